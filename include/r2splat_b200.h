@@ -1,0 +1,366 @@
+/*
+ * r2splat_b200 -- C ABI of the B200 (sm_100a) CT operator library.
+ *
+ * Every entry point takes raw device pointers, sizes, scalars, a dtype tag
+ * (R2S_F32 / R2S_F64) and a cudaStream_t passed as void*. Entry points never
+ * allocate device memory: outputs and scratch workspaces are supplied by the
+ * caller (the Python shim allocates them through the torch caching
+ * allocator). Work is enqueued on the given stream on the CURRENT device.
+ * Each call returns R2S_OK (0) or an error code; r2s_last_error() returns a
+ * thread-local message for the most recent failure.
+ *
+ * Each operator replaces one pybind11 binding of the reference
+ * (MedAPT-group/R2Splat, r2splat/cuda/csrc/ext.cpp) whose C++ declaration is
+ * cited as "Ops.h:line" (r2splat/cuda/include/Ops.h). Where the reference
+ * binding allocates its outputs, the caller here passes them; where it returns
+ * an undefined tensor (absgrad off), the corresponding pointer is NULL.
+ * Array layouts are the reference's: contiguous row-major tensors.
+ */
+#ifndef R2SPLAT_B200_H
+#define R2SPLAT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define R2S_OK 0
+#define R2S_ERR_ARGUMENT 1    /* invalid shape, size or pointer */
+#define R2S_ERR_CUDA 2        /* a CUDA runtime call or kernel launch failed */
+#define R2S_ERR_UNSUPPORTED 3 /* sizes beyond what this build supports */
+#define R2S_ERR_WORKSPACE 4   /* workspace too small */
+
+#define R2S_F32 0
+#define R2S_F64 1
+
+/* Library identification. */
+int r2s_abi_version(void);
+const char* r2s_last_error(void);
+
+/* ---------------------------------------------------------------- geometry */
+
+/* Ops.h:419-422 parameter_transform_fwd_tensor.
+ * quats [N,4] (wxyz, unnormalised), scales [N,3] -> covars [N,6], max_scales [N]. */
+int r2s_parameter_transform_fwd(int dtype, const void* quats, const void* scales,
+                                void* covars, void* max_scales, uint32_t n, void* stream);
+
+/* Ops.h:424-428 parameter_transform_bwd_tensor. -> v_quats [N,4], v_scales [N,3]. */
+int r2s_parameter_transform_bwd(int dtype, const void* quats, const void* scales,
+                                const void* v_covars, void* v_quats, void* v_scales,
+                                uint32_t n, void* stream);
+
+/* Ops.h:397-406 world_to_image_projection_fwd_tensor.
+ * means [N,3], covars [N,6], viewmats [C,4,4], Ks [C,3,3]
+ * -> means2d [C,N,2], cov2d [C,N,6], radii [C,N,2] int32. */
+int r2s_world_to_image_projection_fwd(int dtype, const void* means, const void* covars,
+                                      const void* viewmats, const void* Ks, uint32_t C, uint32_t N,
+                                      uint32_t width, uint32_t height, float eps_blur,
+                                      float radius_clip, void* means2d, void* cov2d,
+                                      int32_t* radii, void* stream);
+
+/* Ops.h:408-417 world_to_image_projection_bwd_tensor. -> v_means [N,3], v_covars [N,6].
+ * Sums over cameras per primitive in a fixed order (no atomics). */
+int r2s_world_to_image_projection_bwd(int dtype, const void* means, const void* covars,
+                                      const void* viewmats, const void* Ks, uint32_t C, uint32_t N,
+                                      uint32_t width, uint32_t height, const void* v_means2d,
+                                      const void* v_cov2d, void* v_means, void* v_covars,
+                                      void* stream);
+
+/* Ops.h:214-217 conics_mu_fwd_tensor. cov2d [total,6] -> conics [total,3], mus [total]. */
+int r2s_conics_mu_fwd(int dtype, const void* cov2d, uint32_t total, double eps,
+                      void* conics, void* mus, void* stream);
+
+/* Ops.h:219-225 conics_mu_bwd_tensor. -> v_cov2d [total,6]. */
+int r2s_conics_mu_bwd(int dtype, const void* cov2d, uint32_t total, double eps,
+                      const void* conics, const void* mus, const void* v_conics,
+                      const void* v_mus, void* v_cov2d, void* stream);
+
+/* Ops.h:430-441 world_to_volume_mapping_fwd_tensor.
+ * -> means3d_v [N,3], conics [N,6], radii [N,3] int32. (max_scales is unused, as in the reference.) */
+int r2s_world_to_volume_mapping_fwd(int dtype, const void* means, const void* covars,
+                                    const void* ranges, const void* centers, uint32_t N,
+                                    uint32_t dim2, uint32_t dim1, uint32_t dim0, double eps3d,
+                                    double radius_clip, void* means3d_v, void* conics,
+                                    int32_t* radii, void* stream);
+
+/* Ops.h:443-454 world_to_volume_mapping_bwd_tensor. -> v_means [N,3], v_covars [N,6]. */
+int r2s_world_to_volume_mapping_bwd(int dtype, const void* means, const void* covars,
+                                    const void* ranges, const void* centers, uint32_t N,
+                                    uint32_t dim2, uint32_t dim1, uint32_t dim0, double eps3d,
+                                    const void* v_means3d_v, const void* v_conics, void* v_means,
+                                    void* v_covars, void* stream);
+
+/* ------------------------------------------------- tile intersection (2D/3D)
+ * Ops.h:46-52 isect_tiles_tensor, Ops.h:54-58 isect_offset_encode_tensor,
+ * Ops.h:60-67 isect_tiles_3d_tensor, Ops.h:69-73 isect_offset_encode_3d_tensor.
+ *
+ * The reference's single call is split at the host read of the intersection
+ * count (IsectTiles.cpp:95-100 reads it with .item()):
+ *   1. r2s_isect_*_count: per-element tile counts (int32) and their inclusive
+ *      prefix sum (int64). The caller reads cum_tiles[n_elems-1].
+ *   2. r2s_isect_*_emit: writes the intersections sorted by key with ties in
+ *      ascending element order (the order of the reference's stable radix
+ *      sort), and optionally the per-key start offsets.
+ * Keys: 2D = camera * tiles_x * tiles_y + tile_y * tiles_x + tile_x (element
+ * c*N+n); 3D = (tz * tiles_y + ty) * tiles_x + tx (element n).
+ * radii: 2D [C,N] (square) or [C,N,2] (rect, radii_is_rect=1); 3D [N,3].
+ */
+size_t r2s_isect_count_workspace(uint64_t n_elems);
+size_t r2s_isect_emit_workspace(uint64_t n_isects, uint64_t n_keys);
+
+int r2s_isect_tiles_count(int dtype, const void* means2d, const int32_t* radii, int radii_is_rect,
+                          uint32_t C, uint32_t N, uint32_t tile_size, uint32_t tiles_x,
+                          uint32_t tiles_y, int32_t* tiles_per_gauss, int64_t* cum_tiles,
+                          void* workspace, size_t workspace_bytes, void* stream);
+int r2s_isect_tiles_emit(int dtype, const void* means2d, const int32_t* radii, int radii_is_rect,
+                         uint32_t C, uint32_t N, uint32_t tile_size, uint32_t tiles_x,
+                         uint32_t tiles_y, const int64_t* cum_tiles, int64_t n_isects,
+                         int64_t* isect_ids, int32_t* flatten_ids, int32_t* offsets,
+                         void* workspace, size_t workspace_bytes, void* stream);
+int r2s_isect_offset_encode(const int64_t* isect_ids, int64_t n_isects, uint32_t C,
+                            uint32_t tiles_x, uint32_t tiles_y, int32_t* offsets, void* stream);
+
+int r2s_isect_tiles_3d_count(int dtype, const void* means3d, const int32_t* radii, uint32_t N,
+                             uint32_t tile_size, uint32_t tiles_x, uint32_t tiles_y,
+                             uint32_t tiles_z, int32_t* tiles_per_gauss, int64_t* cum_tiles,
+                             void* workspace, size_t workspace_bytes, void* stream);
+int r2s_isect_tiles_3d_emit(int dtype, const void* means3d, const int32_t* radii, uint32_t N,
+                            uint32_t tile_size, uint32_t tiles_x, uint32_t tiles_y,
+                            uint32_t tiles_z, const int64_t* cum_tiles, int64_t n_isects,
+                            int64_t* isect_ids, int32_t* flatten_ids, int32_t* offsets,
+                            void* workspace, size_t workspace_bytes, void* stream);
+int r2s_isect_offset_encode_3d(const int64_t* isect_ids, int64_t n_isects, uint32_t tiles_x,
+                               uint32_t tiles_y, uint32_t tiles_z, int32_t* offsets, void* stream);
+
+/* ------------------------------------------------------------ rasterization
+ * Common arguments of the rasterize family (Ops.h:227-396):
+ *   means2d [C,N,2], conics [C,N,3], opacities [C,N], mus [C,N],
+ *   betas [C,N] (Beta variants; the projected exponent beta+1/2),
+ *   uncertainties [N] (mean/variance variants), tile_offsets [C,ty,tx],
+ *   flatten_ids [n_isects], isect_ids [n_isects] (per-primitive variants).
+ *   width = dim1, height = dim0.
+ * Workspace: r2s_raster_workspace(C, N, with_gradients) bytes.
+ */
+size_t r2s_raster_workspace(uint32_t dtype, uint32_t C, uint32_t N, int with_gradients);
+
+/* Ops.h:227-236 rasterize_to_pixels_fwd_tensor / Ops.h:309-319 beta_rasterize_to_pixels_fwd_tensor
+ * (betas NULL selects the Gaussian kernel). -> render [C,H,W]. */
+int r2s_rasterize_to_pixels_fwd(int dtype, const void* means2d, const void* conics,
+                                const void* opacities, const void* mus, const void* betas,
+                                const int32_t* tile_offsets, const int32_t* flatten_ids,
+                                uint32_t C, uint32_t N, uint32_t n_isects, uint32_t width,
+                                uint32_t height, uint32_t tile_size, uint32_t tiles_x,
+                                uint32_t tiles_y, void* render, void* workspace,
+                                size_t workspace_bytes, void* stream);
+
+/* Ops.h:238-248 rasterize_to_pixels_mean_var_fwd_tensor / Ops.h:321-332 beta_... -> render, render_var. */
+int r2s_rasterize_to_pixels_mean_var_fwd(int dtype, const void* means2d, const void* conics,
+                                         const void* opacities, const void* mus, const void* betas,
+                                         const void* uncertainties, const int32_t* tile_offsets,
+                                         const int32_t* flatten_ids, uint32_t C, uint32_t N,
+                                         uint32_t n_isects, uint32_t width, uint32_t height,
+                                         uint32_t tile_size, uint32_t tiles_x, uint32_t tiles_y,
+                                         void* render, void* render_var, void* workspace,
+                                         size_t workspace_bytes, void* stream);
+
+/* Ops.h:250-260 rasterize_to_pixels_uncertainty_bwd_tensor / Ops.h:334-345 beta_...
+ * -> v_uncertainties [N] (zeroed by the call). */
+int r2s_rasterize_to_pixels_uncertainty_bwd(int dtype, const void* means2d, const void* conics,
+                                            const void* opacities, const void* mus,
+                                            const void* betas, const int32_t* tile_offsets,
+                                            const int32_t* flatten_ids, const void* v_render_var,
+                                            uint32_t C, uint32_t N, uint32_t n_isects,
+                                            uint32_t width, uint32_t height, uint32_t tile_size,
+                                            uint32_t tiles_x, uint32_t tiles_y,
+                                            void* v_uncertainties, void* workspace,
+                                            size_t workspace_bytes, void* stream);
+
+/* Ops.h:262-274 rasterize_to_pixels_bwd_tensor ("pixel" mode),
+ * Ops.h:276-289 rasterize_to_pixels_bwd_per_gaussian_tensor ("primitive" mode),
+ * Ops.h:291-307 rasterize_to_pixels_mean_var_bwd_per_gaussian_tensor, and the
+ * Beta counterparts Ops.h:347-396. One entry point serves all of them:
+ *   betas NULL -> Gaussian; v_render_var NULL -> plain VJP;
+ *   uncertainties NULL with v_render_var set -> detached variance branch
+ *   (ext.cpp:106-128 overload); v_means2d_abs NULL -> absgrad off;
+ *   v_betas required iff betas; v_uncertainties required iff v_render_var.
+ * isect_ids may be NULL (the tile of each intersection is implied by the
+ * offsets). Outputs (all zeroed by the call): v_means2d [C,N,2],
+ * v_conics [C,N,3], v_opacities [C,N], v_mus [C,N], v_betas [C,N],
+ * v_uncertainties [N], v_means2d_abs [C,N,2]. */
+int r2s_rasterize_to_pixels_bwd(int dtype, const void* means2d, const void* conics,
+                                const void* opacities, const void* mus, const void* betas,
+                                const int32_t* tile_offsets, const int64_t* isect_ids,
+                                const int32_t* flatten_ids, const void* v_render,
+                                const void* v_render_var, const void* uncertainties,
+                                uint32_t C, uint32_t N, uint32_t n_isects, uint32_t width,
+                                uint32_t height, uint32_t tile_size, uint32_t tiles_x,
+                                uint32_t tiles_y, void* v_means2d_abs, void* v_means2d,
+                                void* v_conics, void* v_opacities, void* v_mus, void* v_betas,
+                                void* v_uncertainties, void* workspace, size_t workspace_bytes,
+                                void* stream);
+
+/* ---------------------------------------------------------- voxelization
+ * Common arguments (Ops.h:75-212): means3d [N,3], conics [N,6],
+ * opacities [N], betas [N] (Beta), uncertainties [N] (mean/variance),
+ * tile_offsets [tz,ty,tx], flatten_ids [n_isects]; dim2 = x, dim1 = y, dim0 = z.
+ * Workspace: r2s_voxel_workspace(N, with_gradients) bytes.
+ */
+size_t r2s_voxel_workspace(uint32_t dtype, uint32_t N, int with_gradients);
+
+/* Ops.h:75-84 voxelize_to_voxels_fwd_tensor / Ops.h:142-152 beta_... -> volume [D,H,W]. */
+int r2s_voxelize_to_voxels_fwd(int dtype, const void* means3d, const void* conics,
+                               const void* opacities, const void* betas,
+                               const int32_t* tile_offsets, const int32_t* flatten_ids,
+                               uint32_t N, uint32_t n_isects, uint32_t dim2, uint32_t dim1,
+                               uint32_t dim0, uint32_t tile_size, uint32_t tiles_x,
+                               uint32_t tiles_y, uint32_t tiles_z, void* volume, void* workspace,
+                               size_t workspace_bytes, void* stream);
+
+/* Ops.h:86-96 voxelize_to_voxels_mean_var_fwd_tensor / Ops.h:154-165 beta_... */
+int r2s_voxelize_to_voxels_mean_var_fwd(int dtype, const void* means3d, const void* conics,
+                                        const void* opacities, const void* betas,
+                                        const void* uncertainties, const int32_t* tile_offsets,
+                                        const int32_t* flatten_ids, uint32_t N, uint32_t n_isects,
+                                        uint32_t dim2, uint32_t dim1, uint32_t dim0,
+                                        uint32_t tile_size, uint32_t tiles_x, uint32_t tiles_y,
+                                        uint32_t tiles_z, void* volume, void* volume_var,
+                                        void* workspace, size_t workspace_bytes, void* stream);
+
+/* Ops.h:98-140 voxelize_to_voxels_bwd / _bwd_per_gaussian / _mean_var_bwd_per_gaussian
+ * and the Beta counterparts Ops.h:167-212 (ext.cpp:42-94 overloads). Same NULL
+ * conventions as r2s_rasterize_to_pixels_bwd. Outputs (zeroed by the call):
+ * v_means3d [N,3], v_conics [N,6], v_opacities [N], v_betas [N], v_uncertainties [N]. */
+int r2s_voxelize_to_voxels_bwd(int dtype, const void* means3d, const void* conics,
+                               const void* opacities, const void* betas,
+                               const int32_t* tile_offsets, const int64_t* isect_ids,
+                               const int32_t* flatten_ids, const void* v_volume,
+                               const void* v_volume_var, const void* uncertainties, uint32_t N,
+                               uint32_t n_isects, uint32_t dim2, uint32_t dim1, uint32_t dim0,
+                               uint32_t tile_size, uint32_t tiles_x, uint32_t tiles_y,
+                               uint32_t tiles_z, void* v_means3d, void* v_conics,
+                               void* v_opacities, void* v_betas, void* v_uncertainties,
+                               void* workspace, size_t workspace_bytes, void* stream);
+
+/* ------------------------------------------------------------------ losses */
+
+/* Ops.h:37-39 volume_loss_fwd (anisotropic TV over [B,D,H,W]).
+ * -> loss [1], tv [1], tv_map [B,D,H,W] (tv_map may be NULL to skip writing it).
+ * Workspace: r2s_volume_loss_workspace(numel). */
+size_t r2s_volume_loss_workspace(uint64_t numel);
+int r2s_volume_loss_fwd(int dtype, const void* volume, uint32_t B, uint32_t D, uint32_t H,
+                        uint32_t W, float lambda_tv, void* loss, void* tv, void* tv_map,
+                        void* workspace, size_t workspace_bytes, void* stream);
+/* Ops.h:41-44 volume_loss_bwd. grad_output [1] -> grad_volume [B,D,H,W] (lambda folded in). */
+int r2s_volume_loss_bwd(int dtype, const void* volume, const void* grad_output, uint32_t B,
+                        uint32_t D, uint32_t H, uint32_t W, float lambda_tv, void* grad_volume,
+                        void* stream);
+
+/* Ops.h:15-18 image_loss_fwd / Ops.h:26-29 image_loss_l1_fwd (mean L1 over [B,H,W]).
+ * -> loss [1], l1 [1], l1_map [B,H,W]. Workspace: r2s_volume_loss_workspace(numel). */
+int r2s_image_loss_l1_fwd(int dtype, const void* prediction, const void* target, uint32_t B,
+                          uint32_t H, uint32_t W, float lambda_l1, void* loss, void* l1,
+                          void* l1_map, void* workspace, size_t workspace_bytes, void* stream);
+/* Ops.h:20-24 image_loss_bwd / Ops.h:31-35 image_loss_l1_bwd. -> grad_prediction [B,H,W]. */
+int r2s_image_loss_l1_bwd(int dtype, const void* prediction, const void* target,
+                          const void* grad_output, uint32_t B, uint32_t H, uint32_t W,
+                          float lambda_l1, void* grad_prediction, void* stream);
+
+/* ------------------------------------------- fused explicit-operator path
+ * These have no single reference counterpart: they implement the pipelines of
+ * the reference's r2splat/explicit.py (rasterize_fwd :102-188,
+ * rasterize_bwd :191-242, voxelize_fwd :245-311, voxelize_bwd :314-351) with
+ * fewer passes over HBM.
+ */
+
+/* Projection + conic/mu + packing (explicit.py:160-170). Writes one 8-slot
+ * record per (camera, primitive) -- x, y, a, b, c, density, mu, beta+1/2 --
+ * into records [C,N,8], the tile rectangle rects [C,N,4] (uint16: x0, y0, x1, y1),
+ * and tiles_per_gauss [C,N]. ratio [N] (Beta path factor) and betas [N] may
+ * be NULL for Gaussians. */
+int r2s_raster_project(int dtype, const void* means, const void* covars, const void* densities,
+                       const void* betas, const void* ratio, const void* viewmats, const void* Ks,
+                       uint32_t C, uint32_t N, uint32_t width, uint32_t height, float eps_blur,
+                       double eps, float radius_clip, uint32_t tile_size, uint32_t tiles_x,
+                       uint32_t tiles_y, void* records, uint16_t* rects, int32_t* tiles_per_gauss,
+                       void* stream);
+
+/* Inclusive prefix sum of int32 tile counts into int64 (the reference's
+ * torch::cumsum(..., kInt64), IsectTiles.cpp:95-97). Workspace: r2s_isect_count_workspace(n). */
+int r2s_scan_tile_counts(const int32_t* counts, uint64_t n, int64_t* cum, void* workspace,
+                         size_t workspace_bytes, void* stream);
+
+/* Emits the sorted 2D intersections from precomputed rectangles (no radii). */
+int r2s_raster_emit(const uint16_t* rects, uint32_t C, uint32_t N, uint32_t tiles_x,
+                    uint32_t tiles_y, const int64_t* cum_tiles, int64_t n_isects,
+                    int64_t* isect_ids, int32_t* flatten_ids, int32_t* offsets, void* workspace,
+                    size_t workspace_bytes, void* stream);
+
+/* Tile accumulation on packed records. uncertainties [N] for the variance image. */
+int r2s_raster_render(int dtype, const void* records, const void* uncertainties, int beta,
+                      const int32_t* tile_offsets, const int32_t* flatten_ids, uint32_t C,
+                      uint32_t N, uint32_t n_isects, uint32_t width, uint32_t height,
+                      uint32_t tile_size, uint32_t tiles_x, uint32_t tiles_y, void* render,
+                      void* render_var, void* stream);
+
+/* Tile VJP on packed records, accumulating packed per-(camera, primitive)
+ * adjoints grads [C,N,8] (x, y, a, b, c, density, mu, beta) and
+ * v_uncertainties [N]; both must be zeroed by the caller. */
+int r2s_raster_render_bwd(int dtype, const void* records, const void* uncertainties, int beta,
+                          int detach_variance, const int32_t* tile_offsets,
+                          const int32_t* flatten_ids, const void* v_render,
+                          const void* v_render_var, uint32_t C, uint32_t N, uint32_t n_isects,
+                          uint32_t width, uint32_t height, uint32_t tile_size, uint32_t tiles_x,
+                          uint32_t tiles_y, void* grads, void* v_means2d_abs,
+                          void* v_uncertainties, void* stream);
+
+/* Chain rule from packed adjoints to physical parameters (explicit.py:225-241):
+ * conic/mu VJP, projection VJP summed over cameras, Beta path factor and the
+ * parameter-transform VJP, per primitive, with no atomics. log_grad [N] and
+ * ratio [N] only for Beta. -> v_means [N,3], v_quats [N,4], v_scales [N,3],
+ * v_densities [N], v_betas [N] (Beta). */
+int r2s_raster_chain_bwd(int dtype, const void* means, const void* quats, const void* scales,
+                         const void* covars, const void* betas, const void* ratio,
+                         const void* log_grad, const void* viewmats, const void* Ks, uint32_t C,
+                         uint32_t N, uint32_t width, uint32_t height, float eps_blur, double eps,
+                         const void* grads, void* v_means, void* v_quats, void* v_scales,
+                         void* v_densities, void* v_betas, void* stream);
+
+/* Volume mapping + packing (explicit.py:290-294): records [N,16] (x, y, z, density,
+ * six conic entries, beta, uncertainty, padding), voxel-space means means_v [N,3],
+ * radii [N,3], tiles_per_gauss [N]. */
+int r2s_voxel_project(int dtype, const void* means, const void* covars, const void* densities,
+                      const void* betas, const void* uncertainties, const void* ranges,
+                      const void* centers, uint32_t N, uint32_t dim2, uint32_t dim1,
+                      uint32_t dim0, double eps3d, double radius_clip, uint32_t tile_size,
+                      uint32_t tiles_x, uint32_t tiles_y, uint32_t tiles_z, void* records,
+                      void* means_v, int32_t* radii, int32_t* tiles_per_gauss, void* stream);
+
+int r2s_voxel_render(int dtype, const void* records, int beta, const int32_t* tile_offsets,
+                     const int32_t* flatten_ids, uint32_t N, uint32_t n_isects, uint32_t dim2,
+                     uint32_t dim1, uint32_t dim0, uint32_t tile_size, uint32_t tiles_x,
+                     uint32_t tiles_y, uint32_t tiles_z, void* volume, void* volume_var,
+                     void* stream);
+
+/* Voxel tile VJP into packed adjoints grads [N,16] (x, y, z, density, six conic
+ * entries, beta, uncertainty, ...), zeroed by the caller. */
+int r2s_voxel_render_bwd(int dtype, const void* records, int beta, int detach_variance,
+                         const int32_t* tile_offsets, const int32_t* flatten_ids,
+                         const void* v_volume, const void* v_volume_var, uint32_t N,
+                         uint32_t n_isects, uint32_t dim2, uint32_t dim1, uint32_t dim0,
+                         uint32_t tile_size, uint32_t tiles_x, uint32_t tiles_y, uint32_t tiles_z,
+                         void* grads, void* stream);
+
+/* Chain rule for voxelization (explicit.py:343-351). */
+int r2s_voxel_chain_bwd(int dtype, const void* means, const void* quats, const void* scales,
+                        const void* covars, const void* ranges, const void* centers, uint32_t N,
+                        uint32_t dim2, uint32_t dim1, uint32_t dim0, double eps3d,
+                        const void* grads, void* v_means, void* v_quats, void* v_scales,
+                        void* v_densities, void* v_betas, void* v_uncertainties, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* R2SPLAT_B200_H */

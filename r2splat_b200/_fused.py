@@ -1,0 +1,235 @@
+"""Fused device pipelines behind the explicit operators.
+
+Rasterize (the reference's explicit.py:160-183 and :204-241):
+  parameter transform -> one fused projection/conic/packing pass writing 32-byte
+  records [C,N,8] + tile rectangles + tile counts -> int64 prefix sum -> host
+  read of the intersection count -> emission + stable radix sort + per-tile
+  offsets -> tile accumulation. The VJP is the tile kernel accumulating packed
+  adjoints [C,N,8] with vector atomics, then one per-primitive chain-rule pass
+  (conic/mu VJP, projection VJP summed over cameras, Beta path factor,
+  parameter-transform VJP) with no atomics.
+
+Voxelize (explicit.py:286-307, :331-350): the same structure in 3D with
+64-byte records [N,16].
+
+All arrays are allocated through the torch caching allocator and passed to the
+C ABI; nothing here computes on the CPU.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+from typing import Optional
+
+import torch
+
+from . import _beta
+from .cuda import _backend
+from .cuda import _wrapper as low
+
+Tensor = torch.Tensor
+RASTER_TILE = 16
+VOXEL_TILE = 8
+
+
+def _ptr(t: Optional[Tensor]):
+    return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+def _stream(device):
+    return ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
+def _dtype(t: Tensor) -> int:
+    return 0 if t.dtype == torch.float32 else 1
+
+
+def _ws(nbytes: int, device) -> Tensor:
+    return torch.empty(max(int(nbytes), 1), dtype=torch.uint8, device=device)
+
+
+@dataclass
+class RasterState:
+    """Device buffers a projection VJP needs (the reference saves 12, explicit.py:184-186)."""
+
+    covars: Tensor
+    records: Tensor
+    offsets: Tensor
+    isect_ids: Tensor
+    flatten_ids: Tensor
+    ratio: Optional[Tensor]
+    n_isects: int
+    width: int
+    height: int
+    tile_size: int = RASTER_TILE
+    extra: dict = field(default_factory=dict)
+
+
+@dataclass
+class VoxelState:
+    covars: Tensor
+    records: Tensor
+    offsets: Tensor
+    isect_ids: Tensor
+    flatten_ids: Tensor
+    n_isects: int
+    shape: tuple
+    tile_size: int = VOXEL_TILE
+
+
+def raster_intersections(means, covars, densities, beta, ratio, viewmats, Ks, width, height, eps, radius_clip,
+                         tile_size=RASTER_TILE):
+    """Projection + packing + sorted tile intersections. Returns (records, offsets, isect_ids, flatten_ids, M)."""
+    device = means.device
+    c, n = viewmats.shape[0], means.shape[0]
+    tx = (width + tile_size - 1) // tile_size
+    ty = (height + tile_size - 1) // tile_size
+    stream = _stream(device)
+    lib = _backend.library()
+    records = means.new_empty((c, n, 8))
+    rects = torch.empty((c, n, 4), dtype=torch.int16, device=device)
+    counts = torch.empty((c, n), dtype=torch.int32, device=device)
+    _backend.call("r2s_raster_project", _dtype(means), _ptr(means), _ptr(covars), _ptr(densities), _ptr(beta),
+                  _ptr(ratio), _ptr(viewmats), _ptr(Ks), c, n, width, height, float(eps), float(eps),
+                  float(radius_clip), tile_size, tx, ty, _ptr(records), _ptr(rects), _ptr(counts), stream)
+    cum = torch.empty((c * n,), dtype=torch.int64, device=device)
+    ws = _ws(lib.r2s_isect_count_workspace(c * n), device)
+    _backend.call("r2s_scan_tile_counts", _ptr(counts), c * n, _ptr(cum), _ptr(ws), ws.numel(), stream)
+    m = int(cum[-1].item())
+    isect_ids = torch.empty((m,), dtype=torch.int64, device=device)
+    flatten_ids = torch.empty((m,), dtype=torch.int32, device=device)
+    offsets = torch.empty((c, ty, tx), dtype=torch.int32, device=device)
+    ws = _ws(lib.r2s_isect_emit_workspace(m, c * tx * ty), device)
+    _backend.call("r2s_raster_emit", _ptr(rects), c, n, tx, ty, _ptr(cum), m, _ptr(isect_ids), _ptr(flatten_ids),
+                  _ptr(offsets), _ptr(ws), ws.numel(), stream)
+    return records, offsets, isect_ids, flatten_ids, m
+
+
+def raster_forward(means, quats, scales, densities, viewmats, Ks, width, height, beta, uncertainty, eps,
+                   radius_clip, tile_size=RASTER_TILE):
+    """Explicit projection forward; returns (image or (image, variance), RasterState)."""
+    device = means.device
+    c = viewmats.shape[0]
+    covars, _ = low.parameter_transform_fwd(quats, scales)
+    ratio = _beta.beta_path_ratio(beta) if beta is not None else None
+    records, offsets, isect_ids, flatten_ids, m = raster_intersections(
+        means, covars, densities, beta, ratio, viewmats, Ks, width, height, eps, radius_clip, tile_size)
+    image = means.new_empty((c, height, width))
+    variance = torch.empty_like(image) if uncertainty is not None else None
+    tx = (width + tile_size - 1) // tile_size
+    ty = (height + tile_size - 1) // tile_size
+    _backend.call("r2s_raster_render", _dtype(means), _ptr(records), _ptr(uncertainty), int(beta is not None),
+                  _ptr(offsets), _ptr(flatten_ids), c, means.shape[0], m, width, height, tile_size, tx, ty,
+                  _ptr(image), _ptr(variance), _stream(device))
+    state = RasterState(covars, records, offsets, isect_ids, flatten_ids, ratio, m, width, height, tile_size)
+    output = image if uncertainty is None else (image, variance)
+    return output, state
+
+
+def raster_backward(state: RasterState, means, quats, scales, densities, beta, uncertainty, viewmats, Ks, eps,
+                    v_image, v_variance, detach_variance):
+    """Explicit projection VJP -> (v_means, v_quats, v_scales, v_densities, v_beta, v_uncertainty)."""
+    device = means.device
+    c, n = viewmats.shape[0], means.shape[0]
+    tile = state.tile_size
+    tx = (state.width + tile - 1) // tile
+    ty = (state.height + tile - 1) // tile
+    stream = _stream(device)
+    grads = means.new_zeros((c, n, 8))
+    v_unc = means.new_zeros((n,)) if v_variance is not None else None
+    _backend.call("r2s_raster_render_bwd", _dtype(means), _ptr(state.records), _ptr(uncertainty),
+                  int(beta is not None), int(bool(detach_variance)), _ptr(state.offsets), _ptr(state.flatten_ids),
+                  _ptr(v_image), _ptr(v_variance), c, n, state.n_isects, state.width, state.height, tile, tx, ty,
+                  _ptr(grads), None, _ptr(v_unc), stream)
+    log_grad = _beta.beta_path_log_grad(beta) if beta is not None else None
+    v_means = means.new_empty((n, 3))
+    v_quats = means.new_empty((n, 4))
+    v_scales = means.new_empty((n, 3))
+    v_dens = means.new_empty((n,))
+    v_beta = means.new_empty((n,)) if beta is not None else None
+    _backend.call("r2s_raster_chain_bwd", _dtype(means), _ptr(means), _ptr(quats), _ptr(scales), _ptr(state.covars),
+                  _ptr(beta), _ptr(state.ratio), _ptr(log_grad), _ptr(viewmats), _ptr(Ks), c, n, state.width,
+                  state.height, float(eps), float(eps), _ptr(grads), _ptr(v_means), _ptr(v_quats), _ptr(v_scales),
+                  _ptr(v_dens), _ptr(v_beta), stream)
+    if v_unc is None and uncertainty is not None:
+        v_unc = torch.zeros_like(uncertainty)
+    return v_means, v_quats, v_scales, v_dens, v_beta, v_unc
+
+
+def voxel_intersections(means, covars, densities, beta, uncertainty, extent, center, shape, eps, radius_clip,
+                        tile_size=VOXEL_TILE):
+    device = means.device
+    depth, height, width = shape
+    n = means.shape[0]
+    tx = (width + tile_size - 1) // tile_size
+    ty = (height + tile_size - 1) // tile_size
+    tz = (depth + tile_size - 1) // tile_size
+    stream = _stream(device)
+    lib = _backend.library()
+    records = means.new_empty((n, 16))
+    means_v = means.new_empty((n, 3))
+    radii = torch.empty((n, 3), dtype=torch.int32, device=device)
+    counts = torch.empty((n,), dtype=torch.int32, device=device)
+    _backend.call("r2s_voxel_project", _dtype(means), _ptr(means), _ptr(covars), _ptr(densities), _ptr(beta),
+                  _ptr(uncertainty), _ptr(extent), _ptr(center), n, width, height, depth, float(eps),
+                  float(radius_clip), tile_size, tx, ty, tz, _ptr(records), _ptr(means_v), _ptr(radii), _ptr(counts),
+                  stream)
+    cum = torch.empty((n,), dtype=torch.int64, device=device)
+    ws = _ws(lib.r2s_isect_count_workspace(n), device)
+    _backend.call("r2s_scan_tile_counts", _ptr(counts), n, _ptr(cum), _ptr(ws), ws.numel(), stream)
+    m = int(cum[-1].item())
+    isect_ids = torch.empty((m,), dtype=torch.int64, device=device)
+    flatten_ids = torch.empty((m,), dtype=torch.int32, device=device)
+    offsets = torch.empty((tz, ty, tx), dtype=torch.int32, device=device)
+    ws = _ws(lib.r2s_isect_emit_workspace(m, tx * ty * tz), device)
+    _backend.call("r2s_isect_tiles_3d_emit", _dtype(means), _ptr(means_v), _ptr(radii), n, tile_size, tx, ty, tz,
+                  _ptr(cum), m, _ptr(isect_ids), _ptr(flatten_ids), _ptr(offsets), _ptr(ws), ws.numel(), stream)
+    return records, offsets, isect_ids, flatten_ids, m
+
+
+def voxel_forward(means, quats, scales, densities, shape, extent, center, beta, uncertainty, eps, radius_clip,
+                  tile_size=VOXEL_TILE):
+    device = means.device
+    depth, height, width = shape
+    covars, _ = low.parameter_transform_fwd(quats, scales)
+    records, offsets, isect_ids, flatten_ids, m = voxel_intersections(
+        means, covars, densities, beta, uncertainty, extent, center, shape, eps, radius_clip, tile_size)
+    volume = means.new_empty(shape)
+    variance = torch.empty_like(volume) if uncertainty is not None else None
+    tx = (width + tile_size - 1) // tile_size
+    ty = (height + tile_size - 1) // tile_size
+    tz = (depth + tile_size - 1) // tile_size
+    _backend.call("r2s_voxel_render", _dtype(means), _ptr(records), int(beta is not None), _ptr(offsets),
+                  _ptr(flatten_ids), means.shape[0], m, width, height, depth, tile_size, tx, ty, tz, _ptr(volume),
+                  _ptr(variance), _stream(device))
+    state = VoxelState(covars, records, offsets, isect_ids, flatten_ids, m, tuple(shape), tile_size)
+    return (volume if uncertainty is None else (volume, variance)), state
+
+
+def voxel_backward(state: VoxelState, means, quats, scales, beta, uncertainty, extent, center, eps, v_volume,
+                   v_variance, detach_variance):
+    device = means.device
+    n = means.shape[0]
+    depth, height, width = state.shape
+    tile = state.tile_size
+    tx = (width + tile - 1) // tile
+    ty = (height + tile - 1) // tile
+    tz = (depth + tile - 1) // tile
+    stream = _stream(device)
+    grads = means.new_zeros((n, 16))
+    _backend.call("r2s_voxel_render_bwd", _dtype(means), _ptr(state.records), int(beta is not None),
+                  int(bool(detach_variance)), _ptr(state.offsets), _ptr(state.flatten_ids), _ptr(v_volume),
+                  _ptr(v_variance), n, state.n_isects, width, height, depth, tile, tx, ty, tz, _ptr(grads), stream)
+    v_means = means.new_empty((n, 3))
+    v_quats = means.new_empty((n, 4))
+    v_scales = means.new_empty((n, 3))
+    v_dens = means.new_empty((n,))
+    v_beta = means.new_empty((n,)) if beta is not None else None
+    v_unc = means.new_empty((n,)) if v_variance is not None else None
+    _backend.call("r2s_voxel_chain_bwd", _dtype(means), _ptr(means), _ptr(quats), _ptr(scales), _ptr(state.covars),
+                  _ptr(extent), _ptr(center), n, width, height, depth, float(eps), _ptr(grads), _ptr(v_means),
+                  _ptr(v_quats), _ptr(v_scales), _ptr(v_dens), _ptr(v_beta), _ptr(v_unc), stream)
+    if v_unc is None and uncertainty is not None:
+        v_unc = torch.zeros_like(uncertainty)
+    return v_means, v_quats, v_scales, v_dens, v_beta, v_unc

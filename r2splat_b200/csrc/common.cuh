@@ -1,0 +1,153 @@
+// Shared device/host helpers for the r2splat_b200 sm_100a library.
+//
+// The library is a plain C-ABI shared object: every entry point takes raw
+// device pointers, sizes and a cudaStream_t, never allocates, and reports
+// failures through an integer status plus r2s_last_error().
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stddef.h>
+
+#include <string>
+
+#include "../../include/r2splat_b200.h"
+
+namespace r2s {
+
+// ---------------------------------------------------------------------------
+// Error reporting (host)
+// ---------------------------------------------------------------------------
+
+void set_error(const std::string& message);
+int fail(int code, const std::string& message);
+int check_launch(const char* what);
+
+#define R2S_REQUIRE(cond, code, msg)             \
+    do {                                         \
+        if (!(cond)) return ::r2s::fail((code), (msg)); \
+    } while (0)
+
+#define R2S_TRY(expr)                            \
+    do {                                         \
+        int _r2s_status = (expr);                \
+        if (_r2s_status != R2S_OK) return _r2s_status; \
+    } while (0)
+
+// Workspace carving: the caller passes one byte buffer; kernels take slices.
+struct Arena {
+    char* base;
+    size_t size;
+    size_t used;
+    __host__ explicit Arena(void* p, size_t n) : base(static_cast<char*>(p)), size(n), used(0) {}
+    template <typename T>
+    __host__ T* take(size_t count) {
+        if (base == nullptr) return nullptr;
+        const uintptr_t start = reinterpret_cast<uintptr_t>(base) + used;
+        const size_t offset = used + (((start + 255) & ~uintptr_t(255)) - start);
+        const size_t bytes = count * sizeof(T);
+        if (offset + bytes > size) return nullptr;
+        used = offset + bytes;
+        return reinterpret_cast<T*>(base + offset);
+    }
+};
+
+// Size accounting mirror of Arena::take.
+struct ArenaSize {
+    size_t used = 0;
+    template <typename T>
+    __host__ void take(size_t count) {
+        used = ((used + 255) & ~size_t(255)) + count * sizeof(T);
+    }
+    __host__ size_t bytes() const { return used + 256; }
+};
+
+// Runs the statement(s) with S bound to the element type of the dtype tag.
+#define R2S_DISPATCH(dtype, ...)                                                    \
+    do {                                                                            \
+        if ((dtype) == R2S_F32) {                                                   \
+            using S = float;                                                        \
+            __VA_ARGS__;                                                            \
+        } else if ((dtype) == R2S_F64) {                                            \
+            using S = double;                                                       \
+            __VA_ARGS__;                                                            \
+        } else {                                                                    \
+            return ::r2s::fail(R2S_ERR_ARGUMENT, "dtype must be R2S_F32 or R2S_F64");      \
+        }                                                                           \
+    } while (0)
+
+inline cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
+
+inline unsigned blocks_for(int64_t n, unsigned threads) {
+    int64_t b = (n + threads - 1) / threads;
+    if (b < 1) b = 1;
+    return static_cast<unsigned>(b);
+}
+
+// ---------------------------------------------------------------------------
+// Device helpers
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ uint64_t global_timer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Asynchronous 16-byte global->shared copy (LDGSTS); used to gather
+// per-primitive records into shared memory while the previous batch computes.
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n"
+                 :: "r"(smem_u32(smem_dst)), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" :: "n"(N) : "memory");
+}
+
+// Vector reductions into global memory (sm_90+ red.global.add.v4.f32).
+__device__ __forceinline__ void red_add_v4(float* addr, float a, float b, float c, float d) {
+    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};\n"
+                 :: "l"(addr), "f"(a), "f"(b), "f"(c), "f"(d) : "memory");
+}
+__device__ __forceinline__ void red_add_v4(double* addr, double a, double b, double c, double d) {
+    atomicAdd(addr + 0, a);
+    atomicAdd(addr + 1, b);
+    atomicAdd(addr + 2, c);
+    atomicAdd(addr + 3, d);
+}
+__device__ __forceinline__ void red_add(float* addr, float v) { atomicAdd(addr, v); }
+__device__ __forceinline__ void red_add(double* addr, double v) { atomicAdd(addr, v); }
+
+template <typename S>
+__device__ __forceinline__ S warp_sum(S v) {
+#pragma unroll
+    for (int offset = 16; offset > 0; offset >>= 1) v += __shfl_xor_sync(0xffffffffu, v, offset);
+    return v;
+}
+
+// Packed per-(camera, primitive) record consumed by the tile kernels.
+// Slot meaning: projected centre (x, y), 2x2 conic (a, b, c), density o,
+// path factor mu, and the projected Beta exponent (beta + 1/2) for Beta
+// primitives (unused otherwise).
+template <typename S>
+struct alignas(16) Rec2D {
+    S x, y, a, b, c, o, mu, beta;
+};
+
+// Packed per-primitive record for voxel tiles: voxel-space centre, density,
+// the 3x3 conic (c00, c01, c02, c11, c12, c22), the Beta exponent, and the
+// uncertainty (relative variance).
+template <typename S>
+struct alignas(16) Rec3D {
+    S x, y, z, o, c00, c01, c02, c11, c12, c22, beta, q, pad0, pad1, pad2, pad3;
+};
+
+}  // namespace r2s

@@ -1,0 +1,446 @@
+// Tile intersection: per-element tile counts, prefix sum, emission of
+// (key, element) pairs, a stable LSD radix sort, and per-key offsets.
+//
+// Ordering contract (IsectTilesKernel.cu:137-217 + the stable radix sort at
+// :398-445): within one key the elements appear in ascending element order.
+// Emission writes each element's pairs contiguously at its prefix-sum slot
+// in ascending element order, and the sort is stable, so any run of equal
+// keys keeps ascending element order -- the same arrays the reference's
+// CUB-sorted output holds.
+#include "geometry.cuh"
+#include "scan.cuh"
+
+namespace r2s {
+
+constexpr unsigned kIsectThreads = 256;
+
+// ----------------------------------------------------------------- counting
+
+template <typename S>
+__device__ __forceinline__ bool rect_2d(const S* means2d, const int32_t* radii, bool rect, size_t idx,
+                                        uint32_t tile_size, uint32_t tiles_x, uint32_t tiles_y, uint32_t& x0,
+                                        uint32_t& x1, uint32_t& y0, uint32_t& y1) {
+    const S radius_x = static_cast<S>(rect ? radii[2 * idx] : radii[idx]);
+    const S radius_y = static_cast<S>(rect ? radii[2 * idx + 1] : radii[idx]);
+    if (radius_x <= 0 || radius_y <= 0) return false;
+    const S mean_x = means2d[2 * idx];
+    const S mean_y = means2d[2 * idx + 1];
+    if (!isfinite(mean_x) || !isfinite(mean_y)) return false;
+    tile_span(mean_x, radius_x, tile_size, tiles_x, x0, x1);
+    tile_span(mean_y, radius_y, tile_size, tiles_y, y0, y1);
+    return x1 > x0 && y1 > y0;
+}
+
+template <typename S>
+__device__ __forceinline__ bool rect_3d(const S* means3d, const int32_t* radii, size_t idx, uint32_t tile_size,
+                                        uint32_t tx, uint32_t ty, uint32_t tz, uint32_t* lo, uint32_t* hi) {
+    const S rx = static_cast<S>(radii[3 * idx]);
+    const S ry = static_cast<S>(radii[3 * idx + 1]);
+    const S rz = static_cast<S>(radii[3 * idx + 2]);
+    if (rx <= 0 || ry <= 0 || rz <= 0) return false;
+    tile_span(means3d[3 * idx + 0], rx, tile_size, tx, lo[0], hi[0]);
+    tile_span(means3d[3 * idx + 1], ry, tile_size, ty, lo[1], hi[1]);
+    tile_span(means3d[3 * idx + 2], rz, tile_size, tz, lo[2], hi[2]);
+    return hi[0] > lo[0] && hi[1] > lo[1] && hi[2] > lo[2];
+}
+
+template <typename S>
+__global__ void count_2d_kernel(const S* __restrict__ means2d, const int32_t* __restrict__ radii, bool rect,
+                                uint32_t total, uint32_t tile_size, uint32_t tiles_x, uint32_t tiles_y,
+                                int32_t* __restrict__ counts) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    uint32_t x0, x1, y0, y1;
+    counts[i] = rect_2d(means2d, radii, rect, i, tile_size, tiles_x, tiles_y, x0, x1, y0, y1)
+                    ? static_cast<int32_t>((y1 - y0) * (x1 - x0)) : 0;
+}
+
+template <typename S>
+__global__ void count_3d_kernel(const S* __restrict__ means3d, const int32_t* __restrict__ radii, uint32_t N,
+                                uint32_t tile_size, uint32_t tx, uint32_t ty, uint32_t tz,
+                                int32_t* __restrict__ counts) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    uint32_t lo[3], hi[3];
+    counts[i] = rect_3d(means3d, radii, i, tile_size, tx, ty, tz, lo, hi)
+                    ? static_cast<int32_t>((hi[2] - lo[2]) * (hi[1] - lo[1]) * (hi[0] - lo[0])) : 0;
+}
+
+// ----------------------------------------------------------------- emission
+
+template <typename S>
+__global__ void emit_2d_kernel(const S* __restrict__ means2d, const int32_t* __restrict__ radii, bool rect,
+                               uint32_t total, uint32_t N, uint32_t tile_size, uint32_t tiles_x, uint32_t tiles_y,
+                               const int64_t* __restrict__ cum, uint32_t* __restrict__ keys,
+                               uint32_t* __restrict__ vals) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    uint32_t x0, x1, y0, y1;
+    if (!rect_2d(means2d, radii, rect, i, tile_size, tiles_x, tiles_y, x0, x1, y0, y1)) return;
+    const uint32_t base_key = (i / N) * (tiles_x * tiles_y);
+    int64_t w = i == 0 ? 0 : cum[i - 1];
+    for (uint32_t y = y0; y < y1; ++y)
+        for (uint32_t x = x0; x < x1; ++x, ++w) {
+            keys[w] = base_key + y * tiles_x + x;
+            vals[w] = i;
+        }
+}
+
+__global__ void emit_rects_kernel(const ushort4* __restrict__ rects, uint32_t total, uint32_t N, uint32_t tiles_x,
+                                  uint32_t tiles_y, const int64_t* __restrict__ cum, uint32_t* __restrict__ keys,
+                                  uint32_t* __restrict__ vals) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    const ushort4 r = rects[i];
+    if (r.z <= r.x || r.w <= r.y) return;
+    const uint32_t base_key = (i / N) * (tiles_x * tiles_y);
+    int64_t w = i == 0 ? 0 : cum[i - 1];
+    for (uint32_t y = r.y; y < r.w; ++y)
+        for (uint32_t x = r.x; x < r.z; ++x, ++w) {
+            keys[w] = base_key + y * tiles_x + x;
+            vals[w] = i;
+        }
+}
+
+template <typename S>
+__global__ void emit_3d_kernel(const S* __restrict__ means3d, const int32_t* __restrict__ radii, uint32_t N,
+                               uint32_t tile_size, uint32_t tx, uint32_t ty, uint32_t tz,
+                               const int64_t* __restrict__ cum, uint32_t* __restrict__ keys,
+                               uint32_t* __restrict__ vals) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    uint32_t lo[3], hi[3];
+    if (!rect_3d(means3d, radii, i, tile_size, tx, ty, tz, lo, hi)) return;
+    int64_t w = i == 0 ? 0 : cum[i - 1];
+    for (uint32_t z = lo[2]; z < hi[2]; ++z)
+        for (uint32_t y = lo[1]; y < hi[1]; ++y)
+            for (uint32_t x = lo[0]; x < hi[0]; ++x, ++w) {
+                keys[w] = (z * ty + y) * tx + x;
+                vals[w] = i;
+            }
+}
+
+// --------------------------------------------------------------- radix sort
+
+constexpr int kSortThreads = 256;
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kSortItems = 16;  // per lane
+constexpr int64_t kSortTile = int64_t(kSortThreads) * kSortItems;
+constexpr int kMaxDigitBits = 10;
+
+// Per-block digit histogram, stored digit-major: hist[d * n_blocks + b].
+__global__ void __launch_bounds__(kSortThreads) radix_upsweep_kernel(const uint32_t* __restrict__ keys, int64_t n,
+                                                                    int shift, uint32_t mask,
+                                                                    uint32_t* __restrict__ hist) {
+    extern __shared__ uint32_t s_hist[];
+    const uint32_t bins = mask + 1;
+    for (uint32_t d = threadIdx.x; d < bins; d += kSortThreads) s_hist[d] = 0;
+    __syncthreads();
+    const int64_t base = int64_t(blockIdx.x) * kSortTile;
+    for (int k = 0; k < kSortItems; ++k) {
+        const int64_t i = base + int64_t(k) * kSortThreads + threadIdx.x;
+        if (i < n) atomicAdd(&s_hist[(keys[i] >> shift) & mask], 1u);
+    }
+    __syncthreads();
+    for (uint32_t d = threadIdx.x; d < bins; d += kSortThreads) hist[size_t(d) * gridDim.x + blockIdx.x] = s_hist[d];
+}
+
+// Stable scatter of one digit. Element order inside a block is (warp, item,
+// lane) = index order; ranks come from warp-wide matching of equal digits.
+template <typename KeyOut, typename ValOut>
+__global__ void __launch_bounds__(kSortThreads) radix_downsweep_kernel(
+    const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals, int64_t n, int shift, uint32_t mask,
+    const uint32_t* __restrict__ offsets, KeyOut* __restrict__ keys_out, ValOut* __restrict__ vals_out) {
+    extern __shared__ uint32_t s_cnt[];  // [kSortWarps][bins]
+    const uint32_t bins = mask + 1;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (uint32_t d = threadIdx.x; d < bins * kSortWarps; d += kSortThreads) s_cnt[d] = 0;
+    __syncthreads();
+    uint32_t* my_cnt = s_cnt + warp * bins;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    const int64_t base = int64_t(blockIdx.x) * kSortTile + int64_t(warp) * (kSortTile / kSortWarps);
+    uint32_t k_key[kSortItems], k_val[kSortItems], k_rank[kSortItems];
+#pragma unroll
+    for (int k = 0; k < kSortItems; ++k) {
+        const int64_t i = base + int64_t(k) * 32 + lane;
+        const bool valid = i < n;
+        const uint32_t key = valid ? keys[i] : 0u;
+        k_key[k] = key;
+        k_val[k] = valid ? vals[i] : 0u;
+        const uint32_t d = valid ? ((key >> shift) & mask) : bins;
+        const uint32_t peers = __match_any_sync(0xffffffffu, d);
+        const uint32_t leader = __ffs(peers) - 1;
+        uint32_t count = 0;
+        if (valid) count = my_cnt[d];
+        __syncwarp();
+        if (valid && lane == static_cast<int>(leader)) my_cnt[d] = count + __popc(peers);
+        __syncwarp();
+        k_rank[k] = count + __popc(peers & lt_mask);
+    }
+    __syncthreads();
+    for (uint32_t d = threadIdx.x; d < bins; d += kSortThreads) {
+        uint32_t running = offsets[size_t(d) * gridDim.x + blockIdx.x];
+#pragma unroll
+        for (int w = 0; w < kSortWarps; ++w) {
+            const uint32_t c = s_cnt[w * bins + d];
+            s_cnt[w * bins + d] = running;
+            running += c;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kSortItems; ++k) {
+        const int64_t i = base + int64_t(k) * 32 + lane;
+        if (i < n) {
+            const uint32_t d = (k_key[k] >> shift) & mask;
+            const uint32_t pos = my_cnt[d] + k_rank[k];
+            keys_out[pos] = static_cast<KeyOut>(k_key[k]);
+            vals_out[pos] = static_cast<ValOut>(k_val[k]);
+        }
+    }
+}
+
+__global__ void widen_kernel(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals, int64_t n,
+                             int64_t* __restrict__ keys_out, int32_t* __restrict__ vals_out) {
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    keys_out[i] = keys[i];
+    vals_out[i] = static_cast<int32_t>(vals[i]);
+}
+
+// offsets[k] = number of sorted keys smaller than k (lower bound).
+__global__ void offsets_kernel(const int64_t* __restrict__ keys, int64_t n, int64_t n_keys,
+                               int32_t* __restrict__ offsets) {
+    const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= n_keys) return;
+    int64_t lo = 0, hi = n;
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (keys[mid] < k) lo = mid + 1; else hi = mid;
+    }
+    offsets[k] = static_cast<int32_t>(lo);
+}
+
+inline int bits_for(uint64_t max_key) {
+    // Number of bits needed for keys in [0, max_key] (IsectTiles.cpp:146-147
+    // sorts on ceil(log2(max_key + 1)) bits of the key).
+    int bits = 0;
+    while (bits < 64 && (uint64_t(1) << bits) <= max_key) ++bits;
+    return bits;
+}
+
+struct SortPlan {
+    int passes = 0;
+    int digit_bits = 0;
+    int64_t blocks = 0;
+};
+
+inline SortPlan plan_sort(int64_t n, uint64_t n_keys) {
+    SortPlan p;
+    const int bits = bits_for(n_keys > 0 ? n_keys - 1 : 0);
+    p.passes = (bits + kMaxDigitBits - 1) / kMaxDigitBits;
+    p.digit_bits = p.passes > 0 ? (bits + p.passes - 1) / p.passes : 0;
+    p.blocks = (n + kSortTile - 1) / kSortTile;
+    return p;
+}
+
+inline size_t emit_workspace(int64_t n, uint64_t n_keys) {
+    const SortPlan p = plan_sort(n, n_keys);
+    ArenaSize a;
+    a.take<uint32_t>(size_t(n));  // keys A
+    a.take<uint32_t>(size_t(n));  // vals A
+    a.take<uint32_t>(size_t(n));  // keys B
+    a.take<uint32_t>(size_t(n));  // vals B
+    const size_t hist = size_t(1u << (p.digit_bits > 0 ? p.digit_bits : 1)) * size_t(p.blocks > 0 ? p.blocks : 1);
+    a.take<uint32_t>(hist);
+    a.take<char>(scan_workspace_bytes<uint32_t>(int64_t(hist)));
+    return a.bytes();
+}
+
+// Sorts (keys, vals) of length n by key bits [0, bits(n_keys-1)), writing
+// the widened result to isect_ids/flatten_ids, then fills offsets.
+inline int sort_and_finish(uint32_t* keys, uint32_t* vals, int64_t n, uint64_t n_keys, Arena& arena,
+                           int64_t* isect_ids, int32_t* flatten_ids, int32_t* offsets, cudaStream_t stream) {
+    const SortPlan p = plan_sort(n, n_keys);
+    if (n > 0) {
+        if (p.passes == 0) {
+            widen_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(keys, vals, n, isect_ids, flatten_ids);
+            R2S_TRY(check_launch("widen"));
+        } else {
+            uint32_t* keys_b = arena.take<uint32_t>(size_t(n));
+            uint32_t* vals_b = arena.take<uint32_t>(size_t(n));
+            const uint32_t bins = 1u << p.digit_bits;
+            uint32_t* hist = arena.take<uint32_t>(size_t(bins) * size_t(p.blocks));
+            R2S_REQUIRE(keys_b && vals_b && hist, R2S_ERR_WORKSPACE, "intersection workspace too small");
+            void* scan_ws = arena.base + arena.used;
+            const size_t scan_bytes = arena.size - arena.used;
+            R2S_REQUIRE(p.blocks < (int64_t(1) << 31), R2S_ERR_UNSUPPORTED, "too many intersections");
+            const size_t up_smem = bins * sizeof(uint32_t);
+            const size_t down_smem = bins * kSortWarps * sizeof(uint32_t);
+            if (down_smem > 48 * 1024) {
+                cudaFuncSetAttribute(radix_downsweep_kernel<uint32_t, uint32_t>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, int(down_smem));
+                cudaFuncSetAttribute(radix_downsweep_kernel<int64_t, int32_t>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, int(down_smem));
+            }
+            uint32_t *src_k = keys, *src_v = vals, *dst_k = keys_b, *dst_v = vals_b;
+            for (int pass = 0; pass < p.passes; ++pass) {
+                const int shift = pass * p.digit_bits;
+                const uint32_t mask = bins - 1;
+                radix_upsweep_kernel<<<unsigned(p.blocks), kSortThreads, up_smem, stream>>>(src_k, n, shift, mask,
+                                                                                           hist);
+                R2S_TRY(check_launch("radix_upsweep"));
+                R2S_TRY((device_scan<uint32_t, uint32_t, false>(hist, hist, int64_t(bins) * p.blocks, scan_ws,
+                                                                scan_bytes, stream)));
+                if (pass == p.passes - 1) {
+                    radix_downsweep_kernel<int64_t, int32_t><<<unsigned(p.blocks), kSortThreads, down_smem, stream>>>(
+                        src_k, src_v, n, shift, mask, hist, isect_ids, flatten_ids);
+                } else {
+                    radix_downsweep_kernel<uint32_t, uint32_t><<<unsigned(p.blocks), kSortThreads, down_smem,
+                                                                 stream>>>(src_k, src_v, n, shift, mask, hist,
+                                                                           dst_k, dst_v);
+                }
+                R2S_TRY(check_launch("radix_downsweep"));
+                uint32_t* t = src_k; src_k = dst_k; dst_k = t;
+                t = src_v; src_v = dst_v; dst_v = t;
+            }
+        }
+    }
+    if (offsets != nullptr && n_keys > 0) {
+        offsets_kernel<<<blocks_for(int64_t(n_keys), 256), 256, 0, stream>>>(isect_ids, n, int64_t(n_keys), offsets);
+        R2S_TRY(check_launch("isect_offsets"));
+    }
+    return R2S_OK;
+}
+
+}  // namespace r2s
+
+using namespace r2s;
+
+extern "C" {
+
+size_t r2s_isect_count_workspace(uint64_t n_elems) { return scan_workspace_bytes<int64_t>(int64_t(n_elems)); }
+
+int r2s_scan_tile_counts(const int32_t* counts, uint64_t n, int64_t* cum, void* workspace, size_t workspace_bytes,
+                         void* stream) {
+    return device_scan<int32_t, int64_t, true>(counts, cum, int64_t(n), workspace, workspace_bytes,
+                                               as_stream(stream));
+}
+
+size_t r2s_isect_emit_workspace(uint64_t n_isects, uint64_t n_keys) {
+    return emit_workspace(int64_t(n_isects), n_keys);
+}
+
+int r2s_isect_tiles_count(int dtype, const void* means2d, const int32_t* radii, int radii_is_rect, uint32_t C,
+                          uint32_t N, uint32_t tile_size, uint32_t tiles_x, uint32_t tiles_y,
+                          int32_t* tiles_per_gauss, int64_t* cum_tiles, void* workspace, size_t workspace_bytes,
+                          void* stream) {
+    const uint64_t total = uint64_t(C) * N;
+    if (total == 0) return R2S_OK;
+    R2S_REQUIRE(total < (uint64_t(1) << 31), R2S_ERR_UNSUPPORTED, "C*N exceeds the int32 element range");
+    R2S_REQUIRE(tile_size > 0, R2S_ERR_ARGUMENT, "tile_size must be positive");
+    R2S_DISPATCH(dtype, count_2d_kernel<S><<<blocks_for(total, kIsectThreads), kIsectThreads, 0, as_stream(stream)>>>(
+        static_cast<const S*>(means2d), radii, radii_is_rect != 0, uint32_t(total), tile_size, tiles_x, tiles_y,
+        tiles_per_gauss));
+    R2S_TRY(check_launch("isect_count"));
+    return device_scan<int32_t, int64_t, true>(tiles_per_gauss, cum_tiles, int64_t(total), workspace,
+                                               workspace_bytes, as_stream(stream));
+}
+
+int r2s_isect_tiles_emit(int dtype, const void* means2d, const int32_t* radii, int radii_is_rect, uint32_t C,
+                         uint32_t N, uint32_t tile_size, uint32_t tiles_x, uint32_t tiles_y,
+                         const int64_t* cum_tiles, int64_t n_isects, int64_t* isect_ids, int32_t* flatten_ids,
+                         int32_t* offsets, void* workspace, size_t workspace_bytes, void* stream) {
+    const uint64_t total = uint64_t(C) * N;
+    const uint64_t n_keys = uint64_t(C) * tiles_x * tiles_y;
+    R2S_REQUIRE(n_keys < (uint64_t(1) << 32), R2S_ERR_UNSUPPORTED, "C*tiles exceeds the 32-bit key range");
+    R2S_REQUIRE(n_isects >= 0 && n_isects < (int64_t(1) << 31), R2S_ERR_UNSUPPORTED,
+                "intersection count exceeds the int32 range");
+    Arena arena(workspace, workspace_bytes);
+    if (n_isects > 0 && total > 0) {
+        uint32_t* keys = arena.take<uint32_t>(size_t(n_isects));
+        uint32_t* vals = arena.take<uint32_t>(size_t(n_isects));
+        R2S_REQUIRE(keys && vals, R2S_ERR_WORKSPACE, "intersection workspace too small");
+        R2S_DISPATCH(dtype, emit_2d_kernel<S><<<blocks_for(total, kIsectThreads), kIsectThreads, 0, as_stream(stream)>>>(
+            static_cast<const S*>(means2d), radii, radii_is_rect != 0, uint32_t(total), N, tile_size, tiles_x, tiles_y,
+            cum_tiles, keys, vals));
+        R2S_TRY(check_launch("isect_emit"));
+        return sort_and_finish(keys, vals, n_isects, n_keys, arena, isect_ids, flatten_ids, offsets,
+                               as_stream(stream));
+    }
+    return sort_and_finish(nullptr, nullptr, 0, n_keys, arena, isect_ids, flatten_ids, offsets, as_stream(stream));
+}
+
+int r2s_raster_emit(const uint16_t* rects, uint32_t C, uint32_t N, uint32_t tiles_x, uint32_t tiles_y,
+                    const int64_t* cum_tiles, int64_t n_isects, int64_t* isect_ids, int32_t* flatten_ids,
+                    int32_t* offsets, void* workspace, size_t workspace_bytes, void* stream) {
+    const uint64_t total = uint64_t(C) * N;
+    const uint64_t n_keys = uint64_t(C) * tiles_x * tiles_y;
+    R2S_REQUIRE(n_keys < (uint64_t(1) << 32), R2S_ERR_UNSUPPORTED, "C*tiles exceeds the 32-bit key range");
+    R2S_REQUIRE(n_isects >= 0 && n_isects < (int64_t(1) << 31), R2S_ERR_UNSUPPORTED,
+                "intersection count exceeds the int32 range");
+    Arena arena(workspace, workspace_bytes);
+    if (n_isects > 0 && total > 0) {
+        uint32_t* keys = arena.take<uint32_t>(size_t(n_isects));
+        uint32_t* vals = arena.take<uint32_t>(size_t(n_isects));
+        R2S_REQUIRE(keys && vals, R2S_ERR_WORKSPACE, "intersection workspace too small");
+        emit_rects_kernel<<<blocks_for(total, kIsectThreads), kIsectThreads, 0, as_stream(stream)>>>(
+            reinterpret_cast<const ushort4*>(rects), uint32_t(total), N, tiles_x, tiles_y, cum_tiles, keys, vals);
+        R2S_TRY(check_launch("raster_emit"));
+        return sort_and_finish(keys, vals, n_isects, n_keys, arena, isect_ids, flatten_ids, offsets,
+                               as_stream(stream));
+    }
+    return sort_and_finish(nullptr, nullptr, 0, n_keys, arena, isect_ids, flatten_ids, offsets, as_stream(stream));
+}
+
+int r2s_isect_offset_encode(const int64_t* isect_ids, int64_t n_isects, uint32_t C, uint32_t tiles_x,
+                            uint32_t tiles_y, int32_t* offsets, void* stream) {
+    const int64_t n_keys = int64_t(C) * tiles_x * tiles_y;
+    if (n_keys == 0) return R2S_OK;
+    offsets_kernel<<<blocks_for(n_keys, 256), 256, 0, as_stream(stream)>>>(isect_ids, n_isects, n_keys, offsets);
+    return check_launch("isect_offset_encode");
+}
+
+int r2s_isect_tiles_3d_count(int dtype, const void* means3d, const int32_t* radii, uint32_t N, uint32_t tile_size,
+                             uint32_t tiles_x, uint32_t tiles_y, uint32_t tiles_z, int32_t* tiles_per_gauss,
+                             int64_t* cum_tiles, void* workspace, size_t workspace_bytes, void* stream) {
+    if (N == 0) return R2S_OK;
+    R2S_REQUIRE(tile_size > 0, R2S_ERR_ARGUMENT, "tile_size must be positive");
+    R2S_DISPATCH(dtype, count_3d_kernel<S><<<blocks_for(N, kIsectThreads), kIsectThreads, 0, as_stream(stream)>>>(
+        static_cast<const S*>(means3d), radii, N, tile_size, tiles_x, tiles_y, tiles_z, tiles_per_gauss));
+    R2S_TRY(check_launch("isect_count_3d"));
+    return device_scan<int32_t, int64_t, true>(tiles_per_gauss, cum_tiles, int64_t(N), workspace, workspace_bytes,
+                                               as_stream(stream));
+}
+
+int r2s_isect_tiles_3d_emit(int dtype, const void* means3d, const int32_t* radii, uint32_t N, uint32_t tile_size,
+                            uint32_t tiles_x, uint32_t tiles_y, uint32_t tiles_z, const int64_t* cum_tiles,
+                            int64_t n_isects, int64_t* isect_ids, int32_t* flatten_ids, int32_t* offsets,
+                            void* workspace, size_t workspace_bytes, void* stream) {
+    const uint64_t n_keys = uint64_t(tiles_x) * tiles_y * tiles_z;
+    R2S_REQUIRE(n_keys < (uint64_t(1) << 32), R2S_ERR_UNSUPPORTED, "tile count exceeds the 32-bit key range");
+    R2S_REQUIRE(n_isects >= 0 && n_isects < (int64_t(1) << 31), R2S_ERR_UNSUPPORTED,
+                "intersection count exceeds the int32 range");
+    Arena arena(workspace, workspace_bytes);
+    if (n_isects > 0 && N > 0) {
+        uint32_t* keys = arena.take<uint32_t>(size_t(n_isects));
+        uint32_t* vals = arena.take<uint32_t>(size_t(n_isects));
+        R2S_REQUIRE(keys && vals, R2S_ERR_WORKSPACE, "intersection workspace too small");
+        R2S_DISPATCH(dtype, emit_3d_kernel<S><<<blocks_for(N, kIsectThreads), kIsectThreads, 0, as_stream(stream)>>>(
+            static_cast<const S*>(means3d), radii, N, tile_size, tiles_x, tiles_y, tiles_z, cum_tiles, keys, vals));
+        R2S_TRY(check_launch("isect_emit_3d"));
+        return sort_and_finish(keys, vals, n_isects, n_keys, arena, isect_ids, flatten_ids, offsets,
+                               as_stream(stream));
+    }
+    return sort_and_finish(nullptr, nullptr, 0, n_keys, arena, isect_ids, flatten_ids, offsets, as_stream(stream));
+}
+
+int r2s_isect_offset_encode_3d(const int64_t* isect_ids, int64_t n_isects, uint32_t tiles_x, uint32_t tiles_y,
+                               uint32_t tiles_z, int32_t* offsets, void* stream) {
+    const int64_t n_keys = int64_t(tiles_x) * tiles_y * tiles_z;
+    if (n_keys == 0) return R2S_OK;
+    offsets_kernel<<<blocks_for(n_keys, 256), 256, 0, as_stream(stream)>>>(isect_ids, n_isects, n_keys, offsets);
+    return check_launch("isect_offset_encode_3d");
+}
+
+}  // extern "C"

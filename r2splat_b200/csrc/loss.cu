@@ -1,0 +1,225 @@
+// Losses: anisotropic total variation over [B,D,H,W] volumes and mean L1 over
+// [B,H,W] images, forward (value + optional per-element map) and VJP.
+//
+// TV forward is one pass over HBM: each voxel reads itself and its +1
+// neighbours (neighbour reads hit L1/L2), writes its map entry if requested,
+// and blocks reduce in double precision into per-block partials that a single
+// block sums in a fixed order -- deterministic, unlike the reference's float
+// atomics (VolumeLossFwd.cu:88-119). TV backward folds 1/edges and lambda into
+// the same pass (the reference applies lambda in a second torch pass,
+// Loss.cpp:187), keeping the reference's rounding order: the sign sum times
+// g/edges, then times lambda.
+#include "common.cuh"
+
+namespace r2s {
+
+constexpr int kLossThreads = 256;
+constexpr int kLossMaxBlocks = 148 * 8;
+
+template <typename S>
+__device__ __forceinline__ S abs_diff(S x) { return x >= S(0) ? x : -x; }
+
+template <typename S>
+__device__ __forceinline__ S sign_of(S x) { return x > S(0) ? S(1) : (x < S(0) ? S(-1) : S(0)); }
+
+__device__ __forceinline__ double block_sum(double v) {
+    __shared__ double warp_part[kLossThreads / 32];
+    v = warp_sum(v);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) warp_part[warp] = v;
+    __syncthreads();
+    double total = 0;
+    if (threadIdx.x == 0) {
+        for (int w = 0; w < kLossThreads / 32; ++w) total += warp_part[w];
+    }
+    return total;
+}
+
+template <typename S>
+__global__ void __launch_bounds__(kLossThreads) tv_fwd_kernel(const S* __restrict__ vol, int64_t B, int64_t D,
+                                                              int64_t H, int64_t W, S* __restrict__ tv_map,
+                                                              double* __restrict__ partials) {
+    const int64_t total = B * D * H * W;
+    const int64_t HW = H * W, DHW = D * HW;
+    double sum = 0;
+    for (int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; idx < total;
+         idx += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t r = idx % DHW;
+        const int64_t d = r / HW;
+        const int64_t hw = r - d * HW;
+        const int64_t h = hw / W;
+        const int64_t w = hw - h * W;
+        const S val = vol[idx];
+        S tv = 0;
+        if (d + 1 < D) tv += abs_diff(vol[idx + HW] - val);
+        if (h + 1 < H) tv += abs_diff(vol[idx + W] - val);
+        if (w + 1 < W) tv += abs_diff(vol[idx + 1] - val);
+        if (tv_map != nullptr) tv_map[idx] = tv;
+        sum += static_cast<double>(tv);
+    }
+    const double total_sum = block_sum(sum);
+    if (threadIdx.x == 0) partials[blockIdx.x] = total_sum;
+}
+
+template <typename S>
+__global__ void __launch_bounds__(kLossThreads) l1_fwd_kernel(const S* __restrict__ pred, const S* __restrict__ tgt,
+                                                              int64_t total, S* __restrict__ l1_map,
+                                                              double* __restrict__ partials) {
+    double sum = 0;
+    for (int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; idx < total;
+         idx += int64_t(gridDim.x) * blockDim.x) {
+        const S v = abs_diff(pred[idx] - tgt[idx]);
+        if (l1_map != nullptr) l1_map[idx] = v;
+        sum += static_cast<double>(v);
+    }
+    const double total_sum = block_sum(sum);
+    if (threadIdx.x == 0) partials[blockIdx.x] = total_sum;
+}
+
+// Sums the per-block partials in order; value = sum / count, loss = lambda * value.
+template <typename S>
+__global__ void finish_mean_kernel(const double* __restrict__ partials, int n_partials, int64_t count,
+                                   float lambda, S* __restrict__ loss, S* __restrict__ value) {
+    __shared__ double s[kLossThreads];
+    double v = 0;
+    for (int i = threadIdx.x; i < n_partials; i += kLossThreads) v += partials[i];
+    s[threadIdx.x] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double total = 0;
+        for (int i = 0; i < kLossThreads; ++i) total += s[i];
+        const S mean = static_cast<S>(total / static_cast<double>(count > 0 ? count : 1));
+        *value = mean;
+        *loss = static_cast<S>(lambda) * mean;
+    }
+}
+
+template <typename S>
+__global__ void tv_bwd_kernel(const S* __restrict__ vol, const S* __restrict__ grad_output, int64_t B, int64_t D,
+                              int64_t H, int64_t W, int64_t edges, float lambda, S* __restrict__ grad) {
+    const int64_t total = B * D * H * W;
+    const int64_t HW = H * W, DHW = D * HW;
+    const S grad_out = grad_output[0] / static_cast<S>(edges);
+    const S lam = static_cast<S>(lambda);
+    for (int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; idx < total;
+         idx += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t r = idx % DHW;
+        const int64_t d = r / HW;
+        const int64_t hw = r - d * HW;
+        const int64_t h = hw / W;
+        const int64_t w = hw - h * W;
+        const S val = vol[idx];
+        S g = 0;
+        if (d + 1 < D) g -= sign_of(vol[idx + HW] - val);
+        if (d > 0) g += sign_of(val - vol[idx - HW]);
+        if (h + 1 < H) g -= sign_of(vol[idx + W] - val);
+        if (h > 0) g += sign_of(val - vol[idx - W]);
+        if (w + 1 < W) g -= sign_of(vol[idx + 1] - val);
+        if (w > 0) g += sign_of(val - vol[idx - 1]);
+        grad[idx] = (g * grad_out) * lam;
+    }
+}
+
+template <typename S>
+__global__ void l1_bwd_kernel(const S* __restrict__ pred, const S* __restrict__ tgt, const S* __restrict__ grad_output,
+                              int64_t total, float lambda, S* __restrict__ grad) {
+    const S lam = static_cast<S>(lambda);
+    for (int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; idx < total;
+         idx += int64_t(gridDim.x) * blockDim.x) {
+        const S s = sign_of(pred[idx] - tgt[idx]);
+        grad[idx] = grad_output[0] * lam * s / static_cast<S>(total);
+    }
+}
+
+inline unsigned loss_blocks(int64_t total) {
+    int64_t b = (total + kLossThreads - 1) / kLossThreads;
+    if (b > kLossMaxBlocks) b = kLossMaxBlocks;
+    if (b < 1) b = 1;
+    return unsigned(b);
+}
+
+}  // namespace r2s
+
+using namespace r2s;
+
+extern "C" {
+
+size_t r2s_volume_loss_workspace(uint64_t numel) {
+    (void)numel;
+    return size_t(kLossMaxBlocks) * sizeof(double) + 256;
+}
+
+int r2s_volume_loss_fwd(int dtype, const void* volume, uint32_t B, uint32_t D, uint32_t H, uint32_t W,
+                        float lambda_tv, void* loss, void* tv, void* tv_map, void* workspace, size_t workspace_bytes,
+                        void* stream) {
+    const int64_t total = int64_t(B) * D * H * W;
+    const int64_t edges_raw = int64_t(B) * ((int64_t(D) - 1) * H * W + int64_t(D) * (H - 1) * W +
+                                            int64_t(D) * H * (int64_t(W) - 1));
+    const int64_t edges = edges_raw > 1 ? edges_raw : 1;
+    Arena arena(workspace, workspace_bytes);
+    const unsigned blocks = loss_blocks(total);
+    double* partials = arena.take<double>(blocks);
+    R2S_REQUIRE(partials, R2S_ERR_WORKSPACE, "loss workspace too small");
+    cudaStream_t st = as_stream(stream);
+    R2S_DISPATCH(dtype, {
+        if (total > 0) {
+            tv_fwd_kernel<S><<<blocks, kLossThreads, 0, st>>>(static_cast<const S*>(volume), B, D, H, W,
+                                                             static_cast<S*>(tv_map), partials);
+            R2S_TRY(check_launch("volume_loss_fwd"));
+        }
+        finish_mean_kernel<S><<<1, kLossThreads, 0, st>>>(partials, total > 0 ? int(blocks) : 0, edges, lambda_tv,
+                                                         static_cast<S*>(loss), static_cast<S*>(tv));
+        return check_launch("volume_loss_finish");
+    });
+}
+
+int r2s_volume_loss_bwd(int dtype, const void* volume, const void* grad_output, uint32_t B, uint32_t D, uint32_t H,
+                        uint32_t W, float lambda_tv, void* grad_volume, void* stream) {
+    const int64_t total = int64_t(B) * D * H * W;
+    if (total == 0) return R2S_OK;
+    const int64_t edges_raw = int64_t(B) * ((int64_t(D) - 1) * H * W + int64_t(D) * (H - 1) * W +
+                                            int64_t(D) * H * (int64_t(W) - 1));
+    const int64_t edges = edges_raw > 1 ? edges_raw : 1;
+    R2S_DISPATCH(dtype, {
+        tv_bwd_kernel<S><<<loss_blocks(total), kLossThreads, 0, as_stream(stream)>>>(
+            static_cast<const S*>(volume), static_cast<const S*>(grad_output), B, D, H, W, edges, lambda_tv,
+            static_cast<S*>(grad_volume));
+        return check_launch("volume_loss_bwd");
+    });
+}
+
+int r2s_image_loss_l1_fwd(int dtype, const void* prediction, const void* target, uint32_t B, uint32_t H, uint32_t W,
+                          float lambda_l1, void* loss, void* l1, void* l1_map, void* workspace,
+                          size_t workspace_bytes, void* stream) {
+    const int64_t total = int64_t(B) * H * W;
+    Arena arena(workspace, workspace_bytes);
+    const unsigned blocks = loss_blocks(total);
+    double* partials = arena.take<double>(blocks);
+    R2S_REQUIRE(partials, R2S_ERR_WORKSPACE, "loss workspace too small");
+    cudaStream_t st = as_stream(stream);
+    R2S_DISPATCH(dtype, {
+        if (total > 0) {
+            l1_fwd_kernel<S><<<blocks, kLossThreads, 0, st>>>(static_cast<const S*>(prediction),
+                                                             static_cast<const S*>(target), total,
+                                                             static_cast<S*>(l1_map), partials);
+            R2S_TRY(check_launch("image_loss_fwd"));
+        }
+        finish_mean_kernel<S><<<1, kLossThreads, 0, st>>>(partials, total > 0 ? int(blocks) : 0, total, lambda_l1,
+                                                         static_cast<S*>(loss), static_cast<S*>(l1));
+        return check_launch("image_loss_finish");
+    });
+}
+
+int r2s_image_loss_l1_bwd(int dtype, const void* prediction, const void* target, const void* grad_output, uint32_t B,
+                          uint32_t H, uint32_t W, float lambda_l1, void* grad_prediction, void* stream) {
+    const int64_t total = int64_t(B) * H * W;
+    if (total == 0) return R2S_OK;
+    R2S_DISPATCH(dtype, {
+        l1_bwd_kernel<S><<<loss_blocks(total), kLossThreads, 0, as_stream(stream)>>>(
+            static_cast<const S*>(prediction), static_cast<const S*>(target), static_cast<const S*>(grad_output), total,
+            lambda_l1, static_cast<S*>(grad_prediction));
+        return check_launch("image_loss_bwd");
+    });
+}
+
+}  // extern "C"

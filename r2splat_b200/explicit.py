@@ -1,0 +1,270 @@
+"""Explicit CUDA forward/VJP calls for physical primitive parameters.
+
+Same public contract as the reference's ``r2splat/explicit.py``:
+``rasterize_fwd`` (:102-188), ``rasterize_bwd`` (:191-242), ``voxelize_fwd``
+(:245-311), ``voxelize_bwd`` (:314-351), the one-shot context with tensor
+version guards (:37-99) and ``ParameterGradients`` (:25-34). Forward returns
+``(output, context)`` without recording an autograd graph; backward consumes
+the context once and returns gradients without writing ``.grad``. Geometry is
+constant; activations and loss derivatives belong to the caller.
+
+The device work runs through the fused sm_100a pipelines in ``_fused``.
+``backward_mode`` is accepted for compatibility: "pixel" and "primitive" give
+the same VJP here (one tile kernel serves both; they differ only in float
+summation order in the reference).
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+from typing import Optional, Sequence, Union
+
+import torch
+
+from . import _fused
+from ._validation import _constant, _options, _primitives, _shape, _tensor, _vector
+
+Tensor = torch.Tensor
+Output = Union[Tensor, tuple[Tensor, Tensor]]
+_PRIMITIVE_NAMES = ("means", "quats", "scales", "densities", "beta", "uncertainty")
+
+
+@dataclass
+class ParameterGradients:
+    """VJP tensors matching the physical inputs; absent optional inputs give None."""
+
+    means: Tensor
+    quats: Tensor
+    scales: Tensor
+    densities: Tensor
+    beta: Optional[Tensor] = None
+    uncertainty: Optional[Tensor] = None
+
+
+@dataclass
+class _Context:
+    kind: str
+    shape: tuple
+    primitives: tuple
+    buffers: dict
+    versions: tuple
+    eps: float
+    backward_mode: str
+    detach_variance: bool
+    used: bool = False
+
+
+def _mode(value):
+    value = str(value).lower()
+    if value not in ("pixel", "primitive"):
+        raise ValueError("backward_mode must be 'pixel' or 'primitive'")
+    return value
+
+
+def _context(kind, shape, primitives, buffers, originals, eps, mode, detach_variance):
+    """Snapshots the version counter of every input and saved tensor."""
+    watched, seen = [], set()
+    entries = list(originals) + list(zip(_PRIMITIVE_NAMES, primitives)) + [
+        (name, value) for name, value in buffers.items() if isinstance(value, Tensor)]
+    for name, value in entries:
+        if isinstance(value, Tensor) and id(value) not in seen:
+            try:
+                version = value._version
+            except RuntimeError as error:
+                raise ValueError("explicit contexts require tensors with version counters") from error
+            watched.append((name, value, version))
+            seen.add(id(value))
+    return _Context(kind, shape, primitives, buffers, tuple(watched), eps, mode, detach_variance)
+
+
+def _check_context(context, kind):
+    if not isinstance(context, _Context) or context.kind != kind:
+        raise TypeError(f"expected a context returned by {kind}_fwd")
+    if context.used:
+        raise RuntimeError("this context has already been consumed by backward")
+    for name, value, version in context.versions:
+        if value._version != version:
+            raise RuntimeError(f"saved input {name} was modified in-place after forward")
+
+
+def _adjoint(name, value, context):
+    return None if value is None else _tensor(name, value, context.shape, context.primitives[0])
+
+
+def _zero_gradients(context):
+    return ParameterGradients(*(None if value is None else torch.zeros_like(value) for value in context.primitives))
+
+
+def _consume(context, gradients):
+    context.used = True
+    context.primitives = ()
+    context.buffers.clear()
+    context.versions = ()
+    return gradients
+
+
+@torch.no_grad()
+def rasterize_fwd(
+    means: Tensor,
+    quats: Tensor,
+    scales: Tensor,
+    densities: Tensor,
+    viewmats: Tensor,
+    Ks: Tensor,
+    image_size: Sequence[int],
+    *,
+    beta: Optional[Tensor] = None,
+    uncertainty: Optional[Tensor] = None,
+    eps: float = 1.0e-8,
+    radius_clip: Optional[float] = None,
+    detach_variance: bool = False,
+    backward_mode: str = "primitive",
+) -> tuple[Output, _Context]:
+    """Project physical primitives, returning a detached image and VJP context.
+
+    World-to-camera ``viewmats [C,4,4]`` and pinhole ``Ks [C,3,3]`` are
+    constant. Output is ``[C,height,width]`` or ``(image, variance)`` with
+    uncertainty. No input needs requires_grad.
+    """
+    originals = list(zip(
+        ("means", "quats", "scales", "densities", "viewmats", "Ks", "beta", "uncertainty"),
+        (means, quats, scales, densities, viewmats, Ks, beta, uncertainty),
+    ))
+    height, width = _shape("image_size", image_size, 2)
+    primitives = _primitives(means, quats, scales, densities, beta, uncertainty)
+    means, quats, scales, densities, beta, uncertainty = primitives
+    eps, radius_clip = _options(beta, eps, radius_clip, detach_variance)
+    mode = _mode(backward_mode)
+    # Check the originals: a contiguous copy under no_grad drops requires_grad.
+    for name, value in (("viewmats", viewmats), ("Ks", Ks)):
+        if isinstance(value, Tensor):
+            _constant(name, value)
+    viewmats = _constant("viewmats", _tensor("viewmats", viewmats, (None, 4, 4), means))
+    cameras = viewmats.shape[0]
+    if cameras == 0:
+        raise ValueError("viewmats must contain at least one camera")
+    if cameras * max(height * width, means.shape[0]) > 2**31 - 1 or cameras > 65535:
+        raise ValueError("camera batch exceeds CUDA indexing or grid limits")
+    if max(height, width) > 16 * 65535:
+        raise ValueError("image_size exceeds CUDA grid limits")
+    Ks = _constant("Ks", _tensor("Ks", Ks, (cameras, 3, 3), means))
+    if bool((Ks[:, (0, 1), (0, 1)] <= 0).any()):
+        raise ValueError("Ks must have positive fx and fy")
+    if bool((Ks[:, (0, 1, 2, 2), (1, 0, 0, 1)] != 0).any()) or bool((Ks[:, 2, 2] != 1).any()):
+        raise ValueError("Ks must be pinhole intrinsics with zero skew and last row [0, 0, 1]")
+    if not torch.equal(viewmats[:, 3], means.new_tensor([0, 0, 0, 1]).expand(cameras, -1)):
+        raise ValueError("viewmats must have homogeneous last row [0, 0, 0, 1]")
+    shape = (cameras, height, width)
+    buffers = {"viewmats": viewmats, "Ks": Ks}
+    if means.shape[0] == 0:
+        image = means.new_zeros(shape)
+        output = image if uncertainty is None else (image, image.clone())
+    else:
+        with torch.cuda.device(means.device):
+            output, state = _fused.raster_forward(means, quats, scales, densities, viewmats, Ks, width, height,
+                                                  beta, uncertainty, eps, radius_clip)
+        buffers.update(state=state, covars=state.covars, records=state.records, offsets=state.offsets,
+                       isect_ids=state.isect_ids, flatten_ids=state.flatten_ids, ratio=state.ratio)
+    context = _context("rasterize", shape, primitives, buffers, originals, eps, mode, detach_variance)
+    return output, context
+
+
+@torch.no_grad()
+def rasterize_bwd(context: _Context, v_image: Optional[Tensor], v_variance: Optional[Tensor] = None
+                  ) -> ParameterGradients:
+    """Consume a projection context and return physical-parameter gradients.
+
+    Adjoint tensors match the output's shape, device, and dtype. None denotes
+    a zero adjoint, including variance-only losses. Inputs must remain unchanged.
+    """
+    _check_context(context, "rasterize")
+    means, quats, scales, densities, beta, uncertainty = context.primitives
+    if v_variance is not None and uncertainty is None:
+        raise ValueError("v_variance requires uncertainty in the forward call")
+    v_image = _adjoint("v_image", v_image, context)
+    v_variance = _adjoint("v_variance", v_variance, context)
+    if means.shape[0] == 0 or (v_image is None and v_variance is None):
+        return _consume(context, _zero_gradients(context))
+    b = context.buffers
+    with torch.cuda.device(means.device):
+        grads = _fused.raster_backward(b["state"], means, quats, scales, densities, beta, uncertainty,
+                                       b["viewmats"], b["Ks"], context.eps, v_image, v_variance,
+                                       context.detach_variance)
+    return _consume(context, ParameterGradients(*grads))
+
+
+@torch.no_grad()
+def voxelize_fwd(
+    means: Tensor,
+    quats: Tensor,
+    scales: Tensor,
+    densities: Tensor,
+    volume_shape: Sequence[int],
+    *,
+    volume_extent: Union[Tensor, Sequence[float]],
+    volume_center: Union[Tensor, Sequence[float]] = (0.0, 0.0, 0.0),
+    beta: Optional[Tensor] = None,
+    uncertainty: Optional[Tensor] = None,
+    eps: float = 1.0e-8,
+    radius_clip: Optional[float] = None,
+    detach_variance: bool = False,
+    backward_mode: str = "primitive",
+) -> tuple[Output, _Context]:
+    """Sample physical primitives, returning a detached volume and VJP context.
+
+    ``volume_shape`` and output use ``[depth,height,width]``; physical extent
+    and center use xyz order. With uncertainty, output is ``(volume, variance)``.
+    """
+    originals = list(zip(
+        ("means", "quats", "scales", "densities", "volume_extent", "volume_center", "beta", "uncertainty"),
+        (means, quats, scales, densities, volume_extent, volume_center, beta, uncertainty),
+    ))
+    depth, height, width = _shape("volume_shape", volume_shape, 3)
+    if max(height, width) > 8 * 65535:
+        raise ValueError("volume_shape exceeds CUDA grid limits")
+    primitives = _primitives(means, quats, scales, densities, beta, uncertainty)
+    means, quats, scales, densities, beta, uncertainty = primitives
+    eps, radius_clip = _options(beta, eps, radius_clip, detach_variance)
+    mode = _mode(backward_mode)
+    for name, value in (("volume_extent", volume_extent), ("volume_center", volume_center)):
+        if isinstance(value, Tensor):
+            _constant(name, value)
+    extent = _vector("volume_extent", volume_extent, means)
+    center = _vector("volume_center", volume_center, means)
+    if bool((extent <= 0).any()):
+        raise ValueError("volume_extent must contain positive physical lengths")
+    shape = (depth, height, width)
+    buffers = {"extent": extent, "center": center}
+    if means.shape[0] == 0:
+        volume = means.new_zeros(shape)
+        output = volume if uncertainty is None else (volume, volume.clone())
+    else:
+        with torch.cuda.device(means.device):
+            output, state = _fused.voxel_forward(means, quats, scales, densities, shape, extent, center, beta,
+                                                 uncertainty, eps, radius_clip)
+        buffers.update(state=state, covars=state.covars, records=state.records, offsets=state.offsets,
+                       isect_ids=state.isect_ids, flatten_ids=state.flatten_ids)
+    context = _context("voxelize", shape, primitives, buffers, originals, eps, mode, detach_variance)
+    return output, context
+
+
+@torch.no_grad()
+def voxelize_bwd(context: _Context, v_volume: Optional[Tensor], v_variance: Optional[Tensor] = None
+                 ) -> ParameterGradients:
+    """Consume a volume context and return gradients without updating inputs."""
+    _check_context(context, "voxelize")
+    means, quats, scales, densities, beta, uncertainty = context.primitives
+    if v_variance is not None and uncertainty is None:
+        raise ValueError("v_variance requires uncertainty in the forward call")
+    v_volume = _adjoint("v_volume", v_volume, context)
+    v_variance = _adjoint("v_variance", v_variance, context)
+    if means.shape[0] == 0 or (v_volume is None and v_variance is None):
+        return _consume(context, _zero_gradients(context))
+    b = context.buffers
+    with torch.cuda.device(means.device):
+        grads = _fused.voxel_backward(b["state"], means, quats, scales, beta, uncertainty, b["extent"],
+                                      b["center"], context.eps, v_volume, v_variance, context.detach_variance)
+    return _consume(context, ParameterGradients(*grads))
+
+
+__all__ = ["ParameterGradients", "rasterize_fwd", "rasterize_bwd", "voxelize_fwd", "voxelize_bwd"]
