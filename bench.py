@@ -1,0 +1,486 @@
+#!/usr/bin/env python
+"""Benchmark: fwd+bwd Gaussian-sample evaluations per second of one CT fit step.
+
+Workload (the CT-scale plain Gaussian scene, fp32): N=200,000 Gaussians
+(means ~ U[-0.5,0.5]^3, quats ~ N(0,1)^4, scales ~ exp(N(log 0.01, 0.4)),
+densities = softplus(N(0,1)), seed 0), C=64 views on a circular cone-beam
+trajectory of radius 3, 512x512 detector (f=600, c=(256,256)). One fit step:
+  rasterize_fwd -> v_image = 2 (image - target) / numel (target rendered once
+  from means perturbed by N(0, 0.005), seed 2) -> rasterize_bwd;
+  voxelize_fwd on 256^3 of extent 1 -> TV loss fwd/bwd (lambda 0.05) ->
+  voxelize_bwd with the TV gradient as the upstream adjoint.
+A "Gaussian-sample evaluation" is one (primitive, pixel) or (primitive, voxel)
+pair inside an intersected tile: per pass, the sum over intersections of the
+in-bounds pixels (voxels) of the intersection's tile. value counts the raster
+and voxel forward and backward passes of a step.
+
+Arms:
+  --impl ours       this package (device-resident inputs for ``value``; the
+                    public API with pinned host buffers for ``e2e``)
+  --impl reference  the reference's own CUDA build (oracle/_ref, compiled
+                    unmodified from the reference sources) driven through a
+                    restatement of the reference's explicit.py call sequence
+
+Under torchrun each rank runs its own replica of the workload (weak scaling,
+no data-path collective); the timing is the max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import torch
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+L2_FLUSH_BYTES = 512 << 20
+FLOPS_PER_EVAL = {
+    # FP32 operations per (primitive, pixel) sample of the Gaussian kernels,
+    # counted from the reference formulas (RasterizeToPixelsFwd.cu:160-177,
+    # RasterizeToPixelsBwd.cu:417-468), an FMA counting as two:
+    # forward: offsets 2, quadratic form 8, exp argument 1 (+1 MUFU), alpha 1,
+    # two threshold compares, accumulate 1 -> 16;
+    # backward: forward part 14 + v_sigma 1 + mean adjoint 8 + 2 accumulates
+    # + conic adjoints 11 + density / mu adjoints 6 -> 44.
+    "raster_render": 16, "raster_render_bwd": 44,
+}
+
+
+# --------------------------------------------------------------------------- utilities
+
+def dist_info():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.samples: list[list[str]] = []
+        self._proc = None
+        self._thread = None
+
+    def __enter__(self):
+        try:
+            self._proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100",
+                 "-i", str(self.gpu)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._thread = threading.Thread(target=self._read, daemon=True)
+            self._thread.start()
+        except (OSError, ValueError):
+            self._proc = None
+        return self
+
+    def _read(self):
+        for line in self._proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.samples.append(parts)
+
+    def __exit__(self, *exc):
+        if self._proc is not None:
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self._proc.kill()
+        if self._thread is not None:
+            self._thread.join(timeout=5)
+        return False
+
+    def summary(self) -> dict:
+        clocks, maxes, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s in self.samples:
+            try:
+                clocks.append(float(s[1]))
+                maxes.append(float(s[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, s[5:9]):
+                if flag.strip().lower() in ("active", "1"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(clocks) if clocks else None,
+                "sm_max_mhz": max(maxes) if maxes else None, "reasons": sorted(reasons),
+                "samples": len(clocks)}
+
+
+def measured_peaks() -> dict:
+    path = ROOT / "MEASURED_PEAKS.json"
+    try:
+        return json.loads(path.read_text())
+    except (OSError, ValueError):
+        return {}
+
+
+def flush_l2(buf: torch.Tensor):
+    buf.add_(1.0)
+
+
+def count_evals_2d(offsets: torch.Tensor, n_isects: int, height: int, width: int, tile: int) -> int:
+    """Sum over intersections of the in-bounds pixels of their tile."""
+    c, ty, tx = offsets.shape
+    flat = offsets.reshape(-1).to(torch.int64)
+    ends = torch.cat([flat[1:], flat.new_tensor([n_isects])])
+    counts = (ends - flat).reshape(c, ty, tx)
+    rows = torch.clamp(height - torch.arange(ty, device=offsets.device) * tile, max=tile)
+    cols = torch.clamp(width - torch.arange(tx, device=offsets.device) * tile, max=tile)
+    pix = rows[:, None] * cols[None, :]
+    return int((counts * pix[None]).sum().item())
+
+
+def count_evals_3d(offsets: torch.Tensor, n_isects: int, shape: tuple, tile: int) -> int:
+    tz, ty, tx = offsets.shape
+    flat = offsets.reshape(-1).to(torch.int64)
+    ends = torch.cat([flat[1:], flat.new_tensor([n_isects])])
+    counts = (ends - flat).reshape(tz, ty, tx)
+    d, h, w = shape
+    ar = lambda n, s: torch.clamp(s - torch.arange(n, device=offsets.device) * tile, max=tile)
+    vox = ar(tz, d)[:, None, None] * ar(ty, h)[None, :, None] * ar(tx, w)[None, None, :]
+    return int((counts * vox).sum().item())
+
+
+# --------------------------------------------------------------------------- the fit step
+
+class OursStep:
+    """One fit step through this package's public explicit operators."""
+
+    def __init__(self, scene, target, lambda_tv=0.05):
+        import r2splat_b200 as r2s
+        from r2splat_b200.cuda import _wrapper as low
+
+        self.r2s, self.low = r2s, low
+        self.scene, self.target, self.lam = scene, target, lambda_tv
+        self.ones = torch.ones(1, device=scene.means.device)
+        self.last = {}
+
+    def __call__(self, means, quats, scales, densities):
+        sc = self.scene
+        image, ctx = self.r2s.rasterize_fwd(means, quats, scales, densities, sc.viewmats, sc.Ks, sc.image_size)
+        self.last["raster_state"] = ctx.buffers["state"]
+        v_image = 2 * (image - self.target) / image.numel()
+        g = self.r2s.rasterize_bwd(ctx, v_image)
+        volume, vctx = self.r2s.voxelize_fwd(means, quats, scales, densities, sc.volume_shape,
+                                             volume_extent=sc.volume_extent)
+        self.last["voxel_state"] = vctx.buffers["state"]
+        vol4 = volume.unsqueeze(0)
+        loss, _, _ = self.low.volume_loss_fwd(vol4, self.lam)
+        g_vol = self.low.volume_loss_bwd(vol4, self.ones, self.lam)[0]
+        gv = self.r2s.voxelize_bwd(vctx, g_vol)
+        return loss, (g.means + gv.means, g.quats + gv.quats, g.scales + gv.scales, g.densities + gv.densities)
+
+    def eval_counts(self):
+        rs, vs = self.last["raster_state"], self.last["voxel_state"]
+        h, w = self.scene.image_size
+        raster = count_evals_2d(rs.offsets, rs.n_isects, h, w, rs.tile_size)
+        voxel = count_evals_3d(vs.offsets, vs.n_isects, vs.shape, vs.tile_size)
+        return raster, voxel, rs.n_isects, vs.n_isects
+
+
+class ReferenceStep:
+    """The same fit step on the reference's own CUDA kernels (oracle/_ref)."""
+
+    def __init__(self, scene, target, lambda_tv=0.05):
+        from oracle import ref_ops
+
+        self.ref_ops = ref_ops
+        self.ref = ref_ops.load()
+        self.scene, self.target, self.lam = scene, target, lambda_tv
+        self.ones = torch.ones(1, device=scene.means.device)
+        self.last = {}
+
+    def __call__(self, means, quats, scales, densities):
+        sc, ro = self.scene, self.ref_ops
+        image, saved = ro.explicit_rasterize_fwd(means, quats, scales, densities, sc.viewmats, sc.Ks, sc.image_size)
+        self.last["raster"] = saved
+        v_image = 2 * (image - self.target) / image.numel()
+        g = ro.explicit_rasterize_bwd(saved, means, quats, scales, None, None, v_image)
+        volume, vsaved = ro.explicit_voxelize_fwd(means, quats, scales, densities, sc.volume_shape,
+                                                  volume_extent=sc.volume_extent)
+        self.last["voxel"] = vsaved
+        vol4 = volume.unsqueeze(0)
+        loss, _, _ = self.ref.volume_loss_fwd(vol4, self.lam)
+        g_vol = self.ref.volume_loss_bwd(vol4, self.ones, self.lam)[0]
+        gv = ro.explicit_voxelize_bwd(vsaved, means, quats, scales, densities, None, None, g_vol)
+        return loss, tuple(a + b for a, b in zip(g[:4], gv[:4]))
+
+    def eval_counts(self):
+        r, v = self.last["raster"], self.last["voxel"]
+        h, w = self.scene.image_size
+        raster = count_evals_2d(r["offsets"], r["isect_ids"].numel(), h, w, 16)
+        voxel = count_evals_3d(v["offsets"], v["isect_ids"].numel(), v["shape"], 8)
+        return raster, voxel, r["isect_ids"].numel(), v["isect_ids"].numel()
+
+
+def build_workload(device, workload: str):
+    from r2splat_b200 import scenes
+
+    if workload == "ct":
+        scene = scenes.ct_scene()
+    elif workload == "small":
+        scene = scenes.small_scene()
+    else:
+        raise SystemExit(f"unknown workload {workload}")
+    scene = scene.to(device)
+    target_scene = scene.to(device)
+    target_scene.means = scenes.perturbed_means(scene.means)
+    import r2splat_b200 as r2s
+
+    target, _ = r2s.rasterize_fwd(*target_scene.primitives, target_scene.viewmats, target_scene.Ks,
+                                  target_scene.image_size)
+    return scene, target
+
+
+def fp32_peak_tflops(device) -> float:
+    """Measured FP32 FMA issue peak (TFLOP/s) on this GPU, CUDA events, best of 5."""
+    import ctypes
+
+    from r2splat_b200.cuda import _backend
+
+    out = torch.zeros(4096, device=device)
+    props = torch.cuda.get_device_properties(device)
+    blocks, threads, iters = props.multi_processor_count * 8, 256, 2048
+    stream = ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+    best = 0.0
+    for _ in range(6):
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        _backend.call("r2s_fp32_peak_probe", ctypes.c_void_p(out.data_ptr()), blocks, threads, iters, stream)
+        end.record()
+        end.synchronize()
+        ms = start.elapsed_time(end)
+        flops = 2.0 * blocks * threads * iters * 128
+        best = max(best, flops / (ms * 1e-3) / 1e12)
+    return best
+
+
+def cpu_baseline(budget_s: float = 15.0) -> dict:
+    """fp64 dense oracle on the host cores: raster fwd+bwd evaluations per second on a bounded sample."""
+    from oracle import dense
+    from r2splat_b200 import scenes
+
+    threads = os.cpu_count() or 1
+    torch.set_num_threads(threads)
+    sc = scenes.ct_scene(dtype=torch.float64)
+    view = slice(0, 1)
+    n = 64
+    prims = [t[:n].clone().requires_grad_(True) for t in sc.primitives]
+    evals = 0
+    t0 = time.perf_counter()
+    reps = 0
+    while True:
+        img = dense.rasterize_dense(*prims, sc.viewmats[view], sc.Ks[view], sc.image_size, eps=1e-8, chunk=16)
+        grads = torch.autograd.grad(img.sum(), prims)
+        evals += 2 * n * sc.image_size[0] * sc.image_size[1]
+        reps += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    elapsed = time.perf_counter() - t0
+    del grads
+    return {"value": evals / elapsed, "unit": "evals/s", "cores": threads, "kind": "port",
+            "sample": f"float64 dense oracle (oracle/dense.py): {n} Gaussians x 1 view x 512x512, raster fwd+bwd "
+                      f"(autograd), {reps} repetitions in {elapsed:.1f}s; dense evals counted"}
+
+
+def timed_run(step, scene, steps, warmup, device, flush_buf):
+    """Device-resident inputs; per-step CUDA events with an L2 flush between steps."""
+    from r2splat_b200 import _fused
+
+    prims = scene.primitives
+    for _ in range(warmup):
+        step(*prims)
+    torch.cuda.synchronize()
+    timer = _fused.StageTimer()
+    total_ms = 0.0
+    for _ in range(steps):
+        flush_l2(flush_buf)
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        _fused.StageTimer.active = timer
+        start.record()
+        step(*prims)
+        end.record()
+        _fused.StageTimer.active = None
+        end.synchronize()
+        total_ms += start.elapsed_time(end)
+    torch.cuda.synchronize()
+    return total_ms, timer.totals_ms()
+
+
+def e2e_run(step, scene, steps, warmup, device):
+    """Public API with pinned host inputs copied in and gradients copied out each step."""
+    host = [t.detach().cpu().pin_memory() for t in scene.primitives]
+    outs = None
+    h2d = sum(t.numel() * t.element_size() for t in host)
+    d2h = 0
+    for i in range(warmup + steps):
+        if i == warmup:
+            torch.cuda.synchronize()
+            start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record()
+        dev = [t.to(device, non_blocking=True) for t in host]
+        loss, grads = step(*dev)
+        if outs is None:
+            outs = [torch.empty(g.shape, dtype=g.dtype, pin_memory=True) for g in grads] + [
+                torch.empty((), dtype=loss.dtype, pin_memory=True)]
+            d2h = sum(o.numel() * o.element_size() for o in outs)
+        for o, g in zip(outs, list(grads) + [loss]):
+            o.copy_(g, non_blocking=True)
+    end.record()
+    end.synchronize()
+    return start.elapsed_time(end), h2d, d2h
+
+
+def count_launches(step, scene, prefix: str) -> int:
+    from torch.profiler import ProfilerActivity, profile
+
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        step(*scene.primitives)
+        torch.cuda.synchronize()
+    return sum(e.count for e in prof.key_averages() if prefix in e.key)
+
+
+def main(argv=None) -> int:
+    parser = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    parser.add_argument("--gpus", type=int, default=1)
+    parser.add_argument("--steps", type=int, default=20)
+    parser.add_argument("--warmup", type=int, default=3)
+    parser.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    parser.add_argument("--workload", choices=("ct", "small"), default="ct")
+    parser.add_argument("--cpu-budget", type=float, default=15.0)
+    parser.add_argument("--no-cpu-baseline", action="store_true")
+    args = parser.parse_args(argv)
+    if args.warmup < 3:
+        parser.error("--warmup must be at least 3")
+
+    world, rank, local = dist_info()
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+
+    if args.impl == "reference":
+        from oracle import ref_ops
+
+        # The reference arm runs on rank 0 only; other ranks wait and exit.
+        if world > 1 and rank != 0:
+            dist.barrier()
+            dist.destroy_process_group()
+            return 0
+        if not ref_ops.available():
+            print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref missing"}))
+            if world > 1:
+                dist.barrier()
+                dist.destroy_process_group()
+            return 0
+
+    scene, target = build_workload(device, args.workload)
+    step = OursStep(scene, target) if args.impl == "ours" else ReferenceStep(scene, target)
+    flush_buf = torch.zeros(L2_FLUSH_BYTES // 4, device=device)
+
+    if world > 1 and args.impl == "ours":
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        total_ms, stages = timed_run(step, scene, args.steps, args.warmup, device, flush_buf)
+    if world > 1 and args.impl == "ours":
+        t = torch.tensor([total_ms], device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    raster_evals, voxel_evals, m2, m3 = step.eval_counts()
+    evals_per_step = 2 * raster_evals + 2 * voxel_evals
+    value = evals_per_step * (world if args.impl == "ours" else 1) / (ms_per_step * 1e-3)
+
+    e2e_ms, h2d, d2h = e2e_run(step, scene, args.steps, args.warmup, device)
+    e2e_value = evals_per_step * (world if args.impl == "ours" else 1) / (e2e_ms / args.steps * 1e-3)
+    prefix = "r2s::" if args.impl == "ours" else "r2splat::"
+    launches = count_launches(step, scene, prefix) * args.steps
+
+    peaks = measured_peaks()
+    result = {
+        "metric": "fwd+bwd Gaussian-sample evals/s (CT fit step: raster 64x512^2 + voxel 256^3 + TV)",
+        "value": value,
+        "unit": "evals/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_per_step,
+        "fit_steps_per_s": (world if args.impl == "ours" else 1) * 1e3 / ms_per_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded scene generator, r2splat_b200/scenes.py)",
+        "config": {
+            "workload": "ct-plain-gaussian: N=200000, C=64 views R=3, 512x512 f=600, volume 256^3, TV lambda 0.05"
+            if args.workload == "ct" else "small: N=2000, C=4, 64x64, volume 32^3",
+            "raster_isects": m2, "voxel_isects": m3,
+            "raster_evals_per_pass": raster_evals, "voxel_evals_per_pass": voxel_evals,
+            "l2": "flushed (512 MiB write) between timed steps",
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+        },
+        "clocks": clocks.summary(),
+        "e2e": {"value": e2e_value, "unit": "evals/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "stages_ms_per_step": {k: v / args.steps for k, v in stages.items()},
+    }
+    if args.impl == "reference":
+        result["impl"] = "reference"
+        result["e2e"] = {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+        result["cpu_baseline"] = {
+            "value": value, "unit": "evals/s", "cores": 0, "kind": "reference",
+            "sample": "the reference's own CUDA kernels (compiled unmodified from its sources for sm_100a) on the "
+                      "same B200, driven by its explicit.py call sequence; the reference has no CPU implementation "
+                      "of these operators",
+        }
+    else:
+        kernel = "raster_render_bwd"
+        kernel_ms = stages.get(kernel, 0.0) / args.steps
+        achieved = FLOPS_PER_EVAL[kernel] * raster_evals / (kernel_ms * 1e-3) / 1e12 if kernel_ms else None
+        peak = fp32_peak_tflops(device)
+        result["roofline"] = {
+            "kernel": "raster_bwd_kernel (tile VJP)",
+            "bound": "fp32",
+            "achieved": achieved,
+            "peak": peak,
+            "unit": "TFLOP/s",
+            "frac": achieved / peak if achieved else None,
+            "traffic": None,
+            "peak_source": "measured in-bench: FP32 FMA probe r2s_fp32_peak_probe (MEASURED_PEAKS.json has no "
+                           "FP32 figure)",
+            "hbm_peak_gbs_measured": peaks.get("hbm_gbs"),
+        }
+        if rank == 0 and not args.no_cpu_baseline:
+            result["cpu_baseline"] = cpu_baseline(args.cpu_budget)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(result))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

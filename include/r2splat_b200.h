@@ -39,6 +39,11 @@ extern "C" {
 int r2s_abi_version(void);
 const char* r2s_last_error(void);
 
+/* Measurement helper (no reference counterpart): launches blocks x threads
+ * threads that each run iters x 128 independent FP32 FMAs, to measure the
+ * FP32 issue peak the accumulate kernels are compared against. */
+int r2s_fp32_peak_probe(float* out, uint32_t blocks, uint32_t threads, int iters, void* stream);
+
 /* ---------------------------------------------------------------- geometry */
 
 /* Ops.h:419-422 parameter_transform_fwd_tensor.

@@ -49,6 +49,45 @@ def _ws(nbytes: int, device) -> Tensor:
     return torch.empty(max(int(nbytes), 1), dtype=torch.uint8, device=device)
 
 
+class StageTimer:
+    """Optional CUDA-event timing of the pipeline stages (used by the benchmark).
+
+    While ``active`` holds a StageTimer, each named stage records a start/end
+    event pair on the current stream; ``totals_ms()`` sums them per stage after
+    a synchronize.
+    """
+
+    active: "Optional[StageTimer]" = None
+
+    def __init__(self):
+        self.records: list[tuple[str, torch.cuda.Event, torch.cuda.Event]] = []
+
+    def totals_ms(self) -> dict:
+        out: dict = {}
+        for name, start, end in self.records:
+            out[name] = out.get(name, 0.0) + start.elapsed_time(end)
+        return out
+
+
+class _stage:
+    def __init__(self, name: str):
+        self.name = name
+        self.start = None
+
+    def __enter__(self):
+        if StageTimer.active is not None:
+            self.start = torch.cuda.Event(enable_timing=True)
+            self.start.record()
+        return self
+
+    def __exit__(self, *exc):
+        if self.start is not None and StageTimer.active is not None:
+            end = torch.cuda.Event(enable_timing=True)
+            end.record()
+            StageTimer.active.records.append((self.name, self.start, end))
+        return False
+
+
 @dataclass
 class RasterState:
     """Device buffers a projection VJP needs (the reference saves 12, explicit.py:184-186)."""
@@ -101,8 +140,9 @@ def raster_intersections(means, covars, densities, beta, ratio, viewmats, Ks, wi
     flatten_ids = torch.empty((m,), dtype=torch.int32, device=device)
     offsets = torch.empty((c, ty, tx), dtype=torch.int32, device=device)
     ws = _ws(lib.r2s_isect_emit_workspace(m, c * tx * ty), device)
-    _backend.call("r2s_raster_emit", _ptr(rects), c, n, tx, ty, _ptr(cum), m, _ptr(isect_ids), _ptr(flatten_ids),
-                  _ptr(offsets), _ptr(ws), ws.numel(), stream)
+    with _stage("raster_sort"):
+        _backend.call("r2s_raster_emit", _ptr(rects), c, n, tx, ty, _ptr(cum), m, _ptr(isect_ids),
+                      _ptr(flatten_ids), _ptr(offsets), _ptr(ws), ws.numel(), stream)
     return records, offsets, isect_ids, flatten_ids, m
 
 
@@ -119,9 +159,10 @@ def raster_forward(means, quats, scales, densities, viewmats, Ks, width, height,
     variance = torch.empty_like(image) if uncertainty is not None else None
     tx = (width + tile_size - 1) // tile_size
     ty = (height + tile_size - 1) // tile_size
-    _backend.call("r2s_raster_render", _dtype(means), _ptr(records), _ptr(uncertainty), int(beta is not None),
-                  _ptr(offsets), _ptr(flatten_ids), c, means.shape[0], m, width, height, tile_size, tx, ty,
-                  _ptr(image), _ptr(variance), _stream(device))
+    with _stage("raster_render"):
+        _backend.call("r2s_raster_render", _dtype(means), _ptr(records), _ptr(uncertainty), int(beta is not None),
+                      _ptr(offsets), _ptr(flatten_ids), c, means.shape[0], m, width, height, tile_size, tx, ty,
+                      _ptr(image), _ptr(variance), _stream(device))
     state = RasterState(covars, records, offsets, isect_ids, flatten_ids, ratio, m, width, height, tile_size)
     output = image if uncertainty is None else (image, variance)
     return output, state
@@ -138,10 +179,11 @@ def raster_backward(state: RasterState, means, quats, scales, densities, beta, u
     stream = _stream(device)
     grads = means.new_zeros((c, n, 8))
     v_unc = means.new_zeros((n,)) if v_variance is not None else None
-    _backend.call("r2s_raster_render_bwd", _dtype(means), _ptr(state.records), _ptr(uncertainty),
-                  int(beta is not None), int(bool(detach_variance)), _ptr(state.offsets), _ptr(state.flatten_ids),
-                  _ptr(v_image), _ptr(v_variance), c, n, state.n_isects, state.width, state.height, tile, tx, ty,
-                  _ptr(grads), None, _ptr(v_unc), stream)
+    with _stage("raster_render_bwd"):
+        _backend.call("r2s_raster_render_bwd", _dtype(means), _ptr(state.records), _ptr(uncertainty),
+                      int(beta is not None), int(bool(detach_variance)), _ptr(state.offsets), _ptr(state.flatten_ids),
+                      _ptr(v_image), _ptr(v_variance), c, n, state.n_isects, state.width, state.height, tile, tx, ty,
+                      _ptr(grads), None, _ptr(v_unc), stream)
     log_grad = _beta.beta_path_log_grad(beta) if beta is not None else None
     v_means = means.new_empty((n, 3))
     v_quats = means.new_empty((n, 4))
@@ -183,8 +225,10 @@ def voxel_intersections(means, covars, densities, beta, uncertainty, extent, cen
     flatten_ids = torch.empty((m,), dtype=torch.int32, device=device)
     offsets = torch.empty((tz, ty, tx), dtype=torch.int32, device=device)
     ws = _ws(lib.r2s_isect_emit_workspace(m, tx * ty * tz), device)
-    _backend.call("r2s_isect_tiles_3d_emit", _dtype(means), _ptr(means_v), _ptr(radii), n, tile_size, tx, ty, tz,
-                  _ptr(cum), m, _ptr(isect_ids), _ptr(flatten_ids), _ptr(offsets), _ptr(ws), ws.numel(), stream)
+    with _stage("voxel_sort"):
+        _backend.call("r2s_isect_tiles_3d_emit", _dtype(means), _ptr(means_v), _ptr(radii), n, tile_size, tx, ty,
+                      tz, _ptr(cum), m, _ptr(isect_ids), _ptr(flatten_ids), _ptr(offsets), _ptr(ws), ws.numel(),
+                      stream)
     return records, offsets, isect_ids, flatten_ids, m
 
 
@@ -200,9 +244,10 @@ def voxel_forward(means, quats, scales, densities, shape, extent, center, beta, 
     tx = (width + tile_size - 1) // tile_size
     ty = (height + tile_size - 1) // tile_size
     tz = (depth + tile_size - 1) // tile_size
-    _backend.call("r2s_voxel_render", _dtype(means), _ptr(records), int(beta is not None), _ptr(offsets),
-                  _ptr(flatten_ids), means.shape[0], m, width, height, depth, tile_size, tx, ty, tz, _ptr(volume),
-                  _ptr(variance), _stream(device))
+    with _stage("voxel_render"):
+        _backend.call("r2s_voxel_render", _dtype(means), _ptr(records), int(beta is not None), _ptr(offsets),
+                      _ptr(flatten_ids), means.shape[0], m, width, height, depth, tile_size, tx, ty, tz,
+                      _ptr(volume), _ptr(variance), _stream(device))
     state = VoxelState(covars, records, offsets, isect_ids, flatten_ids, m, tuple(shape), tile_size)
     return (volume if uncertainty is None else (volume, variance)), state
 
@@ -218,9 +263,10 @@ def voxel_backward(state: VoxelState, means, quats, scales, beta, uncertainty, e
     tz = (depth + tile - 1) // tile
     stream = _stream(device)
     grads = means.new_zeros((n, 16))
-    _backend.call("r2s_voxel_render_bwd", _dtype(means), _ptr(state.records), int(beta is not None),
-                  int(bool(detach_variance)), _ptr(state.offsets), _ptr(state.flatten_ids), _ptr(v_volume),
-                  _ptr(v_variance), n, state.n_isects, width, height, depth, tile, tx, ty, tz, _ptr(grads), stream)
+    with _stage("voxel_render_bwd"):
+        _backend.call("r2s_voxel_render_bwd", _dtype(means), _ptr(state.records), int(beta is not None),
+                      int(bool(detach_variance)), _ptr(state.offsets), _ptr(state.flatten_ids), _ptr(v_volume),
+                      _ptr(v_variance), n, state.n_isects, width, height, depth, tile, tx, ty, tz, _ptr(grads), stream)
     v_means = means.new_empty((n, 3))
     v_quats = means.new_empty((n, 4))
     v_scales = means.new_empty((n, 3))

@@ -162,7 +162,12 @@ constexpr int kBwdThreads = kBwdWarps * 32;
 //   var_q null         -> detached variance branch (no 2 q alpha v_var term)
 //   grads null         -> skip the record-slot adjoints
 //   v_abs / v_unc null -> skip absgrad / uncertainty adjoints
-template <typename S, bool kBeta, int PPL>
+//
+// The per-sample body is branch-free: a skipped sample keeps its arithmetic
+// but has its alpha and visibility selected to zero, so every contribution
+// it would add is an exact zero and the compiler can interleave the lane's
+// pixels (a `continue` per pixel serialises their exp/pow latencies).
+template <typename S, bool kBeta, bool kVar, bool kAbs, int PPL>
 __global__ void __launch_bounds__(kBwdThreads) raster_bwd_kernel(
     const Rec2D<S>* __restrict__ records, const S* __restrict__ var_q, uint32_t N,
     const int32_t* __restrict__ offsets, const int32_t* __restrict__ flatten_ids, int32_t n_isects,
@@ -191,8 +196,7 @@ __global__ void __launch_bounds__(kBwdThreads) raster_bwd_kernel(
     const uint32_t warps_per_sub = kBwdWarps / n_sub;
     const uint32_t my_lane_group = warp / n_sub;
 
-    const bool has_var = v_render_var != nullptr;
-    const bool chain_var = has_var && var_q != nullptr;
+    const bool chain_var = kVar && var_q != nullptr;
     S px[PPL], py[PPL], vr[PPL], vv[PPL];
     bool valid[PPL];
     const size_t cam_base = size_t(cam) * height * width;
@@ -207,7 +211,7 @@ __global__ void __launch_bounds__(kBwdThreads) raster_bwd_kernel(
         py[k] = static_cast<S>(i) + static_cast<S>(0.5);
         const size_t pid = cam_base + size_t(i) * width + j;
         vr[k] = (valid[k] && v_render != nullptr) ? v_render[pid] : S(0);
-        vv[k] = (valid[k] && has_var) ? v_render_var[pid] : S(0);
+        vv[k] = (kVar && valid[k]) ? v_render_var[pid] : S(0);
     }
 
     const int32_t n_batches = (count + kBwdThreads - 1) / kBwdThreads;
@@ -241,26 +245,29 @@ __global__ void __launch_bounds__(kBwdThreads) raster_bwd_kernel(
               g_ay = 0;
 #pragma unroll
             for (int k = 0; k < PPL; ++k) {
-                if (!valid[k]) continue;
                 if (!kBeta) {
                     const S dx = px[k] - r.x;
                     const S dy = py[k] - r.y;
                     const S sigma = static_cast<S>(0.5) * (r.a * dx * dx + r.c * dy * dy) + r.b * dx * dy;
-                    const S vis = exp(-sigma);
-                    const S alpha = om * vis;
-                    if (sigma < static_cast<S>(0) || fabs(alpha) < static_cast<S>(1e-5)) continue;
+                    const S vis_raw = exp(-sigma);
+                    const S alpha_raw = om * vis_raw;
+                    const bool keep = valid[k] && !(sigma < static_cast<S>(0) || fabs(alpha_raw) < static_cast<S>(1e-5));
+                    const S vis = keep ? vis_raw : S(0);
+                    const S alpha = keep ? alpha_raw : S(0);
                     S v = vr[k];
-                    if (has_var) {
+                    if (kVar) {
                         g_q += vv[k] * alpha * alpha;
-                        if (chain_var) v += static_cast<S>(2) * q * alpha * vv[k];
+                        v += static_cast<S>(2) * q * alpha * vv[k];
                     }
                     const S v_sigma = -v * alpha;
                     const S gx = -v_sigma * (r.a * dx + r.b * dy);
                     const S gy = -v_sigma * (r.c * dy + r.b * dx);
                     g_x += gx;
                     g_y += gy;
-                    g_ax += fabs(gx);
-                    g_ay += fabs(gy);
+                    if (kAbs) {
+                        g_ax += fabs(gx);
+                        g_ay += fabs(gy);
+                    }
                     g_a += v_sigma * static_cast<S>(0.5) * dx * dx;
                     g_b += v_sigma * dx * dy;
                     g_c += v_sigma * static_cast<S>(0.5) * dy * dy;
@@ -270,23 +277,28 @@ __global__ void __launch_bounds__(kBwdThreads) raster_bwd_kernel(
                     const S dx = r.x - px[k];
                     const S dy = r.y - py[k];
                     const S d2 = r.a * dx * dx + static_cast<S>(2) * r.b * dx * dy + r.c * dy * dy;
-                    const S h = static_cast<S>(1) - d2;
-                    if (d2 < static_cast<S>(0) || h <= static_cast<S>(0)) continue;
-                    const S vis = pow(h, r.beta);
-                    const S alpha = om * vis;
-                    if (fabs(alpha) < static_cast<S>(1e-5)) continue;
-                    S v = vr[k];
-                    if (has_var) {
+                    const S h_raw = static_cast<S>(1) - d2;
+                    const bool inside = valid[k] && !(d2 < static_cast<S>(0) || h_raw <= static_cast<S>(0));
+                    const S h = inside ? h_raw : S(1);  // keeps pow/log finite on skipped samples
+                    const S vis_raw = pow(h, r.beta);
+                    const S alpha_raw = om * vis_raw;
+                    const bool keep = inside && !(fabs(alpha_raw) < static_cast<S>(1e-5));
+                    const S vis = keep ? vis_raw : S(0);
+                    const S alpha = keep ? alpha_raw : S(0);
+                    S v = keep ? vr[k] : S(0);
+                    if (kVar) {
                         g_q += vv[k] * alpha * alpha;
-                        if (chain_var) v += static_cast<S>(2) * q * alpha * vv[k];
+                        v += static_cast<S>(2) * q * alpha * vv[k];
                     }
                     const S v_d2 = -om * r.beta * pow(h, r.beta - static_cast<S>(1)) * v;
                     const S gx = static_cast<S>(2) * v_d2 * (r.a * dx + r.b * dy);
                     const S gy = static_cast<S>(2) * v_d2 * (r.b * dx + r.c * dy);
                     g_x += gx;
                     g_y += gy;
-                    g_ax += fabs(gx);
-                    g_ay += fabs(gy);
+                    if (kAbs) {
+                        g_ax += fabs(gx);
+                        g_ay += fabs(gy);
+                    }
                     g_a += v_d2 * dx * dx;
                     g_b += static_cast<S>(2) * v_d2 * dx * dy;
                     g_c += v_d2 * dy * dy;
@@ -303,8 +315,8 @@ __global__ void __launch_bounds__(kBwdThreads) raster_bwd_kernel(
             g_o = warp_sum(g_o);
             g_mu = warp_sum(g_mu);
             if (kBeta) g_beta = warp_sum(g_beta);
-            if (has_var) g_q = warp_sum(g_q);
-            if (v_abs != nullptr) {
+            if (kVar) g_q = warp_sum(g_q);
+            if (kAbs) {
                 g_ax = warp_sum(g_ax);
                 g_ay = warp_sum(g_ay);
             }
@@ -313,8 +325,8 @@ __global__ void __launch_bounds__(kBwdThreads) raster_bwd_kernel(
                 if (lane == 0) red_add_v4(dst, g_x, g_y, g_a, g_b);
                 if (lane == 1) red_add_v4(dst + 4, g_c, g_o, g_mu, g_beta);
             }
-            if (lane == 2 && v_unc != nullptr && has_var) red_add(v_unc + (uint32_t(g) % N), g_q);
-            if (lane == 3 && v_abs != nullptr) {
+            if (kVar && lane == 2 && v_unc != nullptr) red_add(v_unc + (uint32_t(g) % N), g_q);
+            if (kAbs && lane == 3) {
                 red_add(v_abs + 2 * size_t(g), g_ax);
                 red_add(v_abs + 2 * size_t(g) + 1, g_ay);
             }
@@ -420,16 +432,46 @@ int launch_fwd(const RasterGeom& g, const Rec2D<S>* rec, const S* unc, bool beta
                : launch_fwd_p<S, false, false>(g, rec, unc, offsets, ids, out, out_var, stream);
 }
 
-template <typename S, bool kBeta, int PPL>
+template <typename S, bool kBeta, bool kVar, bool kAbs, int PPL>
 int launch_bwd_t(const RasterGeom& g, const Rec2D<S>* rec, const S* var_q, const int32_t* offsets,
                  const int32_t* ids, const S* v_render, const S* v_render_var, Rec2D<S>* grads, S* v_abs,
                  S* v_unc, cudaStream_t stream) {
     const size_t smem = 2 * kBwdThreads * (sizeof(Rec2D<S>) + sizeof(S) + sizeof(int32_t));
     dim3 grid(g.tiles_x * g.tiles_y, g.C);
-    raster_bwd_kernel<S, kBeta, PPL><<<grid, kBwdThreads, smem, stream>>>(
+    raster_bwd_kernel<S, kBeta, kVar, kAbs, PPL><<<grid, kBwdThreads, smem, stream>>>(
         rec, var_q, g.N, offsets, ids, int32_t(g.n_isects), g.C, g.width, g.height, g.T, g.tiles_x,
         g.tiles_x * g.tiles_y, v_render, v_render_var, grads, v_abs, v_unc);
     return check_launch("rasterize_to_pixels_bwd");
+}
+
+template <typename S, bool kBeta, bool kVar, bool kAbs>
+int launch_bwd_p(const RasterGeom& g, const Rec2D<S>* rec, const S* var_q, const int32_t* offsets,
+                 const int32_t* ids, const S* v_render, const S* v_render_var, Rec2D<S>* grads, S* v_abs,
+                 S* v_unc, cudaStream_t stream) {
+    // Pixels per lane: 2 for tiles up to 8x8, else 8 (sub-tiles of 256 pixels).
+    if (g.T * g.T <= 64)
+        return launch_bwd_t<S, kBeta, kVar, kAbs, 2>(g, rec, var_q, offsets, ids, v_render, v_render_var, grads,
+                                                     v_abs, v_unc, stream);
+    return launch_bwd_t<S, kBeta, kVar, kAbs, 8>(g, rec, var_q, offsets, ids, v_render, v_render_var, grads,
+                                                 v_abs, v_unc, stream);
+}
+
+template <typename S, bool kBeta>
+int launch_bwd_b(const RasterGeom& g, const Rec2D<S>* rec, const S* var_q, const int32_t* offsets,
+                 const int32_t* ids, const S* v_render, const S* v_render_var, Rec2D<S>* grads, S* v_abs,
+                 S* v_unc, cudaStream_t stream) {
+    const bool var = v_render_var != nullptr, abs = v_abs != nullptr;
+    if (var && abs)
+        return launch_bwd_p<S, kBeta, true, true>(g, rec, var_q, offsets, ids, v_render, v_render_var, grads, v_abs,
+                                                  v_unc, stream);
+    if (var)
+        return launch_bwd_p<S, kBeta, true, false>(g, rec, var_q, offsets, ids, v_render, v_render_var, grads, v_abs,
+                                                   v_unc, stream);
+    if (abs)
+        return launch_bwd_p<S, kBeta, false, true>(g, rec, var_q, offsets, ids, v_render, v_render_var, grads, v_abs,
+                                                   v_unc, stream);
+    return launch_bwd_p<S, kBeta, false, false>(g, rec, var_q, offsets, ids, v_render, v_render_var, grads, v_abs,
+                                                v_unc, stream);
 }
 
 template <typename S>
@@ -438,18 +480,10 @@ int launch_bwd(const RasterGeom& g, const Rec2D<S>* rec, bool beta, const S* var
                cudaStream_t stream) {
     R2S_TRY(check_geom(g));
     if (g.n_isects == 0 || g.tiles_x == 0 || g.tiles_y == 0 || g.C == 0) return R2S_OK;
-    const uint32_t pixels = g.T * g.T;
-    // Pixels per lane: 2 for tiles up to 8x8, else 8 (sub-tiles of 256 pixels).
-    if (pixels <= 64) {
-        return beta ? launch_bwd_t<S, true, 2>(g, rec, var_q, offsets, ids, v_render, v_render_var, grads, v_abs,
-                                               v_unc, stream)
-                    : launch_bwd_t<S, false, 2>(g, rec, var_q, offsets, ids, v_render, v_render_var, grads, v_abs,
-                                                v_unc, stream);
-    }
-    return beta ? launch_bwd_t<S, true, 8>(g, rec, var_q, offsets, ids, v_render, v_render_var, grads, v_abs,
-                                           v_unc, stream)
-                : launch_bwd_t<S, false, 8>(g, rec, var_q, offsets, ids, v_render, v_render_var, grads, v_abs,
-                                            v_unc, stream);
+    return beta ? launch_bwd_b<S, true>(g, rec, var_q, offsets, ids, v_render, v_render_var, grads, v_abs, v_unc,
+                                        stream)
+                : launch_bwd_b<S, false>(g, rec, var_q, offsets, ids, v_render, v_render_var, grads, v_abs, v_unc,
+                                         stream);
 }
 
 template <typename S>

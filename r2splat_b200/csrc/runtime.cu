@@ -25,11 +25,34 @@ int check_launch(const char* what) {
     return R2S_OK;
 }
 
+// FP32 issue-rate probe: every thread runs 8 independent FMA chains, so the
+// kernel is bound by the FMA pipe; 2 flops per FMA.
+__global__ void fp32_peak_kernel(float* out, int iters, float seed) {
+    float a0 = seed + threadIdx.x, a1 = a0 + 1.f, a2 = a0 + 2.f, a3 = a0 + 3.f;
+    float a4 = a0 + 4.f, a5 = a0 + 5.f, a6 = a0 + 6.f, a7 = a0 + 7.f;
+    const float m = 0.9999f, c = 1e-7f;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+            a0 = fmaf(a0, m, c); a1 = fmaf(a1, m, c); a2 = fmaf(a2, m, c); a3 = fmaf(a3, m, c);
+            a4 = fmaf(a4, m, c); a5 = fmaf(a5, m, c); a6 = fmaf(a6, m, c); a7 = fmaf(a7, m, c);
+        }
+    }
+    const float s = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+    if (s == 1234.5f) out[blockIdx.x] = s;  // keeps the chains live
+}
+
 }  // namespace r2s
 
 extern "C" {
 
 int r2s_abi_version(void) { return 1; }
+
+// Launches the FP32 peak probe: blocks x threads x iters x 128 FMAs.
+int r2s_fp32_peak_probe(float* out, uint32_t blocks, uint32_t threads, int iters, void* stream) {
+    r2s::fp32_peak_kernel<<<blocks, threads, 0, static_cast<cudaStream_t>(stream)>>>(out, iters, 0.5f);
+    return r2s::check_launch("fp32_peak_probe");
+}
 
 const char* r2s_last_error(void) { return r2s::t_last_error.c_str(); }
 

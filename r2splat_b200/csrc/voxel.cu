@@ -141,7 +141,7 @@ constexpr int kVoxBwdThreads = kVoxBwdWarps * 32;
 // Null-pointer conventions as in the rasterizer VJP: v_volume null = zero
 // adjoint; v_volume_var null = no variance branch; chain_var false =
 // detached variance branch.
-template <typename S, bool kBeta, int PPL>
+template <typename S, bool kBeta, bool kVar, int PPL>
 __global__ void __launch_bounds__(kVoxBwdThreads) voxel_bwd_kernel(
     const Rec3D<S>* __restrict__ records, bool chain_var, const int32_t* __restrict__ offsets,
     const int32_t* __restrict__ flatten_ids, VoxelGeom g, const S* __restrict__ v_volume,
@@ -168,7 +168,6 @@ __global__ void __launch_bounds__(kVoxBwdThreads) voxel_bwd_kernel(
     const uint32_t warps_per_sub = kVoxBwdWarps / n_sub;
     const uint32_t my_group = warp / n_sub;
 
-    const bool has_var = v_volume_var != nullptr;
     S px[PPL], py[PPL], pz[PPL], vr[PPL], vv[PPL];
     bool valid[PPL];
 #pragma unroll
@@ -183,7 +182,7 @@ __global__ void __launch_bounds__(kVoxBwdThreads) voxel_bwd_kernel(
         pz[k] = static_cast<S>(i) + static_cast<S>(0.5);
         const size_t vid = (size_t(i) * g.dim1 + j) * g.dim2 + kk;
         vr[k] = (valid[k] && v_volume != nullptr) ? v_volume[vid] : S(0);
-        vv[k] = (valid[k] && has_var) ? v_volume_var[vid] : S(0);
+        vv[k] = (kVar && valid[k]) ? v_volume_var[vid] : S(0);
     }
 
     const int32_t n_batches = (count + kVoxBwdThreads - 1) / kVoxBwdThreads;
@@ -212,21 +211,23 @@ __global__ void __launch_bounds__(kVoxBwdThreads) voxel_bwd_kernel(
             const int32_t gid = s_id[stage * kVoxBwdThreads + s];
             const S a = r.c00, p = r.c01, q = r.c02, bb = r.c11, rr = r.c12, c = r.c22;
             const S opac = r.o;
+            const S uq = chain_var ? r.q : S(0);
             S gx = 0, gy = 0, gz = 0, go = 0, g0 = 0, g1 = 0, g2 = 0, g3 = 0, g4 = 0, g5 = 0, gb = 0, gq = 0;
 #pragma unroll
             for (int k = 0; k < PPL; ++k) {
-                if (!valid[k]) continue;
                 if (!kBeta) {
                     const S d1 = px[k] - r.x, d2 = py[k] - r.y, d3 = pz[k] - r.z;
                     const S sigma = static_cast<S>(0.5) * (a * d1 * d1 + bb * d2 * d2 + c * d3 * d3) +
                                     p * d1 * d2 + q * d1 * d3 + rr * d2 * d3;
-                    const S vis = exp(-sigma);
-                    const S alpha = opac * vis;
-                    if (sigma < static_cast<S>(0) || fabs(alpha) < static_cast<S>(1e-6)) continue;
+                    const S vis_raw = exp(-sigma);
+                    const S alpha_raw = opac * vis_raw;
+                    const bool keep = valid[k] && !(sigma < static_cast<S>(0) || fabs(alpha_raw) < static_cast<S>(1e-6));
+                    const S vis = keep ? vis_raw : S(0);
+                    const S alpha = keep ? alpha_raw : S(0);
                     S v_O = vr[k];
-                    if (has_var) {
+                    if (kVar) {
                         gq += vv[k] * alpha * alpha;
-                        if (chain_var) v_O += static_cast<S>(2) * r.q * alpha * vv[k];
+                        v_O += static_cast<S>(2) * uq * alpha * vv[k];
                     }
                     const S v_sigma = -v_O * opac * vis;
                     const S oI = opac * vis;
@@ -244,15 +245,18 @@ __global__ void __launch_bounds__(kVoxBwdThreads) voxel_bwd_kernel(
                     const S d1 = r.x - px[k], d2 = r.y - py[k], d3 = r.z - pz[k];
                     const S qf = a * d1 * d1 + bb * d2 * d2 + c * d3 * d3 + static_cast<S>(2) * p * d1 * d2 +
                                  static_cast<S>(2) * q * d1 * d3 + static_cast<S>(2) * rr * d2 * d3;
-                    const S h = static_cast<S>(1) - qf;
-                    if (qf < static_cast<S>(0) || h <= static_cast<S>(0)) continue;
-                    const S vis = pow(h, r.beta);
-                    const S alpha = opac * vis;
-                    if (fabs(alpha) < static_cast<S>(1e-5)) continue;
-                    S v_O = vr[k];
-                    if (has_var) {
+                    const S h_raw = static_cast<S>(1) - qf;
+                    const bool inside = valid[k] && !(qf < static_cast<S>(0) || h_raw <= static_cast<S>(0));
+                    const S h = inside ? h_raw : S(1);  // keeps pow/log finite on skipped samples
+                    const S vis_raw = pow(h, r.beta);
+                    const S alpha_raw = opac * vis_raw;
+                    const bool keep = inside && !(fabs(alpha_raw) < static_cast<S>(1e-5));
+                    const S vis = keep ? vis_raw : S(0);
+                    const S alpha = keep ? alpha_raw : S(0);
+                    S v_O = keep ? vr[k] : S(0);
+                    if (kVar) {
                         gq += vv[k] * alpha * alpha;
-                        if (chain_var) v_O += static_cast<S>(2) * r.q * alpha * vv[k];
+                        v_O += static_cast<S>(2) * uq * alpha * vv[k];
                     }
                     const S v_q = -opac * r.beta * pow(h, r.beta - static_cast<S>(1)) * v_O;
                     const S wx = a * d1 + p * d2 + q * d3;
@@ -275,7 +279,7 @@ __global__ void __launch_bounds__(kVoxBwdThreads) voxel_bwd_kernel(
             g0 = warp_sum(g0); g1 = warp_sum(g1); g2 = warp_sum(g2); g3 = warp_sum(g3);
             g4 = warp_sum(g4); g5 = warp_sum(g5);
             if (kBeta) gb = warp_sum(gb);
-            if (has_var) gq = warp_sum(gq);
+            if (kVar) gq = warp_sum(gq);
             S* dst = reinterpret_cast<S*>(grads + gid);
             if (lane == 0) red_add_v4(dst, gx, gy, gz, go);
             if (lane == 1) red_add_v4(dst + 4, g0, g1, g2, g3);
@@ -372,16 +376,25 @@ int launch_vfwd(const VoxelGeom& g, const Rec3D<S>* rec, bool beta, const int32_
                : launch_vfwd_p<S, false, false>(g, rec, offsets, ids, vol, vol_var, stream);
 }
 
-template <typename S, bool kBeta, int PPL>
+template <typename S, bool kBeta, bool kVar, int PPL>
 int launch_vbwd_t(const VoxelGeom& g, const Rec3D<S>* rec, bool chain_var, const int32_t* offsets,
                   const int32_t* ids, const S* v_vol, const S* v_vol_var, Rec3D<S>* grads, cudaStream_t stream) {
     const size_t smem = 2 * kVoxBwdThreads * (sizeof(Rec3D<S>) + sizeof(int32_t));
     if (smem > 48 * 1024)
-        cudaFuncSetAttribute(voxel_bwd_kernel<S, kBeta, PPL>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        cudaFuncSetAttribute(voxel_bwd_kernel<S, kBeta, kVar, PPL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(smem));
     const unsigned grid = g.tiles_x * g.tiles_y * g.tiles_z;
-    voxel_bwd_kernel<S, kBeta, PPL><<<grid, kVoxBwdThreads, smem, stream>>>(rec, chain_var, offsets, ids, g, v_vol,
-                                                                             v_vol_var, grads);
+    voxel_bwd_kernel<S, kBeta, kVar, PPL><<<grid, kVoxBwdThreads, smem, stream>>>(rec, chain_var, offsets, ids, g,
+                                                                                   v_vol, v_vol_var, grads);
     return check_launch("voxelize_to_voxels_bwd");
+}
+
+template <typename S, bool kBeta, bool kVar>
+int launch_vbwd_p(const VoxelGeom& g, const Rec3D<S>* rec, bool chain_var, const int32_t* offsets,
+                  const int32_t* ids, const S* v_vol, const S* v_vol_var, Rec3D<S>* grads, cudaStream_t stream) {
+    if (g.T * g.T * g.T <= 64)
+        return launch_vbwd_t<S, kBeta, kVar, 2>(g, rec, chain_var, offsets, ids, v_vol, v_vol_var, grads, stream);
+    return launch_vbwd_t<S, kBeta, kVar, 8>(g, rec, chain_var, offsets, ids, v_vol, v_vol_var, grads, stream);
 }
 
 template <typename S>
@@ -389,11 +402,12 @@ int launch_vbwd(const VoxelGeom& g, const Rec3D<S>* rec, bool beta, bool chain_v
                 const int32_t* ids, const S* v_vol, const S* v_vol_var, Rec3D<S>* grads, cudaStream_t stream) {
     R2S_TRY(check_vgeom(g));
     if (g.n_isects == 0 || uint64_t(g.tiles_x) * g.tiles_y * g.tiles_z == 0) return R2S_OK;
-    if (g.T * g.T * g.T <= 64)
-        return beta ? launch_vbwd_t<S, true, 2>(g, rec, chain_var, offsets, ids, v_vol, v_vol_var, grads, stream)
-                    : launch_vbwd_t<S, false, 2>(g, rec, chain_var, offsets, ids, v_vol, v_vol_var, grads, stream);
-    return beta ? launch_vbwd_t<S, true, 8>(g, rec, chain_var, offsets, ids, v_vol, v_vol_var, grads, stream)
-                : launch_vbwd_t<S, false, 8>(g, rec, chain_var, offsets, ids, v_vol, v_vol_var, grads, stream);
+    const bool var = v_vol_var != nullptr;
+    if (beta)
+        return var ? launch_vbwd_p<S, true, true>(g, rec, chain_var, offsets, ids, v_vol, v_vol_var, grads, stream)
+                   : launch_vbwd_p<S, true, false>(g, rec, chain_var, offsets, ids, v_vol, v_vol_var, grads, stream);
+    return var ? launch_vbwd_p<S, false, true>(g, rec, chain_var, offsets, ids, v_vol, v_vol_var, grads, stream)
+               : launch_vbwd_p<S, false, false>(g, rec, chain_var, offsets, ids, v_vol, v_vol_var, grads, stream);
 }
 
 template <typename S>
