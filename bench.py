@@ -235,6 +235,10 @@ def build_workload(device, workload: str):
 
     if workload == "ct":
         scene = scenes.ct_scene()
+    elif workload == "ct4":
+        # Profiling case: the CT scene with 4 of its 64 views (same per-tile work, 1/16 of the images).
+        scene = scenes.ct_scene()
+        scene.viewmats, scene.Ks = scene.viewmats[::16].contiguous(), scene.Ks[::16].contiguous()
     elif workload == "small":
         scene = scenes.small_scene()
     else:
@@ -310,18 +314,28 @@ def timed_run(step, scene, steps, warmup, device, flush_buf):
     torch.cuda.synchronize()
     timer = _fused.StageTimer()
     total_ms = 0.0
+    launches = 0
     for _ in range(steps):
         flush_l2(flush_buf)
         start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         _fused.StageTimer.active = timer
+        before = library_launches()
         start.record()
         step(*prims)
         end.record()
+        launches += library_launches() - before
         _fused.StageTimer.active = None
         end.synchronize()
         total_ms += start.elapsed_time(end)
     torch.cuda.synchronize()
-    return total_ms, timer.totals_ms()
+    return total_ms, timer.totals_ms(), launches
+
+
+def library_launches() -> int:
+    """Kernels launched so far by this package's library (its own exact counter)."""
+    from r2splat_b200.cuda import _backend
+
+    return int(_backend.library().r2s_launch_count())
 
 
 def e2e_run(step, scene, steps, warmup, device):
@@ -363,7 +377,9 @@ def main(argv=None) -> int:
     parser.add_argument("--steps", type=int, default=20)
     parser.add_argument("--warmup", type=int, default=3)
     parser.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    parser.add_argument("--workload", choices=("ct", "small"), default="ct")
+    parser.add_argument("--workload", choices=("ct", "ct4", "small"), default="ct")
+    parser.add_argument("--profile-only", action="store_true",
+                        help="run the warm-up steps of the workload and exit (profiling driver, no timing)")
     parser.add_argument("--cpu-budget", type=float, default=15.0)
     parser.add_argument("--no-cpu-baseline", action="store_true")
     args = parser.parse_args(argv)
@@ -397,13 +413,18 @@ def main(argv=None) -> int:
 
     scene, target = build_workload(device, args.workload)
     step = OursStep(scene, target) if args.impl == "ours" else ReferenceStep(scene, target)
+    if args.profile_only:
+        for _ in range(args.warmup):
+            step(*scene.primitives)
+        torch.cuda.synchronize()
+        return 0
     flush_buf = torch.zeros(L2_FLUSH_BYTES // 4, device=device)
 
     if world > 1 and args.impl == "ours":
         dist.barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clocks:
-        total_ms, stages = timed_run(step, scene, args.steps, args.warmup, device, flush_buf)
+        total_ms, stages, own_launches = timed_run(step, scene, args.steps, args.warmup, device, flush_buf)
     if world > 1 and args.impl == "ours":
         t = torch.tensor([total_ms], device=device)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -415,8 +436,10 @@ def main(argv=None) -> int:
 
     e2e_ms, h2d, d2h = e2e_run(step, scene, args.steps, args.warmup, device)
     e2e_value = evals_per_step * (world if args.impl == "ours" else 1) / (e2e_ms / args.steps * 1e-3)
-    prefix = "r2s::" if args.impl == "ours" else "r2splat::"
-    launches = count_launches(step, scene, prefix) * args.steps
+    if args.impl == "ours":
+        launches = own_launches
+    else:
+        launches = count_launches(step, scene, "r2splat::") * args.steps
 
     peaks = measured_peaks()
     result = {

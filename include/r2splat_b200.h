@@ -44,6 +44,9 @@ const char* r2s_last_error(void);
  * FP32 issue peak the accumulate kernels are compared against. */
 int r2s_fp32_peak_probe(float* out, uint32_t blocks, uint32_t threads, int iters, void* stream);
 
+/* Number of kernels this library has launched in the process so far. */
+uint64_t r2s_launch_count(void);
+
 /* ---------------------------------------------------------------- geometry */
 
 /* Ops.h:419-422 parameter_transform_fwd_tensor.

@@ -1,12 +1,14 @@
 // Library-wide host runtime: error reporting and identification.
 #include "common.cuh"
 
+#include <atomic>
 #include <string>
 
 namespace r2s {
 
 namespace {
 thread_local std::string t_last_error;
+std::atomic<uint64_t> g_launches{0};
 }
 
 void set_error(const std::string& message) { t_last_error = message; }
@@ -16,8 +18,10 @@ int fail(int code, const std::string& message) {
     return code;
 }
 
-// Converts a pending launch error into an R2S_ERR_CUDA status.
+// Converts a pending launch error into an R2S_ERR_CUDA status. Every kernel
+// launch of the library is followed by exactly one call, which also counts it.
 int check_launch(const char* what) {
+    g_launches.fetch_add(1, std::memory_order_relaxed);
     cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) {
         return fail(R2S_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(err));
@@ -47,6 +51,8 @@ __global__ void fp32_peak_kernel(float* out, int iters, float seed) {
 extern "C" {
 
 int r2s_abi_version(void) { return 1; }
+
+uint64_t r2s_launch_count(void) { return r2s::g_launches.load(std::memory_order_relaxed); }
 
 // Launches the FP32 peak probe: blocks x threads x iters x 128 FMAs.
 int r2s_fp32_peak_probe(float* out, uint32_t blocks, uint32_t threads, int iters, void* stream) {
