@@ -367,6 +367,18 @@ int r2s_voxel_chain_bwd(int dtype, const void* means, const void* quats, const v
                         const void* grads, void* v_means, void* v_quats, void* v_scales,
                         void* v_densities, void* v_betas, void* v_uncertainties, void* stream);
 
+/* ------------------------------------------------ allocation-free variant
+ * No reference counterpart. r2s_scan_tile_counts without a workspace argument:
+ * the scan's scratch is a static per-device array of the library (72 KiB),
+ * so the call needs no device allocation at all. It takes at most
+ * r2s_scan_tile_counts_noalloc_max() elements (2^25); larger n returns
+ * R2S_ERR_UNSUPPORTED with nothing launched. Calls on one device share the
+ * scratch: calls that overlap in time race and must be serialised by the
+ * caller. The first call on a device resolves the scratch address and should
+ * come before any stream capture on that device. */
+uint64_t r2s_scan_tile_counts_noalloc_max(void);
+int r2s_scan_tile_counts_noalloc(const int32_t* counts, uint64_t n, int64_t* cum, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

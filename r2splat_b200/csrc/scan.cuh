@@ -83,7 +83,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_tile_kernel(const In* in, i
 
 // Workspace bytes for scanning n elements of type Out.
 template <typename Out>
-inline size_t scan_workspace_bytes(int64_t n) {
+constexpr size_t scan_workspace_bytes(int64_t n) {
     size_t bytes = 0;
     while (n > kScanTile) {
         const int64_t nb = (n + kScanTile - 1) / kScanTile;

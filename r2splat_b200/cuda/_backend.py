@@ -83,6 +83,8 @@ SIGNATURES: dict[str, tuple] = {
     "r2s_voxel_render_bwd": (I32, [I32, P, I32, I32, P, P, P, P, U32, U32, U32, U32, U32, U32, U32, U32, U32,
                                    P, P]),
     "r2s_voxel_chain_bwd": (I32, [I32, P, P, P, P, P, P, U32, U32, U32, U32, F64, P, P, P, P, P, P, P, P]),
+    "r2s_scan_tile_counts_noalloc_max": (U64, []),
+    "r2s_scan_tile_counts_noalloc": (I32, [P, U64, P, P]),
 }
 
 _lock = threading.Lock()
