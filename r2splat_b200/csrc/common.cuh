@@ -123,6 +123,13 @@ __device__ __forceinline__ void red_add_v4(double* addr, double a, double b, dou
     atomicAdd(addr + 2, c);
     atomicAdd(addr + 3, d);
 }
+__device__ __forceinline__ void red_add_v2(float* addr, float a, float b) {
+    asm volatile("red.global.add.v2.f32 [%0], {%1, %2};\n" :: "l"(addr), "f"(a), "f"(b) : "memory");
+}
+__device__ __forceinline__ void red_add_v2(double* addr, double a, double b) {
+    atomicAdd(addr + 0, a);
+    atomicAdd(addr + 1, b);
+}
 __device__ __forceinline__ void red_add(float* addr, float v) { atomicAdd(addr, v); }
 __device__ __forceinline__ void red_add(double* addr, double v) { atomicAdd(addr, v); }
 
@@ -131,6 +138,51 @@ __device__ __forceinline__ S warp_sum(S v) {
 #pragma unroll
     for (int offset = 16; offset > 0; offset >>= 1) v += __shfl_xor_sync(0xffffffffu, v, offset);
     return v;
+}
+
+// Warp sum of eight per-lane values by recursive halving: each exchange step
+// sends half of the lane's values to its partner and keeps the other half, so
+// the whole reduction costs 4 + 2 + 2 * 3 shuffles instead of 8 * 5. On
+// return every lane of group G = lane / 8 holds the warp totals of values
+// 2G and 2G + 1 in (out0, out1).
+template <typename S>
+__device__ __forceinline__ void warp_sum8_pairs(const S (&v)[8], S& out0, S& out1) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const bool hi16 = (lane & 16u) != 0;
+    S w[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const S send = hi16 ? v[i] : v[i + 4];
+        const S keep = hi16 ? v[i + 4] : v[i];
+        w[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+    }
+    const bool hi8 = (lane & 8u) != 0;
+    S u[2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        const S send = hi8 ? w[i] : w[i + 2];
+        const S keep = hi8 ? w[i + 2] : w[i];
+        u[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+    }
+#pragma unroll
+    for (int offset = 4; offset > 0; offset >>= 1) {
+        u[0] += __shfl_xor_sync(0xffffffffu, u[0], offset);
+        u[1] += __shfl_xor_sync(0xffffffffu, u[1], offset);
+    }
+    out0 = u[0];
+    out1 = u[1];
+}
+
+// Raises a kernel's dynamic shared-memory limit when a launch needs more than
+// the default 48 KB.
+template <typename Kernel>
+inline int allow_dynamic_smem(Kernel kernel, size_t bytes) {
+    if (bytes <= 48 * 1024) return R2S_OK;
+    const cudaError_t err =
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+    if (err != cudaSuccess)
+        return fail(R2S_ERR_CUDA, std::string("cudaFuncSetAttribute(dynamic smem): ") + cudaGetErrorString(err));
+    return R2S_OK;
 }
 
 // Packed per-(camera, primitive) record consumed by the tile kernels.

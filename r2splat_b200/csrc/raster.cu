@@ -10,30 +10,27 @@
 //    staged in shared memory in batches, each thread gathering one 32-byte
 //    record with two 16-byte cp.async copies, double-buffered so the next
 //    batch's gather overlaps the current batch's arithmetic;
-//  * forward: each thread owns up to 4 pixels; backward: each warp owns one
-//    record at a time and evaluates it on every pixel of its sub-tile (8 per
-//    lane), then warp-reduces and issues two vector atomics per record.
+//  * each staged record gets a conservative pixel box on this tile (the
+//    pixels where its sample can pass the contribution test), computed once
+//    per CTA by the thread that staged it;
+//  * forward: one pixel per thread, each warp owning an 8x4 block of the
+//    tile; a warp ballots which staged records' boxes meet its block and
+//    evaluates only those, in list order, so every pixel still sums its
+//    contributions in the reference's order;
+//  * backward: one warp per record, evaluating only the pixels of its box
+//    (about a third of the tile for CT-sized Gaussians), accumulating six to
+//    eight partial sums per lane, reducing them with a recursive-halving warp
+//    sum and adding them to the packed adjoints with vector atomics.
 //
 // Per-sample arithmetic keeps the reference's expression forms
 // (RasterizeToPixelsFwd.cu:160-177, :664-680; RasterizeToPixelsBwd.cu:417-468,
 // :910-945): the contribution thresholds (|alpha| < 1e-5, sigma < 0, d2 >= 1)
 // decide which samples count, so alpha must round exactly as the reference's
-// does. A thread's pixels are placed so that no two share an x or a y
-// coordinate, which keeps every product single-use, as in the reference's
-// one-pixel-per-thread loops, and so the compiler contracts the same
-// multiply-adds.
+// does. Each thread evaluates one pixel per record, as in the reference's
+// one-pixel-per-thread loops, so the compiler contracts the same multiply-adds.
 #include "common.cuh"
 
 namespace r2s {
-
-// Pixel placement: the p-th pixel of a tile sits at row p / T and column
-// (p % T + 7 * row) % T -- a per-row rotation, so rows stay bijective while
-// pixels p and p + 32k (one lane) or p and p + nthreads (one thread) get
-// different columns.
-__device__ __forceinline__ void tile_pixel(uint32_t p, uint32_t T, uint32_t& ly, uint32_t& lx) {
-    ly = p / T;
-    lx = (p - ly * T + 7u * ly) % T;
-}
 
 template <typename S>
 __device__ __forceinline__ void gather_record(Rec2D<S>* dst, const Rec2D<S>* src) {
@@ -44,94 +41,186 @@ __device__ __forceinline__ void gather_record(Rec2D<S>* dst, const Rec2D<S>* src
 }
 
 // --------------------------------------------------------------------------
+// Pixel boxes
+// --------------------------------------------------------------------------
+
+// A record's box on one tile, in tile-local pixel indices: column and row bit
+// masks, the packed origin and extent (x0 | y0 << 8 | width << 16 |
+// height << 24) and ceil(65536 / width), with which (k * magic) >> 16 equals
+// k / width for every k < 1024 and width <= 32. An empty box has zero masks
+// and extent.
+struct alignas(16) TileBox {
+    uint32_t cols, rows, packed, magic;
+};
+
+__device__ __forceinline__ uint32_t low_bits(uint32_t n) { return n >= 32u ? 0xffffffffu : ((1u << n) - 1u); }
+
+// Conservative box of the pixels whose sample can pass the contribution test.
+//
+// Gaussian: a sample counts only if |o mu| exp(-sigma) >= 1e-5, i.e. sigma <=
+// s = ln(|o mu| 1e5), with sigma = d^T Q d / 2 and Q = [[a, b], [b, c]]. When Q
+// is positive definite with condition number <= (a + c)^2 / det <= 1000, the
+// rounded sigma the sample computes is within 8 * 2^-24 * 1000 < 5e-4 of sigma
+// relative (each rounding error is relative to |terms| <= cond * sigma), and
+// the fast exponential and logarithm add < 1e-5 absolute; so every passing
+// pixel lies in the ellipse sigma <= s' = s + 1e-3 |s| + 1e-3, whose bounding
+// box has half-widths sqrt(2 s' c / det) and sqrt(2 s' a / det). Those are
+// widened by 0.1 % plus 0.01 pixel, and by 1e-6 of the coordinates' magnitude
+// for the rounding of the box arithmetic itself.
+// Beta: a sample needs d2 = d^T Q d < 1; by the same argument every passing
+// pixel has d2 < 1.001.
+// Anything outside those conditions (a conic that is not positive definite or
+// badly conditioned, non-finite values) falls back to the whole tile, so the
+// box never drops a sample the reference would count.
+template <typename S, bool kBeta>
+__device__ __forceinline__ TileBox record_box(const Rec2D<S>& r, uint32_t ox, uint32_t oy, uint32_t vx, uint32_t vy) {
+    uint32_t x0 = 0, x1 = vx - 1, y0 = 0, y1 = vy - 1;
+    const S a = r.a, b = r.b, c = r.c;
+    const S det = a * c - b * b;
+    const S tr = a + c;
+    bool bounded = a > S(0) && c > S(0) && det > S(0) && tr * tr <= S(1000) * det;
+    S reach = S(1.001);
+    if (!kBeta) {
+        S s = log(fabs(r.o * r.mu)) + S(11.512925464970229);  // ln(1e5)
+        s = s + S(1e-3) * fabs(s) + S(1e-3);
+        if (bounded && isfinite(s) && s < S(0)) return TileBox{0u, 0u, 0u, 1u};
+        bounded = bounded && isfinite(s);
+        reach = S(2) * s;
+    }
+    if (bounded) {
+        const S hx = sqrt(reach * c / det) * S(1.001) + S(0.01);
+        const S hy = sqrt(reach * a / det) * S(1.001) + S(0.01);
+        // Pixel j (centre j + 0.5) can pass only if |j + 0.5 - x| <= hx.
+        const S cx = r.x - S(0.5) - static_cast<S>(ox);
+        const S cy = r.y - S(0.5) - static_cast<S>(oy);
+        const S mx = S(1e-6) * (fabs(r.x) + hx + static_cast<S>(ox));
+        const S my = S(1e-6) * (fabs(r.y) + hy + static_cast<S>(oy));
+        const S lo_x = ceil(cx - hx - mx), hi_x = floor(cx + hx + mx);
+        const S lo_y = ceil(cy - hy - my), hi_y = floor(cy + hy + my);
+        if (isfinite(lo_x) && isfinite(hi_x) && isfinite(lo_y) && isfinite(hi_y)) {
+            if (hi_x < S(0) || lo_x > static_cast<S>(x1) || hi_y < S(0) || lo_y > static_cast<S>(y1))
+                return TileBox{0u, 0u, 0u, 1u};
+            if (lo_x > S(0)) x0 = static_cast<uint32_t>(lo_x);
+            if (hi_x < static_cast<S>(x1)) x1 = static_cast<uint32_t>(hi_x);
+            if (lo_y > S(0)) y0 = static_cast<uint32_t>(lo_y);
+            if (hi_y < static_cast<S>(y1)) y1 = static_cast<uint32_t>(hi_y);
+            if (x0 > x1 || y0 > y1) return TileBox{0u, 0u, 0u, 1u};
+        }
+    }
+    const uint32_t bw = x1 - x0 + 1, bh = y1 - y0 + 1;
+    TileBox box;
+    box.cols = low_bits(bw) << x0;
+    box.rows = low_bits(bh) << y0;
+    box.packed = x0 | (y0 << 8) | (bw << 16) | (bh << 24);
+    box.magic = (65536u + bw - 1u) / bw;
+    return box;
+}
+
+// --------------------------------------------------------------------------
 // Forward
 // --------------------------------------------------------------------------
 
-template <typename S, bool kBeta, bool kVar, int PPT>
-__global__ void __launch_bounds__(256) raster_fwd_kernel(
+constexpr uint32_t kBlockW = 8;      // one warp's pixel block in the forward: 8 x 4
+constexpr uint32_t kBlockH = 4;
+constexpr uint32_t kFwdBatch = 256;  // records staged per batch (at most)
+
+template <typename S, bool kBeta, bool kVar, int kMaxThreads>
+__global__ void __launch_bounds__(kMaxThreads) raster_fwd_kernel(
     const Rec2D<S>* __restrict__ records, const S* __restrict__ uncertainties, uint32_t N,
     const int32_t* __restrict__ offsets, const int32_t* __restrict__ flatten_ids, int32_t n_isects,
     uint32_t C, uint32_t width, uint32_t height, uint32_t T, uint32_t tiles_x, uint32_t n_tiles,
     S* __restrict__ render, S* __restrict__ render_var) {
     extern __shared__ __align__(16) unsigned char smem[];
-    const uint32_t nthreads = blockDim.x;
-    Rec2D<S>* s_rec = reinterpret_cast<Rec2D<S>*>(smem);                 // [2][nthreads]
-    S* s_q = reinterpret_cast<S*>(s_rec + 2 * nthreads);                   // [2][nthreads]
+    const uint32_t B = blockDim.x < kFwdBatch ? blockDim.x : kFwdBatch;
+    Rec2D<S>* s_rec = reinterpret_cast<Rec2D<S>*>(smem);          // [2][B]
+    S* s_q = reinterpret_cast<S*>(s_rec + 2 * B);                   // [2][B]
+    uint2* s_mask = reinterpret_cast<uint2*>(s_q + 2 * B);          // [B] (column, row) masks
 
     const uint32_t tile = blockIdx.x, cam = blockIdx.y;
     const uint32_t key = cam * n_tiles + tile;
+    const uint32_t ty = tile / tiles_x, tx = tile - ty * tiles_x;
+    const uint32_t ox = tx * T, oy = ty * T;
+    if (ox >= width || oy >= height) return;
+    const uint32_t vx = min(T, width - ox), vy = min(T, height - oy);
     const int32_t start = offsets[key];
     const int32_t end = (key + 1 == C * n_tiles) ? n_isects : offsets[key + 1];
-    const uint32_t ty = tile / tiles_x, tx = tile - ty * tiles_x;
-    const uint32_t t = threadIdx.x;
+    const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
 
-    S px[PPT], py[PPT], acc[PPT], accv[PPT];
-    uint32_t pix[PPT];
-    bool inside[PPT];
-#pragma unroll
-    for (int k = 0; k < PPT; ++k) {
-        const uint32_t p = t + uint32_t(k) * nthreads;
-        uint32_t ly, lx;
-        tile_pixel(p, T, ly, lx);
-        const uint32_t i = ty * T + ly, j = tx * T + lx;
-        inside[k] = p < T * T && i < height && j < width;
-        px[k] = static_cast<S>(j) + static_cast<S>(0.5);
-        py[k] = static_cast<S>(i) + static_cast<S>(0.5);
-        pix[k] = i * width + j;
-        acc[k] = S(0);
-        accv[k] = S(0);
-    }
+    const uint32_t blocks_x = (T + kBlockW - 1) / kBlockW;
+    const uint32_t bx0 = (warp % blocks_x) * kBlockW, by0 = (warp / blocks_x) * kBlockH;
+    const uint32_t lx = bx0 + (lane & 7u), ly = by0 + (lane >> 3);
+    const bool inside = lx < vx && ly < vy;
+    const uint32_t warp_cols = bx0 < 32u ? ((0xffu << bx0) & low_bits(vx)) : 0u;
+    const uint32_t warp_rows = by0 < 32u ? ((0xfu << by0) & low_bits(vy)) : 0u;
+    const bool warp_active = warp_cols != 0u && warp_rows != 0u;
+    const S px = static_cast<S>(ox + lx) + static_cast<S>(0.5);
+    const S py = static_cast<S>(oy + ly) + static_cast<S>(0.5);
+    S acc = S(0), accv = S(0);
 
     const int32_t count = end - start;
-    const int32_t n_batches = count > 0 ? (count + int32_t(nthreads) - 1) / int32_t(nthreads) : 0;
-    auto load = [&](int32_t b, int stage) {
-        const int32_t idx = start + b * int32_t(nthreads) + int32_t(t);
-        if (idx < end) {
+    const int32_t n_batches = count > 0 ? (count + int32_t(B) - 1) / int32_t(B) : 0;
+    auto load = [&](int32_t bi, uint32_t stage) {
+        const int32_t idx = start + bi * int32_t(B) + int32_t(t);
+        if (t < B && idx < end) {
             const int32_t g = flatten_ids[idx];
-            gather_record(s_rec + stage * nthreads + t, records + g);
-            if (kVar) s_q[stage * nthreads + t] = uncertainties[uint32_t(g) % N];
+            gather_record(s_rec + stage * B + t, records + g);
+            if (kVar) s_q[stage * B + t] = uncertainties[uint32_t(g) % N];
         }
         cp_async_commit();
     };
     if (n_batches > 0) load(0, 0);
-    for (int32_t b = 0; b < n_batches; ++b) {
-        if (b + 1 < n_batches) {
-            load(b + 1, (b + 1) & 1);
+    for (int32_t bi = 0; bi < n_batches; ++bi) {
+        if (bi + 1 < n_batches) {
+            load(bi + 1, uint32_t(bi + 1) & 1u);
             cp_async_wait<1>();
         } else {
             cp_async_wait<0>();
         }
         __syncthreads();
-        const Rec2D<S>* buf = s_rec + (b & 1) * nthreads;
-        const S* qbuf = s_q + (b & 1) * nthreads;
-        const int32_t batch = min(int32_t(nthreads), count - b * int32_t(nthreads));
-#pragma unroll 2
-        for (int32_t s = 0; s < batch; ++s) {
-            const Rec2D<S> r = buf[s];
-            const S om = r.o * r.mu;
-            S q = S(0);
-            if (kVar) q = qbuf[s];
-#pragma unroll
-            for (int k = 0; k < PPT; ++k) {
-                if (!kBeta) {
-                    const S dx = px[k] - r.x;
-                    const S dy = py[k] - r.y;
-                    const S sigma = static_cast<S>(0.5) * (r.a * dx * dx + r.c * dy * dy) + r.b * dx * dy;
-                    const S alpha = om * exp(-sigma);
-                    if (!(sigma < static_cast<S>(0) || fabs(alpha) < static_cast<S>(1e-5))) {
-                        acc[k] += alpha;
-                        if (kVar) accv[k] += q * alpha * alpha;
-                    }
-                } else {
-                    const S dx = r.x - px[k];
-                    const S dy = r.y - py[k];
-                    const S d2 = r.a * dx * dx + static_cast<S>(2) * r.b * dx * dy + r.c * dy * dy;
-                    if (!(d2 < static_cast<S>(0) || d2 >= static_cast<S>(1))) {
-                        const S h = static_cast<S>(1) - d2;
-                        const S alpha = om * pow(h, r.beta);
-                        if (!(fabs(alpha) < static_cast<S>(1e-5))) {
-                            acc[k] += alpha;
-                            if (kVar) accv[k] += q * alpha * alpha;
+        const uint32_t stage = uint32_t(bi) & 1u;
+        const Rec2D<S>* buf = s_rec + stage * B;
+        const S* qbuf = s_q + stage * B;
+        const int32_t batch = min(int32_t(B), count - bi * int32_t(B));
+        if (int32_t(t) < batch) {
+            const TileBox box = record_box<S, kBeta>(buf[t], ox, oy, vx, vy);
+            s_mask[t] = make_uint2(box.cols, box.rows);
+        }
+        __syncthreads();
+        if (warp_active) {
+            for (int32_t base = 0; base < batch; base += 32) {
+                bool hit = false;
+                if (base + int32_t(lane) < batch) {
+                    const uint2 m = s_mask[base + int32_t(lane)];
+                    hit = (m.x & warp_cols) != 0u && (m.y & warp_rows) != 0u;
+                }
+                uint32_t pending = __ballot_sync(0xffffffffu, hit);
+                while (pending != 0u) {
+                    const int32_t s = base + __ffs(pending) - 1;
+                    pending &= pending - 1u;
+                    const Rec2D<S> r = buf[s];
+                    const S om = r.o * r.mu;
+                    S q = S(0);
+                    if (kVar) q = qbuf[s];
+                    if (!kBeta) {
+                        const S dx = px - r.x;
+                        const S dy = py - r.y;
+                        const S sigma = static_cast<S>(0.5) * (r.a * dx * dx + r.c * dy * dy) + r.b * dx * dy;
+                        const S alpha = om * exp(-sigma);
+                        if (!(sigma < static_cast<S>(0) || fabs(alpha) < static_cast<S>(1e-5))) {
+                            acc += alpha;
+                            if (kVar) accv += q * alpha * alpha;
+                        }
+                    } else {
+                        const S dx = r.x - px;
+                        const S dy = r.y - py;
+                        const S d2 = r.a * dx * dx + static_cast<S>(2) * r.b * dx * dy + r.c * dy * dy;
+                        if (!(d2 < static_cast<S>(0) || d2 >= static_cast<S>(1))) {
+                            const S h = static_cast<S>(1) - d2;
+                            const S alpha = om * pow(h, r.beta);
+                            if (!(fabs(alpha) < static_cast<S>(1e-5))) {
+                                acc += alpha;
+                                if (kVar) accv += q * alpha * alpha;
+                            }
                         }
                     }
                 }
@@ -139,13 +228,10 @@ __global__ void __launch_bounds__(256) raster_fwd_kernel(
         }
         __syncthreads();
     }
-    const size_t cam_base = size_t(cam) * height * width;
-#pragma unroll
-    for (int k = 0; k < PPT; ++k) {
-        if (inside[k]) {
-            render[cam_base + pix[k]] = acc[k];
-            if (kVar) render_var[cam_base + pix[k]] = accv[k];
-        }
+    if (inside) {
+        const size_t pid = size_t(cam) * height * width + size_t(oy + ly) * width + (ox + lx);
+        render[pid] = acc;
+        if (kVar) render_var[pid] = accv;
     }
 }
 
@@ -163,11 +249,19 @@ constexpr int kBwdThreads = kBwdWarps * 32;
 //   grads null         -> skip the record-slot adjoints
 //   v_abs / v_unc null -> skip absgrad / uncertainty adjoints
 //
-// The per-sample body is branch-free: a skipped sample keeps its arithmetic
-// but has its alpha and visibility selected to zero, so every contribution
-// it would add is an exact zero and the compiler can interleave the lane's
-// pixels (a `continue` per pixel serialises their exp/pow latencies).
-template <typename S, bool kBeta, bool kVar, bool kAbs, int PPL>
+// Per sample the lane accumulates, with g the image adjoint (plus the
+// variance chain term) and w = -g alpha (Gaussian) or the d2 adjoint (Beta):
+//   S0 = sum w dx, S1 = sum w dy, S2 = sum w dx^2, S3 = sum w dx dy,
+//   S4 = sum w dy^2, S5 = sum g vis, S6 = sum g alpha log h (Beta),
+//   S7 = sum v_var alpha^2 (variance),
+// from which the record's adjoints follow once per record: for a Gaussian
+// x = -(a S0 + b S1), y = -(c S1 + b S0), a = S2 / 2, b = S3, c = S4 / 2,
+// o = mu S5, mu = o S5; for a Beta x = 2 (a S0 + b S1), y = 2 (b S0 + c S1),
+// a = S2, b = 2 S3, c = S4, o = mu S5, mu = o S5, beta = S6. These are the
+// reference's per-sample terms with the record's constants factored out.
+// The body is branch-free: a skipped sample keeps its arithmetic but has its
+// alpha and visibility selected to zero.
+template <typename S, bool kBeta, bool kVar, bool kAbs>
 __global__ void __launch_bounds__(kBwdThreads) raster_bwd_kernel(
     const Rec2D<S>* __restrict__ records, const S* __restrict__ var_q, uint32_t N,
     const int32_t* __restrict__ offsets, const int32_t* __restrict__ flatten_ids, int32_t n_isects,
@@ -175,48 +269,38 @@ __global__ void __launch_bounds__(kBwdThreads) raster_bwd_kernel(
     const S* __restrict__ v_render, const S* __restrict__ v_render_var, Rec2D<S>* __restrict__ grads,
     S* __restrict__ v_abs, S* __restrict__ v_unc) {
     extern __shared__ __align__(16) unsigned char smem[];
-    Rec2D<S>* s_rec = reinterpret_cast<Rec2D<S>*>(smem);            // [2][kBwdThreads]
-    S* s_q = reinterpret_cast<S*>(s_rec + 2 * kBwdThreads);           // [2][kBwdThreads]
-    int32_t* s_id = reinterpret_cast<int32_t*>(s_q + 2 * kBwdThreads);  // [2][kBwdThreads]
+    Rec2D<S>* s_rec = reinterpret_cast<Rec2D<S>*>(smem);             // [2][kBwdThreads]
+    TileBox* s_box = reinterpret_cast<TileBox*>(s_rec + 2 * kBwdThreads);  // [kBwdThreads]
+    S* s_q = reinterpret_cast<S*>(s_box + kBwdThreads);                // [2][kBwdThreads]
+    S* s_v = s_q + 2 * kBwdThreads;                                    // [T*T] image adjoint
+    S* s_vv = s_v + T * T;                                             // [T*T] variance adjoint
+    int32_t* s_id = reinterpret_cast<int32_t*>(s_vv + T * T);          // [2][kBwdThreads]
 
     const uint32_t tile = blockIdx.x, cam = blockIdx.y;
     const uint32_t key = cam * n_tiles + tile;
+    const uint32_t ty = tile / tiles_x, tx = tile - ty * tiles_x;
+    const uint32_t ox = tx * T, oy = ty * T;
+    if (ox >= width || oy >= height) return;
+    const uint32_t vx = min(T, width - ox), vy = min(T, height - oy);
     const int32_t start = offsets[key];
     const int32_t end = (key + 1 == C * n_tiles) ? n_isects : offsets[key + 1];
     const int32_t count = end - start;
     if (count <= 0) return;
-    const uint32_t ty = tile / tiles_x, tx = tile - ty * tiles_x;
-    const uint32_t t = threadIdx.x, lane = t & 31, warp = t >> 5;
-
-    // Sub-tiles of 32 * PPL pixels; warps split over sub-tiles, then records.
-    const uint32_t sub_pixels = 32u * PPL;
-    uint32_t n_sub = 1;  // a power of two, so it divides kBwdWarps (tiles are at most 32x32)
-    while (n_sub * sub_pixels < T * T) n_sub <<= 1;
-    const uint32_t my_sub = warp % n_sub;
-    const uint32_t warps_per_sub = kBwdWarps / n_sub;
-    const uint32_t my_lane_group = warp / n_sub;
-
+    const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
     const bool chain_var = kVar && var_q != nullptr;
-    S px[PPL], py[PPL], vr[PPL], vv[PPL];
-    bool valid[PPL];
+
     const size_t cam_base = size_t(cam) * height * width;
-#pragma unroll
-    for (int k = 0; k < PPL; ++k) {
-        const uint32_t p = my_sub * sub_pixels + lane + 32u * k;
-        uint32_t ly, lx;
-        tile_pixel(p, T, ly, lx);
-        const uint32_t i = ty * T + ly, j = tx * T + lx;
-        valid[k] = p < T * T && i < height && j < width;
-        px[k] = static_cast<S>(j) + static_cast<S>(0.5);
-        py[k] = static_cast<S>(i) + static_cast<S>(0.5);
-        const size_t pid = cam_base + size_t(i) * width + j;
-        vr[k] = (valid[k] && v_render != nullptr) ? v_render[pid] : S(0);
-        vv[k] = (kVar && valid[k]) ? v_render_var[pid] : S(0);
+    for (uint32_t p = t; p < T * T; p += kBwdThreads) {
+        const uint32_t py_ = p / T, px_ = p - py_ * T;
+        const bool ok = px_ < vx && py_ < vy;
+        const size_t pid = cam_base + size_t(oy + py_) * width + (ox + px_);
+        s_v[p] = (ok && v_render != nullptr) ? v_render[pid] : S(0);
+        if (kVar) s_vv[p] = ok ? v_render_var[pid] : S(0);
     }
 
     const int32_t n_batches = (count + kBwdThreads - 1) / kBwdThreads;
-    auto load = [&](int32_t b, int stage) {
-        const int32_t idx = start + b * kBwdThreads + int32_t(t);
+    auto load = [&](int32_t bi, uint32_t stage) {
+        const int32_t idx = start + bi * kBwdThreads + int32_t(t);
         if (idx < end) {
             const int32_t g = flatten_ids[idx];
             gather_record(s_rec + stage * kBwdThreads + t, records + g);
@@ -226,109 +310,128 @@ __global__ void __launch_bounds__(kBwdThreads) raster_bwd_kernel(
         cp_async_commit();
     };
     load(0, 0);
-    for (int32_t b = 0; b < n_batches; ++b) {
-        if (b + 1 < n_batches) {
-            load(b + 1, (b + 1) & 1);
+    for (int32_t bi = 0; bi < n_batches; ++bi) {
+        if (bi + 1 < n_batches) {
+            load(bi + 1, uint32_t(bi + 1) & 1u);
             cp_async_wait<1>();
         } else {
             cp_async_wait<0>();
         }
         __syncthreads();
-        const int stage = b & 1;
-        const int32_t batch = min(int32_t(kBwdThreads), count - b * kBwdThreads);
-        for (int32_t s = int32_t(my_lane_group); s < batch; s += int32_t(warps_per_sub)) {
+        const uint32_t stage = uint32_t(bi) & 1u;
+        const int32_t batch = min(int32_t(kBwdThreads), count - bi * kBwdThreads);
+        if (int32_t(t) < batch) s_box[t] = record_box<S, kBeta>(s_rec[stage * kBwdThreads + t], ox, oy, vx, vy);
+        __syncthreads();
+        for (int32_t s = int32_t(warp); s < batch; s += kBwdWarps) {
+            const TileBox box = s_box[s];
+            const uint32_t bw = (box.packed >> 16) & 0xffu, bh = box.packed >> 24;
+            const uint32_t area = bw * bh;
+            if (area == 0u) continue;
+            const uint32_t x0 = box.packed & 0xffu, y0 = (box.packed >> 8) & 0xffu;
             const Rec2D<S> r = s_rec[stage * kBwdThreads + s];
             const int32_t g = s_id[stage * kBwdThreads + s];
             const S q = chain_var ? s_q[stage * kBwdThreads + s] : S(0);
             const S om = r.o * r.mu;
-            S g_x = 0, g_y = 0, g_a = 0, g_b = 0, g_c = 0, g_o = 0, g_mu = 0, g_beta = 0, g_q = 0, g_ax = 0,
-              g_ay = 0;
+            S part[8];
 #pragma unroll
-            for (int k = 0; k < PPL; ++k) {
+            for (int i = 0; i < 8; ++i) part[i] = S(0);
+            S g_ax = S(0), g_ay = S(0);
+            for (uint32_t k = lane; k < area; k += 32u) {
+                const uint32_t row = (k * box.magic) >> 16;
+                const uint32_t col = k - row * bw;
+                const uint32_t lx = x0 + col, ly = y0 + row;
+                const uint32_t p = ly * T + lx;
+                const S px = static_cast<S>(ox + lx) + static_cast<S>(0.5);
+                const S py = static_cast<S>(oy + ly) + static_cast<S>(0.5);
+                S v = s_v[p];
+                const S vv = kVar ? s_vv[p] : S(0);
                 if (!kBeta) {
-                    const S dx = px[k] - r.x;
-                    const S dy = py[k] - r.y;
+                    const S dx = px - r.x;
+                    const S dy = py - r.y;
                     const S sigma = static_cast<S>(0.5) * (r.a * dx * dx + r.c * dy * dy) + r.b * dx * dy;
                     const S vis_raw = exp(-sigma);
                     const S alpha_raw = om * vis_raw;
-                    const bool keep = valid[k] && !(sigma < static_cast<S>(0) || fabs(alpha_raw) < static_cast<S>(1e-5));
+                    const bool keep = !(sigma < static_cast<S>(0) || fabs(alpha_raw) < static_cast<S>(1e-5));
                     const S vis = keep ? vis_raw : S(0);
                     const S alpha = keep ? alpha_raw : S(0);
-                    S v = vr[k];
                     if (kVar) {
-                        g_q += vv[k] * alpha * alpha;
-                        v += static_cast<S>(2) * q * alpha * vv[k];
+                        part[7] += vv * alpha * alpha;
+                        v += static_cast<S>(2) * q * alpha * vv;
                     }
-                    const S v_sigma = -v * alpha;
-                    const S gx = -v_sigma * (r.a * dx + r.b * dy);
-                    const S gy = -v_sigma * (r.c * dy + r.b * dx);
-                    g_x += gx;
-                    g_y += gy;
+                    const S w = -v * alpha;
+                    const S wx = w * dx, wy = w * dy;
+                    part[0] += wx;
+                    part[1] += wy;
+                    part[2] += wx * dx;
+                    part[3] += wx * dy;
+                    part[4] += wy * dy;
+                    part[5] += v * vis;
                     if (kAbs) {
-                        g_ax += fabs(gx);
-                        g_ay += fabs(gy);
+                        g_ax += fabs(r.a * wx + r.b * wy);
+                        g_ay += fabs(r.c * wy + r.b * wx);
                     }
-                    g_a += v_sigma * static_cast<S>(0.5) * dx * dx;
-                    g_b += v_sigma * dx * dy;
-                    g_c += v_sigma * static_cast<S>(0.5) * dy * dy;
-                    g_o += v * r.mu * vis;
-                    g_mu += v * r.o * vis;
                 } else {
-                    const S dx = r.x - px[k];
-                    const S dy = r.y - py[k];
+                    const S dx = r.x - px;
+                    const S dy = r.y - py;
                     const S d2 = r.a * dx * dx + static_cast<S>(2) * r.b * dx * dy + r.c * dy * dy;
                     const S h_raw = static_cast<S>(1) - d2;
-                    const bool inside = valid[k] && !(d2 < static_cast<S>(0) || h_raw <= static_cast<S>(0));
-                    const S h = inside ? h_raw : S(1);  // keeps pow/log finite on skipped samples
+                    const bool in_support = !(d2 < static_cast<S>(0) || h_raw <= static_cast<S>(0));
+                    const S h = in_support ? h_raw : S(1);  // keeps pow/log finite on skipped samples
                     const S vis_raw = pow(h, r.beta);
                     const S alpha_raw = om * vis_raw;
-                    const bool keep = inside && !(fabs(alpha_raw) < static_cast<S>(1e-5));
+                    const bool keep = in_support && !(fabs(alpha_raw) < static_cast<S>(1e-5));
                     const S vis = keep ? vis_raw : S(0);
                     const S alpha = keep ? alpha_raw : S(0);
-                    S v = keep ? vr[k] : S(0);
+                    v = keep ? v : S(0);
                     if (kVar) {
-                        g_q += vv[k] * alpha * alpha;
-                        v += static_cast<S>(2) * q * alpha * vv[k];
+                        part[7] += vv * alpha * alpha;
+                        v += static_cast<S>(2) * q * alpha * vv;
                     }
-                    const S v_d2 = -om * r.beta * pow(h, r.beta - static_cast<S>(1)) * v;
-                    const S gx = static_cast<S>(2) * v_d2 * (r.a * dx + r.b * dy);
-                    const S gy = static_cast<S>(2) * v_d2 * (r.b * dx + r.c * dy);
-                    g_x += gx;
-                    g_y += gy;
+                    const S w = -om * r.beta * pow(h, r.beta - static_cast<S>(1)) * v;
+                    const S wx = w * dx, wy = w * dy;
+                    part[0] += wx;
+                    part[1] += wy;
+                    part[2] += wx * dx;
+                    part[3] += wx * dy;
+                    part[4] += wy * dy;
+                    part[5] += v * vis;
+                    part[6] += v * alpha * log(h);
                     if (kAbs) {
-                        g_ax += fabs(gx);
-                        g_ay += fabs(gy);
+                        g_ax += fabs(static_cast<S>(2) * (r.a * wx + r.b * wy));
+                        g_ay += fabs(static_cast<S>(2) * (r.b * wx + r.c * wy));
                     }
-                    g_a += v_d2 * dx * dx;
-                    g_b += static_cast<S>(2) * v_d2 * dx * dy;
-                    g_c += v_d2 * dy * dy;
-                    g_o += v * r.mu * vis;
-                    g_mu += v * r.o * vis;
-                    g_beta += v * alpha * log(h);
                 }
             }
-            g_x = warp_sum(g_x);
-            g_y = warp_sum(g_y);
-            g_a = warp_sum(g_a);
-            g_b = warp_sum(g_b);
-            g_c = warp_sum(g_c);
-            g_o = warp_sum(g_o);
-            g_mu = warp_sum(g_mu);
-            if (kBeta) g_beta = warp_sum(g_beta);
-            if (kVar) g_q = warp_sum(g_q);
+            S lo, hi;
+            warp_sum8_pairs(part, lo, hi);
+            const uint32_t grp = lane >> 3;
+            if ((lane & 7u) == 0u) {
+                if (grads != nullptr) {
+                    S* dst = reinterpret_cast<S*>(grads + g);
+                    S e0, e1;
+                    if (grp == 0u) {
+                        e0 = kBeta ? static_cast<S>(2) * (r.a * lo + r.b * hi) : -(r.a * lo + r.b * hi);
+                        e1 = kBeta ? static_cast<S>(2) * (r.b * lo + r.c * hi) : -(r.c * hi + r.b * lo);
+                    } else if (grp == 1u) {
+                        e0 = kBeta ? lo : static_cast<S>(0.5) * lo;
+                        e1 = kBeta ? static_cast<S>(2) * hi : hi;
+                    } else {
+                        e0 = kBeta ? lo : static_cast<S>(0.5) * lo;
+                        e1 = r.mu * hi;
+                    }
+                    if (grp < 3u) red_add_v2(dst + 2 * grp, e0, e1);
+                    if (grp == 2u) red_add(dst + 6, r.o * hi);
+                    if (kBeta && grp == 3u) red_add(dst + 7, lo);
+                }
+                if (kVar && grp == 3u && v_unc != nullptr) red_add(v_unc + (uint32_t(g) % N), hi);
+            }
             if (kAbs) {
                 g_ax = warp_sum(g_ax);
                 g_ay = warp_sum(g_ay);
-            }
-            if (grads != nullptr) {
-                S* dst = reinterpret_cast<S*>(grads + g);
-                if (lane == 0) red_add_v4(dst, g_x, g_y, g_a, g_b);
-                if (lane == 1) red_add_v4(dst + 4, g_c, g_o, g_mu, g_beta);
-            }
-            if (kVar && lane == 2 && v_unc != nullptr) red_add(v_unc + (uint32_t(g) % N), g_q);
-            if (kAbs && lane == 3) {
-                red_add(v_abs + 2 * size_t(g), g_ax);
-                red_add(v_abs + 2 * size_t(g) + 1, g_ay);
+                if (lane == 0u) {
+                    red_add(v_abs + 2 * size_t(g), g_ax);
+                    red_add(v_abs + 2 * size_t(g) + 1, g_ay);
+                }
             }
         }
         __syncthreads();
@@ -391,31 +494,28 @@ inline int check_geom(const RasterGeom& g) {
     return R2S_OK;
 }
 
-template <typename S, bool kBeta, bool kVar, int PPT>
-int launch_fwd_t(const RasterGeom& g, const Rec2D<S>* rec, const S* unc, const int32_t* offsets,
-                 const int32_t* ids, S* out, S* out_var, unsigned nthreads, cudaStream_t stream) {
-    const size_t smem = 2 * nthreads * (sizeof(Rec2D<S>) + sizeof(S));
-    dim3 grid(g.tiles_x * g.tiles_y, g.C);
-    raster_fwd_kernel<S, kBeta, kVar, PPT><<<grid, nthreads, smem, stream>>>(
-        rec, unc, g.N, offsets, ids, int32_t(g.n_isects), g.C, g.width, g.height, g.T, g.tiles_x,
-        g.tiles_x * g.tiles_y, out, out_var);
-    return check_launch("rasterize_to_pixels_fwd");
-}
-
 template <typename S, bool kBeta, bool kVar>
 int launch_fwd_p(const RasterGeom& g, const Rec2D<S>* rec, const S* unc, const int32_t* offsets,
                  const int32_t* ids, S* out, S* out_var, cudaStream_t stream) {
-    const uint32_t pixels = g.T * g.T;
-    if (pixels <= 64) {
-        const unsigned nt = (pixels + 31) / 32 * 32;
-        return launch_fwd_t<S, kBeta, kVar, 1>(g, rec, unc, offsets, ids, out, out_var, nt, stream);
+    // One warp per 8x4 block of the tile: at most 4 x 8 warps for 32x32 tiles.
+    const uint32_t blocks = ((g.T + kBlockW - 1) / kBlockW) * ((g.T + kBlockH - 1) / kBlockH);
+    const unsigned nthreads = 32u * blocks;
+    const unsigned batch = nthreads < kFwdBatch ? nthreads : kFwdBatch;
+    const size_t smem = 2 * size_t(batch) * (sizeof(Rec2D<S>) + sizeof(S)) + size_t(batch) * sizeof(uint2);
+    dim3 grid(g.tiles_x * g.tiles_y, g.C);
+    if (nthreads <= 256) {
+        // Tiles up to 16x16: a register budget sized for 256-thread CTAs.
+        R2S_TRY(allow_dynamic_smem(raster_fwd_kernel<S, kBeta, kVar, 256>, smem));
+        raster_fwd_kernel<S, kBeta, kVar, 256><<<grid, nthreads, smem, stream>>>(
+            rec, unc, g.N, offsets, ids, int32_t(g.n_isects), g.C, g.width, g.height, g.T, g.tiles_x,
+            g.tiles_x * g.tiles_y, out, out_var);
+    } else {
+        R2S_TRY(allow_dynamic_smem(raster_fwd_kernel<S, kBeta, kVar, 1024>, smem));
+        raster_fwd_kernel<S, kBeta, kVar, 1024><<<grid, nthreads, smem, stream>>>(
+            rec, unc, g.N, offsets, ids, int32_t(g.n_isects), g.C, g.width, g.height, g.T, g.tiles_x,
+            g.tiles_x * g.tiles_y, out, out_var);
     }
-    if (pixels <= 512) {
-        const unsigned nt = ((pixels + 1) / 2 + 31) / 32 * 32;
-        return launch_fwd_t<S, kBeta, kVar, 2>(g, rec, unc, offsets, ids, out, out_var, nt, stream);
-    }
-    const unsigned nt = ((pixels + 3) / 4 + 31) / 32 * 32;
-    return launch_fwd_t<S, kBeta, kVar, 4>(g, rec, unc, offsets, ids, out, out_var, nt, stream);
+    return check_launch("rasterize_to_pixels_fwd");
 }
 
 template <typename S>
@@ -432,28 +532,18 @@ int launch_fwd(const RasterGeom& g, const Rec2D<S>* rec, const S* unc, bool beta
                : launch_fwd_p<S, false, false>(g, rec, unc, offsets, ids, out, out_var, stream);
 }
 
-template <typename S, bool kBeta, bool kVar, bool kAbs, int PPL>
-int launch_bwd_t(const RasterGeom& g, const Rec2D<S>* rec, const S* var_q, const int32_t* offsets,
-                 const int32_t* ids, const S* v_render, const S* v_render_var, Rec2D<S>* grads, S* v_abs,
-                 S* v_unc, cudaStream_t stream) {
-    const size_t smem = 2 * kBwdThreads * (sizeof(Rec2D<S>) + sizeof(S) + sizeof(int32_t));
-    dim3 grid(g.tiles_x * g.tiles_y, g.C);
-    raster_bwd_kernel<S, kBeta, kVar, kAbs, PPL><<<grid, kBwdThreads, smem, stream>>>(
-        rec, var_q, g.N, offsets, ids, int32_t(g.n_isects), g.C, g.width, g.height, g.T, g.tiles_x,
-        g.tiles_x * g.tiles_y, v_render, v_render_var, grads, v_abs, v_unc);
-    return check_launch("rasterize_to_pixels_bwd");
-}
-
 template <typename S, bool kBeta, bool kVar, bool kAbs>
 int launch_bwd_p(const RasterGeom& g, const Rec2D<S>* rec, const S* var_q, const int32_t* offsets,
                  const int32_t* ids, const S* v_render, const S* v_render_var, Rec2D<S>* grads, S* v_abs,
                  S* v_unc, cudaStream_t stream) {
-    // Pixels per lane: 2 for tiles up to 8x8, else 8 (sub-tiles of 256 pixels).
-    if (g.T * g.T <= 64)
-        return launch_bwd_t<S, kBeta, kVar, kAbs, 2>(g, rec, var_q, offsets, ids, v_render, v_render_var, grads,
-                                                     v_abs, v_unc, stream);
-    return launch_bwd_t<S, kBeta, kVar, kAbs, 8>(g, rec, var_q, offsets, ids, v_render, v_render_var, grads,
-                                                 v_abs, v_unc, stream);
+    const size_t smem = 2 * size_t(kBwdThreads) * (sizeof(Rec2D<S>) + sizeof(S) + sizeof(int32_t)) +
+                        size_t(kBwdThreads) * sizeof(TileBox) + 2 * size_t(g.T) * g.T * sizeof(S);
+    R2S_TRY(allow_dynamic_smem(raster_bwd_kernel<S, kBeta, kVar, kAbs>, smem));
+    dim3 grid(g.tiles_x * g.tiles_y, g.C);
+    raster_bwd_kernel<S, kBeta, kVar, kAbs><<<grid, kBwdThreads, smem, stream>>>(
+        rec, var_q, g.N, offsets, ids, int32_t(g.n_isects), g.C, g.width, g.height, g.T, g.tiles_x,
+        g.tiles_x * g.tiles_y, v_render, v_render_var, grads, v_abs, v_unc);
+    return check_launch("rasterize_to_pixels_bwd");
 }
 
 template <typename S, bool kBeta>

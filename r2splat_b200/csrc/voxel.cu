@@ -138,55 +138,137 @@ __global__ void __launch_bounds__(256) voxel_fwd_kernel(const Rec3D<S>* __restri
 constexpr int kVoxBwdWarps = 8;
 constexpr int kVoxBwdThreads = kVoxBwdWarps * 32;
 
+// A record's box on one 3D tile, tile-local: origin x0 | y0 << 8 | z0 << 16,
+// extent w | h << 8 | d << 16, and ceil(2^20 / w), ceil(2^20 / (w h)), with
+// which (k * magic) >> 20 is the exact quotient for every k < 1024 and divisor
+// <= 1024. An empty box has a zero extent.
+struct alignas(16) VoxelBox {
+    uint32_t origin, extent, magic_w, magic_wh;
+};
+
+// Conservative box of the voxels whose sample can pass the contribution test
+// (the 3D form of the rasterizer's pixel box). Gaussian: |o| exp(-sigma) >=
+// 1e-6 needs sigma <= s = ln(|o| 1e6), sigma = d^T Q d / 2. For Q positive
+// definite with tr(Q)^3 / det(Q) <= 700 (which bounds the ratio of the
+// magnitude of sigma's terms to sigma, tr / lambda_min), the rounded sigma is
+// within 10 * 2^-24 * 700 < 5e-4 of sigma relative, so every passing voxel
+// lies in sigma <= s' = s + 1e-3 |s| + 1e-3, whose bounding box has
+// half-widths sqrt(2 s' adj(Q)_ii / det(Q)). Beta: d^T Q d < 1, so d^T Q d <
+// 1.001. Half-widths are widened by 0.1 % + 0.01 voxel and by 1e-6 of the
+// coordinates' magnitude; any other case takes the whole tile.
+template <typename S, bool kBeta>
+__device__ __forceinline__ VoxelBox voxel_box(const Rec3D<S>& r, uint32_t ox, uint32_t oy, uint32_t oz, uint32_t vx,
+                                              uint32_t vy, uint32_t vz) {
+    uint32_t lo[3] = {0u, 0u, 0u};
+    uint32_t hi[3] = {vx - 1, vy - 1, vz - 1};
+    const VoxelBox empty{0u, 0u, 1u, 1u};
+    const S a = r.c00, p = r.c01, q = r.c02, bb = r.c11, rr = r.c12, c = r.c22;
+    const S adj0 = bb * c - rr * rr;
+    const S adj1 = a * c - q * q;
+    const S adj2 = a * bb - p * p;
+    const S det = a * adj0 - p * (p * c - rr * q) + q * (p * rr - bb * q);
+    const S tr = a + bb + c;
+    bool bounded = a > S(0) && bb > S(0) && c > S(0) && adj0 > S(0) && adj1 > S(0) && adj2 > S(0) &&
+                   det > S(0) && tr * tr * tr <= S(700) * det;
+    S reach = S(1.001);
+    if (!kBeta) {
+        S s = log(fabs(r.o)) + S(13.815510557964274);  // ln(1e6)
+        s = s + S(1e-3) * fabs(s) + S(1e-3);
+        if (bounded && isfinite(s) && s < S(0)) return empty;
+        bounded = bounded && isfinite(s);
+        reach = S(2) * s;
+    }
+    if (bounded) {
+        const S adj[3] = {adj0, adj1, adj2};
+        const S centre[3] = {r.x, r.y, r.z};
+        const uint32_t origin[3] = {ox, oy, oz};
+#pragma unroll
+        for (int axis = 0; axis < 3; ++axis) {
+            const S h = sqrt(reach * adj[axis] / det) * S(1.001) + S(0.01);
+            const S cc = centre[axis] - S(0.5) - static_cast<S>(origin[axis]);
+            const S m = S(1e-6) * (fabs(centre[axis]) + h + static_cast<S>(origin[axis]));
+            const S l = ceil(cc - h - m), u = floor(cc + h + m);
+            if (!(isfinite(l) && isfinite(u))) continue;
+            if (u < S(0) || l > static_cast<S>(hi[axis])) return empty;
+            if (l > S(0)) lo[axis] = static_cast<uint32_t>(l);
+            if (u < static_cast<S>(hi[axis])) hi[axis] = static_cast<uint32_t>(u);
+            if (lo[axis] > hi[axis]) return empty;
+        }
+    }
+    const uint32_t w = hi[0] - lo[0] + 1, h = hi[1] - lo[1] + 1, d = hi[2] - lo[2] + 1;
+    VoxelBox box;
+    box.origin = lo[0] | (lo[1] << 8) | (lo[2] << 16);
+    box.extent = w | (h << 8) | (d << 16);
+    box.magic_w = ((1u << 20) + w - 1u) / w;
+    box.magic_wh = ((1u << 20) + w * h - 1u) / (w * h);
+    return box;
+}
+
+// Voxel centre and image adjoint of one tile voxel.
+template <typename S>
+struct alignas(4 * sizeof(S)) VoxelSample {
+    S x, y, z, v;
+};
+
 // Null-pointer conventions as in the rasterizer VJP: v_volume null = zero
 // adjoint; v_volume_var null = no variance branch; chain_var false =
 // detached variance branch.
-template <typename S, bool kBeta, bool kVar, int PPL>
+//
+// One warp per record, evaluating only the voxels of the record's box. Per
+// sample a lane accumulates, with g the volume adjoint (plus the variance
+// chain term) and w = -g alpha (Gaussian) or the d^T Q d adjoint (Beta):
+//   S1..S3 = sum w d_i, Svis = sum g vis, S_ij = sum w d_i d_j (i <= j),
+//   Sb = sum g alpha log h (Beta), Sq = sum v_var alpha^2 (variance);
+// the record's adjoints follow once per record: for a Gaussian
+// x_i = -(Q d-sums)_i, i.e. x = -(c00 S1 + c01 S2 + c02 S3) and so on,
+// c_ii = S_ii / 2, c_ij = S_ij, o = Svis; for a Beta x = 2 (Q d-sums)_i,
+// c_ii = S_ii, c_ij = 2 S_ij, o = Svis, beta = Sb -- the reference's
+// per-sample terms with the record's constants factored out.
+template <typename S, bool kBeta, bool kVar>
 __global__ void __launch_bounds__(kVoxBwdThreads) voxel_bwd_kernel(
     const Rec3D<S>* __restrict__ records, bool chain_var, const int32_t* __restrict__ offsets,
     const int32_t* __restrict__ flatten_ids, VoxelGeom g, const S* __restrict__ v_volume,
     const S* __restrict__ v_volume_var, Rec3D<S>* __restrict__ grads) {
     extern __shared__ __align__(16) unsigned char smem[];
-    Rec3D<S>* s_rec = reinterpret_cast<Rec3D<S>*>(smem);                    // [2][threads]
-    int32_t* s_id = reinterpret_cast<int32_t*>(s_rec + 2 * kVoxBwdThreads);  // [2][threads]
     const uint32_t T = g.T;
+    const uint32_t tile_voxels = T * T * T;
+    Rec3D<S>* s_rec = reinterpret_cast<Rec3D<S>*>(smem);                          // [2][threads]
+    VoxelBox* s_box = reinterpret_cast<VoxelBox*>(s_rec + 2 * kVoxBwdThreads);     // [threads]
+    VoxelSample<S>* s_vox = reinterpret_cast<VoxelSample<S>*>(s_box + kVoxBwdThreads);  // [T^3]
+    S* s_vv = reinterpret_cast<S*>(s_vox + tile_voxels);                           // [T^3]
+    int32_t* s_id = reinterpret_cast<int32_t*>(s_vv + tile_voxels);                // [2][threads]
+
     const uint32_t n_tiles = g.tiles_x * g.tiles_y * g.tiles_z;
     const uint32_t key = blockIdx.x;
+    const uint32_t tz = key / (g.tiles_x * g.tiles_y);
+    const uint32_t rem = key - tz * g.tiles_x * g.tiles_y;
+    const uint32_t ty = rem / g.tiles_x, tx = rem - ty * g.tiles_x;
+    const uint32_t ox = tx * T, oy = ty * T, oz = tz * T;
+    if (ox >= g.dim2 || oy >= g.dim1 || oz >= g.dim0) return;
+    const uint32_t vx = min(T, g.dim2 - ox), vy = min(T, g.dim1 - oy), vz = min(T, g.dim0 - oz);
     const int32_t start = offsets[key];
     const int32_t end = (key + 1 == n_tiles) ? int32_t(g.n_isects) : offsets[key + 1];
     const int32_t count = end - start;
     if (count <= 0) return;
-    const uint32_t tz = key / (g.tiles_x * g.tiles_y);
-    const uint32_t rem = key - tz * g.tiles_x * g.tiles_y;
-    const uint32_t ty = rem / g.tiles_x, tx = rem - ty * g.tiles_x;
-    const uint32_t t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
 
-    const uint32_t sub_voxels = 32u * PPL;
-    uint32_t n_sub = 1;
-    while (n_sub * sub_voxels < T * T * T) n_sub <<= 1;
-    const uint32_t my_sub = warp % n_sub;
-    const uint32_t warps_per_sub = kVoxBwdWarps / n_sub;
-    const uint32_t my_group = warp / n_sub;
-
-    S px[PPL], py[PPL], pz[PPL], vr[PPL], vv[PPL];
-    bool valid[PPL];
-#pragma unroll
-    for (int k = 0; k < PPL; ++k) {
-        const uint32_t p = my_sub * sub_voxels + lane + 32u * k;
-        uint32_t lz, ly, lx;
-        tile_voxel(p, T, lz, ly, lx);
-        const uint32_t i = tz * T + lz, j = ty * T + ly, kk = tx * T + lx;
-        valid[k] = p < T * T * T && i < g.dim0 && j < g.dim1 && kk < g.dim2;
-        px[k] = static_cast<S>(kk) + static_cast<S>(0.5);
-        py[k] = static_cast<S>(j) + static_cast<S>(0.5);
-        pz[k] = static_cast<S>(i) + static_cast<S>(0.5);
-        const size_t vid = (size_t(i) * g.dim1 + j) * g.dim2 + kk;
-        vr[k] = (valid[k] && v_volume != nullptr) ? v_volume[vid] : S(0);
-        vv[k] = (kVar && valid[k]) ? v_volume_var[vid] : S(0);
+    for (uint32_t p = t; p < tile_voxels; p += kVoxBwdThreads) {
+        const uint32_t lz = p / (T * T);
+        const uint32_t r2 = p - lz * T * T;
+        const uint32_t ly = r2 / T, lx = r2 - ly * T;
+        const bool ok = lx < vx && ly < vy && lz < vz;
+        const size_t vid = (size_t(oz + lz) * g.dim1 + (oy + ly)) * g.dim2 + (ox + lx);
+        VoxelSample<S> sm;
+        sm.x = static_cast<S>(ox + lx) + static_cast<S>(0.5);
+        sm.y = static_cast<S>(oy + ly) + static_cast<S>(0.5);
+        sm.z = static_cast<S>(oz + lz) + static_cast<S>(0.5);
+        sm.v = (ok && v_volume != nullptr) ? v_volume[vid] : S(0);
+        s_vox[p] = sm;
+        if (kVar) s_vv[p] = ok ? v_volume_var[vid] : S(0);
     }
 
     const int32_t n_batches = (count + kVoxBwdThreads - 1) / kVoxBwdThreads;
-    auto load = [&](int32_t b, int stage) {
+    auto load = [&](int32_t b, uint32_t stage) {
         const int32_t idx = start + b * kVoxBwdThreads + int32_t(t);
         if (idx < end) {
             const int32_t gid = flatten_ids[idx];
@@ -198,92 +280,141 @@ __global__ void __launch_bounds__(kVoxBwdThreads) voxel_bwd_kernel(
     load(0, 0);
     for (int32_t b = 0; b < n_batches; ++b) {
         if (b + 1 < n_batches) {
-            load(b + 1, (b + 1) & 1);
+            load(b + 1, uint32_t(b + 1) & 1u);
             cp_async_wait<1>();
         } else {
             cp_async_wait<0>();
         }
         __syncthreads();
-        const int stage = b & 1;
+        const uint32_t stage = uint32_t(b) & 1u;
         const int32_t batch = min(int32_t(kVoxBwdThreads), count - b * kVoxBwdThreads);
-        for (int32_t s = int32_t(my_group); s < batch; s += int32_t(warps_per_sub)) {
+        if (int32_t(t) < batch) s_box[t] = voxel_box<S, kBeta>(s_rec[stage * kVoxBwdThreads + t], ox, oy, oz, vx, vy, vz);
+        __syncthreads();
+        for (int32_t s = int32_t(warp); s < batch; s += kVoxBwdWarps) {
+            const VoxelBox box = s_box[s];
+            const uint32_t w = box.extent & 0xffu, h = (box.extent >> 8) & 0xffu, d = (box.extent >> 16) & 0xffu;
+            const uint32_t wh = w * h, vol = wh * d;
+            if (vol == 0u) continue;
+            const uint32_t base = (((box.origin >> 16) & 0xffu) * T + ((box.origin >> 8) & 0xffu)) * T +
+                                  (box.origin & 0xffu);
             const Rec3D<S> r = s_rec[stage * kVoxBwdThreads + s];
             const int32_t gid = s_id[stage * kVoxBwdThreads + s];
             const S a = r.c00, p = r.c01, q = r.c02, bb = r.c11, rr = r.c12, c = r.c22;
             const S opac = r.o;
             const S uq = chain_var ? r.q : S(0);
-            S gx = 0, gy = 0, gz = 0, go = 0, g0 = 0, g1 = 0, g2 = 0, g3 = 0, g4 = 0, g5 = 0, gb = 0, gq = 0;
+            // part: S1, S2, S3, Svis | S11, S12, S13, S22 | S23, S33, Sb, Sq | unused
+            S part[16];
 #pragma unroll
-            for (int k = 0; k < PPL; ++k) {
+            for (int i = 0; i < 16; ++i) part[i] = S(0);
+            for (uint32_t k = lane; k < vol; k += 32u) {
+                const uint32_t zz = (k * box.magic_wh) >> 20;
+                const uint32_t rem2 = k - zz * wh;
+                const uint32_t yy = (rem2 * box.magic_w) >> 20;
+                const uint32_t xx = rem2 - yy * w;
+                const uint32_t pv = base + (zz * T + yy) * T + xx;
+                const VoxelSample<S> sm = s_vox[pv];
+                S v = sm.v;
+                const S vv = kVar ? s_vv[pv] : S(0);
+                S wgt, d1, d2, d3;
                 if (!kBeta) {
-                    const S d1 = px[k] - r.x, d2 = py[k] - r.y, d3 = pz[k] - r.z;
+                    d1 = sm.x - r.x;
+                    d2 = sm.y - r.y;
+                    d3 = sm.z - r.z;
                     const S sigma = static_cast<S>(0.5) * (a * d1 * d1 + bb * d2 * d2 + c * d3 * d3) +
                                     p * d1 * d2 + q * d1 * d3 + rr * d2 * d3;
                     const S vis_raw = exp(-sigma);
                     const S alpha_raw = opac * vis_raw;
-                    const bool keep = valid[k] && !(sigma < static_cast<S>(0) || fabs(alpha_raw) < static_cast<S>(1e-6));
+                    const bool keep = !(sigma < static_cast<S>(0) || fabs(alpha_raw) < static_cast<S>(1e-6));
                     const S vis = keep ? vis_raw : S(0);
                     const S alpha = keep ? alpha_raw : S(0);
-                    S v_O = vr[k];
                     if (kVar) {
-                        gq += vv[k] * alpha * alpha;
-                        v_O += static_cast<S>(2) * uq * alpha * vv[k];
+                        part[11] += vv * alpha * alpha;
+                        v += static_cast<S>(2) * uq * alpha * vv;
                     }
-                    const S v_sigma = -v_O * opac * vis;
-                    const S oI = opac * vis;
-                    go += v_O * vis;
-                    g0 += v_sigma * static_cast<S>(0.5) * d1 * d1;
-                    g1 += v_sigma * d1 * d2;
-                    g2 += v_sigma * d1 * d3;
-                    g3 += v_sigma * static_cast<S>(0.5) * d2 * d2;
-                    g4 += v_sigma * d2 * d3;
-                    g5 += v_sigma * static_cast<S>(0.5) * d3 * d3;
-                    gx += v_O * oI * (a * d1 + p * d2 + q * d3);
-                    gy += v_O * oI * (bb * d2 + p * d1 + rr * d3);
-                    gz += v_O * oI * (c * d3 + q * d1 + rr * d2);
+                    wgt = -v * alpha;
+                    part[3] += v * vis;
                 } else {
-                    const S d1 = r.x - px[k], d2 = r.y - py[k], d3 = r.z - pz[k];
+                    d1 = r.x - sm.x;
+                    d2 = r.y - sm.y;
+                    d3 = r.z - sm.z;
                     const S qf = a * d1 * d1 + bb * d2 * d2 + c * d3 * d3 + static_cast<S>(2) * p * d1 * d2 +
                                  static_cast<S>(2) * q * d1 * d3 + static_cast<S>(2) * rr * d2 * d3;
                     const S h_raw = static_cast<S>(1) - qf;
-                    const bool inside = valid[k] && !(qf < static_cast<S>(0) || h_raw <= static_cast<S>(0));
-                    const S h = inside ? h_raw : S(1);  // keeps pow/log finite on skipped samples
-                    const S vis_raw = pow(h, r.beta);
+                    const bool in_support = !(qf < static_cast<S>(0) || h_raw <= static_cast<S>(0));
+                    const S hh = in_support ? h_raw : S(1);  // keeps pow/log finite on skipped samples
+                    const S vis_raw = pow(hh, r.beta);
                     const S alpha_raw = opac * vis_raw;
-                    const bool keep = inside && !(fabs(alpha_raw) < static_cast<S>(1e-5));
+                    const bool keep = in_support && !(fabs(alpha_raw) < static_cast<S>(1e-5));
                     const S vis = keep ? vis_raw : S(0);
                     const S alpha = keep ? alpha_raw : S(0);
-                    S v_O = keep ? vr[k] : S(0);
+                    v = keep ? v : S(0);
                     if (kVar) {
-                        gq += vv[k] * alpha * alpha;
-                        v_O += static_cast<S>(2) * uq * alpha * vv[k];
+                        part[11] += vv * alpha * alpha;
+                        v += static_cast<S>(2) * uq * alpha * vv;
                     }
-                    const S v_q = -opac * r.beta * pow(h, r.beta - static_cast<S>(1)) * v_O;
-                    const S wx = a * d1 + p * d2 + q * d3;
-                    const S wy = bb * d2 + p * d1 + rr * d3;
-                    const S wz = c * d3 + q * d1 + rr * d2;
-                    gx += static_cast<S>(2) * v_q * wx;
-                    gy += static_cast<S>(2) * v_q * wy;
-                    gz += static_cast<S>(2) * v_q * wz;
-                    g0 += v_q * d1 * d1;
-                    g1 += static_cast<S>(2) * v_q * d1 * d2;
-                    g2 += static_cast<S>(2) * v_q * d1 * d3;
-                    g3 += v_q * d2 * d2;
-                    g4 += static_cast<S>(2) * v_q * d2 * d3;
-                    g5 += v_q * d3 * d3;
-                    go += v_O * vis;
-                    gb += v_O * alpha * log(h);
+                    wgt = -opac * r.beta * pow(hh, r.beta - static_cast<S>(1)) * v;
+                    part[3] += v * vis;
+                    part[10] += v * alpha * log(hh);
                 }
+                const S t1 = wgt * d1, t2 = wgt * d2, t3 = wgt * d3;
+                part[0] += t1;
+                part[1] += t2;
+                part[2] += t3;
+                part[4] += t1 * d1;
+                part[5] += t1 * d2;
+                part[6] += t1 * d3;
+                part[7] += t2 * d2;
+                part[8] += t2 * d3;
+                part[9] += t3 * d3;
             }
-            gx = warp_sum(gx); gy = warp_sum(gy); gz = warp_sum(gz); go = warp_sum(go);
-            g0 = warp_sum(g0); g1 = warp_sum(g1); g2 = warp_sum(g2); g3 = warp_sum(g3);
-            g4 = warp_sum(g4); g5 = warp_sum(g5);
-            if (kBeta) gb = warp_sum(gb);
-            if (kVar) gq = warp_sum(gq);
-            S* dst = reinterpret_cast<S*>(grads + gid);
-            if (lane == 0) red_add_v4(dst, gx, gy, gz, go);
-            if (lane == 1) red_add_v4(dst + 4, g0, g1, g2, g3);
-            if (lane == 2) red_add_v4(dst + 8, g4, g5, gb, gq);
+            // Recursive halving: 16 -> 8 (lane bit 4) -> 4 (bit 3) values, then
+            // a butterfly over lane bits 2..0; lane group G = lane / 8 ends with
+            // the warp totals of part[4G .. 4G+3].
+            const bool hi16 = (lane & 16u) != 0, hi8 = (lane & 8u) != 0;
+            S w8[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const S send = hi16 ? part[i] : part[i + 8];
+                const S keep = hi16 ? part[i + 8] : part[i];
+                w8[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+            }
+            S w4[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const S send = hi8 ? w8[i] : w8[i + 4];
+                const S keep = hi8 ? w8[i + 4] : w8[i];
+                w4[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+            }
+#pragma unroll
+            for (int offset = 4; offset > 0; offset >>= 1) {
+#pragma unroll
+                for (int i = 0; i < 4; ++i) w4[i] += __shfl_xor_sync(0xffffffffu, w4[i], offset);
+            }
+            const uint32_t grp = lane >> 3;
+            if ((lane & 7u) == 0u && grp < 3u) {
+                const S two = static_cast<S>(2), half = static_cast<S>(0.5);
+                S e0, e1, e2, e3;
+                if (grp == 0u) {
+                    const S sx = a * w4[0] + p * w4[1] + q * w4[2];
+                    const S sy = bb * w4[1] + p * w4[0] + rr * w4[2];
+                    const S sz = c * w4[2] + q * w4[0] + rr * w4[1];
+                    e0 = kBeta ? two * sx : -sx;
+                    e1 = kBeta ? two * sy : -sy;
+                    e2 = kBeta ? two * sz : -sz;
+                    e3 = w4[3];
+                } else if (grp == 1u) {
+                    e0 = kBeta ? w4[0] : half * w4[0];
+                    e1 = kBeta ? two * w4[1] : w4[1];
+                    e2 = kBeta ? two * w4[2] : w4[2];
+                    e3 = kBeta ? w4[3] : half * w4[3];
+                } else {
+                    e0 = kBeta ? two * w4[0] : w4[0];
+                    e1 = kBeta ? w4[1] : half * w4[1];
+                    e2 = w4[2];
+                    e3 = w4[3];
+                }
+                red_add_v4(reinterpret_cast<S*>(grads + gid) + 4 * grp, e0, e1, e2, e3);
+            }
         }
         __syncthreads();
     }
@@ -376,25 +507,17 @@ int launch_vfwd(const VoxelGeom& g, const Rec3D<S>* rec, bool beta, const int32_
                : launch_vfwd_p<S, false, false>(g, rec, offsets, ids, vol, vol_var, stream);
 }
 
-template <typename S, bool kBeta, bool kVar, int PPL>
-int launch_vbwd_t(const VoxelGeom& g, const Rec3D<S>* rec, bool chain_var, const int32_t* offsets,
-                  const int32_t* ids, const S* v_vol, const S* v_vol_var, Rec3D<S>* grads, cudaStream_t stream) {
-    const size_t smem = 2 * kVoxBwdThreads * (sizeof(Rec3D<S>) + sizeof(int32_t));
-    if (smem > 48 * 1024)
-        cudaFuncSetAttribute(voxel_bwd_kernel<S, kBeta, kVar, PPL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(smem));
-    const unsigned grid = g.tiles_x * g.tiles_y * g.tiles_z;
-    voxel_bwd_kernel<S, kBeta, kVar, PPL><<<grid, kVoxBwdThreads, smem, stream>>>(rec, chain_var, offsets, ids, g,
-                                                                                   v_vol, v_vol_var, grads);
-    return check_launch("voxelize_to_voxels_bwd");
-}
-
 template <typename S, bool kBeta, bool kVar>
 int launch_vbwd_p(const VoxelGeom& g, const Rec3D<S>* rec, bool chain_var, const int32_t* offsets,
                   const int32_t* ids, const S* v_vol, const S* v_vol_var, Rec3D<S>* grads, cudaStream_t stream) {
-    if (g.T * g.T * g.T <= 64)
-        return launch_vbwd_t<S, kBeta, kVar, 2>(g, rec, chain_var, offsets, ids, v_vol, v_vol_var, grads, stream);
-    return launch_vbwd_t<S, kBeta, kVar, 8>(g, rec, chain_var, offsets, ids, v_vol, v_vol_var, grads, stream);
+    const size_t tile_voxels = size_t(g.T) * g.T * g.T;
+    const size_t smem = 2 * size_t(kVoxBwdThreads) * (sizeof(Rec3D<S>) + sizeof(int32_t)) +
+                        size_t(kVoxBwdThreads) * sizeof(VoxelBox) + tile_voxels * (sizeof(VoxelSample<S>) + sizeof(S));
+    R2S_TRY(allow_dynamic_smem(voxel_bwd_kernel<S, kBeta, kVar>, smem));
+    const unsigned grid = g.tiles_x * g.tiles_y * g.tiles_z;
+    voxel_bwd_kernel<S, kBeta, kVar><<<grid, kVoxBwdThreads, smem, stream>>>(rec, chain_var, offsets, ids, g, v_vol,
+                                                                           v_vol_var, grads);
+    return check_launch("voxelize_to_voxels_bwd");
 }
 
 template <typename S>
