@@ -323,6 +323,18 @@ int r2s_raster_render_bwd(int dtype, const void* records, const void* uncertaint
                           uint32_t tiles_y, void* grads, void* v_means2d_abs,
                           void* v_uncertainties, void* stream);
 
+/* Record-parallel VJP of r2s_raster_render: one pass over the [C,N] records
+ * (not the intersection lists), each record evaluated on the pixels of its
+ * tile rectangle rects [C,N,4] (uint16 x0, y0, x1, y1 in tiles, upper bounds
+ * exclusive, as r2s_raster_project writes them) and written to grads [C,N,8]
+ * without atomics (every record written; the buffer needs no clearing).
+ * v_means2d_abs [C,N,2] optional (written); v_uncertainties [N] accumulated
+ * (clear it first). Same adjoints as r2s_raster_render_bwd. */
+int r2s_raster_record_bwd(int dtype, const void* records, const uint16_t* rects, const void* uncertainties,
+                          int beta, int detach_variance, const void* v_render, const void* v_render_var,
+                          uint32_t C, uint32_t N, uint32_t width, uint32_t height, uint32_t tile_size,
+                          void* grads, void* v_means2d_abs, void* v_uncertainties, void* stream);
+
 /* Chain rule from packed adjoints to physical parameters (explicit.py:225-241):
  * conic/mu VJP, projection VJP summed over cameras, Beta path factor and the
  * parameter-transform VJP, per primitive, with no atomics. log_grad [N] and

@@ -4,10 +4,11 @@ Rasterize (the reference's explicit.py:160-183 and :204-241):
   parameter transform -> one fused projection/conic/packing pass writing 32-byte
   records [C,N,8] + tile rectangles + tile counts -> int64 prefix sum -> host
   read of the intersection count -> emission + stable radix sort + per-tile
-  offsets -> tile accumulation. The VJP is the tile kernel accumulating packed
-  adjoints [C,N,8] with vector atomics, then one per-primitive chain-rule pass
-  (conic/mu VJP, projection VJP summed over cameras, Beta path factor,
-  parameter-transform VJP) with no atomics.
+  offsets -> tile accumulation. The VJP needs no tile order: one warp per
+  (camera, primitive) record walks the pixels of the record's tile rectangle
+  and writes its packed adjoints [C,N,8] once, then one per-primitive
+  chain-rule pass (conic/mu VJP, projection VJP summed over cameras, Beta path
+  factor, parameter-transform VJP); neither uses atomics.
 
 Voxelize (explicit.py:286-307, :331-350): the same structure in 3D with
 64-byte records [N,16].
@@ -119,7 +120,10 @@ class VoxelState:
 
 def raster_intersections(means, covars, densities, beta, ratio, viewmats, Ks, width, height, eps, radius_clip,
                          tile_size=RASTER_TILE):
-    """Projection + packing + sorted tile intersections. Returns (records, offsets, isect_ids, flatten_ids, M)."""
+    """Projection + packing + sorted tile intersections.
+
+    Returns (records, offsets, isect_ids, flatten_ids, M, rects); rects [C,N,4] are the tile rectangles.
+    """
     device = means.device
     c, n = viewmats.shape[0], means.shape[0]
     tx = (width + tile_size - 1) // tile_size
@@ -143,7 +147,7 @@ def raster_intersections(means, covars, densities, beta, ratio, viewmats, Ks, wi
     with _stage("raster_sort"):
         _backend.call("r2s_raster_emit", _ptr(rects), c, n, tx, ty, _ptr(cum), m, _ptr(isect_ids),
                       _ptr(flatten_ids), _ptr(offsets), _ptr(ws), ws.numel(), stream)
-    return records, offsets, isect_ids, flatten_ids, m
+    return records, offsets, isect_ids, flatten_ids, m, rects
 
 
 def raster_forward(means, quats, scales, densities, viewmats, Ks, width, height, beta, uncertainty, eps,
@@ -153,7 +157,7 @@ def raster_forward(means, quats, scales, densities, viewmats, Ks, width, height,
     c = viewmats.shape[0]
     covars, _ = low.parameter_transform_fwd(quats, scales)
     ratio = _beta.beta_path_ratio(beta) if beta is not None else None
-    records, offsets, isect_ids, flatten_ids, m = raster_intersections(
+    records, offsets, isect_ids, flatten_ids, m, rects = raster_intersections(
         means, covars, densities, beta, ratio, viewmats, Ks, width, height, eps, radius_clip, tile_size)
     image = means.new_empty((c, height, width))
     variance = torch.empty_like(image) if uncertainty is not None else None
@@ -163,7 +167,8 @@ def raster_forward(means, quats, scales, densities, viewmats, Ks, width, height,
         _backend.call("r2s_raster_render", _dtype(means), _ptr(records), _ptr(uncertainty), int(beta is not None),
                       _ptr(offsets), _ptr(flatten_ids), c, means.shape[0], m, width, height, tile_size, tx, ty,
                       _ptr(image), _ptr(variance), _stream(device))
-    state = RasterState(covars, records, offsets, isect_ids, flatten_ids, ratio, m, width, height, tile_size)
+    state = RasterState(covars, records, offsets, isect_ids, flatten_ids, ratio, m, width, height, tile_size,
+                        extra={"rects": rects})
     output = image if uncertainty is None else (image, variance)
     return output, state
 
@@ -174,16 +179,14 @@ def raster_backward(state: RasterState, means, quats, scales, densities, beta, u
     device = means.device
     c, n = viewmats.shape[0], means.shape[0]
     tile = state.tile_size
-    tx = (state.width + tile - 1) // tile
-    ty = (state.height + tile - 1) // tile
     stream = _stream(device)
-    grads = means.new_zeros((c, n, 8))
+    grads = means.new_empty((c, n, 8))  # every record is written by the record-parallel VJP
     v_unc = means.new_zeros((n,)) if v_variance is not None else None
     with _stage("raster_render_bwd"):
-        _backend.call("r2s_raster_render_bwd", _dtype(means), _ptr(state.records), _ptr(uncertainty),
-                      int(beta is not None), int(bool(detach_variance)), _ptr(state.offsets), _ptr(state.flatten_ids),
-                      _ptr(v_image), _ptr(v_variance), c, n, state.n_isects, state.width, state.height, tile, tx, ty,
-                      _ptr(grads), None, _ptr(v_unc), stream)
+        _backend.call("r2s_raster_record_bwd", _dtype(means), _ptr(state.records), _ptr(state.extra["rects"]),
+                      _ptr(uncertainty), int(beta is not None), int(bool(detach_variance)), _ptr(v_image),
+                      _ptr(v_variance), c, n, state.width, state.height, tile, _ptr(grads), None, _ptr(v_unc),
+                      stream)
     log_grad = _beta.beta_path_log_grad(beta) if beta is not None else None
     v_means = means.new_empty((n, 3))
     v_quats = means.new_empty((n, 4))

@@ -55,7 +55,9 @@ struct alignas(16) TileBox {
 
 __device__ __forceinline__ uint32_t low_bits(uint32_t n) { return n >= 32u ? 0xffffffffu : ((1u << n) - 1u); }
 
-// Conservative box of the pixels whose sample can pass the contribution test.
+// Clips the inclusive pixel range [x0, x1] x [y0, y1] (indices relative to
+// (ox, oy)) to a conservative box of the pixels whose sample can pass the
+// contribution test; returns false when no pixel of the range can pass.
 //
 // Gaussian: a sample counts only if |o mu| exp(-sigma) >= 1e-5, i.e. sigma <=
 // s = ln(|o mu| 1e5), with sigma = d^T Q d / 2 and Q = [[a, b], [b, c]]. When Q
@@ -73,8 +75,8 @@ __device__ __forceinline__ uint32_t low_bits(uint32_t n) { return n >= 32u ? 0xf
 // badly conditioned, non-finite values) falls back to the whole tile, so the
 // box never drops a sample the reference would count.
 template <typename S, bool kBeta>
-__device__ __forceinline__ TileBox record_box(const Rec2D<S>& r, uint32_t ox, uint32_t oy, uint32_t vx, uint32_t vy) {
-    uint32_t x0 = 0, x1 = vx - 1, y0 = 0, y1 = vy - 1;
+__device__ __forceinline__ bool clip_to_record(const Rec2D<S>& r, uint32_t ox, uint32_t oy, uint32_t& x0,
+                                               uint32_t& x1, uint32_t& y0, uint32_t& y1) {
     const S a = r.a, b = r.b, c = r.c;
     const S det = a * c - b * b;
     const S tr = a + c;
@@ -83,30 +85,36 @@ __device__ __forceinline__ TileBox record_box(const Rec2D<S>& r, uint32_t ox, ui
     if (!kBeta) {
         S s = log(fabs(r.o * r.mu)) + S(11.512925464970229);  // ln(1e5)
         s = s + S(1e-3) * fabs(s) + S(1e-3);
-        if (bounded && isfinite(s) && s < S(0)) return TileBox{0u, 0u, 0u, 1u};
+        if (bounded && isfinite(s) && s < S(0)) return false;
         bounded = bounded && isfinite(s);
         reach = S(2) * s;
     }
-    if (bounded) {
-        const S hx = sqrt(reach * c / det) * S(1.001) + S(0.01);
-        const S hy = sqrt(reach * a / det) * S(1.001) + S(0.01);
-        // Pixel j (centre j + 0.5) can pass only if |j + 0.5 - x| <= hx.
-        const S cx = r.x - S(0.5) - static_cast<S>(ox);
-        const S cy = r.y - S(0.5) - static_cast<S>(oy);
-        const S mx = S(1e-6) * (fabs(r.x) + hx + static_cast<S>(ox));
-        const S my = S(1e-6) * (fabs(r.y) + hy + static_cast<S>(oy));
-        const S lo_x = ceil(cx - hx - mx), hi_x = floor(cx + hx + mx);
-        const S lo_y = ceil(cy - hy - my), hi_y = floor(cy + hy + my);
-        if (isfinite(lo_x) && isfinite(hi_x) && isfinite(lo_y) && isfinite(hi_y)) {
-            if (hi_x < S(0) || lo_x > static_cast<S>(x1) || hi_y < S(0) || lo_y > static_cast<S>(y1))
-                return TileBox{0u, 0u, 0u, 1u};
-            if (lo_x > S(0)) x0 = static_cast<uint32_t>(lo_x);
-            if (hi_x < static_cast<S>(x1)) x1 = static_cast<uint32_t>(hi_x);
-            if (lo_y > S(0)) y0 = static_cast<uint32_t>(lo_y);
-            if (hi_y < static_cast<S>(y1)) y1 = static_cast<uint32_t>(hi_y);
-            if (x0 > x1 || y0 > y1) return TileBox{0u, 0u, 0u, 1u};
-        }
-    }
+    if (!bounded) return true;
+    const S hx = sqrt(reach * c / det) * S(1.001) + S(0.01);
+    const S hy = sqrt(reach * a / det) * S(1.001) + S(0.01);
+    // Pixel j (centre j + 0.5) can pass only if |j + 0.5 - x| <= hx.
+    const S cx = r.x - S(0.5) - static_cast<S>(ox);
+    const S cy = r.y - S(0.5) - static_cast<S>(oy);
+    const S mx = S(1e-6) * (fabs(r.x) + hx + static_cast<S>(ox));
+    const S my = S(1e-6) * (fabs(r.y) + hy + static_cast<S>(oy));
+    const S lo_x = ceil(cx - hx - mx), hi_x = floor(cx + hx + mx);
+    const S lo_y = ceil(cy - hy - my), hi_y = floor(cy + hy + my);
+    if (!(isfinite(lo_x) && isfinite(hi_x) && isfinite(lo_y) && isfinite(hi_y))) return true;
+    if (hi_x < static_cast<S>(x0) || lo_x > static_cast<S>(x1) || hi_y < static_cast<S>(y0) ||
+        lo_y > static_cast<S>(y1))
+        return false;
+    if (lo_x > static_cast<S>(x0)) x0 = static_cast<uint32_t>(lo_x);
+    if (hi_x < static_cast<S>(x1)) x1 = static_cast<uint32_t>(hi_x);
+    if (lo_y > static_cast<S>(y0)) y0 = static_cast<uint32_t>(lo_y);
+    if (hi_y < static_cast<S>(y1)) y1 = static_cast<uint32_t>(hi_y);
+    return x0 <= x1 && y0 <= y1;
+}
+
+// The record's box on the tile with origin (ox, oy) and valid extent vx x vy.
+template <typename S, bool kBeta>
+__device__ __forceinline__ TileBox record_box(const Rec2D<S>& r, uint32_t ox, uint32_t oy, uint32_t vx, uint32_t vy) {
+    uint32_t x0 = 0, x1 = vx - 1, y0 = 0, y1 = vy - 1;
+    if (!clip_to_record<S, kBeta>(r, ox, oy, x0, x1, y0, y1)) return TileBox{0u, 0u, 0u, 1u};
     const uint32_t bw = x1 - x0 + 1, bh = y1 - y0 + 1;
     TileBox box;
     box.cols = low_bits(bw) << x0;
@@ -239,6 +247,93 @@ __global__ void __launch_bounds__(kMaxThreads) raster_fwd_kernel(
 // Backward
 // --------------------------------------------------------------------------
 
+// One VJP sample: the record's contribution at pixel centre (px, py) with image
+// adjoint v and variance adjoint vv, accumulated into the lane's partial sums
+// (see raster_bwd_kernel for their meaning). Branch-free: a skipped sample has
+// its alpha and visibility selected to zero.
+template <typename S, bool kBeta, bool kVar, bool kAbs>
+__device__ __forceinline__ void vjp_sample(const Rec2D<S>& r, S om, S q, S px, S py, S v, S vv, bool valid,
+                                           S (&part)[8], S& g_ax, S& g_ay) {
+    if (!kBeta) {
+        const S dx = px - r.x;
+        const S dy = py - r.y;
+        const S sigma = static_cast<S>(0.5) * (r.a * dx * dx + r.c * dy * dy) + r.b * dx * dy;
+        const S vis_raw = exp(-sigma);
+        const S alpha_raw = om * vis_raw;
+        const bool keep = valid && !(sigma < static_cast<S>(0) || fabs(alpha_raw) < static_cast<S>(1e-5));
+        const S vis = keep ? vis_raw : S(0);
+        const S alpha = keep ? alpha_raw : S(0);
+        if (kVar) {
+            part[7] += vv * alpha * alpha;
+            v += static_cast<S>(2) * q * alpha * vv;
+        }
+        const S w = -v * alpha;
+        const S wx = w * dx, wy = w * dy;
+        part[0] += wx;
+        part[1] += wy;
+        part[2] += wx * dx;
+        part[3] += wx * dy;
+        part[4] += wy * dy;
+        part[5] += v * vis;
+        if (kAbs) {
+            g_ax += fabs(r.a * wx + r.b * wy);
+            g_ay += fabs(r.c * wy + r.b * wx);
+        }
+    } else {
+        const S dx = r.x - px;
+        const S dy = r.y - py;
+        const S d2 = r.a * dx * dx + static_cast<S>(2) * r.b * dx * dy + r.c * dy * dy;
+        const S h_raw = static_cast<S>(1) - d2;
+        const bool in_support = valid && !(d2 < static_cast<S>(0) || h_raw <= static_cast<S>(0));
+        const S h = in_support ? h_raw : S(1);  // keeps pow/log finite on skipped samples
+        const S vis_raw = pow(h, r.beta);
+        const S alpha_raw = om * vis_raw;
+        const bool keep = in_support && !(fabs(alpha_raw) < static_cast<S>(1e-5));
+        const S vis = keep ? vis_raw : S(0);
+        const S alpha = keep ? alpha_raw : S(0);
+        v = keep ? v : S(0);
+        if (kVar) {
+            part[7] += vv * alpha * alpha;
+            v += static_cast<S>(2) * q * alpha * vv;
+        }
+        const S w = -om * r.beta * pow(h, r.beta - static_cast<S>(1)) * v;
+        const S wx = w * dx, wy = w * dy;
+        part[0] += wx;
+        part[1] += wy;
+        part[2] += wx * dx;
+        part[3] += wx * dy;
+        part[4] += wy * dy;
+        part[5] += v * vis;
+        part[6] += v * alpha * log(h);
+        if (kAbs) {
+            g_ax += fabs(static_cast<S>(2) * (r.a * wx + r.b * wy));
+            g_ay += fabs(static_cast<S>(2) * (r.b * wx + r.c * wy));
+        }
+    }
+}
+
+// The record-slot adjoints held by lane group grp (= lane / 8) after
+// warp_sum8_pairs reduced the partial sums to (lo, hi): group 0 gives
+// (x, y), group 1 (a, b), group 2 (c, o) and mu (in e2), group 3 beta (in e0).
+template <typename S, bool kBeta>
+__device__ __forceinline__ void record_adjoints(const Rec2D<S>& r, uint32_t grp, S lo, S hi, S& e0, S& e1, S& e2) {
+    e2 = S(0);
+    if (grp == 0u) {
+        e0 = kBeta ? static_cast<S>(2) * (r.a * lo + r.b * hi) : -(r.a * lo + r.b * hi);
+        e1 = kBeta ? static_cast<S>(2) * (r.b * lo + r.c * hi) : -(r.c * hi + r.b * lo);
+    } else if (grp == 1u) {
+        e0 = kBeta ? lo : static_cast<S>(0.5) * lo;
+        e1 = kBeta ? static_cast<S>(2) * hi : hi;
+    } else if (grp == 2u) {
+        e0 = kBeta ? lo : static_cast<S>(0.5) * lo;
+        e1 = r.mu * hi;
+        e2 = r.o * hi;
+    } else {
+        e0 = kBeta ? lo : S(0);
+        e1 = S(0);
+    }
+}
+
 constexpr int kBwdWarps = 8;
 constexpr int kBwdThreads = kBwdWarps * 32;
 
@@ -343,64 +438,8 @@ __global__ void __launch_bounds__(kBwdThreads) raster_bwd_kernel(
                 const uint32_t p = ly * T + lx;
                 const S px = static_cast<S>(ox + lx) + static_cast<S>(0.5);
                 const S py = static_cast<S>(oy + ly) + static_cast<S>(0.5);
-                S v = s_v[p];
                 const S vv = kVar ? s_vv[p] : S(0);
-                if (!kBeta) {
-                    const S dx = px - r.x;
-                    const S dy = py - r.y;
-                    const S sigma = static_cast<S>(0.5) * (r.a * dx * dx + r.c * dy * dy) + r.b * dx * dy;
-                    const S vis_raw = exp(-sigma);
-                    const S alpha_raw = om * vis_raw;
-                    const bool keep = !(sigma < static_cast<S>(0) || fabs(alpha_raw) < static_cast<S>(1e-5));
-                    const S vis = keep ? vis_raw : S(0);
-                    const S alpha = keep ? alpha_raw : S(0);
-                    if (kVar) {
-                        part[7] += vv * alpha * alpha;
-                        v += static_cast<S>(2) * q * alpha * vv;
-                    }
-                    const S w = -v * alpha;
-                    const S wx = w * dx, wy = w * dy;
-                    part[0] += wx;
-                    part[1] += wy;
-                    part[2] += wx * dx;
-                    part[3] += wx * dy;
-                    part[4] += wy * dy;
-                    part[5] += v * vis;
-                    if (kAbs) {
-                        g_ax += fabs(r.a * wx + r.b * wy);
-                        g_ay += fabs(r.c * wy + r.b * wx);
-                    }
-                } else {
-                    const S dx = r.x - px;
-                    const S dy = r.y - py;
-                    const S d2 = r.a * dx * dx + static_cast<S>(2) * r.b * dx * dy + r.c * dy * dy;
-                    const S h_raw = static_cast<S>(1) - d2;
-                    const bool in_support = !(d2 < static_cast<S>(0) || h_raw <= static_cast<S>(0));
-                    const S h = in_support ? h_raw : S(1);  // keeps pow/log finite on skipped samples
-                    const S vis_raw = pow(h, r.beta);
-                    const S alpha_raw = om * vis_raw;
-                    const bool keep = in_support && !(fabs(alpha_raw) < static_cast<S>(1e-5));
-                    const S vis = keep ? vis_raw : S(0);
-                    const S alpha = keep ? alpha_raw : S(0);
-                    v = keep ? v : S(0);
-                    if (kVar) {
-                        part[7] += vv * alpha * alpha;
-                        v += static_cast<S>(2) * q * alpha * vv;
-                    }
-                    const S w = -om * r.beta * pow(h, r.beta - static_cast<S>(1)) * v;
-                    const S wx = w * dx, wy = w * dy;
-                    part[0] += wx;
-                    part[1] += wy;
-                    part[2] += wx * dx;
-                    part[3] += wx * dy;
-                    part[4] += wy * dy;
-                    part[5] += v * vis;
-                    part[6] += v * alpha * log(h);
-                    if (kAbs) {
-                        g_ax += fabs(static_cast<S>(2) * (r.a * wx + r.b * wy));
-                        g_ay += fabs(static_cast<S>(2) * (r.b * wx + r.c * wy));
-                    }
-                }
+                vjp_sample<S, kBeta, kVar, kAbs>(r, om, q, px, py, s_v[p], vv, true, part, g_ax, g_ay);
             }
             S lo, hi;
             warp_sum8_pairs(part, lo, hi);
@@ -408,20 +447,11 @@ __global__ void __launch_bounds__(kBwdThreads) raster_bwd_kernel(
             if ((lane & 7u) == 0u) {
                 if (grads != nullptr) {
                     S* dst = reinterpret_cast<S*>(grads + g);
-                    S e0, e1;
-                    if (grp == 0u) {
-                        e0 = kBeta ? static_cast<S>(2) * (r.a * lo + r.b * hi) : -(r.a * lo + r.b * hi);
-                        e1 = kBeta ? static_cast<S>(2) * (r.b * lo + r.c * hi) : -(r.c * hi + r.b * lo);
-                    } else if (grp == 1u) {
-                        e0 = kBeta ? lo : static_cast<S>(0.5) * lo;
-                        e1 = kBeta ? static_cast<S>(2) * hi : hi;
-                    } else {
-                        e0 = kBeta ? lo : static_cast<S>(0.5) * lo;
-                        e1 = r.mu * hi;
-                    }
+                    S e0, e1, e2;
+                    record_adjoints<S, kBeta>(r, grp, lo, hi, e0, e1, e2);
                     if (grp < 3u) red_add_v2(dst + 2 * grp, e0, e1);
-                    if (grp == 2u) red_add(dst + 6, r.o * hi);
-                    if (kBeta && grp == 3u) red_add(dst + 7, lo);
+                    if (grp == 2u) red_add(dst + 6, e2);
+                    if (kBeta && grp == 3u) red_add(dst + 7, e0);
                 }
                 if (kVar && grp == 3u && v_unc != nullptr) red_add(v_unc + (uint32_t(g) % N), hi);
             }
@@ -435,6 +465,167 @@ __global__ void __launch_bounds__(kBwdThreads) raster_bwd_kernel(
             }
         }
         __syncthreads();
+    }
+}
+
+// --------------------------------------------------------------------------
+// Record-parallel backward (explicit pipeline)
+// --------------------------------------------------------------------------
+
+constexpr int kRecBwdThreads = 256;
+
+// The VJP needs no tile order: a record's adjoints are sums over the pixels it
+// covers, which the reference evaluates exactly on the tiles of the record's
+// tile rectangle. So one warp takes one (camera, primitive) record, walks the
+// pixels of its tile rectangle that its conservative box keeps (row-major,
+// 32 lanes per step, the lane position advanced incrementally), reads the
+// pixel adjoints from the camera's adjoint image (L2-resident), and writes the
+// record's adjoints once: no per-tile overhead, no atomics, every slot of
+// grads written (zeros for records without pixels). rects [C,N] hold the
+// tile rectangle (x0, y0, x1, y1), upper bounds exclusive, as the projection
+// writes it.
+// ceil(65536 / w) for w = 1..32: (k * magic) >> 16 == k / w for k < 1024.
+__constant__ uint32_t c_div_magic[33] = {
+    0u,     65536u, 32768u, 21846u, 16384u, 13108u, 10923u, 9363u, 8192u, 7282u, 6554u,
+    5958u,  5462u,  5042u,  4682u,  4370u,  4096u,  3856u,  3641u, 3450u, 3277u, 3121u,
+    2979u,  2850u,  2731u,  2622u,  2521u,  2428u,  2341u,  2260u, 2185u, 2115u, 2048u};
+
+template <typename S, bool kBeta, bool kVar, bool kAbs>
+__global__ void __launch_bounds__(kRecBwdThreads) raster_record_bwd_kernel(
+    const Rec2D<S>* __restrict__ records, const ushort4* __restrict__ rects, const S* __restrict__ var_q,
+    uint32_t C, uint32_t N, uint32_t width, uint32_t height, uint32_t T, const S* __restrict__ v_render,
+    const S* __restrict__ v_render_var, Rec2D<S>* __restrict__ grads, S* __restrict__ v_abs,
+    S* __restrict__ v_unc) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warps_per_block = blockDim.x >> 5;
+    const size_t total = size_t(C) * N;
+    const size_t group_stride = size_t(gridDim.x) * warps_per_block * 32u;
+    const bool chain_var = kVar && var_q != nullptr;
+    // Each warp takes 32 consecutive records at a time. Lane-parallel set-up:
+    // lane L loads record base + L (coalesced) and computes its pixel box and
+    // stepping constants; the warp then walks the 32 records one by one,
+    // broadcasting each record's constants with shuffles.
+    for (size_t base = (size_t(blockIdx.x) * warps_per_block + (threadIdx.x >> 5)) * 32u; base < total;
+         base += group_stride) {
+        const size_t my_rid = base + lane;
+        Rec2D<S> mine;
+        uint32_t x0 = 0u, y0 = 0u, w = 0u, area = 0u;
+        const uint32_t my_cam = uint32_t(my_rid) / N;  // C * N < 2^31
+        S my_q = S(0);
+        if (my_rid < total) {
+            if (chain_var) my_q = var_q[uint32_t(my_rid) - my_cam * N];
+            const ushort4 rect = rects[my_rid];
+            x0 = uint32_t(rect.x) * T;
+            y0 = uint32_t(rect.y) * T;
+            uint32_t x1 = min(uint32_t(rect.z) * T, width), y1 = min(uint32_t(rect.w) * T, height);
+            bool any = rect.z > rect.x && rect.w > rect.y && x0 < x1 && y0 < y1;
+            mine = records[my_rid];
+            if (any) {
+                x1 -= 1u;
+                y1 -= 1u;
+                any = clip_to_record<S, kBeta>(mine, 0u, 0u, x0, x1, y0, y1);
+            }
+            if (any) {
+                w = x1 - x0 + 1u;
+                area = w * (y1 - y0 + 1u);
+            } else {
+                // No pixel can contribute: the record's adjoints are zero.
+                S* dst = reinterpret_cast<S*>(grads + my_rid);
+#pragma unroll
+                for (int i = 0; i < 8; ++i) dst[i] = S(0);
+                if (kAbs) {
+                    v_abs[2 * my_rid] = S(0);
+                    v_abs[2 * my_rid + 1] = S(0);
+                }
+            }
+        }
+        uint32_t pending = __ballot_sync(0xffffffffu, area != 0u);
+        while (pending != 0u) {
+            const uint32_t j = __ffs(pending) - 1u;
+            pending &= pending - 1u;
+            Rec2D<S> r;
+            r.x = __shfl_sync(0xffffffffu, mine.x, j);
+            r.y = __shfl_sync(0xffffffffu, mine.y, j);
+            r.a = __shfl_sync(0xffffffffu, mine.a, j);
+            r.b = __shfl_sync(0xffffffffu, mine.b, j);
+            r.c = __shfl_sync(0xffffffffu, mine.c, j);
+            r.o = __shfl_sync(0xffffffffu, mine.o, j);
+            r.mu = __shfl_sync(0xffffffffu, mine.mu, j);
+            r.beta = kBeta ? __shfl_sync(0xffffffffu, mine.beta, j) : S(0);
+            const uint32_t bx0 = __shfl_sync(0xffffffffu, x0, j);
+            const uint32_t by0 = __shfl_sync(0xffffffffu, y0, j);
+            const uint32_t bw = __shfl_sync(0xffffffffu, w, j);
+            const uint32_t barea = __shfl_sync(0xffffffffu, area, j);
+            const size_t rid = base + j;
+            const uint32_t cam = __shfl_sync(0xffffffffu, my_cam, j);
+            const uint32_t n = uint32_t(rid) - cam * N;
+            const size_t cam_base = size_t(cam) * height * width;
+            const S* vimg = v_render != nullptr ? v_render + cam_base : nullptr;
+            const S* vvar = kVar ? v_render_var + cam_base : nullptr;
+            const S q = chain_var ? __shfl_sync(0xffffffffu, my_q, j) : S(0);
+            const S om = r.o * r.mu;
+            // Lane k of the box (row-major, width bw) starts at k = lane and
+            // steps by 32: dq rows and dr columns, plus one wrap when the
+            // column overflows.
+            uint32_t dq = 0u, dr = 32u, row = 0u, col = lane;
+            if (bw < 32u) {
+                const uint32_t m = c_div_magic[bw];
+                dq = (32u * m) >> 16;
+                dr = 32u - dq * bw;
+                row = (lane * m) >> 16;
+                col = lane - row * bw;
+            }
+            uint32_t off = (by0 + row) * width + bx0 + col;
+            const uint32_t step = dq * width + dr, wrap_step = width - bw;
+            S px = static_cast<S>(bx0 + col) + static_cast<S>(0.5);
+            S py = static_cast<S>(by0 + row) + static_cast<S>(0.5);
+            const S x_end = static_cast<S>(bx0 + bw);  // a centre past the row is >= x0 + w + 0.5
+            const S step_x = static_cast<S>(dr), step_y = static_cast<S>(dq), wrap_x = static_cast<S>(bw);
+            const uint32_t iters = (barea + 31u) >> 5;
+            S part[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) part[i] = S(0);
+            S g_ax = S(0), g_ay = S(0);
+            // A warp-uniform trip count; lanes past the box end in the last step
+            // evaluate nothing (valid = false) and load nothing.
+            uint32_t k = lane;
+            for (uint32_t it = 0; it < iters; ++it, k += 32u) {
+                const bool valid = k < barea;
+                const S v = (valid && vimg != nullptr) ? vimg[off] : S(0);
+                const S vv = (kVar && valid) ? vvar[off] : S(0);
+                vjp_sample<S, kBeta, kVar, kAbs>(r, om, q, px, py, v, vv, valid, part, g_ax, g_ay);
+                px += step_x;
+                py += step_y;
+                off += step;
+                const bool wrap = px > x_end;
+                px = wrap ? px - wrap_x : px;
+                py = wrap ? py + static_cast<S>(1) : py;
+                off = wrap ? off + wrap_step : off;
+            }
+            S lo, hi;
+            warp_sum8_pairs(part, lo, hi);
+            const uint32_t grp = lane >> 3;
+            if ((lane & 7u) == 0u) {
+                S* dst = reinterpret_cast<S*>(grads + rid);
+                S e0, e1, e2;
+                record_adjoints<S, kBeta>(r, grp, lo, hi, e0, e1, e2);
+                if (grp < 3u) {
+                    dst[2 * grp] = e0;
+                    dst[2 * grp + 1] = e1;
+                }
+                if (grp == 2u) dst[6] = e2;
+                if (grp == 3u) dst[7] = e0;
+                if (kVar && grp == 3u && v_unc != nullptr) red_add(v_unc + n, hi);
+            }
+            if (kAbs) {
+                g_ax = warp_sum(g_ax);
+                g_ay = warp_sum(g_ay);
+                if (lane == 0u) {
+                    v_abs[2 * rid] = g_ax;
+                    v_abs[2 * rid + 1] = g_ay;
+                }
+            }
+        }
     }
 }
 
@@ -574,6 +765,45 @@ int launch_bwd(const RasterGeom& g, const Rec2D<S>* rec, bool beta, const S* var
                                         stream)
                 : launch_bwd_b<S, false>(g, rec, var_q, offsets, ids, v_render, v_render_var, grads, v_abs, v_unc,
                                          stream);
+}
+
+template <typename S, bool kBeta, bool kVar, bool kAbs>
+int launch_record_bwd_t(const RasterGeom& g, const Rec2D<S>* rec, const ushort4* rects, const S* var_q,
+                        const S* v_render, const S* v_render_var, Rec2D<S>* grads, S* v_abs, S* v_unc,
+                        cudaStream_t stream) {
+    const size_t total = size_t(g.C) * g.N;
+    const size_t warps_per_block = kRecBwdThreads / 32;
+    int device = 0, sms = 148, per_sm = 4;
+    if (cudaGetDevice(&device) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, raster_record_bwd_kernel<S, kBeta, kVar, kAbs>,
+                                                  kRecBwdThreads, 0);
+    // Persistent grid: exactly the resident blocks, each warp striding over
+    // records, so every warp takes the same number of records and none waits
+    // for a late wave.
+    size_t blocks = (total + warps_per_block - 1) / warps_per_block;
+    const size_t cap = size_t(sms > 0 ? sms : 148) * size_t(per_sm > 0 ? per_sm : 1);
+    if (blocks > cap) blocks = cap;
+    raster_record_bwd_kernel<S, kBeta, kVar, kAbs><<<unsigned(blocks), kRecBwdThreads, 0, stream>>>(
+        rec, rects, var_q, g.C, g.N, g.width, g.height, g.T, v_render, v_render_var, grads, v_abs, v_unc);
+    return check_launch("raster_record_bwd");
+}
+
+template <typename S, bool kBeta>
+int launch_record_bwd_b(const RasterGeom& g, const Rec2D<S>* rec, const ushort4* rects, const S* var_q,
+                        const S* v_render, const S* v_render_var, Rec2D<S>* grads, S* v_abs, S* v_unc,
+                        cudaStream_t stream) {
+    const bool var = v_render_var != nullptr, abs = v_abs != nullptr;
+    if (var && abs)
+        return launch_record_bwd_t<S, kBeta, true, true>(g, rec, rects, var_q, v_render, v_render_var, grads, v_abs,
+                                                         v_unc, stream);
+    if (var)
+        return launch_record_bwd_t<S, kBeta, true, false>(g, rec, rects, var_q, v_render, v_render_var, grads, v_abs,
+                                                          v_unc, stream);
+    if (abs)
+        return launch_record_bwd_t<S, kBeta, false, true>(g, rec, rects, var_q, v_render, v_render_var, grads, v_abs,
+                                                          v_unc, stream);
+    return launch_record_bwd_t<S, kBeta, false, false>(g, rec, rects, var_q, v_render, v_render_var, grads, v_abs,
+                                                       v_unc, stream);
 }
 
 template <typename S>
@@ -743,6 +973,31 @@ int r2s_raster_render_bwd(int dtype, const void* records, const void* uncertaint
                                              static_cast<const S*>(v_render_var), static_cast<Rec2D<S>*>(grads),
                                              static_cast<S*>(v_means2d_abs), static_cast<S*>(v_uncertainties),
                                              as_stream(stream)));
+}
+
+int r2s_raster_record_bwd(int dtype, const void* records, const uint16_t* rects, const void* uncertainties, int beta,
+                          int detach_variance, const void* v_render, const void* v_render_var, uint32_t C,
+                          uint32_t N, uint32_t width, uint32_t height, uint32_t tile_size, void* grads,
+                          void* v_means2d_abs, void* v_uncertainties, void* stream) {
+    const RasterGeom g{C, N, 0u, width, height, tile_size, 1u, 1u};
+    R2S_TRY(check_geom(g));
+    R2S_REQUIRE(uint64_t(width) * height < (uint64_t(1) << 32), R2S_ERR_UNSUPPORTED, "image too large");
+    R2S_REQUIRE(v_render_var == nullptr || v_uncertainties != nullptr, R2S_ERR_ARGUMENT,
+                "variance adjoint needs v_uncertainties");
+    if (uint64_t(C) * N == 0) return R2S_OK;
+    R2S_DISPATCH(dtype, {
+        const S* var_q = detach_variance ? nullptr : static_cast<const S*>(uncertainties);
+        const auto* rec = static_cast<const Rec2D<S>*>(records);
+        const auto* rc = reinterpret_cast<const ushort4*>(rects);
+        return beta ? launch_record_bwd_b<S, true>(g, rec, rc, var_q, static_cast<const S*>(v_render),
+                                                   static_cast<const S*>(v_render_var), static_cast<Rec2D<S>*>(grads),
+                                                   static_cast<S*>(v_means2d_abs), static_cast<S*>(v_uncertainties),
+                                                   as_stream(stream))
+                    : launch_record_bwd_b<S, false>(g, rec, rc, var_q, static_cast<const S*>(v_render),
+                                                    static_cast<const S*>(v_render_var), static_cast<Rec2D<S>*>(grads),
+                                                    static_cast<S*>(v_means2d_abs), static_cast<S*>(v_uncertainties),
+                                                    as_stream(stream));
+    });
 }
 
 }  // extern "C"
