@@ -54,6 +54,9 @@ FLOPS_PER_EVAL = {
     # + conic adjoints 11 + density / mu adjoints 6 -> 44.
     "raster_render": 16, "raster_render_bwd": 44,
 }
+# DRAM bytes (read + write) of one record-parallel raster VJP launch at the CT
+# workload, from ncu (dram__bytes_read.sum + dram__bytes_write.sum, one pass).
+RASTER_VJP_TRAFFIC_BYTES = 569.04e6 + 374.12e6
 
 
 # --------------------------------------------------------------------------- utilities
@@ -484,13 +487,16 @@ def main(argv=None) -> int:
         achieved = FLOPS_PER_EVAL[kernel] * raster_evals / (kernel_ms * 1e-3) / 1e12 if kernel_ms else None
         peak = fp32_peak_tflops(device)
         result["roofline"] = {
-            "kernel": "raster_bwd_kernel (tile VJP)",
+            "kernel": "raster_record_bwd_kernel (record-parallel raster VJP)",
             "bound": "fp32",
+            "work": "algorithmic: 44 FP32 ops x the reference's tile samples of one raster VJP pass; the kernel "
+                    "itself evaluates only the samples inside each record's conservative box",
             "achieved": achieved,
             "peak": peak,
             "unit": "TFLOP/s",
             "frac": achieved / peak if achieved else None,
-            "traffic": None,
+            "traffic": RASTER_VJP_TRAFFIC_BYTES if args.workload == "ct" else None,
+            "traffic_unit": "bytes per launch (ncu)",
             "peak_source": "measured in-bench: FP32 FMA probe r2s_fp32_peak_probe (MEASURED_PEAKS.json has no "
                            "FP32 figure)",
             "hbm_peak_gbs_measured": peaks.get("hbm_gbs"),

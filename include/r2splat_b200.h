@@ -47,6 +47,30 @@ int r2s_fp32_peak_probe(float* out, uint32_t blocks, uint32_t threads, int iters
 /* Number of kernels this library has launched in the process so far. */
 uint64_t r2s_launch_count(void);
 
+/* ------------------------------------------------------- input value checks
+ * Batched form of the value checks of r2splat/_validation.py:35-48 (_tensor's
+ * finiteness), :63-86 (_primitives' ranges) and r2splat/explicit.py's camera
+ * checks: one launch evaluates up to 32 checks and sets bit `bit` of *flags
+ * (cleared first) for each check that fails on any element, so the caller
+ * reads one word instead of one host read per check. Elements are counted in
+ * units of the check: scalars for FINITE / POSITIVE / NONNEGATIVE, rows of 4
+ * for ZERO_ROW4, 3x3 matrices for FOCAL / PINHOLE, 4x4 for HOMOGENEOUS_ROW. */
+#define R2S_CHECK_FINITE 0          /* fails on a non-finite value */
+#define R2S_CHECK_ZERO_ROW4 1       /* fails on a row of four zeros (quaternion) */
+#define R2S_CHECK_POSITIVE 2        /* fails on a value <= 0 */
+#define R2S_CHECK_NONNEGATIVE 3     /* fails on a value < 0 */
+#define R2S_CHECK_FOCAL 4           /* fails on K[0][0] <= 0 or K[1][1] <= 0 */
+#define R2S_CHECK_PINHOLE 5         /* fails on nonzero skew or a last row other than [0, 0, 1] */
+#define R2S_CHECK_HOMOGENEOUS_ROW 6 /* fails on a last row other than [0, 0, 0, 1] */
+typedef struct {
+    const void* data;
+    uint64_t count;
+    uint32_t kind;
+    uint32_t bit;
+} r2s_value_check;
+int r2s_check_values(int dtype, const r2s_value_check* checks, uint32_t n_checks, uint32_t* flags,
+                     void* stream);
+
 /* ---------------------------------------------------------------- geometry */
 
 /* Ops.h:419-422 parameter_transform_fwd_tensor.

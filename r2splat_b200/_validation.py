@@ -5,11 +5,21 @@ Mirrors the error contract of the reference's ``r2splat/_validation.py``
 :51-54, ``_vector`` :57-60, ``_primitives`` :63-86, ``_options`` :89-96): the
 same exception types and messages are raised before any native call, because
 callers and tests match on them.
+
+The reference evaluates each value check (finiteness, ranges, camera
+structure) with its own device reduction and host read. Here, inside
+``deferred_value_checks()``, value checks are queued in the order they are
+made and evaluated together by one kernel (``r2s_check_values``) and one host
+read, when the block ends or when a host-side check raises; the first failing
+check in call order raises, so the error a caller sees is the reference's.
 """
 
 from __future__ import annotations
 
+import contextlib
+import ctypes
 import math
+import threading
 from numbers import Integral, Real
 from typing import Optional, Sequence, Union
 
@@ -17,6 +27,85 @@ import torch
 
 Tensor = torch.Tensor
 INT32_MAX = 2**31 - 1
+
+# Check kinds of r2s_check_values (include/r2splat_b200.h).
+FINITE, ZERO_ROW4, POSITIVE, NONNEGATIVE, FOCAL, PINHOLE, HOMOGENEOUS_ROW = range(7)
+_ELEMENT_SIZE = {FINITE: 1, ZERO_ROW4: 4, POSITIVE: 1, NONNEGATIVE: 1, FOCAL: 9, PINHOLE: 9, HOMOGENEOUS_ROW: 16}
+
+
+class _ValueCheck(ctypes.Structure):
+    _fields_ = [("data", ctypes.c_void_p), ("count", ctypes.c_uint64), ("kind", ctypes.c_uint32),
+                ("bit", ctypes.c_uint32)]
+
+
+class _ValueChecks:
+    """Value checks queued in call order: (tensor, kind, exception type, message)."""
+
+    def __init__(self):
+        self.items: list = []
+
+    def first_failure(self):
+        """Evaluates the queued checks; returns the first failing one's exception, or None."""
+        items, self.items = self.items, []
+        live = [(i, item) for i, item in enumerate(items) if item[0].numel() > 0]
+        failed: set = set()
+        groups: dict = {}
+        for index, item in live:
+            groups.setdefault((item[0].device, item[0].dtype), []).append((index, item))
+        from .cuda import _backend  # late import: the loader imports nothing from here
+
+        for (device, dtype), group in groups.items():
+            for start in range(0, len(group), 32):
+                chunk = group[start:start + 32]
+                table = (_ValueCheck * len(chunk))()
+                for bit, (_, (tensor, kind, _, _)) in enumerate(chunk):
+                    table[bit] = _ValueCheck(tensor.data_ptr(), tensor.numel() // _ELEMENT_SIZE[kind], kind, bit)
+                with torch.cuda.device(device):
+                    flags = torch.empty(1, dtype=torch.int32, device=device)
+                    _backend.call("r2s_check_values", 0 if dtype == torch.float32 else 1, table, len(chunk),
+                                  flags.data_ptr(), torch.cuda.current_stream(device).cuda_stream)
+                    word = int(flags.item())
+                failed.update(index for bit, (index, _) in enumerate(chunk) if word >> bit & 1)
+        for index, (_, _, exc_type, message) in enumerate(items):
+            if index in failed:
+                return exc_type(message)
+        return None
+
+
+_active = threading.local()
+
+
+@contextlib.contextmanager
+def deferred_value_checks():
+    """Queue the value checks made inside the block and evaluate them with one host read."""
+    checks = _ValueChecks()
+    previous = getattr(_active, "checks", None)
+    _active.checks = checks
+    try:
+        yield checks
+    except BaseException:
+        _active.checks = previous
+        earlier = checks.first_failure()  # checks made before the failing host-side check
+        if earlier is not None:
+            raise earlier from None
+        raise
+    _active.checks = previous
+    failure = checks.first_failure()
+    if failure is not None:
+        raise failure
+
+
+def _value_check(tensor: Tensor, kind: int, exc_type, message: str) -> None:
+    """Fails with exc_type(message) if the check fails on any element (queued inside deferred_value_checks)."""
+    checks = getattr(_active, "checks", None)
+    if checks is not None:
+        checks.items.append((tensor, kind, exc_type, message))
+        return
+    single = _ValueChecks()
+    single.items.append((tensor, kind, exc_type, message))
+    failure = single.first_failure()
+    if failure is not None:
+        raise failure
 
 
 def _shape(name: str, value: Sequence[int], rank: int) -> tuple[int, ...]:
@@ -52,9 +141,9 @@ def _tensor(name: str, value: Tensor, shape: tuple, reference: Optional[Tensor] 
         raise ValueError(f"{name} must be a CUDA tensor")
     if reference is not None and (value.device != reference.device or value.dtype != reference.dtype):
         raise ValueError(f"{name} must have the same device and dtype as means")
-    if not bool(torch.isfinite(value).all()):
-        raise ValueError(f"{name} must contain only finite values")
-    return value.contiguous()
+    value = value.contiguous()
+    _value_check(value, FINITE, ValueError, f"{name} must contain only finite values")
+    return value
 
 
 def _constant(name: str, value: Tensor) -> Tensor:
@@ -78,20 +167,15 @@ def _primitives(means, quats, scales, densities, beta, uncertainty):
     scales = _tensor("scales", scales, (n, 3), means)
     densities = _tensor("densities", densities, (n,), means)
     # Quaternions are normalised on the device; only all-zero rows are invalid.
-    if bool((quats == 0).all(dim=-1).any()):
-        raise ValueError("quats must have nonzero norm")
-    if bool((scales <= 0).any()):
-        raise ValueError("scales must be strictly positive physical lengths")
-    if bool((densities < 0).any()):
-        raise ValueError("densities must be nonnegative")
+    _value_check(quats, ZERO_ROW4, ValueError, "quats must have nonzero norm")
+    _value_check(scales, POSITIVE, ValueError, "scales must be strictly positive physical lengths")
+    _value_check(densities, NONNEGATIVE, ValueError, "densities must be nonnegative")
     if beta is not None:
         beta = _tensor("beta", beta, (n,), means)
-        if bool((beta <= 0).any()):
-            raise ValueError("beta must contain positive 3D exponents")
+        _value_check(beta, POSITIVE, ValueError, "beta must contain positive 3D exponents")
     if uncertainty is not None:
         uncertainty = _tensor("uncertainty", uncertainty, (n,), means)
-        if bool((uncertainty < 0).any()):
-            raise ValueError("uncertainty must be nonnegative relative variance")
+        _value_check(uncertainty, NONNEGATIVE, ValueError, "uncertainty must be nonnegative relative variance")
     return means, quats, scales, densities, beta, uncertainty
 
 

@@ -22,7 +22,8 @@ from typing import Optional, Sequence, Union
 import torch
 
 from . import _fused
-from ._validation import _constant, _options, _primitives, _shape, _tensor, _vector
+from ._validation import (FOCAL, HOMOGENEOUS_ROW, PINHOLE, POSITIVE, _constant, _options, _primitives, _shape,
+                          _tensor, _value_check, _vector, deferred_value_checks)
 
 Tensor = torch.Tensor
 Output = Union[Tensor, tuple[Tensor, Tensor]]
@@ -130,30 +131,28 @@ def rasterize_fwd(
         ("means", "quats", "scales", "densities", "viewmats", "Ks", "beta", "uncertainty"),
         (means, quats, scales, densities, viewmats, Ks, beta, uncertainty),
     ))
-    height, width = _shape("image_size", image_size, 2)
-    primitives = _primitives(means, quats, scales, densities, beta, uncertainty)
-    means, quats, scales, densities, beta, uncertainty = primitives
-    eps, radius_clip = _options(beta, eps, radius_clip, detach_variance)
-    mode = _mode(backward_mode)
-    # Check the originals: a contiguous copy under no_grad drops requires_grad.
-    for name, value in (("viewmats", viewmats), ("Ks", Ks)):
-        if isinstance(value, Tensor):
-            _constant(name, value)
-    viewmats = _constant("viewmats", _tensor("viewmats", viewmats, (None, 4, 4), means))
-    cameras = viewmats.shape[0]
-    if cameras == 0:
-        raise ValueError("viewmats must contain at least one camera")
-    if cameras * max(height * width, means.shape[0]) > 2**31 - 1 or cameras > 65535:
-        raise ValueError("camera batch exceeds CUDA indexing or grid limits")
-    if max(height, width) > 16 * 65535:
-        raise ValueError("image_size exceeds CUDA grid limits")
-    Ks = _constant("Ks", _tensor("Ks", Ks, (cameras, 3, 3), means))
-    if bool((Ks[:, (0, 1), (0, 1)] <= 0).any()):
-        raise ValueError("Ks must have positive fx and fy")
-    if bool((Ks[:, (0, 1, 2, 2), (1, 0, 0, 1)] != 0).any()) or bool((Ks[:, 2, 2] != 1).any()):
-        raise ValueError("Ks must be pinhole intrinsics with zero skew and last row [0, 0, 1]")
-    if not torch.equal(viewmats[:, 3], means.new_tensor([0, 0, 0, 1]).expand(cameras, -1)):
-        raise ValueError("viewmats must have homogeneous last row [0, 0, 0, 1]")
+    with deferred_value_checks():
+        height, width = _shape("image_size", image_size, 2)
+        primitives = _primitives(means, quats, scales, densities, beta, uncertainty)
+        means, quats, scales, densities, beta, uncertainty = primitives
+        eps, radius_clip = _options(beta, eps, radius_clip, detach_variance)
+        mode = _mode(backward_mode)
+        # Check the originals: a contiguous copy under no_grad drops requires_grad.
+        for name, value in (("viewmats", viewmats), ("Ks", Ks)):
+            if isinstance(value, Tensor):
+                _constant(name, value)
+        viewmats = _constant("viewmats", _tensor("viewmats", viewmats, (None, 4, 4), means))
+        cameras = viewmats.shape[0]
+        if cameras == 0:
+            raise ValueError("viewmats must contain at least one camera")
+        if cameras * max(height * width, means.shape[0]) > 2**31 - 1 or cameras > 65535:
+            raise ValueError("camera batch exceeds CUDA indexing or grid limits")
+        if max(height, width) > 16 * 65535:
+            raise ValueError("image_size exceeds CUDA grid limits")
+        Ks = _constant("Ks", _tensor("Ks", Ks, (cameras, 3, 3), means))
+        _value_check(Ks, FOCAL, ValueError, "Ks must have positive fx and fy")
+        _value_check(Ks, PINHOLE, ValueError, "Ks must be pinhole intrinsics with zero skew and last row [0, 0, 1]")
+        _value_check(viewmats, HOMOGENEOUS_ROW, ValueError, "viewmats must have homogeneous last row [0, 0, 0, 1]")
     shape = (cameras, height, width)
     buffers = {"viewmats": viewmats, "Ks": Ks}
     if means.shape[0] == 0:
@@ -181,8 +180,9 @@ def rasterize_bwd(context: _Context, v_image: Optional[Tensor], v_variance: Opti
     means, quats, scales, densities, beta, uncertainty = context.primitives
     if v_variance is not None and uncertainty is None:
         raise ValueError("v_variance requires uncertainty in the forward call")
-    v_image = _adjoint("v_image", v_image, context)
-    v_variance = _adjoint("v_variance", v_variance, context)
+    with deferred_value_checks():
+        v_image = _adjoint("v_image", v_image, context)
+        v_variance = _adjoint("v_variance", v_variance, context)
     if means.shape[0] == 0 or (v_image is None and v_variance is None):
         return _consume(context, _zero_gradients(context))
     b = context.buffers
@@ -219,20 +219,20 @@ def voxelize_fwd(
         ("means", "quats", "scales", "densities", "volume_extent", "volume_center", "beta", "uncertainty"),
         (means, quats, scales, densities, volume_extent, volume_center, beta, uncertainty),
     ))
-    depth, height, width = _shape("volume_shape", volume_shape, 3)
-    if max(height, width) > 8 * 65535:
-        raise ValueError("volume_shape exceeds CUDA grid limits")
-    primitives = _primitives(means, quats, scales, densities, beta, uncertainty)
-    means, quats, scales, densities, beta, uncertainty = primitives
-    eps, radius_clip = _options(beta, eps, radius_clip, detach_variance)
-    mode = _mode(backward_mode)
-    for name, value in (("volume_extent", volume_extent), ("volume_center", volume_center)):
-        if isinstance(value, Tensor):
-            _constant(name, value)
-    extent = _vector("volume_extent", volume_extent, means)
-    center = _vector("volume_center", volume_center, means)
-    if bool((extent <= 0).any()):
-        raise ValueError("volume_extent must contain positive physical lengths")
+    with deferred_value_checks():
+        depth, height, width = _shape("volume_shape", volume_shape, 3)
+        if max(height, width) > 8 * 65535:
+            raise ValueError("volume_shape exceeds CUDA grid limits")
+        primitives = _primitives(means, quats, scales, densities, beta, uncertainty)
+        means, quats, scales, densities, beta, uncertainty = primitives
+        eps, radius_clip = _options(beta, eps, radius_clip, detach_variance)
+        mode = _mode(backward_mode)
+        for name, value in (("volume_extent", volume_extent), ("volume_center", volume_center)):
+            if isinstance(value, Tensor):
+                _constant(name, value)
+        extent = _vector("volume_extent", volume_extent, means)
+        center = _vector("volume_center", volume_center, means)
+        _value_check(extent, POSITIVE, ValueError, "volume_extent must contain positive physical lengths")
     shape = (depth, height, width)
     buffers = {"extent": extent, "center": center}
     if means.shape[0] == 0:
@@ -256,8 +256,9 @@ def voxelize_bwd(context: _Context, v_volume: Optional[Tensor], v_variance: Opti
     means, quats, scales, densities, beta, uncertainty = context.primitives
     if v_variance is not None and uncertainty is None:
         raise ValueError("v_variance requires uncertainty in the forward call")
-    v_volume = _adjoint("v_volume", v_volume, context)
-    v_variance = _adjoint("v_variance", v_variance, context)
+    with deferred_value_checks():
+        v_volume = _adjoint("v_volume", v_volume, context)
+        v_variance = _adjoint("v_variance", v_variance, context)
     if means.shape[0] == 0 or (v_volume is None and v_variance is None):
         return _consume(context, _zero_gradients(context))
     b = context.buffers
