@@ -147,18 +147,28 @@ __global__ void __launch_bounds__(kSortThreads) radix_upsweep_kernel(const uint3
 
 // Stable scatter of one digit. Element order inside a block is (warp, item,
 // lane) = index order; ranks come from warp-wide matching of equal digits.
+// The block's elements are first placed in shared memory in digit order, then
+// written out in that order, so consecutive threads store consecutive
+// positions of one digit's run (coalesced) instead of scattering 4-byte stores.
+// Shared memory: [kSortWarps][bins] warp offsets, [bins] block-local digit
+// starts, [bins] global digit bases, then kSortTile staged keys and values.
 template <typename KeyOut, typename ValOut>
 __global__ void __launch_bounds__(kSortThreads) radix_downsweep_kernel(
     const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals, int64_t n, int shift, uint32_t mask,
     const uint32_t* __restrict__ offsets, KeyOut* __restrict__ keys_out, ValOut* __restrict__ vals_out) {
-    extern __shared__ uint32_t s_cnt[];  // [kSortWarps][bins]
+    extern __shared__ uint32_t s_cnt[];
     const uint32_t bins = mask + 1;
+    uint32_t* s_local = s_cnt + kSortWarps * bins;  // block-local start of each digit
+    uint32_t* s_global = s_local + bins;             // global position of each digit's first element
+    uint32_t* s_key = s_global + bins;               // [kSortTile]
+    uint32_t* s_val = s_key + kSortTile;             // [kSortTile]
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (uint32_t d = threadIdx.x; d < bins * kSortWarps; d += kSortThreads) s_cnt[d] = 0;
     __syncthreads();
     uint32_t* my_cnt = s_cnt + warp * bins;
     const uint32_t lt_mask = (1u << lane) - 1u;
-    const int64_t base = int64_t(blockIdx.x) * kSortTile + int64_t(warp) * (kSortTile / kSortWarps);
+    const int64_t block_base = int64_t(blockIdx.x) * kSortTile;
+    const int64_t base = block_base + int64_t(warp) * (kSortTile / kSortWarps);
     uint32_t k_key[kSortItems], k_val[kSortItems], k_rank[kSortItems];
 #pragma unroll
     for (int k = 0; k < kSortItems; ++k) {
@@ -178,13 +188,33 @@ __global__ void __launch_bounds__(kSortThreads) radix_downsweep_kernel(
         k_rank[k] = count + __popc(peers & lt_mask);
     }
     __syncthreads();
+    // Per digit: total over warps, and warp counts -> block-local warp offsets.
     for (uint32_t d = threadIdx.x; d < bins; d += kSortThreads) {
-        uint32_t running = offsets[size_t(d) * gridDim.x + blockIdx.x];
+        uint32_t running = 0;
 #pragma unroll
         for (int w = 0; w < kSortWarps; ++w) {
             const uint32_t c = s_cnt[w * bins + d];
             s_cnt[w * bins + d] = running;
             running += c;
+        }
+        s_local[d] = running;  // digit total for now
+        s_global[d] = offsets[size_t(d) * gridDim.x + blockIdx.x];
+    }
+    __syncthreads();
+    // Exclusive scan of the digit totals (one warp; at most 1024 digits).
+    if (warp == 0) {
+        uint32_t carry = 0;
+        for (uint32_t d0 = 0; d0 < bins; d0 += 32) {
+            const uint32_t d = d0 + lane;
+            const uint32_t v = d < bins ? s_local[d] : 0u;
+            uint32_t inc = v;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const uint32_t o = __shfl_up_sync(0xffffffffu, inc, off);
+                if (lane >= off) inc += o;
+            }
+            if (d < bins) s_local[d] = carry + inc - v;
+            carry += __shfl_sync(0xffffffffu, inc, 31);
         }
     }
     __syncthreads();
@@ -193,10 +223,20 @@ __global__ void __launch_bounds__(kSortThreads) radix_downsweep_kernel(
         const int64_t i = base + int64_t(k) * 32 + lane;
         if (i < n) {
             const uint32_t d = (k_key[k] >> shift) & mask;
-            const uint32_t pos = my_cnt[d] + k_rank[k];
-            keys_out[pos] = static_cast<KeyOut>(k_key[k]);
-            vals_out[pos] = static_cast<ValOut>(k_val[k]);
+            const uint32_t slot = s_local[d] + my_cnt[d] + k_rank[k];
+            s_key[slot] = k_key[k];
+            s_val[slot] = k_val[k];
         }
+    }
+    __syncthreads();
+    const int64_t remaining = n - block_base;
+    const uint32_t count = remaining < kSortTile ? uint32_t(remaining) : uint32_t(kSortTile);
+    for (uint32_t j = threadIdx.x; j < count; j += kSortThreads) {
+        const uint32_t key = s_key[j];
+        const uint32_t d = (key >> shift) & mask;
+        const uint32_t pos = s_global[d] + (j - s_local[d]);
+        keys_out[pos] = static_cast<KeyOut>(key);
+        vals_out[pos] = static_cast<ValOut>(s_val[j]);
     }
 }
 
@@ -276,7 +316,7 @@ inline int sort_and_finish(uint32_t* keys, uint32_t* vals, int64_t n, uint64_t n
             const size_t scan_bytes = arena.size - arena.used;
             R2S_REQUIRE(p.blocks < (int64_t(1) << 31), R2S_ERR_UNSUPPORTED, "too many intersections");
             const size_t up_smem = bins * sizeof(uint32_t);
-            const size_t down_smem = bins * kSortWarps * sizeof(uint32_t);
+            const size_t down_smem = (bins * (kSortWarps + 2) + 2 * size_t(kSortTile)) * sizeof(uint32_t);
             if (down_smem > 48 * 1024) {
                 cudaFuncSetAttribute(radix_downsweep_kernel<uint32_t, uint32_t>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, int(down_smem));
