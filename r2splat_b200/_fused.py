@@ -173,6 +173,37 @@ def raster_forward(means, quats, scales, densities, viewmats, Ks, width, height,
     return output, state
 
 
+def raster_vjp_state(means, quats, scales, densities, viewmats, Ks, width, height, beta, eps, radius_clip,
+                     tile_size=RASTER_TILE):
+    """What the raster VJP reads (covariances, packed records, tile rectangles), rebuilt without the image.
+
+    The record-parallel VJP needs neither the intersection lists nor their
+    order, so recomputation is the parameter transform and the projection only.
+    """
+    device = means.device
+    c, n = viewmats.shape[0], means.shape[0]
+    tx = (width + tile_size - 1) // tile_size
+    ty = (height + tile_size - 1) // tile_size
+    covars, _ = low.parameter_transform_fwd(quats, scales)
+    ratio = _beta.beta_path_ratio(beta) if beta is not None else None
+    records = means.new_empty((c, n, 8))
+    rects = torch.empty((c, n, 4), dtype=torch.int16, device=device)
+    counts = torch.empty((c, n), dtype=torch.int32, device=device)
+    _backend.call("r2s_raster_project", _dtype(means), _ptr(means), _ptr(covars), _ptr(densities), _ptr(beta),
+                  _ptr(ratio), _ptr(viewmats), _ptr(Ks), c, n, width, height, float(eps), float(eps),
+                  float(radius_clip), tile_size, tx, ty, _ptr(records), _ptr(rects), _ptr(counts), _stream(device))
+    return RasterState(covars, records, None, None, None, ratio, 0, width, height, tile_size, extra={"rects": rects})
+
+
+def voxel_vjp_state(means, quats, scales, densities, shape, extent, center, beta, uncertainty, eps, radius_clip,
+                    tile_size=VOXEL_TILE):
+    """What the voxel VJP reads (covariances, records, sorted tile lists), rebuilt without the volume."""
+    covars, _ = low.parameter_transform_fwd(quats, scales)
+    records, offsets, isect_ids, flatten_ids, m = voxel_intersections(
+        means, covars, densities, beta, uncertainty, extent, center, shape, eps, radius_clip, tile_size)
+    return VoxelState(covars, records, offsets, isect_ids, flatten_ids, m, tuple(shape), tile_size)
+
+
 def raster_backward(state: RasterState, means, quats, scales, densities, beta, uncertainty, viewmats, Ks, eps,
                     v_image, v_variance, detach_variance):
     """Explicit projection VJP -> (v_means, v_quats, v_scales, v_densities, v_beta, v_uncertainty)."""
