@@ -403,6 +403,55 @@ int r2s_voxel_chain_bwd(int dtype, const void* means, const void* quats, const v
                         const void* grads, void* v_means, void* v_quats, void* v_scales,
                         void* v_densities, void* v_betas, void* v_uncertainties, void* stream);
 
+/* ------------------------------------------- capacity-bounded (graph) mode
+ * No reference counterpart: variants of the fused pipeline whose intersection
+ * count stays on the device, so a whole fit step can be captured in a CUDA
+ * graph (no host read of the count). The lists live in buffers of a fixed
+ * `capacity`; *n_used receives the count (0 when it exceeds the capacity, in
+ * which case nothing is written past the capacity and *overflow gets bit 0
+ * set; the caller clears *overflow, grows the capacity and repeats the step).
+ * Workspace: r2s_isect_emit_workspace(capacity, n_keys). The render entries
+ * read the count from n_used. */
+int r2s_raster_emit_capacity(const uint16_t* rects, uint32_t C, uint32_t N, uint32_t tiles_x, uint32_t tiles_y,
+                             const int64_t* cum_tiles, int64_t capacity, int64_t* n_used, uint32_t* overflow,
+                             int64_t* isect_ids, int32_t* flatten_ids, int32_t* offsets, void* workspace,
+                             size_t workspace_bytes, void* stream);
+int r2s_voxel_emit_capacity(int dtype, const void* means3d, const int32_t* radii, uint32_t N, uint32_t tile_size,
+                            uint32_t tiles_x, uint32_t tiles_y, uint32_t tiles_z, const int64_t* cum_tiles,
+                            int64_t capacity, int64_t* n_used, uint32_t* overflow, int64_t* isect_ids,
+                            int32_t* flatten_ids, int32_t* offsets, void* workspace, size_t workspace_bytes,
+                            void* stream);
+/* stage_batch: records staged in shared memory per batch of the tile kernel
+ * (0 = the default 256; capped at the kernel's thread count). */
+int r2s_raster_render_capacity(int dtype, const void* records, const void* uncertainties, int beta,
+                               const int32_t* tile_offsets, const int32_t* flatten_ids, const int64_t* n_used,
+                               uint32_t C, uint32_t N, uint32_t width, uint32_t height, uint32_t tile_size,
+                               uint32_t tiles_x, uint32_t tiles_y, uint32_t stage_batch, void* render,
+                               void* render_var, void* stream);
+int r2s_voxel_render_capacity(int dtype, const void* records, int beta, const int32_t* tile_offsets,
+                              const int32_t* flatten_ids, const int64_t* n_used, uint32_t N, uint32_t dim2,
+                              uint32_t dim1, uint32_t dim0, uint32_t tile_size, uint32_t tiles_x, uint32_t tiles_y,
+                              uint32_t tiles_z, void* volume, void* volume_var, void* stream);
+int r2s_voxel_render_bwd_capacity(int dtype, const void* records, int beta, int detach_variance,
+                                  const int32_t* tile_offsets, const int32_t* flatten_ids, const int64_t* n_used,
+                                  const void* v_volume, const void* v_volume_var, uint32_t N, uint32_t dim2,
+                                  uint32_t dim1, uint32_t dim0, uint32_t tile_size, uint32_t tiles_x,
+                                  uint32_t tiles_y, uint32_t tiles_z, void* grads, void* stream);
+
+/* Fused fit-loop update, no reference counterpart (the reference's example
+ * loop, examples/optimize.py, does it with torch ops): sums two physical VJPs
+ * grads_a/grads_b (each an array of 5 pointers: means [N,3], quats [N,4],
+ * scales [N,3], densities [N], beta [N] or NULL; grads_b may be NULL),
+ * applies the activation derivatives of scales = exp(raw_scales), densities =
+ * softplus(raw_densities), beta = exp(raw_beta), takes one Adam step (torch's
+ * order of operations; moments [N,12]) on the raw parameters in place, writes
+ * the activated scales/densities/beta, and advances *step. A nonzero *skip
+ * makes the call a no-op. raw_beta and beta are both NULL without Beta. */
+int r2s_adam_activation_step(int dtype, uint32_t N, void* means, void* quats, void* raw_scales, void* raw_densities,
+                             void* raw_beta, void* scales, void* densities, void* beta, void* adam_m, void* adam_v,
+                             const void* const* grads_a, const void* const* grads_b, double lr, double beta1,
+                             double beta2, double eps, int32_t* step, const uint32_t* skip, void* stream);
+
 /* ------------------------------------------------ allocation-free variant
  * No reference counterpart. r2s_scan_tile_counts without a workspace argument:
  * the scan's scratch is a static per-device array of the library (72 KiB),

@@ -86,15 +86,18 @@ __global__ void emit_2d_kernel(const S* __restrict__ means2d, const int32_t* __r
         }
 }
 
+// Writes element i's intersections at [cum[i-1], cum[i]); positions at or past
+// `capacity` are not written (the caller flags that case as an overflow).
 __global__ void emit_rects_kernel(const ushort4* __restrict__ rects, uint32_t total, uint32_t N, uint32_t tiles_x,
-                                  uint32_t tiles_y, const int64_t* __restrict__ cum, uint32_t* __restrict__ keys,
-                                  uint32_t* __restrict__ vals) {
+                                  uint32_t tiles_y, const int64_t* __restrict__ cum, int64_t capacity,
+                                  uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= total) return;
     const ushort4 r = rects[i];
     if (r.z <= r.x || r.w <= r.y) return;
     const uint32_t base_key = (i / N) * (tiles_x * tiles_y);
     int64_t w = i == 0 ? 0 : cum[i - 1];
+    if (cum[i] > capacity) return;
     for (uint32_t y = r.y; y < r.w; ++y)
         for (uint32_t x = r.x; x < r.z; ++x, ++w) {
             keys[w] = base_key + y * tiles_x + x;
@@ -105,13 +108,14 @@ __global__ void emit_rects_kernel(const ushort4* __restrict__ rects, uint32_t to
 template <typename S>
 __global__ void emit_3d_kernel(const S* __restrict__ means3d, const int32_t* __restrict__ radii, uint32_t N,
                                uint32_t tile_size, uint32_t tx, uint32_t ty, uint32_t tz,
-                               const int64_t* __restrict__ cum, uint32_t* __restrict__ keys,
+                               const int64_t* __restrict__ cum, int64_t capacity, uint32_t* __restrict__ keys,
                                uint32_t* __restrict__ vals) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
     uint32_t lo[3], hi[3];
     if (!rect_3d(means3d, radii, i, tile_size, tx, ty, tz, lo, hi)) return;
     int64_t w = i == 0 ? 0 : cum[i - 1];
+    if (cum[i] > capacity) return;
     for (uint32_t z = lo[2]; z < hi[2]; ++z)
         for (uint32_t y = lo[1]; y < hi[1]; ++y)
             for (uint32_t x = lo[0]; x < hi[0]; ++x, ++w) {
@@ -129,10 +133,13 @@ constexpr int64_t kSortTile = int64_t(kSortThreads) * kSortItems;
 constexpr int kMaxDigitBits = 10;
 
 // Per-block digit histogram, stored digit-major: hist[d * n_blocks + b].
+// With n_dev non-null the element count is *n_dev (at most n, the capacity the
+// grid was sized for); blocks past it contribute empty histograms.
 __global__ void __launch_bounds__(kSortThreads) radix_upsweep_kernel(const uint32_t* __restrict__ keys, int64_t n,
-                                                                    int shift, uint32_t mask,
-                                                                    uint32_t* __restrict__ hist) {
+                                                                    const int64_t* __restrict__ n_dev, int shift,
+                                                                    uint32_t mask, uint32_t* __restrict__ hist) {
     extern __shared__ uint32_t s_hist[];
+    if (n_dev != nullptr && *n_dev < n) n = *n_dev;
     const uint32_t bins = mask + 1;
     for (uint32_t d = threadIdx.x; d < bins; d += kSortThreads) s_hist[d] = 0;
     __syncthreads();
@@ -154,9 +161,12 @@ __global__ void __launch_bounds__(kSortThreads) radix_upsweep_kernel(const uint3
 // starts, [bins] global digit bases, then kSortTile staged keys and values.
 template <typename KeyOut, typename ValOut>
 __global__ void __launch_bounds__(kSortThreads) radix_downsweep_kernel(
-    const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals, int64_t n, int shift, uint32_t mask,
-    const uint32_t* __restrict__ offsets, KeyOut* __restrict__ keys_out, ValOut* __restrict__ vals_out) {
+    const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals, int64_t n, const int64_t* __restrict__ n_dev,
+    int shift, uint32_t mask, const uint32_t* __restrict__ offsets, KeyOut* __restrict__ keys_out,
+    ValOut* __restrict__ vals_out) {
     extern __shared__ uint32_t s_cnt[];
+    if (n_dev != nullptr && *n_dev < n) n = *n_dev;
+    if (int64_t(blockIdx.x) * kSortTile >= n) return;  // the whole block is past the count
     const uint32_t bins = mask + 1;
     uint32_t* s_local = s_cnt + kSortWarps * bins;  // block-local start of each digit
     uint32_t* s_global = s_local + bins;             // global position of each digit's first element
@@ -241,24 +251,41 @@ __global__ void __launch_bounds__(kSortThreads) radix_downsweep_kernel(
 }
 
 __global__ void widen_kernel(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals, int64_t n,
-                             int64_t* __restrict__ keys_out, int32_t* __restrict__ vals_out) {
+                             const int64_t* __restrict__ n_dev, int64_t* __restrict__ keys_out,
+                             int32_t* __restrict__ vals_out) {
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (n_dev != nullptr && *n_dev < n) n = *n_dev;
     if (i >= n) return;
     keys_out[i] = keys[i];
     vals_out[i] = static_cast<int32_t>(vals[i]);
 }
 
 // offsets[k] = number of sorted keys smaller than k (lower bound).
-__global__ void offsets_kernel(const int64_t* __restrict__ keys, int64_t n, int64_t n_keys,
-                               int32_t* __restrict__ offsets) {
+__global__ void offsets_kernel(const int64_t* __restrict__ keys, int64_t n, const int64_t* __restrict__ n_dev,
+                               int64_t n_keys, int32_t* __restrict__ offsets) {
     const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (k >= n_keys) return;
+    if (n_dev != nullptr && *n_dev < n) n = *n_dev;
     int64_t lo = 0, hi = n;
     while (lo < hi) {
         const int64_t mid = (lo + hi) >> 1;
         if (keys[mid] < k) lo = mid + 1; else hi = mid;
     }
     offsets[k] = static_cast<int32_t>(lo);
+}
+
+// Device-side intersection count for capacity-bounded (graph-capturable)
+// pipelines: n_used = total when it fits the capacity, else 0 with the
+// overflow flag raised (the emission wrote nothing past the capacity).
+__global__ void count_finish_kernel(const int64_t* __restrict__ cum, int64_t last, int64_t capacity,
+                                    int64_t* __restrict__ n_used, uint32_t* __restrict__ overflow) {
+    const int64_t total = last >= 0 ? cum[last] : 0;
+    if (total > capacity) {
+        *n_used = 0;
+        atomicOr(overflow, 1u);
+    } else {
+        *n_used = total;
+    }
 }
 
 inline int bits_for(uint64_t max_key) {
@@ -300,11 +327,12 @@ inline size_t emit_workspace(int64_t n, uint64_t n_keys) {
 // Sorts (keys, vals) of length n by key bits [0, bits(n_keys-1)), writing
 // the widened result to isect_ids/flatten_ids, then fills offsets.
 inline int sort_and_finish(uint32_t* keys, uint32_t* vals, int64_t n, uint64_t n_keys, Arena& arena,
-                           int64_t* isect_ids, int32_t* flatten_ids, int32_t* offsets, cudaStream_t stream) {
+                           int64_t* isect_ids, int32_t* flatten_ids, int32_t* offsets, cudaStream_t stream,
+                           const int64_t* n_dev = nullptr) {
     const SortPlan p = plan_sort(n, n_keys);
     if (n > 0) {
         if (p.passes == 0) {
-            widen_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(keys, vals, n, isect_ids, flatten_ids);
+            widen_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(keys, vals, n, n_dev, isect_ids, flatten_ids);
             R2S_TRY(check_launch("widen"));
         } else {
             uint32_t* keys_b = arena.take<uint32_t>(size_t(n));
@@ -327,17 +355,17 @@ inline int sort_and_finish(uint32_t* keys, uint32_t* vals, int64_t n, uint64_t n
             for (int pass = 0; pass < p.passes; ++pass) {
                 const int shift = pass * p.digit_bits;
                 const uint32_t mask = bins - 1;
-                radix_upsweep_kernel<<<unsigned(p.blocks), kSortThreads, up_smem, stream>>>(src_k, n, shift, mask,
-                                                                                           hist);
+                radix_upsweep_kernel<<<unsigned(p.blocks), kSortThreads, up_smem, stream>>>(src_k, n, n_dev, shift,
+                                                                                           mask, hist);
                 R2S_TRY(check_launch("radix_upsweep"));
                 R2S_TRY((device_scan<uint32_t, uint32_t, false>(hist, hist, int64_t(bins) * p.blocks, scan_ws,
                                                                 scan_bytes, stream)));
                 if (pass == p.passes - 1) {
                     radix_downsweep_kernel<int64_t, int32_t><<<unsigned(p.blocks), kSortThreads, down_smem, stream>>>(
-                        src_k, src_v, n, shift, mask, hist, isect_ids, flatten_ids);
+                        src_k, src_v, n, n_dev, shift, mask, hist, isect_ids, flatten_ids);
                 } else {
                     radix_downsweep_kernel<uint32_t, uint32_t><<<unsigned(p.blocks), kSortThreads, down_smem,
-                                                                 stream>>>(src_k, src_v, n, shift, mask, hist,
+                                                                 stream>>>(src_k, src_v, n, n_dev, shift, mask, hist,
                                                                            dst_k, dst_v);
                 }
                 R2S_TRY(check_launch("radix_downsweep"));
@@ -347,7 +375,8 @@ inline int sort_and_finish(uint32_t* keys, uint32_t* vals, int64_t n, uint64_t n
         }
     }
     if (offsets != nullptr && n_keys > 0) {
-        offsets_kernel<<<blocks_for(int64_t(n_keys), 256), 256, 0, stream>>>(isect_ids, n, int64_t(n_keys), offsets);
+        offsets_kernel<<<blocks_for(int64_t(n_keys), 256), 256, 0, stream>>>(isect_ids, n, n_dev, int64_t(n_keys),
+                                                                            offsets);
         R2S_TRY(check_launch("isect_offsets"));
     }
     return R2S_OK;
@@ -425,7 +454,8 @@ int r2s_raster_emit(const uint16_t* rects, uint32_t C, uint32_t N, uint32_t tile
         uint32_t* vals = arena.take<uint32_t>(size_t(n_isects));
         R2S_REQUIRE(keys && vals, R2S_ERR_WORKSPACE, "intersection workspace too small");
         emit_rects_kernel<<<blocks_for(total, kIsectThreads), kIsectThreads, 0, as_stream(stream)>>>(
-            reinterpret_cast<const ushort4*>(rects), uint32_t(total), N, tiles_x, tiles_y, cum_tiles, keys, vals);
+            reinterpret_cast<const ushort4*>(rects), uint32_t(total), N, tiles_x, tiles_y, cum_tiles, INT64_MAX, keys,
+            vals);
         R2S_TRY(check_launch("raster_emit"));
         return sort_and_finish(keys, vals, n_isects, n_keys, arena, isect_ids, flatten_ids, offsets,
                                as_stream(stream));
@@ -437,7 +467,8 @@ int r2s_isect_offset_encode(const int64_t* isect_ids, int64_t n_isects, uint32_t
                             uint32_t tiles_y, int32_t* offsets, void* stream) {
     const int64_t n_keys = int64_t(C) * tiles_x * tiles_y;
     if (n_keys == 0) return R2S_OK;
-    offsets_kernel<<<blocks_for(n_keys, 256), 256, 0, as_stream(stream)>>>(isect_ids, n_isects, n_keys, offsets);
+    offsets_kernel<<<blocks_for(n_keys, 256), 256, 0, as_stream(stream)>>>(isect_ids, n_isects, nullptr, n_keys,
+                                                                            offsets);
     return check_launch("isect_offset_encode");
 }
 
@@ -467,7 +498,8 @@ int r2s_isect_tiles_3d_emit(int dtype, const void* means3d, const int32_t* radii
         uint32_t* vals = arena.take<uint32_t>(size_t(n_isects));
         R2S_REQUIRE(keys && vals, R2S_ERR_WORKSPACE, "intersection workspace too small");
         R2S_DISPATCH(dtype, emit_3d_kernel<S><<<blocks_for(N, kIsectThreads), kIsectThreads, 0, as_stream(stream)>>>(
-            static_cast<const S*>(means3d), radii, N, tile_size, tiles_x, tiles_y, tiles_z, cum_tiles, keys, vals));
+            static_cast<const S*>(means3d), radii, N, tile_size, tiles_x, tiles_y, tiles_z, cum_tiles, INT64_MAX, keys,
+            vals));
         R2S_TRY(check_launch("isect_emit_3d"));
         return sort_and_finish(keys, vals, n_isects, n_keys, arena, isect_ids, flatten_ids, offsets,
                                as_stream(stream));
@@ -479,8 +511,61 @@ int r2s_isect_offset_encode_3d(const int64_t* isect_ids, int64_t n_isects, uint3
                                uint32_t tiles_z, int32_t* offsets, void* stream) {
     const int64_t n_keys = int64_t(tiles_x) * tiles_y * tiles_z;
     if (n_keys == 0) return R2S_OK;
-    offsets_kernel<<<blocks_for(n_keys, 256), 256, 0, as_stream(stream)>>>(isect_ids, n_isects, n_keys, offsets);
+    offsets_kernel<<<blocks_for(n_keys, 256), 256, 0, as_stream(stream)>>>(isect_ids, n_isects, nullptr, n_keys,
+                                                                            offsets);
     return check_launch("isect_offset_encode_3d");
+}
+
+int r2s_raster_emit_capacity(const uint16_t* rects, uint32_t C, uint32_t N, uint32_t tiles_x, uint32_t tiles_y,
+                             const int64_t* cum_tiles, int64_t capacity, int64_t* n_used, uint32_t* overflow,
+                             int64_t* isect_ids, int32_t* flatten_ids, int32_t* offsets, void* workspace,
+                             size_t workspace_bytes, void* stream) {
+    const uint64_t total = uint64_t(C) * N;
+    const uint64_t n_keys = uint64_t(C) * tiles_x * tiles_y;
+    R2S_REQUIRE(n_keys < (uint64_t(1) << 32), R2S_ERR_UNSUPPORTED, "C*tiles exceeds the 32-bit key range");
+    R2S_REQUIRE(capacity >= 1 && capacity < (int64_t(1) << 31), R2S_ERR_UNSUPPORTED,
+                "capacity must be in [1, 2^31)");
+    R2S_REQUIRE(n_used != nullptr && overflow != nullptr, R2S_ERR_ARGUMENT, "n_used and overflow must be non-null");
+    cudaStream_t st = as_stream(stream);
+    count_finish_kernel<<<1, 1, 0, st>>>(cum_tiles, int64_t(total) - 1, capacity, n_used, overflow);
+    R2S_TRY(check_launch("count_finish"));
+    Arena arena(workspace, workspace_bytes);
+    uint32_t* keys = arena.take<uint32_t>(size_t(capacity));
+    uint32_t* vals = arena.take<uint32_t>(size_t(capacity));
+    R2S_REQUIRE(keys && vals, R2S_ERR_WORKSPACE, "intersection workspace too small");
+    if (total > 0) {
+        emit_rects_kernel<<<blocks_for(total, kIsectThreads), kIsectThreads, 0, st>>>(
+            reinterpret_cast<const ushort4*>(rects), uint32_t(total), N, tiles_x, tiles_y, cum_tiles, capacity, keys,
+            vals);
+        R2S_TRY(check_launch("raster_emit"));
+    }
+    return sort_and_finish(keys, vals, capacity, n_keys, arena, isect_ids, flatten_ids, offsets, st, n_used);
+}
+
+int r2s_voxel_emit_capacity(int dtype, const void* means3d, const int32_t* radii, uint32_t N, uint32_t tile_size,
+                            uint32_t tiles_x, uint32_t tiles_y, uint32_t tiles_z, const int64_t* cum_tiles,
+                            int64_t capacity, int64_t* n_used, uint32_t* overflow, int64_t* isect_ids,
+                            int32_t* flatten_ids, int32_t* offsets, void* workspace, size_t workspace_bytes,
+                            void* stream) {
+    const uint64_t n_keys = uint64_t(tiles_x) * tiles_y * tiles_z;
+    R2S_REQUIRE(n_keys < (uint64_t(1) << 32), R2S_ERR_UNSUPPORTED, "tile count exceeds the 32-bit key range");
+    R2S_REQUIRE(capacity >= 1 && capacity < (int64_t(1) << 31), R2S_ERR_UNSUPPORTED,
+                "capacity must be in [1, 2^31)");
+    R2S_REQUIRE(n_used != nullptr && overflow != nullptr, R2S_ERR_ARGUMENT, "n_used and overflow must be non-null");
+    cudaStream_t st = as_stream(stream);
+    count_finish_kernel<<<1, 1, 0, st>>>(cum_tiles, int64_t(N) - 1, capacity, n_used, overflow);
+    R2S_TRY(check_launch("count_finish"));
+    Arena arena(workspace, workspace_bytes);
+    uint32_t* keys = arena.take<uint32_t>(size_t(capacity));
+    uint32_t* vals = arena.take<uint32_t>(size_t(capacity));
+    R2S_REQUIRE(keys && vals, R2S_ERR_WORKSPACE, "intersection workspace too small");
+    if (N > 0) {
+        R2S_DISPATCH(dtype, emit_3d_kernel<S><<<blocks_for(N, kIsectThreads), kIsectThreads, 0, st>>>(
+            static_cast<const S*>(means3d), radii, N, tile_size, tiles_x, tiles_y, tiles_z, cum_tiles, capacity, keys,
+            vals));
+        R2S_TRY(check_launch("isect_emit_3d"));
+    }
+    return sort_and_finish(keys, vals, capacity, n_keys, arena, isect_ids, flatten_ids, offsets, st, n_used);
 }
 
 }  // extern "C"

@@ -136,10 +136,10 @@ template <typename S, bool kBeta, bool kVar, int kMaxThreads>
 __global__ void __launch_bounds__(kMaxThreads) raster_fwd_kernel(
     const Rec2D<S>* __restrict__ records, const S* __restrict__ uncertainties, uint32_t N,
     const int32_t* __restrict__ offsets, const int32_t* __restrict__ flatten_ids, int32_t n_isects,
+    const int64_t* __restrict__ n_dev,
     uint32_t C, uint32_t width, uint32_t height, uint32_t T, uint32_t tiles_x, uint32_t n_tiles,
-    S* __restrict__ render, S* __restrict__ render_var) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    const uint32_t B = blockDim.x < kFwdBatch ? blockDim.x : kFwdBatch;
+    S* __restrict__ render, S* __restrict__ render_var, uint32_t B) {
+    extern __shared__ __align__(16) unsigned char smem[];  // B = records staged per batch (<= blockDim.x)
     Rec2D<S>* s_rec = reinterpret_cast<Rec2D<S>*>(smem);          // [2][B]
     S* s_q = reinterpret_cast<S*>(s_rec + 2 * B);                   // [2][B]
     uint2* s_mask = reinterpret_cast<uint2*>(s_q + 2 * B);          // [B] (column, row) masks
@@ -151,7 +151,9 @@ __global__ void __launch_bounds__(kMaxThreads) raster_fwd_kernel(
     if (ox >= width || oy >= height) return;
     const uint32_t vx = min(T, width - ox), vy = min(T, height - oy);
     const int32_t start = offsets[key];
-    const int32_t end = (key + 1 == C * n_tiles) ? n_isects : offsets[key + 1];
+    // n_dev: the intersection count kept on the device (capacity-bounded pipelines).
+    const int32_t n_total = n_dev != nullptr ? int32_t(*n_dev) : n_isects;
+    const int32_t end = (key + 1 == C * n_tiles) ? n_total : offsets[key + 1];
     const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
 
     const uint32_t blocks_x = (T + kBlockW - 1) / kBlockW;
@@ -360,6 +362,7 @@ template <typename S, bool kBeta, bool kVar, bool kAbs>
 __global__ void __launch_bounds__(kBwdThreads) raster_bwd_kernel(
     const Rec2D<S>* __restrict__ records, const S* __restrict__ var_q, uint32_t N,
     const int32_t* __restrict__ offsets, const int32_t* __restrict__ flatten_ids, int32_t n_isects,
+    const int64_t* __restrict__ n_dev,
     uint32_t C, uint32_t width, uint32_t height, uint32_t T, uint32_t tiles_x, uint32_t n_tiles,
     const S* __restrict__ v_render, const S* __restrict__ v_render_var, Rec2D<S>* __restrict__ grads,
     S* __restrict__ v_abs, S* __restrict__ v_unc) {
@@ -378,7 +381,9 @@ __global__ void __launch_bounds__(kBwdThreads) raster_bwd_kernel(
     if (ox >= width || oy >= height) return;
     const uint32_t vx = min(T, width - ox), vy = min(T, height - oy);
     const int32_t start = offsets[key];
-    const int32_t end = (key + 1 == C * n_tiles) ? n_isects : offsets[key + 1];
+    // n_dev: the intersection count kept on the device (capacity-bounded pipelines).
+    const int32_t n_total = n_dev != nullptr ? int32_t(*n_dev) : n_isects;
+    const int32_t end = (key + 1 == C * n_tiles) ? n_total : offsets[key + 1];
     const int32_t count = end - start;
     if (count <= 0) return;
     const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
@@ -674,6 +679,8 @@ __global__ void unpack_grads_kernel(const Rec2D<S>* __restrict__ grads, size_t t
 
 struct RasterGeom {
     uint32_t C, N, n_isects, width, height, T, tiles_x, tiles_y;
+    const int64_t* n_dev = nullptr;  // device-side intersection count, overrides n_isects
+    uint32_t stage_batch = kFwdBatch;  // forward: records staged in shared memory per batch
 };
 
 inline int check_geom(const RasterGeom& g) {
@@ -691,20 +698,22 @@ int launch_fwd_p(const RasterGeom& g, const Rec2D<S>* rec, const S* unc, const i
     // One warp per 8x4 block of the tile: at most 4 x 8 warps for 32x32 tiles.
     const uint32_t blocks = ((g.T + kBlockW - 1) / kBlockW) * ((g.T + kBlockH - 1) / kBlockH);
     const unsigned nthreads = 32u * blocks;
-    const unsigned batch = nthreads < kFwdBatch ? nthreads : kFwdBatch;
+    unsigned batch = g.stage_batch < kFwdBatch ? g.stage_batch : kFwdBatch;
+    if (batch > nthreads) batch = nthreads;
+    if (batch < 1) batch = 1;
     const size_t smem = 2 * size_t(batch) * (sizeof(Rec2D<S>) + sizeof(S)) + size_t(batch) * sizeof(uint2);
     dim3 grid(g.tiles_x * g.tiles_y, g.C);
     if (nthreads <= 256) {
         // Tiles up to 16x16: a register budget sized for 256-thread CTAs.
         R2S_TRY(allow_dynamic_smem(raster_fwd_kernel<S, kBeta, kVar, 256>, smem));
         raster_fwd_kernel<S, kBeta, kVar, 256><<<grid, nthreads, smem, stream>>>(
-            rec, unc, g.N, offsets, ids, int32_t(g.n_isects), g.C, g.width, g.height, g.T, g.tiles_x,
-            g.tiles_x * g.tiles_y, out, out_var);
+            rec, unc, g.N, offsets, ids, int32_t(g.n_isects), g.n_dev, g.C, g.width, g.height, g.T, g.tiles_x,
+            g.tiles_x * g.tiles_y, out, out_var, batch);
     } else {
         R2S_TRY(allow_dynamic_smem(raster_fwd_kernel<S, kBeta, kVar, 1024>, smem));
         raster_fwd_kernel<S, kBeta, kVar, 1024><<<grid, nthreads, smem, stream>>>(
-            rec, unc, g.N, offsets, ids, int32_t(g.n_isects), g.C, g.width, g.height, g.T, g.tiles_x,
-            g.tiles_x * g.tiles_y, out, out_var);
+            rec, unc, g.N, offsets, ids, int32_t(g.n_isects), g.n_dev, g.C, g.width, g.height, g.T, g.tiles_x,
+            g.tiles_x * g.tiles_y, out, out_var, batch);
     }
     return check_launch("rasterize_to_pixels_fwd");
 }
@@ -732,7 +741,7 @@ int launch_bwd_p(const RasterGeom& g, const Rec2D<S>* rec, const S* var_q, const
     R2S_TRY(allow_dynamic_smem(raster_bwd_kernel<S, kBeta, kVar, kAbs>, smem));
     dim3 grid(g.tiles_x * g.tiles_y, g.C);
     raster_bwd_kernel<S, kBeta, kVar, kAbs><<<grid, kBwdThreads, smem, stream>>>(
-        rec, var_q, g.N, offsets, ids, int32_t(g.n_isects), g.C, g.width, g.height, g.T, g.tiles_x,
+        rec, var_q, g.N, offsets, ids, int32_t(g.n_isects), g.n_dev, g.C, g.width, g.height, g.T, g.tiles_x,
         g.tiles_x * g.tiles_y, v_render, v_render_var, grads, v_abs, v_unc);
     return check_launch("rasterize_to_pixels_bwd");
 }
@@ -998,6 +1007,21 @@ int r2s_raster_record_bwd(int dtype, const void* records, const uint16_t* rects,
                                                     static_cast<S*>(v_means2d_abs), static_cast<S*>(v_uncertainties),
                                                     as_stream(stream));
     });
+}
+
+int r2s_raster_render_capacity(int dtype, const void* records, const void* uncertainties, int beta,
+                               const int32_t* tile_offsets, const int32_t* flatten_ids, const int64_t* n_used,
+                               uint32_t C, uint32_t N, uint32_t width, uint32_t height, uint32_t tile_size,
+                               uint32_t tiles_x, uint32_t tiles_y, uint32_t stage_batch, void* render,
+                               void* render_var, void* stream) {
+    R2S_REQUIRE(n_used != nullptr, R2S_ERR_ARGUMENT, "n_used must be non-null");
+    RasterGeom g{C, N, 1u, width, height, tile_size, tiles_x, tiles_y};
+    g.n_dev = n_used;
+    if (stage_batch != 0) g.stage_batch = stage_batch;
+    R2S_DISPATCH(dtype, return launch_fwd<S>(g, static_cast<const Rec2D<S>*>(records),
+                                             static_cast<const S*>(uncertainties), beta != 0, tile_offsets,
+                                             flatten_ids, static_cast<S*>(render), static_cast<S*>(render_var),
+                                             as_stream(stream)));
 }
 
 }  // extern "C"

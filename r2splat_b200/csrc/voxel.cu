@@ -39,6 +39,7 @@ __device__ __forceinline__ void gather_record3(Rec3D<S>* dst, const Rec3D<S>* sr
 
 struct VoxelGeom {
     uint32_t N, n_isects, dim2, dim1, dim0, T, tiles_x, tiles_y, tiles_z;
+    const int64_t* n_dev = nullptr;  // device-side intersection count, overrides n_isects
 };
 
 template <typename S, bool kBeta, bool kVar, int PPT>
@@ -53,7 +54,8 @@ __global__ void __launch_bounds__(256) voxel_fwd_kernel(const Rec3D<S>* __restri
     const uint32_t n_tiles = g.tiles_x * g.tiles_y * g.tiles_z;
     const uint32_t key = blockIdx.x;
     const int32_t start = offsets[key];
-    const int32_t end = (key + 1 == n_tiles) ? int32_t(g.n_isects) : offsets[key + 1];
+    const int32_t n_total = g.n_dev != nullptr ? int32_t(*g.n_dev) : int32_t(g.n_isects);
+    const int32_t end = (key + 1 == n_tiles) ? n_total : offsets[key + 1];
     const uint32_t tz = key / (g.tiles_x * g.tiles_y);
     const uint32_t rem = key - tz * g.tiles_x * g.tiles_y;
     const uint32_t ty = rem / g.tiles_x, tx = rem - ty * g.tiles_x;
@@ -247,7 +249,8 @@ __global__ void __launch_bounds__(kVoxBwdThreads) voxel_bwd_kernel(
     if (ox >= g.dim2 || oy >= g.dim1 || oz >= g.dim0) return;
     const uint32_t vx = min(T, g.dim2 - ox), vy = min(T, g.dim1 - oy), vz = min(T, g.dim0 - oz);
     const int32_t start = offsets[key];
-    const int32_t end = (key + 1 == n_tiles) ? int32_t(g.n_isects) : offsets[key + 1];
+    const int32_t n_total = g.n_dev != nullptr ? int32_t(*g.n_dev) : int32_t(g.n_isects);
+    const int32_t end = (key + 1 == n_tiles) ? n_total : offsets[key + 1];
     const int32_t count = end - start;
     if (count <= 0) return;
     const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
@@ -654,6 +657,32 @@ int r2s_voxel_render_bwd(int dtype, const void* records, int beta, int detach_va
                          uint32_t n_isects, uint32_t dim2, uint32_t dim1, uint32_t dim0, uint32_t tile_size,
                          uint32_t tiles_x, uint32_t tiles_y, uint32_t tiles_z, void* grads, void* stream) {
     const VoxelGeom g{N, n_isects, dim2, dim1, dim0, tile_size, tiles_x, tiles_y, tiles_z};
+    R2S_DISPATCH(dtype, return launch_vbwd<S>(g, static_cast<const Rec3D<S>*>(records), beta != 0,
+                                              detach_variance == 0, tile_offsets, flatten_ids,
+                                              static_cast<const S*>(v_volume), static_cast<const S*>(v_volume_var),
+                                              static_cast<Rec3D<S>*>(grads), as_stream(stream)));
+}
+
+int r2s_voxel_render_capacity(int dtype, const void* records, int beta, const int32_t* tile_offsets,
+                              const int32_t* flatten_ids, const int64_t* n_used, uint32_t N, uint32_t dim2,
+                              uint32_t dim1, uint32_t dim0, uint32_t tile_size, uint32_t tiles_x, uint32_t tiles_y,
+                              uint32_t tiles_z, void* volume, void* volume_var, void* stream) {
+    R2S_REQUIRE(n_used != nullptr, R2S_ERR_ARGUMENT, "n_used must be non-null");
+    VoxelGeom g{N, 1u, dim2, dim1, dim0, tile_size, tiles_x, tiles_y, tiles_z};
+    g.n_dev = n_used;
+    R2S_DISPATCH(dtype, return launch_vfwd<S>(g, static_cast<const Rec3D<S>*>(records), beta != 0, tile_offsets,
+                                              flatten_ids, static_cast<S*>(volume), static_cast<S*>(volume_var),
+                                              as_stream(stream)));
+}
+
+int r2s_voxel_render_bwd_capacity(int dtype, const void* records, int beta, int detach_variance,
+                                  const int32_t* tile_offsets, const int32_t* flatten_ids, const int64_t* n_used,
+                                  const void* v_volume, const void* v_volume_var, uint32_t N, uint32_t dim2,
+                                  uint32_t dim1, uint32_t dim0, uint32_t tile_size, uint32_t tiles_x,
+                                  uint32_t tiles_y, uint32_t tiles_z, void* grads, void* stream) {
+    R2S_REQUIRE(n_used != nullptr, R2S_ERR_ARGUMENT, "n_used must be non-null");
+    VoxelGeom g{N, 1u, dim2, dim1, dim0, tile_size, tiles_x, tiles_y, tiles_z};
+    g.n_dev = n_used;
     R2S_DISPATCH(dtype, return launch_vbwd<S>(g, static_cast<const Rec3D<S>*>(records), beta != 0,
                                               detach_variance == 0, tile_offsets, flatten_ids,
                                               static_cast<const S*>(v_volume), static_cast<const S*>(v_volume_var),

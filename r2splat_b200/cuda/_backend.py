@@ -85,6 +85,14 @@ SIGNATURES: dict[str, tuple] = {
     "r2s_voxel_render_bwd": (I32, [I32, P, I32, I32, P, P, P, P, U32, U32, U32, U32, U32, U32, U32, U32, U32,
                                    P, P]),
     "r2s_voxel_chain_bwd": (I32, [I32, P, P, P, P, P, P, U32, U32, U32, U32, F64, P, P, P, P, P, P, P, P]),
+    "r2s_raster_emit_capacity": (I32, [P, U32, U32, U32, U32, P, I64, P, P, P, P, P, P, SZ, P]),
+    "r2s_voxel_emit_capacity": (I32, [I32, P, P, U32, U32, U32, U32, U32, P, I64, P, P, P, P, P, P, SZ, P]),
+    "r2s_raster_render_capacity": (I32, [I32, P, P, I32, P, P, P, U32, U32, U32, U32, U32, U32, U32, U32, P, P,
+                                         P]),
+    "r2s_voxel_render_capacity": (I32, [I32, P, I32, P, P, P, U32, U32, U32, U32, U32, U32, U32, U32, P, P, P]),
+    "r2s_voxel_render_bwd_capacity": (I32, [I32, P, I32, I32, P, P, P, P, P, U32, U32, U32, U32, U32, U32, U32,
+                                            U32, P, P]),
+    "r2s_adam_activation_step": (I32, [I32, U32, P, P, P, P, P, P, P, P, P, P, P, P, F64, F64, F64, F64, P, P, P]),
     "r2s_scan_tile_counts_noalloc_max": (U64, []),
     "r2s_scan_tile_counts_noalloc": (I32, [P, U64, P, P]),
 }
