@@ -1,0 +1,272 @@
+"""Continuous-batching fit-step server over many resident reconstructions.
+
+Requests name a reconstruction and ask for one fit step of it. The server
+keeps every admitted reconstruction's parameters and Adam moments resident on
+the device, and runs requests as follows:
+
+* Admission is by an HBM budget. A reconstruction whose full fit-step
+  footprint (all buffers of a ``FitScene`` plus its captured graph) fits the
+  remaining budget is kept *graphed*: one CUDA-graph replay per step. One that
+  does not fit is kept *lean*: parameters, Adam moments, cameras and target
+  resident, every other buffer allocated for the step and released after it.
+  A lean step runs the explicit API (which rebuilds the intersection lists each
+  step) plus the same fused activation + Adam update. A reconstruction that
+  does not fit even lean waits until memory frees up.
+* Scheduling is continuous. A scheduler thread of control launches each
+  arrived request as soon as its reconstruction has no step in flight and one
+  of ``slots`` CUDA streams is free, so requests that arrive while others run
+  are started immediately and their kernels overlap on the device. Completion
+  is detected with CUDA events; latency is arrival to completion.
+
+``serve()`` replays a list of (arrival time, reconstruction) requests against
+the wall clock and reports fit-steps/s with p50/p99 latency. ``serve_serially``
+runs the same requests one at a time through the plain explicit API: the
+baseline the served form is compared with.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import heapq
+import time
+from collections import deque
+from dataclasses import dataclass, field
+from typing import Callable, Optional
+
+import torch
+
+from . import batched, explicit
+from .cuda import _backend
+from .cuda import _wrapper as low
+
+Tensor = torch.Tensor
+
+
+@dataclass
+class Reconstruction:
+    key: object
+    scene: batched.FitScene
+    graphed: bool
+    graph: Optional[torch.cuda.CUDAGraph] = None
+    busy: bool = False
+    steps: int = 0
+    footprint: int = 0
+
+
+@dataclass
+class ServeStats:
+    completed: int
+    wall_s: float
+    latencies_ms: list = field(default_factory=list)
+    lean: int = 0
+    graphed: int = 0
+    waited_for_memory: int = 0
+
+    @property
+    def steps_per_s(self) -> float:
+        return self.completed / self.wall_s if self.wall_s > 0 else 0.0
+
+    def percentile(self, q: float) -> float:
+        if not self.latencies_ms:
+            return float("nan")
+        values = sorted(self.latencies_ms)
+        index = min(len(values) - 1, max(0, int(round(q / 100.0 * (len(values) - 1)))))
+        return values[index]
+
+    def summary(self) -> dict:
+        return {"completed": self.completed, "wall_s": self.wall_s, "fit_steps_per_s": self.steps_per_s,
+                "p50_ms": self.percentile(50), "p99_ms": self.percentile(99), "graphed": self.graphed,
+                "lean": self.lean, "waited_for_memory": self.waited_for_memory}
+
+
+def lean_step(scene: batched.FitScene):
+    """One fit step through the explicit API with transient buffers, then the fused update."""
+    cfg = scene.cfg
+    image, ctx = explicit.rasterize_fwd(scene.means, scene.quats, scene.scales, scene.densities, scene.viewmats,
+                                        scene.Ks, cfg.image_size, beta=scene.beta, eps=cfg.eps,
+                                        radius_clip=cfg.radius_clip)
+    v_image = (image - scene.target).mul_(2.0 / image.numel())
+    g = explicit.rasterize_bwd(ctx, v_image)
+    volume, vctx = explicit.voxelize_fwd(scene.means, scene.quats, scene.scales, scene.densities, cfg.volume_shape,
+                                         volume_extent=cfg.volume_extent, volume_center=cfg.volume_center,
+                                         beta=scene.beta, eps=cfg.eps, radius_clip=cfg.radius_clip)
+    vol4 = volume.unsqueeze(0)
+    tv, _, _ = low.volume_loss_fwd(vol4, cfg.lambda_tv)
+    g_vol = low.volume_loss_bwd(vol4, scene.ones, cfg.lambda_tv)[0]
+    gv = explicit.voxelize_bwd(vctx, g_vol)
+    torch.add(torch.sum(v_image * v_image) * (image.numel() / 4.0), tv.reshape(1), out=scene.loss)
+    ga = (ctypes.c_void_p * 5)(*[None if t is None else t.data_ptr() for t in (g.means, g.quats, g.scales,
+                                                                               g.densities, g.beta)])
+    gb = (ctypes.c_void_p * 5)(*[None if t is None else t.data_ptr() for t in (gv.means, gv.quats, gv.scales,
+                                                                               gv.densities, gv.beta)])
+    _backend.call("r2s_adam_activation_step", 0 if scene.means.dtype == torch.float32 else 1, scene.n,
+                  ctypes.c_void_p(scene.means.data_ptr()), ctypes.c_void_p(scene.quats.data_ptr()),
+                  ctypes.c_void_p(scene.raw_scales.data_ptr()), ctypes.c_void_p(scene.raw_densities.data_ptr()),
+                  None if scene.raw_beta is None else ctypes.c_void_p(scene.raw_beta.data_ptr()),
+                  ctypes.c_void_p(scene.scales.data_ptr()), ctypes.c_void_p(scene.densities.data_ptr()),
+                  None if scene.beta is None else ctypes.c_void_p(scene.beta.data_ptr()),
+                  ctypes.c_void_p(scene.adam_m.data_ptr()), ctypes.c_void_p(scene.adam_v.data_ptr()), ga, gb,
+                  float(cfg.lr), 0.9, 0.999, 1e-8, ctypes.c_void_p(scene.step_count.data_ptr()), None,
+                  torch.cuda.current_stream().cuda_stream)
+
+
+class FitServer:
+    """Admits reconstructions against an HBM budget and serves fit-step requests continuously."""
+
+    def __init__(self, budget_bytes: int, slots: int = 8, device="cuda"):
+        self.device = torch.device(device)
+        self.budget = int(budget_bytes)
+        self.used = 0
+        self.streams = [torch.cuda.Stream(device=self.device) for _ in range(slots)]
+        self.recons: dict = {}
+        self.waiting: deque = deque()  # (key, factory) not yet admitted
+
+    # ----------------------------------------------------------- admission
+    def admit(self, key, factory: Callable[[], batched.FitScene]) -> bool:
+        """Creates and admits a reconstruction; returns False (queued) when memory is short."""
+        torch.cuda.synchronize(self.device)
+        before = torch.cuda.memory_allocated(self.device)
+        scene = factory()
+        torch.cuda.synchronize(self.device)
+        full = torch.cuda.memory_allocated(self.device) - before
+        if self.used + full <= self.budget:
+            recon = Reconstruction(key, scene, graphed=True, footprint=full)
+            self._capture(recon)
+        else:
+            # Lean: release every fit-step buffer; keep parameters, moments, cameras, target.
+            self._make_lean(scene)
+            torch.cuda.synchronize(self.device)
+            lean = torch.cuda.memory_allocated(self.device) - before
+            if self.used + lean > self.budget:
+                del scene
+                self.waiting.append((key, factory))
+                return False
+            recon = Reconstruction(key, scene, graphed=False, footprint=lean)
+        self.used += recon.footprint
+        self.recons[key] = recon
+        return True
+
+    @staticmethod
+    def _make_lean(scene: batched.FitScene):
+        keep = {"means", "quats", "raw_scales", "raw_densities", "raw_beta", "scales", "densities", "beta",
+                "adam_m", "adam_v", "step_count", "viewmats", "Ks", "target", "extent", "center", "loss", "ones",
+                "cfg", "device", "n", "c", "height", "width", "depth", "vheight", "vwidth", "radius_clip"}
+        for name in list(vars(scene)):
+            if name not in keep and isinstance(getattr(scene, name), (torch.Tensor, list)):
+                setattr(scene, name, None)
+
+    def _capture(self, recon: Reconstruction):
+        scene = recon.scene
+        scene.step()  # warm-up outside capture (a real step)
+        recon.steps += 1
+        torch.cuda.synchronize(self.device)
+        before = torch.cuda.memory_allocated(self.device)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            scene.enqueue(torch.cuda.current_stream(self.device))
+        torch.cuda.synchronize(self.device)
+        recon.footprint += torch.cuda.memory_allocated(self.device) - before
+        recon.graph = graph
+
+    def evict(self, key):
+        recon = self.recons.pop(key)
+        self.used -= recon.footprint
+        del recon
+        torch.cuda.synchronize(self.device)
+        while self.waiting:
+            k, factory = self.waiting[0]
+            if not self.admit(k, factory):
+                self.waiting.pop()  # admit() queued it again at the back; keep its place at the front
+                self.waiting.appendleft((k, factory))
+                break
+            self.waiting.popleft()
+
+    # ----------------------------------------------------------- serving
+    def _launch(self, recon: Reconstruction, stream: torch.cuda.Stream) -> torch.cuda.Event:
+        with torch.cuda.stream(stream):
+            if recon.graphed:
+                recon.graph.replay()
+            else:
+                lean_step(recon.scene)
+            done = torch.cuda.Event()
+            done.record(stream)
+        return done
+
+    def serve(self, requests: list, poll_s: float = 2e-5) -> ServeStats:
+        """requests: [(arrival_s, key)] sorted by arrival, relative to the call. Runs them all."""
+        pending: dict = {key: deque() for key in self.recons}
+        arrivals = deque(sorted(requests, key=lambda r: r[0]))
+        free = list(range(len(self.streams)))
+        in_flight: list = []  # (event, slot, key, arrival)
+        ready: list = []  # heap of (arrival, seq, key)
+        stats = ServeStats(0, 0.0)
+        stats.graphed = sum(r.graphed for r in self.recons.values())
+        stats.lean = len(self.recons) - stats.graphed
+        stats.waited_for_memory = len(self.waiting)
+        seq = 0
+        start = time.perf_counter()
+        while arrivals or in_flight or ready or any(pending.values()):
+            now = time.perf_counter() - start
+            while arrivals and arrivals[0][0] <= now:
+                t, key = arrivals.popleft()
+                pending[key].append(t)
+                if len(pending[key]) == 1 and not self.recons[key].busy:
+                    heapq.heappush(ready, (t, seq, key))
+                    seq += 1
+            progressed = False
+            still = []
+            for event, slot, key, t in in_flight:
+                if event.query():
+                    stats.completed += 1
+                    stats.latencies_ms.append((time.perf_counter() - start - t) * 1e3)
+                    recon = self.recons[key]
+                    recon.busy = False
+                    recon.steps += 1
+                    free.append(slot)
+                    if pending[key]:
+                        heapq.heappush(ready, (pending[key][0], seq, key))
+                        seq += 1
+                    progressed = True
+                else:
+                    still.append((event, slot, key, t))
+            in_flight = still
+            while free and ready:
+                t, _, key = heapq.heappop(ready)
+                recon = self.recons[key]
+                pending[key].popleft()
+                recon.busy = True
+                slot = free.pop()
+                in_flight.append((self._launch(recon, self.streams[slot]), slot, key, t))
+                progressed = True
+            if not progressed:
+                time.sleep(poll_s)
+        stats.wall_s = time.perf_counter() - start
+        return stats
+
+
+def serve_serially(recons: dict, requests: list) -> ServeStats:
+    """The baseline: each request's fit step through the plain explicit API, one at a time, in arrival order."""
+    stats = ServeStats(0, 0.0)
+    start = time.perf_counter()
+    for t, key in sorted(requests, key=lambda r: r[0]):
+        now = time.perf_counter() - start
+        if t > now:
+            time.sleep(t - now)
+        lean_step(recons[key])
+        torch.cuda.synchronize()
+        stats.completed += 1
+        stats.latencies_ms.append((time.perf_counter() - start - t) * 1e3)
+    stats.wall_s = time.perf_counter() - start
+    return stats
+
+
+def poisson_requests(keys: list, rate_per_s: float, count: int, seed: int = 0) -> list:
+    """`count` requests over `keys` (uniformly) with exponential inter-arrival times."""
+    gen = torch.Generator().manual_seed(seed)
+    gaps = torch.empty(count, dtype=torch.float64).exponential_(rate_per_s, generator=gen)
+    times = torch.cumsum(gaps, 0).tolist()
+    picks = torch.randint(len(keys), (count,), generator=gen).tolist()
+    return [(t, keys[i]) for t, i in zip(times, picks)]
+
+
+__all__ = ["FitServer", "ServeStats", "lean_step", "poisson_requests", "serve_serially"]
