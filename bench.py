@@ -374,13 +374,108 @@ def count_launches(step, scene, prefix: str) -> int:
     return sum(e.count for e in prof.key_averages() if prefix in e.key)
 
 
+def _mixed_scene_specs(count: int, small: bool):
+    """Scene shapes of the batched benchmark: per scene, N log-uniform in [10k, 400k], C in {16, 32, 64,
+    128}, square detector side in {256, 512, 1024}, cubic volume side in {128, 256, 384}, Gaussian or Beta
+    by a coin flip, seed = scene index. small: the serving shapes (N in [10k, 100k], C in {8, 16, 32},
+    side in {128, 256}, volume in {64, 128}), sized so one GPU can keep up with the offered load."""
+    specs = []
+    for i in range(count):
+        g = torch.Generator().manual_seed(i)
+        lo, hi = (1e4, 1e5) if small else (1e4, 4e5)
+        n = int(math.exp(math.log(lo) + (math.log(hi) - math.log(lo)) * torch.rand(1, generator=g).item()))
+        cams = (8, 16, 32) if small else (16, 32, 64, 128)
+        sides = (128, 256) if small else (256, 512, 1024)
+        vols = (64, 128) if small else (128, 256, 384)
+        pick = lambda options: options[int(torch.randint(len(options), (1,), generator=g).item())]
+        specs.append({"n": n, "cameras": pick(cams), "side": pick(sides), "volume": pick(vols),
+                      "beta": bool(torch.randint(2, (1,), generator=g).item()), "seed": i})
+    return specs
+
+
+def mixed_workload(args, device) -> dict:
+    """Aggregate fit-steps/s of the batched (one CUDA graph) or served form vs the plain drop-in run
+    scene by scene (explicit API + the same update), on many uneven reconstructions."""
+    from r2splat_b200 import batched, serve
+
+    small = args.workload == "serve"
+    specs = _mixed_scene_specs(args.scenes, small)
+    tuner = batched.Autotuner(steps=2)
+    tuner.BATCHES = (256,)
+    makers = []
+    for spec in specs:
+        def make(tile, stage_batch, spec=spec):
+            return batched.make_synthetic_scene(spec["n"], spec["cameras"], spec["side"], spec["volume"],
+                                                beta=spec["beta"], seed=spec["seed"], tile=tile,
+                                                stage_batch=stage_batch, device=device)
+        tile, stage = tuner.choose(make, spec["n"], spec["cameras"], (spec["side"], spec["side"]),
+                                   "beta" if spec["beta"] else "gaussian")
+        spec["tile"] = tile
+        makers.append(lambda make=make, tile=tile, stage=stage: make(tile, stage))
+    server = None
+    if small:
+        # Admission builds each reconstruction inside the budget accounting.
+        server = serve.FitServer(budget_bytes=150 << 30, slots=8, device=device)
+        for i, maker in enumerate(makers):
+            server.admit(i, maker)
+        scenes = [server.recons[i].scene for i in sorted(server.recons)]
+    else:
+        scenes = [maker() for maker in makers]
+    torch.cuda.synchronize(device)
+    # Plain: each scene's fit step through the explicit API, one scene after another.
+    for scene in scenes:
+        serve.lean_step(scene)
+    torch.cuda.synchronize(device)
+    rounds = max(1, args.steps // 4)
+    start = time.perf_counter()
+    for _ in range(rounds):
+        for scene in scenes:
+            serve.lean_step(scene)
+    torch.cuda.synchronize(device)
+    plain_s = (time.perf_counter() - start) / rounds
+    config = {"workload": ("served" if small else "batched") + f" mix of {len(scenes)} reconstructions",
+              "scenes": [{k: v for k, v in spec.items() if k != "seed"} for spec in specs]}
+    result = {"metric": "aggregate fit-steps/s over uneven reconstructions", "unit": "fit-steps/s",
+              "higher_is_better": True, "n_gpus": 1, "dtype": "f32", "data": "synthetic", "config": config,
+              "plain_fit_steps_per_s": len(scenes) / plain_s}
+    if not small:
+        fit = batched.BatchedFit(scenes)
+        fit.capture()
+        for _ in range(args.warmup):
+            fit.step()
+        torch.cuda.synchronize(device)
+        start_ev, end_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start_ev.record()
+        for _ in range(args.steps):
+            fit.step(check=False)
+        end_ev.record()
+        torch.cuda.synchronize(device)
+        fit.step()  # one checked step: overflow handling stays exercised
+        ms = start_ev.elapsed_time(end_ev) / args.steps
+        result.update({"value": len(scenes) * 1e3 / ms, "ms_per_batched_step": ms, "steps": args.steps,
+                       "warmup": args.warmup, "recaptures": fit.recaptures,
+                       "vs_plain": len(scenes) * 1e3 / ms / result["plain_fit_steps_per_s"]})
+        return result
+    requests = serve.poisson_requests(list(server.recons), args.rate, args.requests, seed=1)
+    served = server.serve(requests)
+    serial = serve.serve_serially({k: r.scene for k, r in server.recons.items()}, requests)
+    result.update({"value": served.steps_per_s, "served": served.summary(), "serial": serial.summary(),
+                   "offered_rate_per_s": args.rate, "requests": args.requests,
+                   "vs_serial": served.steps_per_s / serial.steps_per_s if serial.steps_per_s else None})
+    return result
+
+
 def main(argv=None) -> int:
     parser = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     parser.add_argument("--gpus", type=int, default=1)
     parser.add_argument("--steps", type=int, default=20)
     parser.add_argument("--warmup", type=int, default=3)
     parser.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    parser.add_argument("--workload", choices=("ct", "ct4", "small"), default="ct")
+    parser.add_argument("--workload", choices=("ct", "ct4", "small", "batched", "serve"), default="ct",
+                        help="ct: the CT fit step (default); batched / serve: the multi-reconstruction forms")
+    parser.add_argument("--scenes", type=int, default=32, help="reconstructions for --workload batched/serve")
+    parser.add_argument("--requests", type=int, default=400, help="requests for --workload serve")
+    parser.add_argument("--rate", type=float, default=400.0, help="Poisson request rate for --workload serve")
     parser.add_argument("--profile-only", action="store_true",
                         help="run the warm-up steps of the workload and exit (profiling driver, no timing)")
     parser.add_argument("--cpu-budget", type=float, default=15.0)
@@ -398,6 +493,12 @@ def main(argv=None) -> int:
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
+    if args.workload in ("batched", "serve"):
+        if rank == 0:
+            print(json.dumps(mixed_workload(args, device)))
+        if world > 1:
+            dist.destroy_process_group()
+        return 0
 
     if args.impl == "reference":
         from oracle import ref_ops

@@ -6,6 +6,8 @@ int64 inclusive prefix sums (bit-exact: integer work), on two calls in a row,
 since the second call reuses the static scratch the first one left behind.
 """
 
+import gc
+
 import pytest
 import torch
 
@@ -43,11 +45,13 @@ def test_no_alloc_scan_matches_workspace_scan_twice(device, n):
     for counts in (first, second):
         expected = _scan_with_workspace(counts)
         cum = torch.full((n,), -1, dtype=torch.int64, device=device)
+        gc.collect()
         torch.cuda.synchronize(device)
-        allocated = torch.cuda.memory_allocated(device)
+        allocations = torch.cuda.memory_stats(device).get("allocation.all.allocated", 0)
         _scan_no_alloc(counts, cum)
         torch.cuda.synchronize(device)
-        assert torch.cuda.memory_allocated(device) == allocated
+        # The cumulative allocation count of the caching allocator must not move.
+        assert torch.cuda.memory_stats(device).get("allocation.all.allocated", 0) == allocations
         assert torch.equal(cum, expected)
         assert torch.equal(cum, torch.cumsum(counts.to(torch.int64), 0))
 
