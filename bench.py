@@ -68,6 +68,22 @@ def dist_info():
     return world, rank, local
 
 
+def max_over_ranks(ms: float, world: int, device) -> float:
+    """The job's time for a multi-rank measurement: the slowest rank's (identity on one rank)."""
+    if world <= 1:
+        return ms
+    import torch.distributed as dist
+
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(units_per_rank_step: float, ranks: int, ms_per_step: float) -> float:
+    """Whole-job throughput: every rank processes its own units per step (weak scaling, replicas)."""
+    return units_per_rank_step * ranks / (ms_per_step * 1e-3)
+
+
 class ClockSampler:
     """Samples nvidia-smi clocks and throttle reasons during the timed region."""
 
@@ -256,27 +272,36 @@ def build_workload(device, workload: str):
     return scene, target
 
 
-def fp32_peak_tflops(device) -> float:
-    """Measured FP32 FMA issue peak (TFLOP/s) on this GPU, CUDA events, best of 5."""
+def _probe_rate(name: str, device, ops_per_iter: float, iters: int) -> float:
+    """Best-of-6 rate (ops/s) of a peak probe, timed with CUDA events."""
     import ctypes
 
     from r2splat_b200.cuda import _backend
 
     out = torch.zeros(4096, device=device)
     props = torch.cuda.get_device_properties(device)
-    blocks, threads, iters = props.multi_processor_count * 8, 256, 2048
+    blocks, threads = props.multi_processor_count * 8, 256
     stream = ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
     best = 0.0
     for _ in range(6):
         start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         start.record()
-        _backend.call("r2s_fp32_peak_probe", ctypes.c_void_p(out.data_ptr()), blocks, threads, iters, stream)
+        _backend.call(name, ctypes.c_void_p(out.data_ptr()), blocks, threads, iters, stream)
         end.record()
         end.synchronize()
         ms = start.elapsed_time(end)
-        flops = 2.0 * blocks * threads * iters * 128
-        best = max(best, flops / (ms * 1e-3) / 1e12)
+        best = max(best, ops_per_iter * blocks * threads * iters / (ms * 1e-3))
     return best
+
+
+def fp32_peak_tflops(device) -> float:
+    """Measured FP32 FMA issue peak (TFLOP/s) on this GPU: 128 FMAs = 256 flops per thread and step."""
+    return _probe_rate("r2s_fp32_peak_probe", device, 256.0, 2048) / 1e12
+
+
+def sfu_peak_gops(device) -> float:
+    """Measured SFU ex2 issue peak (G ex2/s) on this GPU: 128 ex2 per thread and step."""
+    return _probe_rate("r2s_sfu_peak_probe", device, 128.0, 512) / 1e9
 
 
 def cpu_baseline(budget_s: float = 15.0) -> dict:
@@ -529,17 +554,16 @@ def main(argv=None) -> int:
     torch.cuda.synchronize()
     with ClockSampler(local) as clocks:
         total_ms, stages, own_launches = timed_run(step, scene, args.steps, args.warmup, device, flush_buf)
-    if world > 1 and args.impl == "ours":
-        t = torch.tensor([total_ms], device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    ranks = world if args.impl == "ours" else 1
+    total_ms = max_over_ranks(total_ms, ranks, device)
     ms_per_step = total_ms / args.steps
     raster_evals, voxel_evals, m2, m3 = step.eval_counts()
     evals_per_step = 2 * raster_evals + 2 * voxel_evals
-    value = evals_per_step * (world if args.impl == "ours" else 1) / (ms_per_step * 1e-3)
+    value = job_rate(evals_per_step, ranks, ms_per_step)
 
     e2e_ms, h2d, d2h = e2e_run(step, scene, args.steps, args.warmup, device)
-    e2e_value = evals_per_step * (world if args.impl == "ours" else 1) / (e2e_ms / args.steps * 1e-3)
+    e2e_ms = max_over_ranks(e2e_ms, ranks, device)
+    e2e_value = job_rate(evals_per_step, ranks, e2e_ms / args.steps)
     if args.impl == "ours":
         launches = own_launches
     else:
@@ -601,6 +625,7 @@ def main(argv=None) -> int:
             "peak_source": "measured in-bench: FP32 FMA probe r2s_fp32_peak_probe (MEASURED_PEAKS.json has no "
                            "FP32 figure)",
             "hbm_peak_gbs_measured": peaks.get("hbm_gbs"),
+            "sfu_peak_gex2_s_measured": sfu_peak_gops(device),
         }
         if rank == 0 and not args.no_cpu_baseline:
             result["cpu_baseline"] = cpu_baseline(args.cpu_budget)

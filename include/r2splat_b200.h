@@ -44,6 +44,11 @@ const char* r2s_last_error(void);
  * FP32 issue peak the accumulate kernels are compared against. */
 int r2s_fp32_peak_probe(float* out, uint32_t blocks, uint32_t threads, int iters, void* stream);
 
+/* Measurement helper (no reference counterpart): blocks x threads threads
+ * that each run iters x 128 independent fast base-2 exponentials (one SFU ex2
+ * each), to measure the SFU issue peak of the exp/pow-bound loops. */
+int r2s_sfu_peak_probe(float* out, uint32_t blocks, uint32_t threads, int iters, void* stream);
+
 /* Number of kernels this library has launched in the process so far. */
 uint64_t r2s_launch_count(void);
 

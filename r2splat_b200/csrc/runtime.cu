@@ -46,6 +46,25 @@ __global__ void fp32_peak_kernel(float* out, int iters, float seed) {
     if (s == 1234.5f) out[blockIdx.x] = s;  // keeps the chains live
 }
 
+// SFU (MUFU) issue probe: 8 independent chains x = 2^(-x) per thread. The
+// fast exponential compiles to one ex2 per step; x stays in (0, 1).
+__global__ void sfu_peak_kernel(float* out, int iters, float seed) {
+    float x[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) x[k] = seed * float(k + 1) / 8.f + 1e-3f * float(threadIdx.x & 7);
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) x[k] = exp2f(-x[k]);
+        }
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s += x[k];
+    if (s == 1234.5f) out[blockIdx.x] = s;  // keeps the chains live
+}
+
 }  // namespace r2s
 
 extern "C" {
@@ -58,6 +77,12 @@ uint64_t r2s_launch_count(void) { return r2s::g_launches.load(std::memory_order_
 int r2s_fp32_peak_probe(float* out, uint32_t blocks, uint32_t threads, int iters, void* stream) {
     r2s::fp32_peak_kernel<<<blocks, threads, 0, static_cast<cudaStream_t>(stream)>>>(out, iters, 0.5f);
     return r2s::check_launch("fp32_peak_probe");
+}
+
+// Launches the SFU peak probe: blocks x threads x iters x 128 ex2.
+int r2s_sfu_peak_probe(float* out, uint32_t blocks, uint32_t threads, int iters, void* stream) {
+    r2s::sfu_peak_kernel<<<blocks, threads, 0, static_cast<cudaStream_t>(stream)>>>(out, iters, 0.5f);
+    return r2s::check_launch("sfu_peak_probe");
 }
 
 const char* r2s_last_error(void) { return r2s::t_last_error.c_str(); }

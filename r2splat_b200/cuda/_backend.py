@@ -30,6 +30,7 @@ SIGNATURES: dict[str, tuple] = {
     "r2s_abi_version": (I32, []),
     "r2s_last_error": (ctypes.c_char_p, []),
     "r2s_fp32_peak_probe": (I32, [P, U32, U32, I32, P]),
+    "r2s_sfu_peak_probe": (I32, [P, U32, U32, I32, P]),
     "r2s_launch_count": (U64, []),
     "r2s_check_values": (I32, [I32, P, U32, P, P]),
     "r2s_parameter_transform_fwd": (I32, [I32, P, P, P, P, U32, P]),
