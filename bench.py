@@ -327,9 +327,16 @@ def cpu_baseline(budget_s: float = 15.0) -> dict:
             break
     elapsed = time.perf_counter() - t0
     del grads
-    return {"value": evals / elapsed, "unit": "evals/s", "cores": threads, "kind": "port",
+    rate = evals / elapsed
+    # The dense oracle evaluates every (primitive, pixel) and (primitive, voxel) pair: a whole CT fit step
+    # (200k primitives, 64 views x 512^2, 256^3 volume, forward + backward) is this many dense evaluations.
+    full = sc.means.shape[0]
+    dense_per_step = 2 * full * (sc.viewmats.shape[0] * sc.image_size[0] * sc.image_size[1] + 256 ** 3)
+    return {"value": rate, "unit": "evals/s", "cores": threads, "kind": "port",
             "sample": f"float64 dense oracle (oracle/dense.py): {n} Gaussians x 1 view x 512x512, raster fwd+bwd "
-                      f"(autograd), {reps} repetitions in {elapsed:.1f}s; dense evals counted"}
+                      f"(autograd), {reps} repetitions in {elapsed:.1f}s; dense evals counted",
+            "extrapolated_ct_fit_step_s": dense_per_step / rate,
+            "extrapolation": "not measured: dense evaluations of one full CT fit step divided by the measured rate"}
 
 
 def timed_run(step, scene, steps, warmup, device, flush_buf):

@@ -143,6 +143,7 @@ __global__ void __launch_bounds__(kMaxThreads) raster_fwd_kernel(
     Rec2D<S>* s_rec = reinterpret_cast<Rec2D<S>*>(smem);          // [2][B]
     S* s_q = reinterpret_cast<S*>(s_rec + 2 * B);                   // [2][B]
     uint2* s_mask = reinterpret_cast<uint2*>(s_q + 2 * B);          // [B] (column, row) masks
+    uint16_t* s_hits = reinterpret_cast<uint16_t*>(s_mask + B);     // [warps][32] hit lists
 
     const uint32_t tile = blockIdx.x, cam = blockIdx.y;
     const uint32_t key = cam * n_tiles + tile;
@@ -203,10 +204,14 @@ __global__ void __launch_bounds__(kMaxThreads) raster_fwd_kernel(
                     const uint2 m = s_mask[base + int32_t(lane)];
                     hit = (m.x & warp_cols) != 0u && (m.y & warp_rows) != 0u;
                 }
-                uint32_t pending = __ballot_sync(0xffffffffu, hit);
-                while (pending != 0u) {
-                    const int32_t s = base + __ffs(pending) - 1;
-                    pending &= pending - 1u;
+                // The warp's hits, compacted in lane (= list) order.
+                const uint32_t hits = __ballot_sync(0xffffffffu, hit);
+                uint16_t* my_hits = s_hits + warp * 32u;
+                if (hit) my_hits[__popc(hits & ((1u << lane) - 1u))] = uint16_t(base + int32_t(lane));
+                __syncwarp();
+                const int32_t n_hits = __popc(hits);
+                for (int32_t e = 0; e < n_hits; ++e) {
+                    const int32_t s = my_hits[e];
                     const Rec2D<S> r = buf[s];
                     const S om = r.o * r.mu;
                     S q = S(0);
@@ -234,6 +239,7 @@ __global__ void __launch_bounds__(kMaxThreads) raster_fwd_kernel(
                         }
                     }
                 }
+                __syncwarp();  // the list is rewritten for the next 32 records
             }
         }
         __syncthreads();
@@ -701,7 +707,8 @@ int launch_fwd_p(const RasterGeom& g, const Rec2D<S>* rec, const S* unc, const i
     unsigned batch = g.stage_batch < kFwdBatch ? g.stage_batch : kFwdBatch;
     if (batch > nthreads) batch = nthreads;
     if (batch < 1) batch = 1;
-    const size_t smem = 2 * size_t(batch) * (sizeof(Rec2D<S>) + sizeof(S)) + size_t(batch) * sizeof(uint2);
+    const size_t smem = 2 * size_t(batch) * (sizeof(Rec2D<S>) + sizeof(S)) + size_t(batch) * sizeof(uint2) +
+                        size_t(nthreads) * sizeof(uint16_t);
     dim3 grid(g.tiles_x * g.tiles_y, g.C);
     if (nthreads <= 256) {
         // Tiles up to 16x16: a register budget sized for 256-thread CTAs.
