@@ -1,0 +1,53 @@
+"""Host-side logic of the serving and batched drivers (no GPU needed)."""
+
+import pytest
+import torch
+
+from r2splat_b200 import batched, serve
+
+
+def test_poisson_requests_are_sorted_seeded_and_cover_keys():
+    a = serve.poisson_requests(["x", "y", "z"], rate_per_s=400.0, count=2000, seed=3)
+    b = serve.poisson_requests(["x", "y", "z"], rate_per_s=400.0, count=2000, seed=3)
+    assert a == b
+    times = [t for t, _ in a]
+    assert times == sorted(times) and times[0] > 0
+    assert {k for _, k in a} == {"x", "y", "z"}
+    # Mean inter-arrival time of an exponential with rate 400/s is 2.5 ms.
+    assert abs(times[-1] / len(times) - 1 / 400.0) < 2e-4
+
+
+def test_serve_stats_percentiles_and_summary():
+    stats = serve.ServeStats(completed=5, wall_s=2.0, latencies_ms=[5.0, 1.0, 3.0, 2.0, 4.0])
+    assert stats.steps_per_s == 2.5
+    assert stats.percentile(50) == 3.0
+    assert stats.percentile(99) == 5.0
+    assert stats.percentile(0) == 1.0
+    summary = stats.summary()
+    assert summary["p50_ms"] == 3.0 and summary["fit_steps_per_s"] == 2.5
+    assert serve.ServeStats(0, 0.0).steps_per_s == 0.0
+    assert serve.ServeStats(0, 1.0).percentile(50) != serve.ServeStats(0, 1.0).percentile(50)  # nan
+
+
+def test_scene_config_defaults_and_autotuner_keys():
+    cfg = batched.SceneConfig(image_size=(64, 64), volume_shape=(32, 32, 32))
+    assert cfg.tile == 16 and cfg.voxel_tile == 8 and cfg.stage_batch == 256 and cfg.capacity_slack > 1
+    k1 = batched.Autotuner.key(100_000, 32, (512, 512), "gaussian")
+    k2 = batched.Autotuner.key(120_000, 32, (512, 512), "gaussian")
+    k3 = batched.Autotuner.key(100_000, 32, (512, 512), "beta")
+    assert k1 == k2 and k1 != k3
+    assert set(batched.Autotuner.TILES) == {8, 16, 32}
+
+
+def test_mixed_benchmark_scene_shapes_follow_the_stated_distribution():
+    import bench
+
+    specs = bench._mixed_scene_specs(64, small=False)
+    assert all(10_000 <= s["n"] <= 400_000 for s in specs)
+    assert {s["cameras"] for s in specs} <= {16, 32, 64, 128}
+    assert {s["side"] for s in specs} <= {256, 512, 1024}
+    assert {s["volume"] for s in specs} <= {128, 256, 384}
+    assert {s["beta"] for s in specs} == {False, True}
+    assert specs == bench._mixed_scene_specs(64, small=False)
+    small = bench._mixed_scene_specs(16, small=True)
+    assert all(s["n"] <= 100_000 and s["side"] <= 256 for s in small)
