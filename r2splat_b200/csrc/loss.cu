@@ -35,27 +35,48 @@ __device__ __forceinline__ double block_sum(double v) {
     return total;
 }
 
+// Each block takes a contiguous range of rows (a row is one (b, d, h) line of W
+// voxels) and its threads stride along x. The first row's (d, h) is derived
+// once per block and then advanced by one per row, so no voxel pays an index
+// division; blocks walk fixed row ranges in a fixed order, so the double
+// partial sums (and the loss) are deterministic.
+__device__ __forceinline__ void first_row(uint64_t rows, uint32_t D, uint32_t H, uint64_t& r0, uint64_t& r1,
+                                          uint32_t& d, uint32_t& h) {
+    const uint64_t per = (rows + gridDim.x - 1) / gridDim.x;
+    r0 = uint64_t(blockIdx.x) * per;
+    r1 = r0 + per < rows ? r0 + per : rows;
+    h = uint32_t(r0 % H);
+    d = uint32_t((r0 / H) % D);
+}
+
+__device__ __forceinline__ void next_row(uint32_t D, uint32_t H, uint32_t& d, uint32_t& h) {
+    if (++h == H) {
+        h = 0;
+        if (++d == D) d = 0;
+    }
+}
+
 template <typename S>
-__global__ void __launch_bounds__(kLossThreads) tv_fwd_kernel(const S* __restrict__ vol, int64_t B, int64_t D,
-                                                              int64_t H, int64_t W, S* __restrict__ tv_map,
+__global__ void __launch_bounds__(kLossThreads) tv_fwd_kernel(const S* __restrict__ vol, uint32_t D, uint32_t H,
+                                                              uint32_t W, uint64_t rows, S* __restrict__ tv_map,
                                                               double* __restrict__ partials) {
-    const int64_t total = B * D * H * W;
-    const int64_t HW = H * W, DHW = D * HW;
     double sum = 0;
-    for (int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; idx < total;
-         idx += int64_t(gridDim.x) * blockDim.x) {
-        const int64_t r = idx % DHW;
-        const int64_t d = r / HW;
-        const int64_t hw = r - d * HW;
-        const int64_t h = hw / W;
-        const int64_t w = hw - h * W;
-        const S val = vol[idx];
-        S tv = 0;
-        if (d + 1 < D) tv += abs_diff(vol[idx + HW] - val);
-        if (h + 1 < H) tv += abs_diff(vol[idx + W] - val);
-        if (w + 1 < W) tv += abs_diff(vol[idx + 1] - val);
-        if (tv_map != nullptr) tv_map[idx] = tv;
-        sum += static_cast<double>(tv);
+    const uint64_t HW = uint64_t(H) * W;
+    uint64_t r0, r1;
+    uint32_t d, h;
+    first_row(rows, D, H, r0, r1, d, h);
+    for (uint64_t row = r0; row < r1; ++row, next_row(D, H, d, h)) {
+        const uint64_t base = row * W;
+        for (uint32_t x = threadIdx.x; x < W; x += kLossThreads) {
+            const uint64_t idx = base + x;
+            const S val = vol[idx];
+            S tv = 0;
+            if (d + 1 < D) tv += abs_diff(vol[idx + HW] - val);
+            if (h + 1 < H) tv += abs_diff(vol[idx + W] - val);
+            if (x + 1 < W) tv += abs_diff(vol[idx + 1] - val);
+            if (tv_map != nullptr) tv_map[idx] = tv;
+            sum += static_cast<double>(tv);
+        }
     }
     const double total_sum = block_sum(sum);
     if (threadIdx.x == 0) partials[blockIdx.x] = total_sum;
@@ -95,28 +116,28 @@ __global__ void finish_mean_kernel(const double* __restrict__ partials, int n_pa
 }
 
 template <typename S>
-__global__ void tv_bwd_kernel(const S* __restrict__ vol, const S* __restrict__ grad_output, int64_t B, int64_t D,
-                              int64_t H, int64_t W, int64_t edges, float lambda, S* __restrict__ grad) {
-    const int64_t total = B * D * H * W;
-    const int64_t HW = H * W, DHW = D * HW;
+__global__ void tv_bwd_kernel(const S* __restrict__ vol, const S* __restrict__ grad_output, uint32_t D, uint32_t H,
+                              uint32_t W, uint64_t rows, int64_t edges, float lambda, S* __restrict__ grad) {
     const S grad_out = grad_output[0] / static_cast<S>(edges);
     const S lam = static_cast<S>(lambda);
-    for (int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; idx < total;
-         idx += int64_t(gridDim.x) * blockDim.x) {
-        const int64_t r = idx % DHW;
-        const int64_t d = r / HW;
-        const int64_t hw = r - d * HW;
-        const int64_t h = hw / W;
-        const int64_t w = hw - h * W;
-        const S val = vol[idx];
-        S g = 0;
-        if (d + 1 < D) g -= sign_of(vol[idx + HW] - val);
-        if (d > 0) g += sign_of(val - vol[idx - HW]);
-        if (h + 1 < H) g -= sign_of(vol[idx + W] - val);
-        if (h > 0) g += sign_of(val - vol[idx - W]);
-        if (w + 1 < W) g -= sign_of(vol[idx + 1] - val);
-        if (w > 0) g += sign_of(val - vol[idx - 1]);
-        grad[idx] = (g * grad_out) * lam;
+    const uint64_t HW = uint64_t(H) * W;
+    uint64_t r0, r1;
+    uint32_t d, h;
+    first_row(rows, D, H, r0, r1, d, h);
+    for (uint64_t row = r0; row < r1; ++row, next_row(D, H, d, h)) {
+        const uint64_t base = row * W;
+        for (uint32_t x = threadIdx.x; x < W; x += blockDim.x) {
+            const uint64_t idx = base + x;
+            const S val = vol[idx];
+            S g = 0;
+            if (d + 1 < D) g -= sign_of(vol[idx + HW] - val);
+            if (d > 0) g += sign_of(val - vol[idx - HW]);
+            if (h + 1 < H) g -= sign_of(vol[idx + W] - val);
+            if (h > 0) g += sign_of(val - vol[idx - W]);
+            if (x + 1 < W) g -= sign_of(vol[idx + 1] - val);
+            if (x > 0) g += sign_of(val - vol[idx - 1]);
+            grad[idx] = (g * grad_out) * lam;
+        }
     }
 }
 
@@ -163,7 +184,8 @@ int r2s_volume_loss_fwd(int dtype, const void* volume, uint32_t B, uint32_t D, u
     cudaStream_t st = as_stream(stream);
     R2S_DISPATCH(dtype, {
         if (total > 0) {
-            tv_fwd_kernel<S><<<blocks, kLossThreads, 0, st>>>(static_cast<const S*>(volume), B, D, H, W,
+            const uint64_t rows = uint64_t(B) * D * H;
+            tv_fwd_kernel<S><<<blocks, kLossThreads, 0, st>>>(static_cast<const S*>(volume), D, H, W, rows,
                                                              static_cast<S*>(tv_map), partials);
             R2S_TRY(check_launch("volume_loss_fwd"));
         }
@@ -180,9 +202,10 @@ int r2s_volume_loss_bwd(int dtype, const void* volume, const void* grad_output, 
     const int64_t edges_raw = int64_t(B) * ((int64_t(D) - 1) * H * W + int64_t(D) * (H - 1) * W +
                                             int64_t(D) * H * (int64_t(W) - 1));
     const int64_t edges = edges_raw > 1 ? edges_raw : 1;
+    const uint64_t rows = uint64_t(B) * D * H;
     R2S_DISPATCH(dtype, {
         tv_bwd_kernel<S><<<loss_blocks(total), kLossThreads, 0, as_stream(stream)>>>(
-            static_cast<const S*>(volume), static_cast<const S*>(grad_output), B, D, H, W, edges, lambda_tv,
+            static_cast<const S*>(volume), static_cast<const S*>(grad_output), D, H, W, rows, edges, lambda_tv,
             static_cast<S*>(grad_volume));
         return check_launch("volume_loss_bwd");
     });
