@@ -244,9 +244,11 @@ __global__ void raster_project_kernel(const S* __restrict__ means, const S* __re
     tiles_per_gauss[idx] = count;
 }
 
-// Chain rule for the rasterizer, one thread per primitive looping over the
-// cameras in order. grads [C,N,8] holds the tile-accumulated adjoints of the
-// packed record slots.
+// Chain rule for the rasterizer: four lanes per primitive, each looping over
+// every fourth camera, partial sums combined by shuffles (no atomics). grads
+// [C,N,8] holds the adjoints of the packed record slots.
+constexpr uint32_t kChainGroup = 4;  // lanes per primitive in the chain-rule pass
+
 template <typename S>
 __global__ void raster_chain_bwd_kernel(const S* __restrict__ means, const S* __restrict__ quats,
                                         const S* __restrict__ scales, const S* __restrict__ covars,
@@ -256,17 +258,26 @@ __global__ void raster_chain_bwd_kernel(const S* __restrict__ means, const S* __
                                         const Rec2D<S>* __restrict__ grads, S* __restrict__ v_means,
                                         S* __restrict__ v_quats, S* __restrict__ v_scales,
                                         S* __restrict__ v_densities, S* __restrict__ v_betas) {
-    const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= N) return;
+    // kChainGroup consecutive lanes share a primitive, each taking every
+    // kChainGroup-th camera; their partial sums are combined by shuffles in a
+    // fixed order (deterministic).
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t part = tid % kChainGroup;
+    const bool active = tid / kChainGroup < N;
+    const uint32_t n = active ? tid / kChainGroup : N - 1;
     S sig[6];
 #pragma unroll
     for (int k = 0; k < 6; ++k) sig[k] = covars[size_t(n) * 6 + k];
     const S px = means[size_t(n) * 3 + 0], py = means[size_t(n) * 3 + 1], pz = means[size_t(n) * 3 + 2];
     const bool is_beta = ratio != nullptr;
     const S beta_ratio = is_beta ? ratio[n] : S(1);
-    S acc_p[3] = {0, 0, 0}, acc_s[6] = {0, 0, 0, 0, 0, 0};
-    S acc_o = 0, acc_beta = 0, acc_mu_mu = 0;
-    for (uint32_t c = 0; c < C; ++c) {
+    S acc[12] = {};  // means 0-2, covariance 3-8, density 9, beta 10, mu * mu 11
+    S* acc_p = acc;
+    S* acc_s = acc + 3;
+    S& acc_o = acc[9];
+    S& acc_beta = acc[10];
+    S& acc_mu_mu = acc[11];
+    for (uint32_t c = active ? part : C; c < C; c += kChainGroup) {
         const Rec2D<S> g = grads[size_t(c) * N + n];
         acc_o += g.o;
         if (g.x == S(0) && g.y == S(0) && g.a == S(0) && g.b == S(0) && g.c == S(0) && g.mu == S(0) &&
@@ -292,6 +303,12 @@ __global__ void raster_chain_bwd_kernel(const S* __restrict__ means, const S* __
 #pragma unroll
         for (int k = 0; k < 6; ++k) acc_s[k] += vs[k];
     }
+#pragma unroll
+    for (int offset = 1; offset < kChainGroup; offset <<= 1) {
+#pragma unroll
+        for (int k = 0; k < 12; ++k) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], offset);
+    }
+    if (!active || part != 0) return;
     S q[4], s[3], vq[4], vsc[3];
 #pragma unroll
     for (int k = 0; k < 4; ++k) q[k] = quats[size_t(n) * 4 + k];
@@ -512,7 +529,8 @@ int r2s_raster_chain_bwd(int dtype, const void* means, const void* quats, const 
     const bool beta = betas != nullptr;
     R2S_REQUIRE(!beta || (ratio != nullptr && log_grad != nullptr && v_betas != nullptr), R2S_ERR_ARGUMENT,
                 "Beta chain rule needs ratio, log_grad and v_betas");
-    R2S_DISPATCH(dtype, raster_chain_bwd_kernel<S><<<blocks_for(N, 128), 128, 0, as_stream(stream)>>>(
+    R2S_DISPATCH(dtype, raster_chain_bwd_kernel<S><<<blocks_for(uint64_t(N) * kChainGroup, 128), 128, 0,
+                                                    as_stream(stream)>>>(
         static_cast<const S*>(means), static_cast<const S*>(quats), static_cast<const S*>(scales),
         static_cast<const S*>(covars), beta ? static_cast<const S*>(ratio) : nullptr,
         beta ? static_cast<const S*>(log_grad) : nullptr, static_cast<const S*>(viewmats),
