@@ -141,11 +141,11 @@ constexpr int kVoxBwdWarps = 8;
 constexpr int kVoxBwdThreads = kVoxBwdWarps * 32;
 
 // A record's box on one 3D tile, tile-local: origin x0 | y0 << 8 | z0 << 16,
-// extent w | h << 8 | d << 16, and ceil(2^20 / w), ceil(2^20 / (w h)), with
-// which (k * magic) >> 20 is the exact quotient for every k < 1024 and divisor
-// <= 1024. An empty box has a zero extent.
+// extent w | h << 8 | d << 16, and ceil(65536 / h), with which
+// (k * magic_h) >> 16 == k / h for every k < 1024 and h <= 32. An empty box has
+// a zero extent.
 struct alignas(16) VoxelBox {
-    uint32_t origin, extent, magic_w, magic_wh;
+    uint32_t origin, extent, magic_h, unused;
 };
 
 // Conservative box of the voxels whose sample can pass the contribution test
@@ -163,7 +163,7 @@ __device__ __forceinline__ VoxelBox voxel_box(const Rec3D<S>& r, uint32_t ox, ui
                                               uint32_t vy, uint32_t vz) {
     uint32_t lo[3] = {0u, 0u, 0u};
     uint32_t hi[3] = {vx - 1, vy - 1, vz - 1};
-    const VoxelBox empty{0u, 0u, 1u, 1u};
+    const VoxelBox empty{0u, 0u, 1u, 0u};
     const S a = r.c00, p = r.c01, q = r.c02, bb = r.c11, rr = r.c12, c = r.c22;
     const S adj0 = bb * c - rr * rr;
     const S adj1 = a * c - q * q;
@@ -201,31 +201,34 @@ __device__ __forceinline__ VoxelBox voxel_box(const Rec3D<S>& r, uint32_t ox, ui
     VoxelBox box;
     box.origin = lo[0] | (lo[1] << 8) | (lo[2] << 16);
     box.extent = w | (h << 8) | (d << 16);
-    box.magic_w = ((1u << 20) + w - 1u) / w;
-    box.magic_wh = ((1u << 20) + w * h - 1u) / (w * h);
+    box.magic_h = (65536u + h - 1u) / h;
+    box.unused = 0u;
     return box;
 }
-
-// Voxel centre and image adjoint of one tile voxel.
-template <typename S>
-struct alignas(4 * sizeof(S)) VoxelSample {
-    S x, y, z, v;
-};
 
 // Null-pointer conventions as in the rasterizer VJP: v_volume null = zero
 // adjoint; v_volume_var null = no variance branch; chain_var false =
 // detached variance branch.
 //
-// One warp per record, evaluating only the voxels of the record's box. Per
-// sample a lane accumulates, with g the volume adjoint (plus the variance
-// chain term) and w = -g alpha (Gaussian) or the d^T Q d adjoint (Beta):
+// One warp per record over the record's box, one lane per box row (the box's
+// voxels at one (y, z)), walking x with a warp-uniform trip count. Along a row
+// d2 and d3 are fixed, so the quadratic form is a per-row constant plus a
+// linear and a quadratic term in d1, and each lane keeps four row sums
+// (sum w, sum w d1, sum w d1^2, sum g vis; plus the variance and Beta sums)
+// that it folds into the record sums once per row. With g the volume adjoint
+// (plus the variance chain term) and w = -g alpha (Gaussian) or the d^T Q d
+// adjoint (Beta), the record sums are
 //   S1..S3 = sum w d_i, Svis = sum g vis, S_ij = sum w d_i d_j (i <= j),
-//   Sb = sum g alpha log h (Beta), Sq = sum v_var alpha^2 (variance);
-// the record's adjoints follow once per record: for a Gaussian
+//   Sb = sum g alpha log h (Beta), Sq = sum v_var alpha^2 (variance),
+// and the record's adjoints follow once per record: for a Gaussian
 // x_i = -(Q d-sums)_i, i.e. x = -(c00 S1 + c01 S2 + c02 S3) and so on,
 // c_ii = S_ii / 2, c_ij = S_ij, o = Svis; for a Beta x = 2 (Q d-sums)_i,
 // c_ii = S_ii, c_ij = 2 S_ij, o = Svis, beta = Sb -- the reference's
-// per-sample terms with the record's constants factored out.
+// per-sample terms with the record's constants factored out. The factored
+// quadratic form rounds differently from the reference's per-sample
+// expression (by about an ulp); the VJP is held to a tolerance, and a
+// contribution-threshold decision that flips moves a gradient by one
+// threshold-sized sample at most.
 template <typename S, bool kBeta, bool kVar>
 __global__ void __launch_bounds__(kVoxBwdThreads) voxel_bwd_kernel(
     const Rec3D<S>* __restrict__ records, bool chain_var, const int32_t* __restrict__ offsets,
@@ -236,8 +239,8 @@ __global__ void __launch_bounds__(kVoxBwdThreads) voxel_bwd_kernel(
     const uint32_t tile_voxels = T * T * T;
     Rec3D<S>* s_rec = reinterpret_cast<Rec3D<S>*>(smem);                          // [2][threads]
     VoxelBox* s_box = reinterpret_cast<VoxelBox*>(s_rec + 2 * kVoxBwdThreads);     // [threads]
-    VoxelSample<S>* s_vox = reinterpret_cast<VoxelSample<S>*>(s_box + kVoxBwdThreads);  // [T^3]
-    S* s_vv = reinterpret_cast<S*>(s_vox + tile_voxels);                           // [T^3]
+    S* s_v = reinterpret_cast<S*>(s_box + kVoxBwdThreads);                         // [T^3] adjoint
+    S* s_vv = s_v + tile_voxels;                                                   // [T^3] variance adjoint
     int32_t* s_id = reinterpret_cast<int32_t*>(s_vv + tile_voxels);                // [2][threads]
 
     const uint32_t n_tiles = g.tiles_x * g.tiles_y * g.tiles_z;
@@ -261,12 +264,7 @@ __global__ void __launch_bounds__(kVoxBwdThreads) voxel_bwd_kernel(
         const uint32_t ly = r2 / T, lx = r2 - ly * T;
         const bool ok = lx < vx && ly < vy && lz < vz;
         const size_t vid = (size_t(oz + lz) * g.dim1 + (oy + ly)) * g.dim2 + (ox + lx);
-        VoxelSample<S> sm;
-        sm.x = static_cast<S>(ox + lx) + static_cast<S>(0.5);
-        sm.y = static_cast<S>(oy + ly) + static_cast<S>(0.5);
-        sm.z = static_cast<S>(oz + lz) + static_cast<S>(0.5);
-        sm.v = (ok && v_volume != nullptr) ? v_volume[vid] : S(0);
-        s_vox[p] = sm;
+        s_v[p] = (ok && v_volume != nullptr) ? v_volume[vid] : S(0);
         if (kVar) s_vv[p] = ok ? v_volume_var[vid] : S(0);
     }
 
@@ -296,79 +294,98 @@ __global__ void __launch_bounds__(kVoxBwdThreads) voxel_bwd_kernel(
         for (int32_t s = int32_t(warp); s < batch; s += kVoxBwdWarps) {
             const VoxelBox box = s_box[s];
             const uint32_t w = box.extent & 0xffu, h = (box.extent >> 8) & 0xffu, d = (box.extent >> 16) & 0xffu;
-            const uint32_t wh = w * h, vol = wh * d;
-            if (vol == 0u) continue;
-            const uint32_t base = (((box.origin >> 16) & 0xffu) * T + ((box.origin >> 8) & 0xffu)) * T +
-                                  (box.origin & 0xffu);
+            const uint32_t rows = h * d;
+            if (rows * w == 0u) continue;
+            const uint32_t x0 = box.origin & 0xffu, y0 = (box.origin >> 8) & 0xffu, z0 = (box.origin >> 16) & 0xffu;
             const Rec3D<S> r = s_rec[stage * kVoxBwdThreads + s];
             const int32_t gid = s_id[stage * kVoxBwdThreads + s];
             const S a = r.c00, p = r.c01, q = r.c02, bb = r.c11, rr = r.c12, c = r.c22;
             const S opac = r.o;
             const S uq = chain_var ? r.q : S(0);
+            const S half_a = static_cast<S>(0.5) * a;
+            const S px0 = static_cast<S>(ox + x0) + static_cast<S>(0.5);
             // part: S1, S2, S3, Svis | S11, S12, S13, S22 | S23, S33, Sb, Sq | unused
             S part[16];
 #pragma unroll
             for (int i = 0; i < 16; ++i) part[i] = S(0);
-            for (uint32_t k = lane; k < vol; k += 32u) {
-                const uint32_t zz = (k * box.magic_wh) >> 20;
-                const uint32_t rem2 = k - zz * wh;
-                const uint32_t yy = (rem2 * box.magic_w) >> 20;
-                const uint32_t xx = rem2 - yy * w;
-                const uint32_t pv = base + (zz * T + yy) * T + xx;
-                const VoxelSample<S> sm = s_vox[pv];
-                S v = sm.v;
-                const S vv = kVar ? s_vv[pv] : S(0);
-                S wgt, d1, d2, d3;
+            for (uint32_t r0 = 0; r0 < rows; r0 += 32u) {
+                const uint32_t row = r0 + lane;
+                const bool valid = row < rows;
+                const uint32_t zz = valid ? (row * box.magic_h) >> 16 : 0u;
+                const uint32_t yy = valid ? row - zz * h : 0u;
+                const uint32_t p0 = ((z0 + zz) * T + (y0 + yy)) * T + x0;
+                const S py = static_cast<S>(oy + y0 + yy) + static_cast<S>(0.5);
+                const S pz = static_cast<S>(oz + z0 + zz) + static_cast<S>(0.5);
+                S d2, d3, K, L;
                 if (!kBeta) {
-                    d1 = sm.x - r.x;
-                    d2 = sm.y - r.y;
-                    d3 = sm.z - r.z;
-                    const S sigma = static_cast<S>(0.5) * (a * d1 * d1 + bb * d2 * d2 + c * d3 * d3) +
-                                    p * d1 * d2 + q * d1 * d3 + rr * d2 * d3;
-                    const S vis_raw = exp(-sigma);
-                    const S alpha_raw = opac * vis_raw;
-                    const bool keep = !(sigma < static_cast<S>(0) || fabs(alpha_raw) < static_cast<S>(1e-6));
-                    const S vis = keep ? vis_raw : S(0);
-                    const S alpha = keep ? alpha_raw : S(0);
-                    if (kVar) {
-                        part[11] += vv * alpha * alpha;
-                        v += static_cast<S>(2) * uq * alpha * vv;
-                    }
-                    wgt = -v * alpha;
-                    part[3] += v * vis;
+                    d2 = py - r.y;
+                    d3 = pz - r.z;
+                    K = static_cast<S>(0.5) * (bb * d2 * d2 + c * d3 * d3) + rr * d2 * d3;
+                    L = p * d2 + q * d3;
                 } else {
-                    d1 = r.x - sm.x;
-                    d2 = r.y - sm.y;
-                    d3 = r.z - sm.z;
-                    const S qf = a * d1 * d1 + bb * d2 * d2 + c * d3 * d3 + static_cast<S>(2) * p * d1 * d2 +
-                                 static_cast<S>(2) * q * d1 * d3 + static_cast<S>(2) * rr * d2 * d3;
-                    const S h_raw = static_cast<S>(1) - qf;
-                    const bool in_support = !(qf < static_cast<S>(0) || h_raw <= static_cast<S>(0));
-                    const S hh = in_support ? h_raw : S(1);  // keeps pow/log finite on skipped samples
-                    const S vis_raw = pow(hh, r.beta);
-                    const S alpha_raw = opac * vis_raw;
-                    const bool keep = in_support && !(fabs(alpha_raw) < static_cast<S>(1e-5));
-                    const S vis = keep ? vis_raw : S(0);
-                    const S alpha = keep ? alpha_raw : S(0);
-                    v = keep ? v : S(0);
-                    if (kVar) {
-                        part[11] += vv * alpha * alpha;
-                        v += static_cast<S>(2) * uq * alpha * vv;
-                    }
-                    wgt = -opac * r.beta * pow(hh, r.beta - static_cast<S>(1)) * v;
-                    part[3] += v * vis;
-                    part[10] += v * alpha * log(hh);
+                    d2 = r.y - py;
+                    d3 = r.z - pz;
+                    K = bb * d2 * d2 + c * d3 * d3 + static_cast<S>(2) * rr * d2 * d3;
+                    L = static_cast<S>(2) * (p * d2 + q * d3);
                 }
-                const S t1 = wgt * d1, t2 = wgt * d2, t3 = wgt * d3;
-                part[0] += t1;
-                part[1] += t2;
-                part[2] += t3;
-                part[4] += t1 * d1;
-                part[5] += t1 * d2;
-                part[6] += t1 * d3;
-                part[7] += t2 * d2;
-                part[8] += t2 * d3;
-                part[9] += t3 * d3;
+                S A0 = S(0), A1 = S(0), A2 = S(0), A3 = S(0), A4 = S(0), A5 = S(0);
+                S px = px0;
+                for (uint32_t i = 0; i < w; ++i, px += S(1)) {
+                    S v = valid ? s_v[p0 + i] : S(0);
+                    const S vv = (kVar && valid) ? s_vv[p0 + i] : S(0);
+                    S wgt, d1;
+                    if (!kBeta) {
+                        d1 = px - r.x;
+                        const S sigma = half_a * d1 * d1 + L * d1 + K;
+                        const S vis_raw = exp(-sigma);
+                        const S alpha_raw = opac * vis_raw;
+                        const bool keep =
+                            valid && !(sigma < static_cast<S>(0) || fabs(alpha_raw) < static_cast<S>(1e-6));
+                        const S vis = keep ? vis_raw : S(0);
+                        const S alpha = keep ? alpha_raw : S(0);
+                        if (kVar) {
+                            A4 += vv * alpha * alpha;
+                            v += static_cast<S>(2) * uq * alpha * vv;
+                        }
+                        wgt = -v * alpha;
+                        A3 += v * vis;
+                    } else {
+                        d1 = r.x - px;
+                        const S qf = a * d1 * d1 + L * d1 + K;
+                        const S h_raw = static_cast<S>(1) - qf;
+                        const bool in_support = valid && !(qf < static_cast<S>(0) || h_raw <= static_cast<S>(0));
+                        const S hh = in_support ? h_raw : S(1);  // keeps pow/log finite on skipped samples
+                        const S vis_raw = pow(hh, r.beta);
+                        const S alpha_raw = opac * vis_raw;
+                        const bool keep = in_support && !(fabs(alpha_raw) < static_cast<S>(1e-5));
+                        const S vis = keep ? vis_raw : S(0);
+                        const S alpha = keep ? alpha_raw : S(0);
+                        v = keep ? v : S(0);
+                        if (kVar) {
+                            A4 += vv * alpha * alpha;
+                            v += static_cast<S>(2) * uq * alpha * vv;
+                        }
+                        wgt = -opac * r.beta * pow(hh, r.beta - static_cast<S>(1)) * v;
+                        A3 += v * vis;
+                        A5 += v * alpha * log(hh);
+                    }
+                    const S wd = wgt * d1;
+                    A0 += wgt;
+                    A1 += wd;
+                    A2 += wd * d1;
+                }
+                part[0] += A1;
+                part[1] += d2 * A0;
+                part[2] += d3 * A0;
+                part[3] += A3;
+                part[4] += A2;
+                part[5] += d2 * A1;
+                part[6] += d3 * A1;
+                part[7] += d2 * d2 * A0;
+                part[8] += d2 * d3 * A0;
+                part[9] += d3 * d3 * A0;
+                part[10] += A5;
+                part[11] += A4;
             }
             // Recursive halving: 16 -> 8 (lane bit 4) -> 4 (bit 3) values, then
             // a butterfly over lane bits 2..0; lane group G = lane / 8 ends with
@@ -515,7 +532,7 @@ int launch_vbwd_p(const VoxelGeom& g, const Rec3D<S>* rec, bool chain_var, const
                   const int32_t* ids, const S* v_vol, const S* v_vol_var, Rec3D<S>* grads, cudaStream_t stream) {
     const size_t tile_voxels = size_t(g.T) * g.T * g.T;
     const size_t smem = 2 * size_t(kVoxBwdThreads) * (sizeof(Rec3D<S>) + sizeof(int32_t)) +
-                        size_t(kVoxBwdThreads) * sizeof(VoxelBox) + tile_voxels * (sizeof(VoxelSample<S>) + sizeof(S));
+                        size_t(kVoxBwdThreads) * sizeof(VoxelBox) + 2 * tile_voxels * sizeof(S);
     R2S_TRY(allow_dynamic_smem(voxel_bwd_kernel<S, kBeta, kVar>, smem));
     const unsigned grid = g.tiles_x * g.tiles_y * g.tiles_z;
     voxel_bwd_kernel<S, kBeta, kVar><<<grid, kVoxBwdThreads, smem, stream>>>(rec, chain_var, offsets, ids, g, v_vol,
