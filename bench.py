@@ -56,7 +56,7 @@ FLOPS_PER_EVAL = {
 }
 # DRAM bytes (read + write) of one record-parallel raster VJP launch at the CT
 # workload, from ncu (dram__bytes_read.sum + dram__bytes_write.sum, one pass).
-RASTER_VJP_TRAFFIC_BYTES = 569.04e6 + 374.12e6
+RASTER_VJP_TRAFFIC_BYTES = 569.6e6 + 371.2e6
 
 
 # --------------------------------------------------------------------------- utilities
