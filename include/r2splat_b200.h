@@ -443,6 +443,33 @@ int r2s_voxel_render_bwd_capacity(int dtype, const void* records, int beta, int 
                                   uint32_t dim1, uint32_t dim0, uint32_t tile_size, uint32_t tiles_x,
                                   uint32_t tiles_y, uint32_t tiles_z, void* grads, void* stream);
 
+/* ------------------------------------------ forward with fused image loss
+ * Replaces, in a fit step, the separate image-loss pass after
+ * rasterize_to_pixels_fwd (caller-side in examples/optimize.py; the L1 form is
+ * image_loss_l1_fwd/bwd, Loss.cpp:12-113, ImageLossFwd.cu:19-31,
+ * ImageLossBwd.cu:14-30). r2s_raster_render plus an epilogue: each pixel also
+ * writes v_render = d(loss)/d(render) for the mean loss over the C*H*W pixels
+ * and adds its term to a per-tile fp64 partial, summed in a fixed order:
+ *   R2S_IMAGE_LOSS_MSE: loss = lambda * mean((render - target)^2),
+ *                       v_render = (render - target) * (2 lambda / numel);
+ *   R2S_IMAGE_LOSS_L1:  loss = lambda * mean|render - target|,
+ *                       v_render = lambda * sign(render - target) / numel
+ *                       (image_loss_l1_bwd with grad_output = 1).
+ * loss_value = the mean without lambda. n_used, when non-NULL, overrides
+ * n_isects (capacity-bounded mode). Workspace:
+ * r2s_raster_image_loss_workspace(C, tiles_x, tiles_y). render must not
+ * alias target or v_render. */
+#define R2S_IMAGE_LOSS_MSE 0
+#define R2S_IMAGE_LOSS_L1 1
+size_t r2s_raster_image_loss_workspace(uint32_t C, uint32_t tiles_x, uint32_t tiles_y);
+int r2s_raster_render_image_loss(int dtype, const void* records, const void* uncertainties, int beta,
+                                 const int32_t* tile_offsets, const int32_t* flatten_ids, uint32_t n_isects,
+                                 const int64_t* n_used, uint32_t C, uint32_t N, uint32_t width, uint32_t height,
+                                 uint32_t tile_size, uint32_t tiles_x, uint32_t tiles_y, uint32_t stage_batch,
+                                 const void* target, int loss_kind, float lambda, void* render, void* render_var,
+                                 void* v_render, void* loss, void* loss_value, void* workspace,
+                                 size_t workspace_bytes, void* stream);
+
 /* Fused fit-loop update, no reference counterpart (the reference's example
  * loop, examples/optimize.py, does it with torch ops): sums two physical VJPs
  * grads_a/grads_b (each an array of 5 pointers: means [N,3], quats [N,4],

@@ -150,9 +150,38 @@ def raster_intersections(means, covars, densities, beta, ratio, viewmats, Ks, wi
     return records, offsets, isect_ids, flatten_ids, m, rects
 
 
+IMAGE_LOSS_KINDS = {"mse": 0, "l1": 1}  # R2S_IMAGE_LOSS_MSE, R2S_IMAGE_LOSS_L1
+
+
+def render_image_loss(records, uncertainty, beta: bool, offsets, flatten_ids, m, n, width, height, tile_size,
+                      target, kind, weight, image, variance, device):
+    """Tile forward with the fused image-loss epilogue; returns (v_image, loss, loss_value).
+
+    ``records`` and ``flatten_ids`` may be None when ``m`` is 0 (no
+    intersections): the epilogue then sees an all-zero image.
+    """
+    c = target.shape[0]
+    tx = (width + tile_size - 1) // tile_size
+    ty = (height + tile_size - 1) // tile_size
+    lib = _backend.library()
+    ws = _ws(int(lib.r2s_raster_image_loss_workspace(c, tx, ty)), device)
+    v_image = torch.empty_like(target)
+    loss = target.new_empty(())
+    value = target.new_empty(())
+    _backend.call("r2s_raster_render_image_loss", _dtype(target), _ptr(records), _ptr(uncertainty), int(beta),
+                  _ptr(offsets), _ptr(flatten_ids), m, None, c, n, width, height, tile_size, tx, ty, 0,
+                  _ptr(target), IMAGE_LOSS_KINDS[kind], float(weight), _ptr(image), _ptr(variance), _ptr(v_image),
+                  _ptr(loss), _ptr(value), _ptr(ws), ws.numel(), _stream(device))
+    return v_image, loss, value
+
+
 def raster_forward(means, quats, scales, densities, viewmats, Ks, width, height, beta, uncertainty, eps,
-                   radius_clip, tile_size=RASTER_TILE):
-    """Explicit projection forward; returns (image or (image, variance), RasterState)."""
+                   radius_clip, tile_size=RASTER_TILE, image_loss=None):
+    """Explicit projection forward; returns (image or (image, variance), RasterState).
+
+    With ``image_loss = (target, kind, weight)`` the tile kernel also writes the
+    loss gradient; the return is then (output, state, (v_image, loss, loss_value)).
+    """
     device = means.device
     c = viewmats.shape[0]
     covars, _ = low.parameter_transform_fwd(quats, scales)
@@ -163,14 +192,23 @@ def raster_forward(means, quats, scales, densities, viewmats, Ks, width, height,
     variance = torch.empty_like(image) if uncertainty is not None else None
     tx = (width + tile_size - 1) // tile_size
     ty = (height + tile_size - 1) // tile_size
+    loss_out = None
     with _stage("raster_render"):
-        _backend.call("r2s_raster_render", _dtype(means), _ptr(records), _ptr(uncertainty), int(beta is not None),
-                      _ptr(offsets), _ptr(flatten_ids), c, means.shape[0], m, width, height, tile_size, tx, ty,
-                      _ptr(image), _ptr(variance), _stream(device))
+        if image_loss is None:
+            _backend.call("r2s_raster_render", _dtype(means), _ptr(records), _ptr(uncertainty),
+                          int(beta is not None), _ptr(offsets), _ptr(flatten_ids), c, means.shape[0], m, width,
+                          height, tile_size, tx, ty, _ptr(image), _ptr(variance), _stream(device))
+        else:
+            target, kind, weight = image_loss
+            loss_out = render_image_loss(records, uncertainty, beta is not None, offsets, flatten_ids, m,
+                                         means.shape[0], width, height, tile_size, target, kind, weight, image,
+                                         variance, device)
     state = RasterState(covars, records, offsets, isect_ids, flatten_ids, ratio, m, width, height, tile_size,
                         extra={"rects": rects})
     output = image if uncertainty is None else (image, variance)
-    return output, state
+    if image_loss is None:
+        return output, state
+    return output, state, loss_out
 
 
 def raster_vjp_state(means, quats, scales, densities, viewmats, Ks, width, height, beta, eps, radius_clip,

@@ -11,7 +11,8 @@ A ``FitScene`` owns one reconstruction on the device:
 synchronisation:
 * raster forward (parameter transform, projection, capacity-bounded intersection lists,
   tile accumulation);
-* the MSE image gradient ``2 (image - target) / numel``;
+* the MSE image loss and its gradient ``2 (image - target) / numel``, written by
+  the forward's tile kernel (fused epilogue);
 * the record-parallel raster VJP and its chain rule;
 * voxel forward, TV loss forward and backward, the voxel VJP and its chain rule;
 * the fused activation-chain + Adam update.
@@ -135,6 +136,9 @@ class FitScene:
         self.n_used = torch.zeros(1, dtype=torch.int64, device=dev)
         self.image = torch.empty((c, self.height, self.width), dtype=dt, device=dev)
         self.v_image = torch.empty_like(self.image)
+        self.image_loss = torch.empty(1, dtype=dt, device=dev)
+        self.image_loss_value = torch.empty(1, dtype=dt, device=dev)
+        self.image_loss_ws = _ws(lib.r2s_raster_image_loss_workspace(c, self.tx, self.ty), dev)
         self.grads2d = torch.empty((c, n, 8), dtype=dt, device=dev)
         self.g_raster = [torch.empty((n, 3), dtype=dt, device=dev), torch.empty((n, 4), dtype=dt, device=dev),
                          torch.empty((n, 3), dtype=dt, device=dev), torch.empty((n,), dtype=dt, device=dev),
@@ -219,11 +223,12 @@ class FitScene:
             _backend.call("r2s_raster_emit_capacity", _p(self.rects), self.c, self.n, self.tx, self.ty, _p(self.cum),
                           self.capacity_2d, _p(self.n_used), _p(self.overflow), _p(self.isect_ids),
                           _p(self.flatten_ids), _p(self.offsets), _p(self.emit_ws), self.emit_ws.numel(), s)
-            _backend.call("r2s_raster_render_capacity", d, _p(self.records), None, beta_flag, _p(self.offsets),
-                          _p(self.flatten_ids), _p(self.n_used), self.c, self.n, self.width, self.height,
-                          self.cfg.tile, self.tx, self.ty, self.cfg.stage_batch, _p(self.image), None, s)
-            torch.sub(self.image, self.target, out=self.v_image)
-            self.v_image.mul_(2.0 / self.image.numel())
+            # Tile forward with the MSE image loss and its gradient in the epilogue.
+            _backend.call("r2s_raster_render_image_loss", d, _p(self.records), None, beta_flag, _p(self.offsets),
+                          _p(self.flatten_ids), 0, _p(self.n_used), self.c, self.n, self.width, self.height,
+                          self.cfg.tile, self.tx, self.ty, self.cfg.stage_batch, _p(self.target), 0, 1.0,
+                          _p(self.image), None, _p(self.v_image), _p(self.image_loss), _p(self.image_loss_value),
+                          _p(self.image_loss_ws), self.image_loss_ws.numel(), s)
             _backend.call("r2s_raster_record_bwd", d, _p(self.records), _p(self.rects), None, beta_flag, 0,
                           _p(self.v_image), None, self.c, self.n, self.width, self.height, self.cfg.tile,
                           _p(self.grads2d), None, None, s)
@@ -258,8 +263,7 @@ class FitScene:
                           float(self.cfg.eps), _p(self.grads3d), _p(v[0]), _p(v[1]), _p(v[2]), _p(v[3]), _p(v[4]),
                           None, s)
             # Loss (image MSE + lambda TV), then the update unless this step overflowed.
-            torch.add(torch.sum(self.v_image * self.v_image) * (self.image.numel() / 4.0), self.tv_loss,
-                      out=self.loss)
+            torch.add(self.image_loss, self.tv_loss, out=self.loss)
             grads_a = (ctypes.c_void_p * 5)(*[None if t is None else t.data_ptr() for t in self.g_raster])
             grads_b = (ctypes.c_void_p * 5)(*[None if t is None else t.data_ptr() for t in self.g_voxel])
             self._grad_tables = (grads_a, grads_b)  # kept alive for the captured call's duration

@@ -202,4 +202,8 @@ struct alignas(16) Rec3D {
     S x, y, z, o, c00, c01, c02, c11, c12, c22, beta, q, pad0, pad1, pad2, pad3;
 };
 
+// Defined in loss.cu: fixed-order sum of fp64 partials into a mean and lambda * mean.
+int launch_finish_mean(int dtype, const double* partials, int n_partials, int64_t count, float lambda, void* loss,
+                       void* value, cudaStream_t stream);
+
 }  // namespace r2s

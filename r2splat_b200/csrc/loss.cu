@@ -159,6 +159,17 @@ inline unsigned loss_blocks(int64_t total) {
     return unsigned(b);
 }
 
+// Sums `n_partials` fp64 partials in a fixed order into value = sum / count and
+// loss = lambda * value; shared with the forward's fused image-loss epilogue.
+int launch_finish_mean(int dtype, const double* partials, int n_partials, int64_t count, float lambda, void* loss,
+                       void* value, cudaStream_t stream) {
+    R2S_DISPATCH(dtype, {
+        finish_mean_kernel<S><<<1, kLossThreads, 0, stream>>>(partials, n_partials, count, lambda,
+                                                             static_cast<S*>(loss), static_cast<S*>(value));
+        return check_launch("loss_finish");
+    });
+}
+
 }  // namespace r2s
 
 using namespace r2s;

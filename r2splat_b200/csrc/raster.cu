@@ -132,13 +132,31 @@ constexpr uint32_t kBlockW = 8;      // one warp's pixel block in the forward: 8
 constexpr uint32_t kBlockH = 4;
 constexpr uint32_t kFwdBatch = 256;  // records staged per batch (at most)
 
+// Image-loss epilogue of the forward. With a target image, every pixel also
+// writes the gradient of the mean image loss with respect to the rendered value
+// and adds its loss term to its CTA's partial sum (fp64, fixed order):
+//   mse: v = (img - tgt) * scale with scale = 2 / numel (as torch computes
+//        `(img - tgt).mul_(2 / numel)`), term (img - tgt)^2;
+//   l1:  v = lambda * sign(img - tgt) / numel, the reference's L1 gradient with
+//        an upstream gradient of one (ImageLossBwd.cu:14-30), term |img - tgt|
+//        (ImageLossFwd.cu:19-31).
+template <typename S>
+struct ImageLossEpilogue {
+    const S* target = nullptr;   // [C, H, W]; null: no epilogue
+    S* v_render = nullptr;       // [C, H, W]
+    double* partials = nullptr;  // [C * n_tiles] per-tile loss sums
+    S scale = S(0);              // mse: 2 / numel; l1: lambda
+    S numel = S(1);              // l1: numel as S
+    uint32_t l1 = 0u;
+};
+
 template <typename S, bool kBeta, bool kVar, int kMaxThreads>
 __global__ void __launch_bounds__(kMaxThreads) raster_fwd_kernel(
     const Rec2D<S>* __restrict__ records, const S* __restrict__ uncertainties, uint32_t N,
     const int32_t* __restrict__ offsets, const int32_t* __restrict__ flatten_ids, int32_t n_isects,
     const int64_t* __restrict__ n_dev,
     uint32_t C, uint32_t width, uint32_t height, uint32_t T, uint32_t tiles_x, uint32_t n_tiles,
-    S* __restrict__ render, S* __restrict__ render_var, uint32_t B) {
+    S* __restrict__ render, S* __restrict__ render_var, uint32_t B, ImageLossEpilogue<S> loss) {
     extern __shared__ __align__(16) unsigned char smem[];  // B = records staged per batch (<= blockDim.x)
     Rec2D<S>* s_rec = reinterpret_cast<Rec2D<S>*>(smem);          // [2][B]
     S* s_q = reinterpret_cast<S*>(s_rec + 2 * B);                   // [2][B]
@@ -149,7 +167,10 @@ __global__ void __launch_bounds__(kMaxThreads) raster_fwd_kernel(
     const uint32_t key = cam * n_tiles + tile;
     const uint32_t ty = tile / tiles_x, tx = tile - ty * tiles_x;
     const uint32_t ox = tx * T, oy = ty * T;
-    if (ox >= width || oy >= height) return;
+    if (ox >= width || oy >= height) {
+        if (loss.target != nullptr && threadIdx.x == 0) loss.partials[key] = 0.0;
+        return;
+    }
     const uint32_t vx = min(T, width - ox), vy = min(T, height - oy);
     const int32_t start = offsets[key];
     // n_dev: the intersection count kept on the device (capacity-bounded pipelines).
@@ -244,10 +265,40 @@ __global__ void __launch_bounds__(kMaxThreads) raster_fwd_kernel(
         }
         __syncthreads();
     }
+    const size_t pid = size_t(cam) * height * width + size_t(oy + ly) * width + (ox + lx);
     if (inside) {
-        const size_t pid = size_t(cam) * height * width + size_t(oy + ly) * width + (ox + lx);
         render[pid] = acc;
         if (kVar) render_var[pid] = accv;
+    }
+    if (loss.target != nullptr) {
+        double term = 0.0;
+        if (inside) {
+            const S diff = acc - loss.target[pid];
+            S v;
+            if (loss.l1) {
+                const S sgn = diff > S(0) ? S(1) : (diff < S(0) ? S(-1) : S(0));
+                v = loss.scale * sgn / loss.numel;
+                term = fabs(static_cast<double>(diff));
+            } else {
+                v = diff * loss.scale;
+                term = static_cast<double>(diff) * static_cast<double>(diff);
+            }
+            loss.v_render[pid] = v;
+        }
+        // Fixed-order CTA sum: warp butterfly, then warp 0 over the warp sums.
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) term += __shfl_xor_sync(0xffffffffu, term, o);
+        double* s_sum = reinterpret_cast<double*>(s_hits);  // hit lists are no longer read
+        const uint32_t n_warps = blockDim.x >> 5;
+        __syncthreads();
+        if (lane == 0) s_sum[warp] = term;
+        __syncthreads();
+        if (warp == 0) {
+            double w = lane < n_warps ? s_sum[lane] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+            if (lane == 0) loss.partials[key] = w;
+        }
     }
 }
 
@@ -700,7 +751,7 @@ inline int check_geom(const RasterGeom& g) {
 
 template <typename S, bool kBeta, bool kVar>
 int launch_fwd_p(const RasterGeom& g, const Rec2D<S>* rec, const S* unc, const int32_t* offsets,
-                 const int32_t* ids, S* out, S* out_var, cudaStream_t stream) {
+                 const int32_t* ids, S* out, S* out_var, const ImageLossEpilogue<S>& loss, cudaStream_t stream) {
     // One warp per 8x4 block of the tile: at most 4 x 8 warps for 32x32 tiles.
     const uint32_t blocks = ((g.T + kBlockW - 1) / kBlockW) * ((g.T + kBlockH - 1) / kBlockH);
     const unsigned nthreads = 32u * blocks;
@@ -715,28 +766,29 @@ int launch_fwd_p(const RasterGeom& g, const Rec2D<S>* rec, const S* unc, const i
         R2S_TRY(allow_dynamic_smem(raster_fwd_kernel<S, kBeta, kVar, 256>, smem));
         raster_fwd_kernel<S, kBeta, kVar, 256><<<grid, nthreads, smem, stream>>>(
             rec, unc, g.N, offsets, ids, int32_t(g.n_isects), g.n_dev, g.C, g.width, g.height, g.T, g.tiles_x,
-            g.tiles_x * g.tiles_y, out, out_var, batch);
+            g.tiles_x * g.tiles_y, out, out_var, batch, loss);
     } else {
         R2S_TRY(allow_dynamic_smem(raster_fwd_kernel<S, kBeta, kVar, 1024>, smem));
         raster_fwd_kernel<S, kBeta, kVar, 1024><<<grid, nthreads, smem, stream>>>(
             rec, unc, g.N, offsets, ids, int32_t(g.n_isects), g.n_dev, g.C, g.width, g.height, g.T, g.tiles_x,
-            g.tiles_x * g.tiles_y, out, out_var, batch);
+            g.tiles_x * g.tiles_y, out, out_var, batch, loss);
     }
     return check_launch("rasterize_to_pixels_fwd");
 }
 
 template <typename S>
 int launch_fwd(const RasterGeom& g, const Rec2D<S>* rec, const S* unc, bool beta, const int32_t* offsets,
-               const int32_t* ids, S* out, S* out_var, cudaStream_t stream) {
+               const int32_t* ids, S* out, S* out_var, cudaStream_t stream,
+               const ImageLossEpilogue<S>& loss = ImageLossEpilogue<S>{}) {
     R2S_TRY(check_geom(g));
     if (g.tiles_x == 0 || g.tiles_y == 0 || g.C == 0) return R2S_OK;
     const bool var = out_var != nullptr;
     if (beta) {
-        return var ? launch_fwd_p<S, true, true>(g, rec, unc, offsets, ids, out, out_var, stream)
-                   : launch_fwd_p<S, true, false>(g, rec, unc, offsets, ids, out, out_var, stream);
+        return var ? launch_fwd_p<S, true, true>(g, rec, unc, offsets, ids, out, out_var, loss, stream)
+                   : launch_fwd_p<S, true, false>(g, rec, unc, offsets, ids, out, out_var, loss, stream);
     }
-    return var ? launch_fwd_p<S, false, true>(g, rec, unc, offsets, ids, out, out_var, stream)
-               : launch_fwd_p<S, false, false>(g, rec, unc, offsets, ids, out, out_var, stream);
+    return var ? launch_fwd_p<S, false, true>(g, rec, unc, offsets, ids, out, out_var, loss, stream)
+               : launch_fwd_p<S, false, false>(g, rec, unc, offsets, ids, out, out_var, loss, stream);
 }
 
 template <typename S, bool kBeta, bool kVar, bool kAbs>
@@ -1029,6 +1081,51 @@ int r2s_raster_render_capacity(int dtype, const void* records, const void* uncer
                                              static_cast<const S*>(uncertainties), beta != 0, tile_offsets,
                                              flatten_ids, static_cast<S*>(render), static_cast<S*>(render_var),
                                              as_stream(stream)));
+}
+
+size_t r2s_raster_image_loss_workspace(uint32_t C, uint32_t tiles_x, uint32_t tiles_y) {
+    ArenaSize a;
+    a.take<double>(size_t(C) * tiles_x * tiles_y);
+    return a.bytes();
+}
+
+int r2s_raster_render_image_loss(int dtype, const void* records, const void* uncertainties, int beta,
+                                 const int32_t* tile_offsets, const int32_t* flatten_ids, uint32_t n_isects,
+                                 const int64_t* n_used, uint32_t C, uint32_t N, uint32_t width, uint32_t height,
+                                 uint32_t tile_size, uint32_t tiles_x, uint32_t tiles_y, uint32_t stage_batch,
+                                 const void* target, int loss_kind, float lambda, void* render, void* render_var,
+                                 void* v_render, void* loss, void* loss_value, void* workspace,
+                                 size_t workspace_bytes, void* stream) {
+    R2S_REQUIRE(loss_kind == R2S_IMAGE_LOSS_MSE || loss_kind == R2S_IMAGE_LOSS_L1, R2S_ERR_ARGUMENT,
+                "loss_kind must be R2S_IMAGE_LOSS_MSE or R2S_IMAGE_LOSS_L1");
+    R2S_REQUIRE(target != nullptr && v_render != nullptr && loss != nullptr && loss_value != nullptr,
+                R2S_ERR_ARGUMENT, "target, v_render, loss and loss_value must be non-null");
+    RasterGeom g{C, N, n_isects, width, height, tile_size, tiles_x, tiles_y};
+    g.n_dev = n_used;
+    if (stage_batch != 0) g.stage_batch = stage_batch;
+    const uint64_t n_keys = uint64_t(C) * tiles_x * tiles_y;
+    R2S_REQUIRE(n_keys < (uint64_t(1) << 31), R2S_ERR_UNSUPPORTED, "too many tiles");
+    Arena arena(workspace, workspace_bytes);
+    double* partials = arena.take<double>(n_keys);
+    R2S_REQUIRE(partials || n_keys == 0, R2S_ERR_WORKSPACE, "image-loss workspace too small");
+    const int64_t numel = int64_t(C) * height * width;
+    cudaStream_t st = as_stream(stream);
+    R2S_DISPATCH(dtype, {
+        ImageLossEpilogue<S> ep;
+        ep.target = static_cast<const S*>(target);
+        ep.v_render = static_cast<S*>(v_render);
+        ep.partials = partials;
+        ep.l1 = loss_kind == R2S_IMAGE_LOSS_L1 ? 1u : 0u;
+        // mse: the factor torch applies in `(img - tgt).mul_(2 / numel)`, rounded to S once.
+        ep.scale = ep.l1 ? static_cast<S>(lambda)
+                         : static_cast<S>(2.0 * double(lambda) / double(numel > 0 ? numel : 1));
+        ep.numel = static_cast<S>(numel > 0 ? numel : 1);
+        R2S_TRY(launch_fwd<S>(g, static_cast<const Rec2D<S>*>(records), static_cast<const S*>(uncertainties),
+                              beta != 0, tile_offsets, flatten_ids, static_cast<S*>(render),
+                              static_cast<S*>(render_var), st, ep));
+        const bool launched = g.tiles_x != 0 && g.tiles_y != 0 && g.C != 0;
+        return launch_finish_mean(dtype, partials, launched ? int(n_keys) : 0, numel, lambda, loss, loss_value, st);
+    });
 }
 
 }  // extern "C"

@@ -93,6 +93,11 @@ SIGNATURES: dict[str, tuple] = {
     "r2s_voxel_render_capacity": (I32, [I32, P, I32, P, P, P, U32, U32, U32, U32, U32, U32, U32, U32, P, P, P]),
     "r2s_voxel_render_bwd_capacity": (I32, [I32, P, I32, I32, P, P, P, P, P, U32, U32, U32, U32, U32, U32, U32,
                                             U32, P, P]),
+    "r2s_raster_image_loss_workspace": (SZ, [U32, U32, U32]),
+    # dtype, records, unc, beta, offsets, ids, n_isects, n_used, C, N, W, H, tile, tiles_x, tiles_y, stage_batch,
+    # target, kind, lambda, render, render_var, v_render, loss, loss_value, workspace, bytes, stream
+    "r2s_raster_render_image_loss": (I32, [I32, P, P, I32, P, P, U32, P, U32, U32, U32, U32, U32, U32, U32, U32,
+                                           P, I32, F32, P, P, P, P, P, P, SZ, P]),
     "r2s_adam_activation_step": (I32, [I32, U32, P, P, P, P, P, P, P, P, P, P, P, P, F64, F64, F64, F64, P, P, P]),
     "r2s_scan_tile_counts_noalloc_max": (U64, []),
     "r2s_scan_tile_counts_noalloc": (I32, [P, U64, P, P]),

@@ -127,6 +127,59 @@ def rasterize_fwd(
     constant. Output is ``[C,height,width]`` or ``(image, variance)`` with
     uncertainty. No input needs requires_grad.
     """
+    return _rasterize_fwd(means, quats, scales, densities, viewmats, Ks, image_size, beta, uncertainty, eps,
+                          radius_clip, detach_variance, backward_mode, None)
+
+
+def rasterize_fwd_with_loss(
+    means: Tensor,
+    quats: Tensor,
+    scales: Tensor,
+    densities: Tensor,
+    viewmats: Tensor,
+    Ks: Tensor,
+    image_size: Sequence[int],
+    target: Tensor,
+    *,
+    loss: str = "mse",
+    loss_weight: float = 1.0,
+    beta: Optional[Tensor] = None,
+    uncertainty: Optional[Tensor] = None,
+    eps: float = 1.0e-8,
+    radius_clip: Optional[float] = None,
+    detach_variance: bool = False,
+    backward_mode: str = "primitive",
+) -> tuple[Output, _Context, Tensor, Tensor, Tensor]:
+    """``rasterize_fwd`` with the mean image loss against ``target`` fused into the tile kernel.
+
+    No reference counterpart: the reference's fit loop (examples/optimize.py)
+    computes the image loss and its gradient with separate passes after the
+    forward; its L1 form is ``image_loss_l1_fwd/bwd`` (Loss.cpp:12-113). Here
+    the tile kernel's epilogue writes them while the image is in registers.
+
+    ``target`` is ``[C,height,width]`` with the primitives' device and dtype.
+    ``loss`` is "mse" (``weight * mean((image - target)^2)``, gradient
+    ``(image - target) * (2 weight / numel)``) or "l1" (``weight * mean|image -
+    target|``, gradient ``weight * sign(image - target) / numel``, the
+    reference's L1 backward with an upstream gradient of one). The loss is on
+    the image only; with ``uncertainty`` the variance is returned as usual.
+
+    Returns ``(output, context, v_image, loss, loss_value)``: ``v_image`` is
+    the adjoint to pass to ``rasterize_bwd``; ``loss`` is the weighted mean
+    (0-dim) and ``loss_value`` the unweighted one, both summed in fp64 in a
+    fixed order.
+    """
+    if loss not in _fused.IMAGE_LOSS_KINDS:
+        raise ValueError('loss must be "mse" or "l1"')
+    weight = float(loss_weight)
+    if not (weight == weight and abs(weight) != float("inf")):
+        raise ValueError("loss_weight must be finite")
+    return _rasterize_fwd(means, quats, scales, densities, viewmats, Ks, image_size, beta, uncertainty, eps,
+                          radius_clip, detach_variance, backward_mode, (target, loss, weight))
+
+
+def _rasterize_fwd(means, quats, scales, densities, viewmats, Ks, image_size, beta, uncertainty, eps, radius_clip,
+                   detach_variance, backward_mode, image_loss):
     originals = list(zip(
         ("means", "quats", "scales", "densities", "viewmats", "Ks", "beta", "uncertainty"),
         (means, quats, scales, densities, viewmats, Ks, beta, uncertainty),
@@ -153,19 +206,37 @@ def rasterize_fwd(
         _value_check(Ks, FOCAL, ValueError, "Ks must have positive fx and fy")
         _value_check(Ks, PINHOLE, ValueError, "Ks must be pinhole intrinsics with zero skew and last row [0, 0, 1]")
         _value_check(viewmats, HOMOGENEOUS_ROW, ValueError, "viewmats must have homogeneous last row [0, 0, 0, 1]")
+        if image_loss is not None:
+            target = _constant("target", _tensor("target", image_loss[0], (cameras, height, width), means))
+            image_loss = (target,) + tuple(image_loss[1:])
     shape = (cameras, height, width)
     buffers = {"viewmats": viewmats, "Ks": Ks}
+    loss_out = None
     if means.shape[0] == 0:
         image = means.new_zeros(shape)
         output = image if uncertainty is None else (image, image.clone())
+        if image_loss is not None:
+            # No primitives, no intersections: every tile list is empty.
+            tile = _fused.RASTER_TILE
+            offsets = torch.zeros((cameras * ((height + tile - 1) // tile) * ((width + tile - 1) // tile),),
+                                  dtype=torch.int32, device=means.device)
+            with torch.cuda.device(means.device):
+                loss_out = _fused.render_image_loss(None, None, False, offsets, None, 0, 1, width, height, tile,
+                                                    image_loss[0], image_loss[1], image_loss[2], image, None,
+                                                    means.device)
     else:
         with torch.cuda.device(means.device):
-            output, state = _fused.raster_forward(means, quats, scales, densities, viewmats, Ks, width, height,
-                                                  beta, uncertainty, eps, radius_clip)
+            result = _fused.raster_forward(means, quats, scales, densities, viewmats, Ks, width, height, beta,
+                                           uncertainty, eps, radius_clip, image_loss=image_loss)
+        output, state = result[0], result[1]
+        if image_loss is not None:
+            loss_out = result[2]
         buffers.update(state=state, covars=state.covars, records=state.records, offsets=state.offsets,
                        isect_ids=state.isect_ids, flatten_ids=state.flatten_ids, ratio=state.ratio)
     context = _context("rasterize", shape, primitives, buffers, originals, eps, mode, detach_variance)
-    return output, context
+    if image_loss is None:
+        return output, context
+    return (output, context) + tuple(loss_out)
 
 
 @torch.no_grad()
@@ -268,4 +339,6 @@ def voxelize_bwd(context: _Context, v_volume: Optional[Tensor], v_variance: Opti
     return _consume(context, ParameterGradients(*grads))
 
 
+# rasterize_fwd_with_loss is an extension outside the reference's surface: it is
+# reached as r2splat_b200.explicit.rasterize_fwd_with_loss and not re-exported.
 __all__ = ["ParameterGradients", "rasterize_fwd", "rasterize_bwd", "voxelize_fwd", "voxelize_bwd"]

@@ -82,10 +82,9 @@ class ServeStats:
 def lean_step(scene: batched.FitScene):
     """One fit step through the explicit API with transient buffers, then the fused update."""
     cfg = scene.cfg
-    image, ctx = explicit.rasterize_fwd(scene.means, scene.quats, scene.scales, scene.densities, scene.viewmats,
-                                        scene.Ks, cfg.image_size, beta=scene.beta, eps=cfg.eps,
-                                        radius_clip=cfg.radius_clip)
-    v_image = (image - scene.target).mul_(2.0 / image.numel())
+    _, ctx, v_image, image_loss, _ = explicit.rasterize_fwd_with_loss(
+        scene.means, scene.quats, scene.scales, scene.densities, scene.viewmats, scene.Ks, cfg.image_size,
+        scene.target, loss="mse", beta=scene.beta, eps=cfg.eps, radius_clip=cfg.radius_clip)
     g = explicit.rasterize_bwd(ctx, v_image)
     volume, vctx = explicit.voxelize_fwd(scene.means, scene.quats, scene.scales, scene.densities, cfg.volume_shape,
                                          volume_extent=cfg.volume_extent, volume_center=cfg.volume_center,
@@ -94,7 +93,7 @@ def lean_step(scene: batched.FitScene):
     tv, _, _ = low.volume_loss_fwd(vol4, cfg.lambda_tv)
     g_vol = low.volume_loss_bwd(vol4, scene.ones, cfg.lambda_tv)[0]
     gv = explicit.voxelize_bwd(vctx, g_vol)
-    torch.add(torch.sum(v_image * v_image) * (image.numel() / 4.0), tv.reshape(1), out=scene.loss)
+    torch.add(image_loss.reshape(1), tv.reshape(1), out=scene.loss)
     ga = (ctypes.c_void_p * 5)(*[None if t is None else t.data_ptr() for t in (g.means, g.quats, g.scales,
                                                                                g.densities, g.beta)])
     gb = (ctypes.c_void_p * 5)(*[None if t is None else t.data_ptr() for t in (gv.means, gv.quats, gv.scales,

@@ -63,6 +63,10 @@ def test_fit_step_matches_explicit_api(device, beta):
     volume, vctx = r2s.voxelize_fwd(means, quats, scales, densities, cfg.volume_shape,
                                     volume_extent=cfg.volume_extent, beta=b)
     assert torch.equal(scene.volume, volume)
+    # The step's loss: MSE from the forward's fused epilogue plus lambda TV.
+    tv = low.volume_loss_fwd(volume.unsqueeze(0), cfg.lambda_tv)[0]
+    want = ((image.double() - scene.target.double()) ** 2).mean().item() + tv.item()
+    assert abs(scene.loss.item() - want) <= 1e-5 * want
     g_vol = low.volume_loss_bwd(volume.unsqueeze(0), torch.ones(1, device=device), cfg.lambda_tv)[0]
     gv = r2s.voxelize_bwd(vctx, g_vol)
     for mine, ref in zip(scene.g_voxel, (gv.means, gv.quats, gv.scales, gv.densities, gv.beta)):
