@@ -173,6 +173,21 @@ __device__ __forceinline__ void warp_sum8_pairs(const S (&v)[8], S& out0, S& out
     out1 = u[1];
 }
 
+// Packed FP32x2 arithmetic (sm_100 FADD2 / FMUL2 / FFMA2): one instruction
+// evaluates two independent samples, each component rounded like the scalar
+// operation (round to nearest even).
+__device__ __forceinline__ float2 splat2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
+// 1.0f when a > b, else 0.0f (also 0.0f when either is NaN), as one PTX set.
+__device__ __forceinline__ float gt_mask(float a, float b) {
+    float m;
+    asm("set.gt.f32.f32 %0, %1, %2;" : "=f"(m) : "f"(a), "f"(b));
+    return m;
+}
+
 // Raises a kernel's dynamic shared-memory limit when a launch needs more than
 // the default 48 KB.
 template <typename Kernel>

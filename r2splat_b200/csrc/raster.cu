@@ -28,6 +28,8 @@
 // decide which samples count, so alpha must round exactly as the reference's
 // does. Each thread evaluates one pixel per record, as in the reference's
 // one-pixel-per-thread loops, so the compiler contracts the same multiply-adds.
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace r2s {
@@ -552,6 +554,83 @@ __constant__ uint32_t c_div_magic[33] = {
     5958u,  5462u,  5042u,  4682u,  4370u,  4096u,  3856u,  3641u, 3450u, 3277u, 3121u,
     2979u,  2850u,  2731u,  2622u,  2521u,  2428u,  2341u,  2260u, 2185u, 2115u, 2048u};
 
+// -(log2 e): exp(-s) = 2^(-s log2 e).
+constexpr float kNegLog2e = -1.4426950408889634f;
+
+// The walk of one Gaussian record (no variance branch, no absgrad) in packed
+// FP32x2 form: each lane evaluates two samples per step, k and k + 32 of the
+// row-major box order (k = lane + 64 it), so one FADD2/FMUL2/FFMA2 serves both.
+// Pixel centres are stepped exactly in float (integers + 0.5); the pixel's
+// element offset py * width + px - (width + 1) / 2 is formed exactly in float
+// as well and read out through the 2^23 bias (valid while width * height <
+// 2^22). The six partial sums are those of vjp_sample (S0..S5), with the
+// quadratic form evaluated as dx (a/2 dx + b dy) + c/2 dy^2; the contribution
+// decisions (sigma < 0, |alpha| < 1e-5) are the reference's.
+__device__ __forceinline__ void record_walk_packed(const Rec2D<float>& r, float om, const float* vimg,
+                                                   uint32_t bx0, uint32_t by0, uint32_t bw, uint32_t barea,
+                                                   uint32_t magic, uint32_t width, float (&part)[8]) {
+    const uint32_t lane = threadIdx.x & 31u;
+    // (k * magic) >> 16 == k / bw for k <= 64 (magic = ceil(2^16 / bw)).
+    const uint32_t dq = (64u * magic) >> 16, dr = 64u - dq * bw;
+    const uint32_t ra = (lane * magic) >> 16, rb = ((lane + 32u) * magic) >> 16;
+    const uint32_t ca = lane - ra * bw, cb = lane + 32u - rb * bw;
+    float2 px = make_float2(static_cast<float>(bx0 + ca) + 0.5f, static_cast<float>(bx0 + cb) + 0.5f);
+    float2 py = make_float2(static_cast<float>(by0 + ra) + 0.5f, static_cast<float>(by0 + rb) + 0.5f);
+    const float x_end = static_cast<float>(bx0 + bw);
+    const float2 step_x = splat2(static_cast<float>(dr)), step_y = splat2(static_cast<float>(dq));
+    const float2 neg_bw = splat2(-static_cast<float>(bw));
+    const float2 fw = splat2(static_cast<float>(width));
+    // 2^23 - (width + 1) / 2: exact in float for width < 2^22.
+    const float2 bias = splat2(8388608.0f - 0.5f * static_cast<float>(width) - 0.5f);
+    const uint64_t vbase = reinterpret_cast<uint64_t>(vimg) - uint64_t(0x4B000000u) * sizeof(float);
+    const float2 nx = splat2(-r.x), ny = splat2(-r.y);
+    const float2 ha = splat2(0.5f * r.a), hb = splat2(r.b), hc = splat2(0.5f * r.c);
+    const float2 nom = splat2(-om), nl2e = splat2(kNegLog2e);
+    float2 acc0 = splat2(0.f), acc1 = acc0, acc2 = acc0, acc3 = acc0, acc4 = acc0, acc5 = acc0;
+    const uint32_t iters = (barea + 63u) >> 6;
+    uint32_t k = lane;
+    for (uint32_t it = 0; it < iters; ++it, k += 64u) {
+        const bool va = k < barea, vb = k + 32u < barea;
+        const float2 offb = add2(fma2(py, fw, px), bias);
+        const float* pa = reinterpret_cast<const float*>(vbase + uint64_t(__float_as_uint(offb.x)) * sizeof(float));
+        const float* pb = reinterpret_cast<const float*>(vbase + uint64_t(__float_as_uint(offb.y)) * sizeof(float));
+        const float ga = va ? __ldg(pa) : 0.f;
+        const float gb = vb ? __ldg(pb) : 0.f;
+        const float2 dx = add2(px, nx), dy = add2(py, ny);
+        const float2 t = fma2(ha, dx, mul2(hb, dy));
+        const float2 sigma = fma2(dx, t, mul2(mul2(hc, dy), dy));
+        const float2 e = mul2(sigma, nl2e);
+        const float2 vis = make_float2(exp2f(e.x), exp2f(e.y));
+        const float2 nalpha = mul2(nom, vis);  // -alpha
+        const bool ka = va && !(sigma.x < 0.f || fabsf(nalpha.x) < 1e-5f);
+        const bool kb = vb && !(sigma.y < 0.f || fabsf(nalpha.y) < 1e-5f);
+        const float2 g = make_float2(ka ? ga : 0.f, kb ? gb : 0.f);
+        const float2 w = mul2(g, nalpha);  // -g alpha
+        const float2 wx = mul2(w, dx), wy = mul2(w, dy);
+        acc0 = add2(acc0, wx);
+        acc1 = add2(acc1, wy);
+        acc2 = fma2(wx, dx, acc2);
+        acc3 = fma2(wx, dy, acc3);
+        acc4 = fma2(wy, dy, acc4);
+        acc5 = fma2(g, vis, acc5);
+        // Advance both samples by 64 box positions: dq rows and dr columns,
+        // plus one wrap where the column passes the box's width.
+        px = add2(px, step_x);
+        py = add2(py, step_y);
+        const float2 wrap = make_float2(gt_mask(px.x, x_end), gt_mask(px.y, x_end));
+        px = fma2(wrap, neg_bw, px);
+        py = add2(py, wrap);
+    }
+    part[0] = acc0.x + acc0.y;
+    part[1] = acc1.x + acc1.y;
+    part[2] = acc2.x + acc2.y;
+    part[3] = acc3.x + acc3.y;
+    part[4] = acc4.x + acc4.y;
+    part[5] = acc5.x + acc5.y;
+    part[6] = 0.f;
+    part[7] = 0.f;
+}
+
 template <typename S, bool kBeta, bool kVar, bool kAbs>
 __global__ void __launch_bounds__(kRecBwdThreads) raster_record_bwd_kernel(
     const Rec2D<S>* __restrict__ records, const ushort4* __restrict__ rects, const S* __restrict__ var_q,
@@ -563,6 +642,9 @@ __global__ void __launch_bounds__(kRecBwdThreads) raster_record_bwd_kernel(
     const size_t total = size_t(C) * N;
     const size_t group_stride = size_t(gridDim.x) * warps_per_block * 32u;
     const bool chain_var = kVar && var_q != nullptr;
+    // The packed two-samples-per-lane walk serves the plain Gaussian VJP.
+    constexpr bool kPacked = std::is_same<S, float>::value && !kBeta && !kVar && !kAbs;
+    const bool packed = kPacked && v_render != nullptr && uint64_t(width) * height < (uint64_t(1) << 22);
     // Each warp takes 32 consecutive records at a time. Lane-parallel set-up:
     // lane L loads record base + L (coalesced) and computes its pixel box and
     // stepping constants; the warp then walks the 32 records one by one,
@@ -571,7 +653,7 @@ __global__ void __launch_bounds__(kRecBwdThreads) raster_record_bwd_kernel(
          base += group_stride) {
         const size_t my_rid = base + lane;
         Rec2D<S> mine;
-        uint32_t x0 = 0u, y0 = 0u, w = 0u, area = 0u;
+        uint32_t x0 = 0u, y0 = 0u, w = 0u, area = 0u, magic = 0u;
         const uint32_t my_cam = uint32_t(my_rid) / N;  // C * N < 2^31
         S my_q = S(0);
         if (my_rid < total) {
@@ -590,6 +672,7 @@ __global__ void __launch_bounds__(kRecBwdThreads) raster_record_bwd_kernel(
             if (any) {
                 w = x1 - x0 + 1u;
                 area = w * (y1 - y0 + 1u);
+                if (kPacked) magic = (65536u + w - 1u) / w;
             } else {
                 // No pixel can contribute: the record's adjoints are zero.
                 S* dst = reinterpret_cast<S*>(grads + my_rid);
@@ -626,43 +709,53 @@ __global__ void __launch_bounds__(kRecBwdThreads) raster_record_bwd_kernel(
             const S* vvar = kVar ? v_render_var + cam_base : nullptr;
             const S q = chain_var ? __shfl_sync(0xffffffffu, my_q, j) : S(0);
             const S om = r.o * r.mu;
-            // Lane k of the box (row-major, width bw) starts at k = lane and
-            // steps by 32: dq rows and dr columns, plus one wrap when the
-            // column overflows.
-            uint32_t dq = 0u, dr = 32u, row = 0u, col = lane;
-            if (bw < 32u) {
-                const uint32_t m = c_div_magic[bw];
-                dq = (32u * m) >> 16;
-                dr = 32u - dq * bw;
-                row = (lane * m) >> 16;
-                col = lane - row * bw;
-            }
-            uint32_t off = (by0 + row) * width + bx0 + col;
-            const uint32_t step = dq * width + dr, wrap_step = width - bw;
-            S px = static_cast<S>(bx0 + col) + static_cast<S>(0.5);
-            S py = static_cast<S>(by0 + row) + static_cast<S>(0.5);
-            const S x_end = static_cast<S>(bx0 + bw);  // a centre past the row is >= x0 + w + 0.5
-            const S step_x = static_cast<S>(dr), step_y = static_cast<S>(dq), wrap_x = static_cast<S>(bw);
-            const uint32_t iters = (barea + 31u) >> 5;
             S part[8];
-#pragma unroll
-            for (int i = 0; i < 8; ++i) part[i] = S(0);
             S g_ax = S(0), g_ay = S(0);
-            // A warp-uniform trip count; lanes past the box end in the last step
-            // evaluate nothing (valid = false) and load nothing.
-            uint32_t k = lane;
-            for (uint32_t it = 0; it < iters; ++it, k += 32u) {
-                const bool valid = k < barea;
-                const S v = (valid && vimg != nullptr) ? vimg[off] : S(0);
-                const S vv = (kVar && valid) ? vvar[off] : S(0);
-                vjp_sample<S, kBeta, kVar, kAbs>(r, om, q, px, py, v, vv, valid, part, g_ax, g_ay);
-                px += step_x;
-                py += step_y;
-                off += step;
-                const bool wrap = px > x_end;
-                px = wrap ? px - wrap_x : px;
-                py = wrap ? py + static_cast<S>(1) : py;
-                off = wrap ? off + wrap_step : off;
+            bool walked = false;
+            if constexpr (kPacked) {
+                if (packed) {
+                    const uint32_t bmagic = __shfl_sync(0xffffffffu, magic, j);
+                    record_walk_packed(r, om, vimg, bx0, by0, bw, barea, bmagic, width, part);
+                    walked = true;
+                }
+            }
+            if (!walked) {
+                // Lane k of the box (row-major, width bw) starts at k = lane and
+                // steps by 32: dq rows and dr columns, plus one wrap when the
+                // column overflows.
+                uint32_t dq = 0u, dr = 32u, row = 0u, col = lane;
+                if (bw < 32u) {
+                    const uint32_t m = c_div_magic[bw];
+                    dq = (32u * m) >> 16;
+                    dr = 32u - dq * bw;
+                    row = (lane * m) >> 16;
+                    col = lane - row * bw;
+                }
+                uint32_t off = (by0 + row) * width + bx0 + col;
+                const uint32_t step = dq * width + dr, wrap_step = width - bw;
+                S px = static_cast<S>(bx0 + col) + static_cast<S>(0.5);
+                S py = static_cast<S>(by0 + row) + static_cast<S>(0.5);
+                const S x_end = static_cast<S>(bx0 + bw);  // a centre past the row is >= x0 + w + 0.5
+                const S step_x = static_cast<S>(dr), step_y = static_cast<S>(dq), wrap_x = static_cast<S>(bw);
+                const uint32_t iters = (barea + 31u) >> 5;
+#pragma unroll
+                for (int i = 0; i < 8; ++i) part[i] = S(0);
+                // A warp-uniform trip count; lanes past the box end in the last step
+                // evaluate nothing (valid = false) and load nothing.
+                uint32_t k = lane;
+                for (uint32_t it = 0; it < iters; ++it, k += 32u) {
+                    const bool valid = k < barea;
+                    const S v = (valid && vimg != nullptr) ? vimg[off] : S(0);
+                    const S vv = (kVar && valid) ? vvar[off] : S(0);
+                    vjp_sample<S, kBeta, kVar, kAbs>(r, om, q, px, py, v, vv, valid, part, g_ax, g_ay);
+                    px += step_x;
+                    py += step_y;
+                    off += step;
+                    const bool wrap = px > x_end;
+                    px = wrap ? px - wrap_x : px;
+                    py = wrap ? py + static_cast<S>(1) : py;
+                    off = wrap ? off + wrap_step : off;
+                }
             }
             S lo, hi;
             warp_sum8_pairs(part, lo, hi);
