@@ -13,6 +13,8 @@
 // :853-895) so the |alpha| thresholds (1e-6 Gaussian, 1e-5 Beta) select the
 // same samples. The tile size is a run-time value, so the compiler cannot
 // merge arithmetic across a thread's voxels.
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace r2s {
@@ -229,6 +231,9 @@ __device__ __forceinline__ VoxelBox voxel_box(const Rec3D<S>& r, uint32_t ox, ui
 // expression (by about an ulp); the VJP is held to a tolerance, and a
 // contribution-threshold decision that flips moves a gradient by one
 // threshold-sized sample at most.
+// -(log2 e): exp(-s) = 2^(-s log2 e).
+constexpr float kVoxNegLog2e = -1.4426950408889634f;
+
 template <typename S, bool kBeta, bool kVar>
 __global__ void __launch_bounds__(kVoxBwdThreads) voxel_bwd_kernel(
     const Rec3D<S>* __restrict__ records, bool chain_var, const int32_t* __restrict__ offsets,
@@ -257,6 +262,8 @@ __global__ void __launch_bounds__(kVoxBwdThreads) voxel_bwd_kernel(
     const int32_t count = end - start;
     if (count <= 0) return;
     const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+    // The plain Gaussian VJP walks its rows two voxels per packed step.
+    constexpr bool kPackedRow = std::is_same<S, float>::value && !kBeta && !kVar;
 
     for (uint32_t p = t; p < tile_voxels; p += kVoxBwdThreads) {
         const uint32_t lz = p / (T * T);
@@ -329,8 +336,42 @@ __global__ void __launch_bounds__(kVoxBwdThreads) voxel_bwd_kernel(
                     L = static_cast<S>(2) * (p * d2 + q * d3);
                 }
                 S A0 = S(0), A1 = S(0), A2 = S(0), A3 = S(0), A4 = S(0), A5 = S(0);
+                bool walked = false;
+                if constexpr (kPackedRow) {
+                    // Two voxels of the row per step (x and x + 1) in packed
+                    // FP32x2 form; sigma by Horner in d1.
+                    const float2 nx = splat2(-r.x), ha2 = splat2(half_a), l2 = splat2(L), k2 = splat2(K);
+                    const float2 nop = splat2(-opac), nl2e = splat2(kVoxNegLog2e), two = splat2(2.f);
+                    float2 px2 = make_float2(px0, px0 + 1.f);
+                    float2 a0 = splat2(0.f), a1 = a0, a2 = a0, a3 = a0;
+                    for (uint32_t i = 0; i < w; i += 2u) {
+                        const bool va = valid, vb = valid && i + 1u < w;
+                        const float ga = va ? s_v[p0 + i] : 0.f;
+                        const float gb = vb ? s_v[p0 + i + 1u] : 0.f;
+                        const float2 d1 = add2(px2, nx);
+                        const float2 sigma = fma2(fma2(ha2, d1, l2), d1, k2);
+                        const float2 e = mul2(sigma, nl2e);
+                        const float2 vis = make_float2(exp2f(e.x), exp2f(e.y));
+                        const float2 nalpha = mul2(nop, vis);  // -alpha
+                        const bool ka = va && !(sigma.x < 0.f || fabsf(nalpha.x) < 1e-6f);
+                        const bool kb = vb && !(sigma.y < 0.f || fabsf(nalpha.y) < 1e-6f);
+                        const float2 g2 = make_float2(ka ? ga : 0.f, kb ? gb : 0.f);
+                        const float2 wgt = mul2(g2, nalpha);  // -g alpha
+                        a3 = fma2(g2, vis, a3);
+                        const float2 wd = mul2(wgt, d1);
+                        a0 = add2(a0, wgt);
+                        a1 = add2(a1, wd);
+                        a2 = fma2(wd, d1, a2);
+                        px2 = add2(px2, two);
+                    }
+                    A0 = a0.x + a0.y;
+                    A1 = a1.x + a1.y;
+                    A2 = a2.x + a2.y;
+                    A3 = a3.x + a3.y;
+                    walked = true;
+                }
                 S px = px0;
-                for (uint32_t i = 0; i < w; ++i, px += S(1)) {
+                for (uint32_t i = 0; !walked && i < w; ++i, px += S(1)) {
                     S v = valid ? s_v[p0 + i] : S(0);
                     const S vv = (kVar && valid) ? s_vv[p0 + i] : S(0);
                     S wgt, d1;
