@@ -242,11 +242,15 @@ __global__ void __launch_bounds__(kVoxBwdThreads) voxel_bwd_kernel(
     extern __shared__ __align__(16) unsigned char smem[];
     const uint32_t T = g.T;
     const uint32_t tile_voxels = T * T * T;
+    // The tile's adjoints are stored by rows of T voxels at a stride of T + 1,
+    // so the lanes of a warp (one box row each) read distinct banks.
+    const uint32_t RS = T + 1u;
+    const uint32_t tile_slots = T * T * RS;
     Rec3D<S>* s_rec = reinterpret_cast<Rec3D<S>*>(smem);                          // [2][threads]
     VoxelBox* s_box = reinterpret_cast<VoxelBox*>(s_rec + 2 * kVoxBwdThreads);     // [threads]
-    S* s_v = reinterpret_cast<S*>(s_box + kVoxBwdThreads);                         // [T^3] adjoint
-    S* s_vv = s_v + tile_voxels;                                                   // [T^3] variance adjoint
-    int32_t* s_id = reinterpret_cast<int32_t*>(s_vv + tile_voxels);                // [2][threads]
+    S* s_v = reinterpret_cast<S*>(s_box + kVoxBwdThreads);                         // [T^2][T+1] adjoint
+    S* s_vv = s_v + tile_slots;                                                    // [T^2][T+1] variance adjoint
+    int32_t* s_id = reinterpret_cast<int32_t*>(s_vv + tile_slots);                 // [2][threads]
 
     const uint32_t n_tiles = g.tiles_x * g.tiles_y * g.tiles_z;
     const uint32_t key = blockIdx.x;
@@ -271,8 +275,9 @@ __global__ void __launch_bounds__(kVoxBwdThreads) voxel_bwd_kernel(
         const uint32_t ly = r2 / T, lx = r2 - ly * T;
         const bool ok = lx < vx && ly < vy && lz < vz;
         const size_t vid = (size_t(oz + lz) * g.dim1 + (oy + ly)) * g.dim2 + (ox + lx);
-        s_v[p] = (ok && v_volume != nullptr) ? v_volume[vid] : S(0);
-        if (kVar) s_vv[p] = ok ? v_volume_var[vid] : S(0);
+        const uint32_t slot = (lz * T + ly) * RS + lx;
+        s_v[slot] = (ok && v_volume != nullptr) ? v_volume[vid] : S(0);
+        if (kVar) s_vv[slot] = ok ? v_volume_var[vid] : S(0);
     }
 
     const int32_t n_batches = (count + kVoxBwdThreads - 1) / kVoxBwdThreads;
@@ -310,6 +315,9 @@ __global__ void __launch_bounds__(kVoxBwdThreads) voxel_bwd_kernel(
             const S opac = r.o;
             const S uq = chain_var ? r.q : S(0);
             const S half_a = static_cast<S>(0.5) * a;
+            // Packed rows: |alpha| < 1e-6 <=> 2^e < 1e-6 / |opac| <=> e < e_min.
+            float e_min = 0.f;
+            if constexpr (kPackedRow) e_min = log2f(1e-6f / fabsf(opac));
             const S px0 = static_cast<S>(ox + x0) + static_cast<S>(0.5);
             // part: S1, S2, S3, Svis | S11, S12, S13, S22 | S23, S33, Sb, Sq | unused
             S part[16];
@@ -320,7 +328,7 @@ __global__ void __launch_bounds__(kVoxBwdThreads) voxel_bwd_kernel(
                 const bool valid = row < rows;
                 const uint32_t zz = valid ? (row * box.magic_h) >> 16 : 0u;
                 const uint32_t yy = valid ? row - zz * h : 0u;
-                const uint32_t p0 = ((z0 + zz) * T + (y0 + yy)) * T + x0;
+                const uint32_t p0 = ((z0 + zz) * T + (y0 + yy)) * RS + x0;
                 const S py = static_cast<S>(oy + y0 + yy) + static_cast<S>(0.5);
                 const S pz = static_cast<S>(oz + z0 + zz) + static_cast<S>(0.5);
                 S d2, d3, K, L;
@@ -339,35 +347,33 @@ __global__ void __launch_bounds__(kVoxBwdThreads) voxel_bwd_kernel(
                 bool walked = false;
                 if constexpr (kPackedRow) {
                     // Two voxels of the row per step (x and x + 1) in packed
-                    // FP32x2 form; sigma by Horner in d1.
-                    const float2 nx = splat2(-r.x), ha2 = splat2(half_a), l2 = splat2(L), k2 = splat2(K);
-                    const float2 nop = splat2(-opac), nl2e = splat2(kVoxNegLog2e), two = splat2(2.f);
-                    float2 px2 = make_float2(px0, px0 + 1.f);
-                    float2 a0 = splat2(0.f), a1 = a0, a2 = a0, a3 = a0;
+                    // FP32x2 form. The exponent e = -sigma log2(e) comes from
+                    // prescaled coefficients by Horner in d1, so vis = 2^e; a
+                    // sample counts when e <= 0 (sigma >= 0) and e >= e_min
+                    // (|alpha| >= 1e-6). With w = -g alpha = -opac g vis, the
+                    // row sums carry g vis and are scaled by -opac once per row.
+                    const float2 qa = splat2(half_a * kVoxNegLog2e), ql = splat2(L * kVoxNegLog2e);
+                    const float2 qk = splat2(K * kVoxNegLog2e), two = splat2(2.f);
+                    float2 d1 = make_float2(px0 - r.x, px0 + 1.f - r.x);
+                    float2 a1 = splat2(0.f), a2 = a1, a3 = a1;
                     for (uint32_t i = 0; i < w; i += 2u) {
-                        const bool va = valid, vb = valid && i + 1u < w;
-                        const float ga = va ? s_v[p0 + i] : 0.f;
-                        const float gb = vb ? s_v[p0 + i + 1u] : 0.f;
-                        const float2 d1 = add2(px2, nx);
-                        const float2 sigma = fma2(fma2(ha2, d1, l2), d1, k2);
-                        const float2 e = mul2(sigma, nl2e);
+                        const float ga = valid ? s_v[p0 + i] : 0.f;
+                        const float gb = (valid && i + 1u < w) ? s_v[p0 + i + 1u] : 0.f;
+                        const float2 e = fma2(fma2(qa, d1, ql), d1, qk);
                         const float2 vis = make_float2(exp2f(e.x), exp2f(e.y));
-                        const float2 nalpha = mul2(nop, vis);  // -alpha
-                        const bool ka = va && !(sigma.x < 0.f || fabsf(nalpha.x) < 1e-6f);
-                        const bool kb = vb && !(sigma.y < 0.f || fabsf(nalpha.y) < 1e-6f);
-                        const float2 g2 = make_float2(ka ? ga : 0.f, kb ? gb : 0.f);
-                        const float2 wgt = mul2(g2, nalpha);  // -g alpha
-                        a3 = fma2(g2, vis, a3);
-                        const float2 wd = mul2(wgt, d1);
-                        a0 = add2(a0, wgt);
-                        a1 = add2(a1, wd);
-                        a2 = fma2(wd, d1, a2);
-                        px2 = add2(px2, two);
+                        const bool ka = !(e.x > 0.f || e.x < e_min);
+                        const bool kb = !(e.y > 0.f || e.y < e_min);
+                        const float2 gv = mul2(make_float2(ka ? ga : 0.f, kb ? gb : 0.f), vis);
+                        a3 = add2(a3, gv);
+                        const float2 gvd = mul2(gv, d1);
+                        a1 = add2(a1, gvd);
+                        a2 = fma2(gvd, d1, a2);
+                        d1 = add2(d1, two);
                     }
-                    A0 = a0.x + a0.y;
-                    A1 = a1.x + a1.y;
-                    A2 = a2.x + a2.y;
                     A3 = a3.x + a3.y;
+                    A0 = -opac * A3;
+                    A1 = -opac * (a1.x + a1.y);
+                    A2 = -opac * (a2.x + a2.y);
                     walked = true;
                 }
                 S px = px0;
@@ -571,9 +577,9 @@ int launch_vfwd(const VoxelGeom& g, const Rec3D<S>* rec, bool beta, const int32_
 template <typename S, bool kBeta, bool kVar>
 int launch_vbwd_p(const VoxelGeom& g, const Rec3D<S>* rec, bool chain_var, const int32_t* offsets,
                   const int32_t* ids, const S* v_vol, const S* v_vol_var, Rec3D<S>* grads, cudaStream_t stream) {
-    const size_t tile_voxels = size_t(g.T) * g.T * g.T;
+    const size_t tile_slots = size_t(g.T) * g.T * (g.T + 1);
     const size_t smem = 2 * size_t(kVoxBwdThreads) * (sizeof(Rec3D<S>) + sizeof(int32_t)) +
-                        size_t(kVoxBwdThreads) * sizeof(VoxelBox) + 2 * tile_voxels * sizeof(S);
+                        size_t(kVoxBwdThreads) * sizeof(VoxelBox) + 2 * tile_slots * sizeof(S);
     R2S_TRY(allow_dynamic_smem(voxel_bwd_kernel<S, kBeta, kVar>, smem));
     const unsigned grid = g.tiles_x * g.tiles_y * g.tiles_z;
     voxel_bwd_kernel<S, kBeta, kVar><<<grid, kVoxBwdThreads, smem, stream>>>(rec, chain_var, offsets, ids, g, v_vol,
