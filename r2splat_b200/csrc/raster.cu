@@ -563,9 +563,13 @@ constexpr float kNegLog2e = -1.4426950408889634f;
 // Pixel centres are stepped exactly in float (integers + 0.5); the pixel's
 // element offset py * width + px - (width + 1) / 2 is formed exactly in float
 // as well and read out through the 2^23 bias (valid while width * height <
-// 2^22). The six partial sums are those of vjp_sample (S0..S5), with the
-// quadratic form evaluated as dx (a/2 dx + b dy) + c/2 dy^2; the contribution
-// decisions (sigma < 0, |alpha| < 1e-5) are the reference's.
+// 2^22). The exponent e = -sigma log2(e) is evaluated from prescaled conic
+// coefficients as dx (a' dx + b' dy) + c' dy^2, so vis = 2^e. A sample counts
+// when e <= 0 (sigma >= 0) and e >= e_min, e_min = log2(1e-5 / |o mu|)
+// (|alpha| >= 1e-5): the reference's two decisions, taken on the exponent.
+// With w = -g alpha = -(o mu) g vis, the walk sums g vis and its moments and
+// scales them by -(o mu) once: part[0..4] are S0..S4 and part[5] = S5 of
+// vjp_sample.
 __device__ __forceinline__ void record_walk_packed(const Rec2D<float>& r, float om, const float* vimg,
                                                    uint32_t bx0, uint32_t by0, uint32_t bw, uint32_t barea,
                                                    uint32_t magic, uint32_t width, float (&part)[8]) {
@@ -584,35 +588,34 @@ __device__ __forceinline__ void record_walk_packed(const Rec2D<float>& r, float 
     const float2 bias = splat2(8388608.0f - 0.5f * static_cast<float>(width) - 0.5f);
     const uint64_t vbase = reinterpret_cast<uint64_t>(vimg) - uint64_t(0x4B000000u) * sizeof(float);
     const float2 nx = splat2(-r.x), ny = splat2(-r.y);
-    const float2 ha = splat2(0.5f * r.a), hb = splat2(r.b), hc = splat2(0.5f * r.c);
-    const float2 nom = splat2(-om), nl2e = splat2(kNegLog2e);
+    const float2 qa = splat2(0.5f * r.a * kNegLog2e), qb = splat2(r.b * kNegLog2e);
+    const float2 qc = splat2(0.5f * r.c * kNegLog2e);
+    const float e_min = log2f(1e-5f / fabsf(om));
     float2 acc0 = splat2(0.f), acc1 = acc0, acc2 = acc0, acc3 = acc0, acc4 = acc0, acc5 = acc0;
     const uint32_t iters = (barea + 63u) >> 6;
     uint32_t k = lane;
     for (uint32_t it = 0; it < iters; ++it, k += 64u) {
-        const bool va = k < barea, vb = k + 32u < barea;
         const float2 offb = add2(fma2(py, fw, px), bias);
         const float* pa = reinterpret_cast<const float*>(vbase + uint64_t(__float_as_uint(offb.x)) * sizeof(float));
         const float* pb = reinterpret_cast<const float*>(vbase + uint64_t(__float_as_uint(offb.y)) * sizeof(float));
-        const float ga = va ? __ldg(pa) : 0.f;
-        const float gb = vb ? __ldg(pb) : 0.f;
+        const float ga = k < barea ? __ldg(pa) : 0.f;
+        const float gb = k + 32u < barea ? __ldg(pb) : 0.f;
         const float2 dx = add2(px, nx), dy = add2(py, ny);
-        const float2 t = fma2(ha, dx, mul2(hb, dy));
-        const float2 sigma = fma2(dx, t, mul2(mul2(hc, dy), dy));
-        const float2 e = mul2(sigma, nl2e);
+        const float2 t = fma2(qa, dx, mul2(qb, dy));
+        const float2 e = fma2(dx, t, mul2(mul2(qc, dy), dy));
         const float2 vis = make_float2(exp2f(e.x), exp2f(e.y));
-        const float2 nalpha = mul2(nom, vis);  // -alpha
-        const bool ka = va && !(sigma.x < 0.f || fabsf(nalpha.x) < 1e-5f);
-        const bool kb = vb && !(sigma.y < 0.f || fabsf(nalpha.y) < 1e-5f);
-        const float2 g = make_float2(ka ? ga : 0.f, kb ? gb : 0.f);
-        const float2 w = mul2(g, nalpha);  // -g alpha
-        const float2 wx = mul2(w, dx), wy = mul2(w, dy);
+        const bool ka = !(e.x > 0.f || e.x < e_min);
+        const bool kb = !(e.y > 0.f || e.y < e_min);
+        // Select after the product: a skipped sample may have vis = inf (e > 0).
+        const float2 gvr = mul2(make_float2(ga, gb), vis);
+        const float2 gv = make_float2(ka ? gvr.x : 0.f, kb ? gvr.y : 0.f);
+        const float2 wx = mul2(gv, dx), wy = mul2(gv, dy);
         acc0 = add2(acc0, wx);
         acc1 = add2(acc1, wy);
         acc2 = fma2(wx, dx, acc2);
         acc3 = fma2(wx, dy, acc3);
         acc4 = fma2(wy, dy, acc4);
-        acc5 = fma2(g, vis, acc5);
+        acc5 = add2(acc5, gv);
         // Advance both samples by 64 box positions: dq rows and dr columns,
         // plus one wrap where the column passes the box's width.
         px = add2(px, step_x);
@@ -621,11 +624,12 @@ __device__ __forceinline__ void record_walk_packed(const Rec2D<float>& r, float 
         px = fma2(wrap, neg_bw, px);
         py = add2(py, wrap);
     }
-    part[0] = acc0.x + acc0.y;
-    part[1] = acc1.x + acc1.y;
-    part[2] = acc2.x + acc2.y;
-    part[3] = acc3.x + acc3.y;
-    part[4] = acc4.x + acc4.y;
+    const float nom = -om;
+    part[0] = nom * (acc0.x + acc0.y);
+    part[1] = nom * (acc1.x + acc1.y);
+    part[2] = nom * (acc2.x + acc2.y);
+    part[3] = nom * (acc3.x + acc3.y);
+    part[4] = nom * (acc4.x + acc4.y);
     part[5] = acc5.x + acc5.y;
     part[6] = 0.f;
     part[7] = 0.f;

@@ -363,7 +363,9 @@ __global__ void __launch_bounds__(kVoxBwdThreads) voxel_bwd_kernel(
                         const float2 vis = make_float2(exp2f(e.x), exp2f(e.y));
                         const bool ka = !(e.x > 0.f || e.x < e_min);
                         const bool kb = !(e.y > 0.f || e.y < e_min);
-                        const float2 gv = mul2(make_float2(ka ? ga : 0.f, kb ? gb : 0.f), vis);
+                        // Select after the product: a skipped sample may have vis = inf (e > 0).
+                        const float2 gvr = mul2(make_float2(ga, gb), vis);
+                        const float2 gv = make_float2(ka ? gvr.x : 0.f, kb ? gvr.y : 0.f);
                         a3 = add2(a3, gv);
                         const float2 gvd = mul2(gv, d1);
                         a1 = add2(a1, gvd);

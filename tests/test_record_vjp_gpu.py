@@ -1,0 +1,90 @@
+"""Record-parallel raster VJP (``r2s_raster_record_bwd``) against a float64 restatement.
+
+Each (camera, primitive) record's adjoints are sums over the pixels of its tile
+rectangle, with the reference's per-sample rules (RasterizeToPixelsBwd.cu:350-563):
+a sample counts when sigma >= 0 and |alpha| >= 1e-5, alpha = o mu exp(-sigma),
+sigma = (a dx^2 + c dy^2) / 2 + b dx dy at pixel centres. The records here include
+what the projection never makes: indefinite and negative-definite conics, negative
+and tiny o mu. Such records fall back to the whole rectangle; their skipped
+samples (sigma < 0, where exp(-sigma) overflows) must contribute nothing.
+"""
+
+import pytest
+import torch
+
+from r2splat_b200.cuda import _backend
+
+pytestmark = pytest.mark.gpu
+
+W, H, T = 64, 48, 16
+
+
+def _records(device, n=96, seed=0):
+    gen = torch.Generator(device="cpu").manual_seed(seed)
+    x = torch.rand(n, generator=gen, dtype=torch.float64) * (W + 8) - 4
+    y = torch.rand(n, generator=gen, dtype=torch.float64) * (H + 8) - 4
+    s = torch.exp(torch.randn(n, 2, generator=gen, dtype=torch.float64) * 0.5) * 2.5
+    th = torch.rand(n, generator=gen, dtype=torch.float64) * 3.14159
+    cth, sth = torch.cos(th), torch.sin(th)
+    # Conic = inverse covariance of an ellipse with axes s rotated by th.
+    ia, ib = 1 / s[:, 0] ** 2, 1 / s[:, 1] ** 2
+    a = cth ** 2 * ia + sth ** 2 * ib
+    c = sth ** 2 * ia + cth ** 2 * ib
+    b = cth * sth * (ia - ib)
+    o = torch.rand(n, generator=gen, dtype=torch.float64) * 0.9 + 0.05
+    mu = torch.rand(n, generator=gen, dtype=torch.float64) * 2 + 0.1
+    # Records the projection never produces.
+    a[0], b[0], c[0] = 0.2, 0.5, 0.2            # indefinite
+    a[1], b[1], c[1] = -0.1, 0.0, -0.2          # negative definite
+    a[2], b[2], c[2] = 0.0, 0.3, 0.1            # singular, indefinite
+    o[3] = -0.7                                 # negative o mu
+    o[4] = 2e-6                                 # |alpha| < 1e-5 everywhere
+    rec = torch.stack([x, y, a, b, c, o, mu, torch.zeros_like(x)], 1)
+    return rec.float().to(device)
+
+
+def _expected(rec, v):
+    """float64 adjoints over every pixel of the full-image rectangle."""
+    r = rec.double()
+    x, y, a, b, c, o, mu = [r[:, i, None, None] for i in range(7)]
+    py, px = torch.meshgrid(torch.arange(H, device=rec.device, dtype=torch.float64) + 0.5,
+                            torch.arange(W, device=rec.device, dtype=torch.float64) + 0.5, indexing="ij")
+    dx, dy = px - x, py - y
+    sigma = 0.5 * (a * dx * dx + c * dy * dy) + b * dx * dy
+    alpha = o * mu * torch.exp(-sigma.clamp(min=-80.0))
+    keep = (sigma >= 0) & (alpha.abs() >= 1e-5)
+    g = v.double()[None]
+    vis = torch.where(keep, torch.exp(-sigma.clamp(min=-80.0)), torch.zeros_like(sigma))
+    w = torch.where(keep, -g * alpha, torch.zeros_like(sigma))
+    s = [(w * dx).sum((1, 2)), (w * dy).sum((1, 2)), (w * dx * dx).sum((1, 2)), (w * dx * dy).sum((1, 2)),
+         (w * dy * dy).sum((1, 2)), (g * vis).sum((1, 2))]
+    a, b, c, o, mu = [r[:, i] for i in range(2, 7)]
+    return torch.stack([-(a * s[0] + b * s[1]), -(c * s[1] + b * s[0]), 0.5 * s[2], s[3], 0.5 * s[4], mu * s[5],
+                        o * s[5], torch.zeros_like(a)], 1)
+
+
+def _record_vjp(rec, v):
+    """Packed FP32x2 walk for float32 inputs, the scalar walk for float64."""
+    n = rec.shape[0]
+    rects = torch.tensor([0, 0, (W + T - 1) // T, (H + T - 1) // T], dtype=torch.int16,
+                         device=rec.device).repeat(n, 1)
+    grads = torch.full((n, 8), float("nan"), device=rec.device, dtype=rec.dtype)
+    dtype = 0 if rec.dtype == torch.float32 else 1
+    _backend.call("r2s_raster_record_bwd", dtype, rec.data_ptr(), rects.data_ptr(), None, 0, 0, v.data_ptr(), None,
+                  1, n, W, H, T, grads.data_ptr(), None, None, torch.cuda.current_stream(rec.device).cuda_stream)
+    return grads
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+@pytest.mark.parametrize("seed", [0, 1])
+def test_record_vjp_matches_float64_with_degenerate_records(device, seed, dtype):
+    rec = _records(device, seed=seed).to(dtype)
+    gen = torch.Generator(device="cpu").manual_seed(seed + 10)
+    v = torch.randn((H, W), generator=gen).to(device=device, dtype=dtype)
+    got = _record_vjp(rec, v)
+    want = _expected(rec, v)
+    assert torch.isfinite(got).all()
+    assert not got[4].any()  # |alpha| below the threshold everywhere
+    scale = want.abs().amax(0).clamp(min=1e-12)
+    err = ((got.double() - want).abs() / scale).amax(0)
+    assert (err < 1e-4).all(), err.tolist()
