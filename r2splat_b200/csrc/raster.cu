@@ -216,8 +216,10 @@ __global__ void __launch_bounds__(kMaxThreads) raster_fwd_kernel(
         const S* qbuf = s_q + stage * B;
         const int32_t batch = min(int32_t(B), count - bi * int32_t(B));
         if (int32_t(t) < batch) {
-            const TileBox box = record_box<S, kBeta>(buf[t], ox, oy, vx, vy);
+            Rec2D<S>& rec = s_rec[stage * B + t];
+            const TileBox box = record_box<S, kBeta>(rec, ox, oy, vx, vy);
             s_mask[t] = make_uint2(box.cols, box.rows);
+            rec.o = rec.o * rec.mu;  // o mu, once per record (the samples use only the product)
         }
         __syncthreads();
         if (warp_active) {
@@ -235,8 +237,8 @@ __global__ void __launch_bounds__(kMaxThreads) raster_fwd_kernel(
                 const int32_t n_hits = __popc(hits);
                 for (int32_t e = 0; e < n_hits; ++e) {
                     const int32_t s = my_hits[e];
-                    const Rec2D<S> r = buf[s];
-                    const S om = r.o * r.mu;
+                    const Rec2D<S>& r = buf[s];
+                    const S om = r.o;  // o mu
                     S q = S(0);
                     if (kVar) q = qbuf[s];
                     if (!kBeta) {
