@@ -132,6 +132,19 @@ constexpr int kSortItems = 16;  // per lane
 constexpr int64_t kSortTile = int64_t(kSortThreads) * kSortItems;
 constexpr int kMaxDigitBits = 10;
 
+// Digit histogram of elements [begin, end) into shared memory (zeroed here).
+template <typename Digit>
+__device__ __forceinline__ void block_histogram(const uint32_t* __restrict__ keys, int64_t begin, int64_t end,
+                                                Digit digit, uint32_t bins, uint32_t* s_hist) {
+    for (uint32_t d = threadIdx.x; d < bins; d += kSortThreads) s_hist[d] = 0;
+    __syncthreads();
+    for (int k = 0; k < kSortItems; ++k) {
+        const int64_t i = begin + int64_t(k) * kSortThreads + threadIdx.x;
+        if (i < end) atomicAdd(&s_hist[digit(keys[i])], 1u);
+    }
+    __syncthreads();
+}
+
 // Per-block digit histogram, stored digit-major: hist[d * n_blocks + b].
 // With n_dev non-null the element count is *n_dev (at most n, the capacity the
 // grid was sized for); blocks past it contribute empty histograms.
@@ -141,33 +154,26 @@ __global__ void __launch_bounds__(kSortThreads) radix_upsweep_kernel(const uint3
     extern __shared__ uint32_t s_hist[];
     if (n_dev != nullptr && *n_dev < n) n = *n_dev;
     const uint32_t bins = mask + 1;
-    for (uint32_t d = threadIdx.x; d < bins; d += kSortThreads) s_hist[d] = 0;
-    __syncthreads();
     const int64_t base = int64_t(blockIdx.x) * kSortTile;
-    for (int k = 0; k < kSortItems; ++k) {
-        const int64_t i = base + int64_t(k) * kSortThreads + threadIdx.x;
-        if (i < n) atomicAdd(&s_hist[(keys[i] >> shift) & mask], 1u);
-    }
-    __syncthreads();
+    block_histogram(keys, base, min(n, base + kSortTile), [=](uint32_t key) { return (key >> shift) & mask; }, bins,
+                    s_hist);
     for (uint32_t d = threadIdx.x; d < bins; d += kSortThreads) hist[size_t(d) * gridDim.x + blockIdx.x] = s_hist[d];
 }
 
-// Stable scatter of one digit. Element order inside a block is (warp, item,
-// lane) = index order; ranks come from warp-wide matching of equal digits.
-// The block's elements are first placed in shared memory in digit order, then
-// written out in that order, so consecutive threads store consecutive
-// positions of one digit's run (coalesced) instead of scattering 4-byte stores.
+// Stable scatter of one digit for the block's elements [block_base, end).
+// Element order inside a block is (warp, item, lane) = index order; ranks come
+// from warp-wide matching of equal digits. The block's elements are first
+// placed in shared memory in digit order, then written out in that order, so
+// consecutive threads store consecutive positions of one digit's run
+// (coalesced) instead of scattering 4-byte stores. global(d) is the output
+// position of the block's first element of digit d.
 // Shared memory: [kSortWarps][bins] warp offsets, [bins] block-local digit
 // starts, [bins] global digit bases, then kSortTile staged keys and values.
-template <typename KeyOut, typename ValOut>
-__global__ void __launch_bounds__(kSortThreads) radix_downsweep_kernel(
-    const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals, int64_t n, const int64_t* __restrict__ n_dev,
-    int shift, uint32_t mask, const uint32_t* __restrict__ offsets, KeyOut* __restrict__ keys_out,
-    ValOut* __restrict__ vals_out) {
-    extern __shared__ uint32_t s_cnt[];
-    if (n_dev != nullptr && *n_dev < n) n = *n_dev;
-    if (int64_t(blockIdx.x) * kSortTile >= n) return;  // the whole block is past the count
-    const uint32_t bins = mask + 1;
+template <typename KeyOut, typename ValOut, typename Digit, typename Global>
+__device__ __forceinline__ void block_scatter(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
+                                              int64_t block_base, int64_t end, Digit digit, uint32_t bins,
+                                              Global global, KeyOut* __restrict__ keys_out,
+                                              ValOut* __restrict__ vals_out, uint32_t* s_cnt) {
     uint32_t* s_local = s_cnt + kSortWarps * bins;  // block-local start of each digit
     uint32_t* s_global = s_local + bins;             // global position of each digit's first element
     uint32_t* s_key = s_global + bins;               // [kSortTile]
@@ -177,17 +183,16 @@ __global__ void __launch_bounds__(kSortThreads) radix_downsweep_kernel(
     __syncthreads();
     uint32_t* my_cnt = s_cnt + warp * bins;
     const uint32_t lt_mask = (1u << lane) - 1u;
-    const int64_t block_base = int64_t(blockIdx.x) * kSortTile;
     const int64_t base = block_base + int64_t(warp) * (kSortTile / kSortWarps);
     uint32_t k_key[kSortItems], k_val[kSortItems], k_rank[kSortItems];
 #pragma unroll
     for (int k = 0; k < kSortItems; ++k) {
         const int64_t i = base + int64_t(k) * 32 + lane;
-        const bool valid = i < n;
+        const bool valid = i < end;
         const uint32_t key = valid ? keys[i] : 0u;
         k_key[k] = key;
         k_val[k] = valid ? vals[i] : 0u;
-        const uint32_t d = valid ? ((key >> shift) & mask) : bins;
+        const uint32_t d = valid ? digit(key) : bins;
         const uint32_t peers = __match_any_sync(0xffffffffu, d);
         const uint32_t leader = __ffs(peers) - 1;
         uint32_t count = 0;
@@ -208,7 +213,7 @@ __global__ void __launch_bounds__(kSortThreads) radix_downsweep_kernel(
             running += c;
         }
         s_local[d] = running;  // digit total for now
-        s_global[d] = offsets[size_t(d) * gridDim.x + blockIdx.x];
+        s_global[d] = global(d);
     }
     __syncthreads();
     // Exclusive scan of the digit totals (one warp; at most 1024 digits).
@@ -231,23 +236,126 @@ __global__ void __launch_bounds__(kSortThreads) radix_downsweep_kernel(
 #pragma unroll
     for (int k = 0; k < kSortItems; ++k) {
         const int64_t i = base + int64_t(k) * 32 + lane;
-        if (i < n) {
-            const uint32_t d = (k_key[k] >> shift) & mask;
+        if (i < end) {
+            const uint32_t d = digit(k_key[k]);
             const uint32_t slot = s_local[d] + my_cnt[d] + k_rank[k];
             s_key[slot] = k_key[k];
             s_val[slot] = k_val[k];
         }
     }
     __syncthreads();
-    const int64_t remaining = n - block_base;
+    const int64_t remaining = end - block_base;
     const uint32_t count = remaining < kSortTile ? uint32_t(remaining) : uint32_t(kSortTile);
     for (uint32_t j = threadIdx.x; j < count; j += kSortThreads) {
         const uint32_t key = s_key[j];
-        const uint32_t d = (key >> shift) & mask;
+        const uint32_t d = digit(key);
         const uint32_t pos = s_global[d] + (j - s_local[d]);
         keys_out[pos] = static_cast<KeyOut>(key);
         vals_out[pos] = static_cast<ValOut>(s_val[j]);
     }
+}
+
+template <typename KeyOut, typename ValOut>
+__global__ void __launch_bounds__(kSortThreads) radix_downsweep_kernel(
+    const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals, int64_t n, const int64_t* __restrict__ n_dev,
+    int shift, uint32_t mask, const uint32_t* __restrict__ offsets, KeyOut* __restrict__ keys_out,
+    ValOut* __restrict__ vals_out) {
+    extern __shared__ uint32_t s_cnt[];
+    if (n_dev != nullptr && *n_dev < n) n = *n_dev;
+    const int64_t block_base = int64_t(blockIdx.x) * kSortTile;
+    if (block_base >= n) return;  // the whole block is past the count
+    const uint32_t b = blockIdx.x, nb = gridDim.x;
+    block_scatter(keys, vals, block_base, min(n, block_base + kSortTile),
+                  [=](uint32_t key) { return (key >> shift) & mask; }, mask + 1,
+                  [=](uint32_t d) { return offsets[size_t(d) * nb + b]; }, keys_out, vals_out, s_cnt);
+}
+
+// ------------------------------------------------ camera-segmented 2D sort
+//
+// 2D keys are cam * n_tiles + tile and emission is camera-major, so the key
+// array is already ordered by camera: one stable pass on the tile digit
+// inside each camera's segment sorts it completely. Each sort block takes
+// kSortTile elements of one camera. The histogram of camera c, tile d, block
+// j (of nb_c) sits at n_tiles * first_block_c + d * nb_c + j, so one
+// exclusive scan over all of them gives every block's output position per
+// tile directly (cameras before c, then tiles before d, then earlier blocks).
+
+struct CamSegment {
+    int64_t begin, end;    // elements of the camera
+    uint32_t first_block;  // sort blocks before this camera's
+    uint32_t n_blocks;
+};
+
+// One thread: segment bounds from the inclusive tile-count prefix (one entry
+// per (camera, element) pair, C*N in all) and the block layout; the blocks of
+// the grid past the last camera's zero-fill the unused histogram tail.
+__global__ void cam_segments_kernel(const int64_t* __restrict__ cum, uint32_t C, uint32_t N, int64_t n,
+                                    const int64_t* __restrict__ n_dev, CamSegment* __restrict__ seg,
+                                    uint32_t* __restrict__ total_blocks) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (n_dev != nullptr && *n_dev < n) n = *n_dev;
+    int64_t begin = 0;
+    uint32_t blocks = 0;
+    for (uint32_t c = 0; c < C; ++c) {
+        int64_t end = cum[(int64_t(c) + 1) * N - 1];
+        if (end > n) end = n;
+        if (end < begin) end = begin;
+        const uint32_t nb = uint32_t((end - begin + kSortTile - 1) / kSortTile);
+        seg[c] = CamSegment{begin, end, blocks, nb};
+        blocks += nb;
+        begin = end;
+    }
+    *total_blocks = blocks;
+}
+
+// The camera holding sort block b (binary search over first_block).
+__device__ __forceinline__ uint32_t block_camera(const CamSegment* seg, uint32_t C, uint32_t b) {
+    uint32_t lo = 0, hi = C;  // first_block[lo] <= b < first_block[hi]
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (seg[mid].first_block <= b) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(kSortThreads) segmented_upsweep_kernel(
+    const uint32_t* __restrict__ keys, const CamSegment* __restrict__ seg, uint32_t C, uint32_t n_tiles,
+    const uint32_t* __restrict__ total_blocks, uint32_t* __restrict__ hist) {
+    extern __shared__ uint32_t s_hist[];
+    const uint32_t b = blockIdx.x, used = *total_blocks;
+    if (b >= used) {
+        // Zero the histogram tail that no camera uses (gridDim.x - used blocks of n_tiles).
+        uint32_t* tail = hist + size_t(n_tiles) * used + size_t(b - used) * n_tiles;
+        for (uint32_t d = threadIdx.x; d < n_tiles; d += kSortThreads) tail[d] = 0;
+        return;
+    }
+    const uint32_t c = block_camera(seg, C, b);
+    const CamSegment sg = seg[c];
+    const uint32_t j = b - sg.first_block;
+    const int64_t begin = sg.begin + int64_t(j) * kSortTile;
+    const uint32_t key0 = c * n_tiles;
+    block_histogram(keys, begin, min(sg.end, begin + kSortTile), [=](uint32_t key) { return key - key0; }, n_tiles,
+                    s_hist);
+    uint32_t* out = hist + size_t(n_tiles) * sg.first_block + j;
+    for (uint32_t d = threadIdx.x; d < n_tiles; d += kSortThreads) out[size_t(d) * sg.n_blocks] = s_hist[d];
+}
+
+__global__ void __launch_bounds__(kSortThreads) segmented_downsweep_kernel(
+    const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals, const CamSegment* __restrict__ seg,
+    uint32_t C, uint32_t n_tiles, const uint32_t* __restrict__ total_blocks, const uint32_t* __restrict__ offsets,
+    int64_t* __restrict__ keys_out, int32_t* __restrict__ vals_out) {
+    extern __shared__ uint32_t s_cnt[];
+    const uint32_t b = blockIdx.x;
+    if (b >= *total_blocks) return;
+    const uint32_t c = block_camera(seg, C, b);
+    const CamSegment sg = seg[c];
+    const uint32_t j = b - sg.first_block;
+    const int64_t begin = sg.begin + int64_t(j) * kSortTile;
+    const uint32_t key0 = c * n_tiles;
+    const uint32_t* base = offsets + size_t(n_tiles) * sg.first_block + j;
+    const uint32_t nb = sg.n_blocks;
+    block_scatter(keys, vals, begin, min(sg.end, begin + kSortTile), [=](uint32_t key) { return key - key0; },
+                  n_tiles, [=](uint32_t d) { return base[size_t(d) * nb]; }, keys_out, vals_out, s_cnt);
 }
 
 __global__ void widen_kernel(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals, int64_t n,
@@ -311,6 +419,17 @@ inline SortPlan plan_sort(int64_t n, uint64_t n_keys) {
     return p;
 }
 
+// Camera layout of 2D keys (cam * n_tiles + tile, emitted camera-major) for
+// the one-pass segmented sort; cum is the inclusive tile-count prefix over the
+// C * N (camera, element) pairs.
+struct CamLayout {
+    const int64_t* cum;
+    uint32_t C, N, n_tiles;
+};
+
+constexpr uint32_t kMaxSegmentedTiles = 1024;  // digit bins of the segmented pass
+constexpr uint32_t kMaxCameras = 65535;
+
 inline size_t emit_workspace(int64_t n, uint64_t n_keys) {
     const SortPlan p = plan_sort(n, n_keys);
     ArenaSize a;
@@ -318,22 +437,61 @@ inline size_t emit_workspace(int64_t n, uint64_t n_keys) {
     a.take<uint32_t>(size_t(n));  // vals A
     a.take<uint32_t>(size_t(n));  // keys B
     a.take<uint32_t>(size_t(n));  // vals B
-    const size_t hist = size_t(1u << (p.digit_bits > 0 ? p.digit_bits : 1)) * size_t(p.blocks > 0 ? p.blocks : 1);
+    const size_t blocks = size_t(p.blocks > 0 ? p.blocks : 1);
+    const size_t hist_generic = size_t(1u << (p.digit_bits > 0 ? p.digit_bits : 1)) * blocks;
+    // Segmented: n_tiles * (blocks + C) <= kMaxSegmentedTiles * blocks + n_keys.
+    const size_t hist_segmented = size_t(kMaxSegmentedTiles) * blocks + size_t(n_keys);
+    const size_t hist = hist_generic > hist_segmented ? hist_generic : hist_segmented;
+    a.take<CamSegment>(size_t(n_keys < kMaxCameras ? n_keys : kMaxCameras));
+    a.take<uint32_t>(1);
     a.take<uint32_t>(hist);
     a.take<char>(scan_workspace_bytes<uint32_t>(int64_t(hist)));
     return a.bytes();
 }
 
+// One stable pass on the tile digit inside each camera's segment, writing the
+// widened result to isect_ids/flatten_ids.
+inline int segmented_sort(const uint32_t* keys, const uint32_t* vals, int64_t n, const CamLayout& cams,
+                          Arena& arena, int64_t* isect_ids, int32_t* flatten_ids, cudaStream_t stream,
+                          const int64_t* n_dev) {
+    const int64_t max_blocks = (n + kSortTile - 1) / kSortTile + int64_t(cams.C);
+    R2S_REQUIRE(max_blocks < (int64_t(1) << 31), R2S_ERR_UNSUPPORTED, "too many intersections");
+    CamSegment* seg = arena.take<CamSegment>(cams.C);
+    uint32_t* total_blocks = arena.take<uint32_t>(1);
+    const int64_t hist_len = int64_t(cams.n_tiles) * max_blocks;
+    uint32_t* hist = arena.take<uint32_t>(size_t(hist_len));
+    R2S_REQUIRE(seg && total_blocks && hist, R2S_ERR_WORKSPACE, "intersection workspace too small");
+    void* scan_ws = arena.base + arena.used;
+    const size_t scan_bytes = arena.size - arena.used;
+    cam_segments_kernel<<<1, 32, 0, stream>>>(cams.cum, cams.C, cams.N, n, n_dev, seg, total_blocks);
+    R2S_TRY(check_launch("cam_segments"));
+    segmented_upsweep_kernel<<<unsigned(max_blocks), kSortThreads, cams.n_tiles * sizeof(uint32_t), stream>>>(
+        keys, seg, cams.C, cams.n_tiles, total_blocks, hist);
+    R2S_TRY(check_launch("segmented_upsweep"));
+    R2S_TRY((device_scan<uint32_t, uint32_t, false>(hist, hist, hist_len, scan_ws, scan_bytes, stream)));
+    const size_t down_smem = (size_t(cams.n_tiles) * (kSortWarps + 2) + 2 * size_t(kSortTile)) * sizeof(uint32_t);
+    R2S_TRY(allow_dynamic_smem(segmented_downsweep_kernel, down_smem));
+    segmented_downsweep_kernel<<<unsigned(max_blocks), kSortThreads, down_smem, stream>>>(
+        keys, vals, seg, cams.C, cams.n_tiles, total_blocks, hist, isect_ids, flatten_ids);
+    return check_launch("segmented_downsweep");
+}
+
 // Sorts (keys, vals) of length n by key bits [0, bits(n_keys-1)), writing
-// the widened result to isect_ids/flatten_ids, then fills offsets.
+// the widened result to isect_ids/flatten_ids, then fills offsets. With a
+// camera layout of at most kMaxSegmentedTiles tiles per camera the sort is
+// the one-pass segmented one.
 inline int sort_and_finish(uint32_t* keys, uint32_t* vals, int64_t n, uint64_t n_keys, Arena& arena,
                            int64_t* isect_ids, int32_t* flatten_ids, int32_t* offsets, cudaStream_t stream,
-                           const int64_t* n_dev = nullptr) {
+                           const int64_t* n_dev = nullptr, const CamLayout* cams = nullptr) {
     const SortPlan p = plan_sort(n, n_keys);
+    const bool segmented = cams != nullptr && cams->C >= 1 && cams->C <= kMaxCameras && cams->n_tiles >= 1 &&
+                           cams->n_tiles <= kMaxSegmentedTiles && p.passes > 1;
     if (n > 0) {
         if (p.passes == 0) {
             widen_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(keys, vals, n, n_dev, isect_ids, flatten_ids);
             R2S_TRY(check_launch("widen"));
+        } else if (segmented) {
+            R2S_TRY(segmented_sort(keys, vals, n, *cams, arena, isect_ids, flatten_ids, stream, n_dev));
         } else {
             uint32_t* keys_b = arena.take<uint32_t>(size_t(n));
             uint32_t* vals_b = arena.take<uint32_t>(size_t(n));
@@ -434,8 +592,9 @@ int r2s_isect_tiles_emit(int dtype, const void* means2d, const int32_t* radii, i
             static_cast<const S*>(means2d), radii, radii_is_rect != 0, uint32_t(total), N, tile_size, tiles_x, tiles_y,
             cum_tiles, keys, vals));
         R2S_TRY(check_launch("isect_emit"));
+        const CamLayout cams{cum_tiles, C, N, tiles_x * tiles_y};
         return sort_and_finish(keys, vals, n_isects, n_keys, arena, isect_ids, flatten_ids, offsets,
-                               as_stream(stream));
+                               as_stream(stream), nullptr, &cams);
     }
     return sort_and_finish(nullptr, nullptr, 0, n_keys, arena, isect_ids, flatten_ids, offsets, as_stream(stream));
 }
@@ -457,8 +616,9 @@ int r2s_raster_emit(const uint16_t* rects, uint32_t C, uint32_t N, uint32_t tile
             reinterpret_cast<const ushort4*>(rects), uint32_t(total), N, tiles_x, tiles_y, cum_tiles, INT64_MAX, keys,
             vals);
         R2S_TRY(check_launch("raster_emit"));
+        const CamLayout cams{cum_tiles, C, N, tiles_x * tiles_y};
         return sort_and_finish(keys, vals, n_isects, n_keys, arena, isect_ids, flatten_ids, offsets,
-                               as_stream(stream));
+                               as_stream(stream), nullptr, &cams);
     }
     return sort_and_finish(nullptr, nullptr, 0, n_keys, arena, isect_ids, flatten_ids, offsets, as_stream(stream));
 }
@@ -539,7 +699,9 @@ int r2s_raster_emit_capacity(const uint16_t* rects, uint32_t C, uint32_t N, uint
             vals);
         R2S_TRY(check_launch("raster_emit"));
     }
-    return sort_and_finish(keys, vals, capacity, n_keys, arena, isect_ids, flatten_ids, offsets, st, n_used);
+    const CamLayout cams{cum_tiles, C, N, tiles_x * tiles_y};
+    return sort_and_finish(keys, vals, capacity, n_keys, arena, isect_ids, flatten_ids, offsets, st, n_used,
+                           total > 0 ? &cams : nullptr);
 }
 
 int r2s_voxel_emit_capacity(int dtype, const void* means3d, const int32_t* radii, uint32_t N, uint32_t tile_size,
