@@ -119,10 +119,11 @@ class VoxelState:
 
 
 def raster_intersections(means, covars, densities, beta, ratio, viewmats, Ks, width, height, eps, radius_clip,
-                         tile_size=RASTER_TILE):
+                         tile_size=RASTER_TILE, before_count=None):
     """Projection + packing + sorted tile intersections.
 
     Returns (records, offsets, isect_ids, flatten_ids, M, rects); rects [C,N,4] are the tile rectangles.
+    ``before_count`` runs just before the host reads the intersection count (the pending input checks).
     """
     device = means.device
     c, n = viewmats.shape[0], means.shape[0]
@@ -139,6 +140,8 @@ def raster_intersections(means, covars, densities, beta, ratio, viewmats, Ks, wi
     cum = torch.empty((c * n,), dtype=torch.int64, device=device)
     ws = _ws(lib.r2s_isect_count_workspace(c * n), device)
     _backend.call("r2s_scan_tile_counts", _ptr(counts), c * n, _ptr(cum), _ptr(ws), ws.numel(), stream)
+    if before_count is not None:
+        before_count()
     m = int(cum[-1].item())
     isect_ids = torch.empty((m,), dtype=torch.int64, device=device)
     flatten_ids = torch.empty((m,), dtype=torch.int32, device=device)
@@ -176,7 +179,7 @@ def render_image_loss(records, uncertainty, beta: bool, offsets, flatten_ids, m,
 
 
 def raster_forward(means, quats, scales, densities, viewmats, Ks, width, height, beta, uncertainty, eps,
-                   radius_clip, tile_size=RASTER_TILE, image_loss=None):
+                   radius_clip, tile_size=RASTER_TILE, image_loss=None, before_count=None):
     """Explicit projection forward; returns (image or (image, variance), RasterState).
 
     With ``image_loss = (target, kind, weight)`` the tile kernel also writes the
@@ -187,7 +190,8 @@ def raster_forward(means, quats, scales, densities, viewmats, Ks, width, height,
     covars, _ = low.parameter_transform_fwd(quats, scales)
     ratio = _beta.beta_path_ratio(beta) if beta is not None else None
     records, offsets, isect_ids, flatten_ids, m, rects = raster_intersections(
-        means, covars, densities, beta, ratio, viewmats, Ks, width, height, eps, radius_clip, tile_size)
+        means, covars, densities, beta, ratio, viewmats, Ks, width, height, eps, radius_clip, tile_size,
+        before_count)
     image = means.new_empty((c, height, width))
     variance = torch.empty_like(image) if uncertainty is not None else None
     tx = (width + tile_size - 1) // tile_size
@@ -272,7 +276,7 @@ def raster_backward(state: RasterState, means, quats, scales, densities, beta, u
 
 
 def voxel_intersections(means, covars, densities, beta, uncertainty, extent, center, shape, eps, radius_clip,
-                        tile_size=VOXEL_TILE):
+                        tile_size=VOXEL_TILE, before_count=None):
     device = means.device
     depth, height, width = shape
     n = means.shape[0]
@@ -292,6 +296,8 @@ def voxel_intersections(means, covars, densities, beta, uncertainty, extent, cen
     cum = torch.empty((n,), dtype=torch.int64, device=device)
     ws = _ws(lib.r2s_isect_count_workspace(n), device)
     _backend.call("r2s_scan_tile_counts", _ptr(counts), n, _ptr(cum), _ptr(ws), ws.numel(), stream)
+    if before_count is not None:
+        before_count()
     m = int(cum[-1].item())
     isect_ids = torch.empty((m,), dtype=torch.int64, device=device)
     flatten_ids = torch.empty((m,), dtype=torch.int32, device=device)
@@ -305,12 +311,13 @@ def voxel_intersections(means, covars, densities, beta, uncertainty, extent, cen
 
 
 def voxel_forward(means, quats, scales, densities, shape, extent, center, beta, uncertainty, eps, radius_clip,
-                  tile_size=VOXEL_TILE):
+                  tile_size=VOXEL_TILE, before_count=None):
     device = means.device
     depth, height, width = shape
     covars, _ = low.parameter_transform_fwd(quats, scales)
     records, offsets, isect_ids, flatten_ids, m = voxel_intersections(
-        means, covars, densities, beta, uncertainty, extent, center, shape, eps, radius_clip, tile_size)
+        means, covars, densities, beta, uncertainty, extent, center, shape, eps, radius_clip, tile_size,
+        before_count)
     volume = means.new_empty(shape)
     variance = torch.empty_like(volume) if uncertainty is not None else None
     tx = (width + tile_size - 1) // tile_size

@@ -43,17 +43,19 @@ class _ValueChecks:
 
     def __init__(self):
         self.items: list = []
+        self._launched = None
 
-    def first_failure(self):
-        """Evaluates the queued checks; returns the first failing one's exception, or None."""
+    def launch(self) -> None:
+        """Enqueues the queued checks: one kernel per (device, dtype, 32 checks) and an
+        asynchronous copy of its flag word to pinned host memory, followed by an event."""
         items, self.items = self.items, []
         live = [(i, item) for i, item in enumerate(items) if item[0].numel() > 0]
-        failed: set = set()
         groups: dict = {}
         for index, item in live:
             groups.setdefault((item[0].device, item[0].dtype), []).append((index, item))
         from .cuda import _backend  # late import: the loader imports nothing from here
 
+        words = []
         for (device, dtype), group in groups.items():
             for start in range(0, len(group), 32):
                 chunk = group[start:start + 32]
@@ -61,23 +63,60 @@ class _ValueChecks:
                 for bit, (_, (tensor, kind, _, _)) in enumerate(chunk):
                     table[bit] = _ValueCheck(tensor.data_ptr(), tensor.numel() // _ELEMENT_SIZE[kind], kind, bit)
                 with torch.cuda.device(device):
+                    stream = torch.cuda.current_stream(device)
                     flags = torch.empty(1, dtype=torch.int32, device=device)
                     _backend.call("r2s_check_values", 0 if dtype == torch.float32 else 1, table, len(chunk),
-                                  flags.data_ptr(), torch.cuda.current_stream(device).cuda_stream)
-                    word = int(flags.item())
-                failed.update(index for bit, (index, _) in enumerate(chunk) if word >> bit & 1)
+                                  flags.data_ptr(), stream.cuda_stream)
+                    host = torch.empty(1, dtype=torch.int32, pin_memory=True)
+                    host.copy_(flags, non_blocking=True)
+                    done = torch.cuda.Event()
+                    done.record(stream)
+                words.append(([index for index, _ in chunk], host, done))
+        self._launched = (items, words)
+
+    def resolve(self):
+        """Waits for the launched checks only (work queued after them keeps running);
+        returns the first failing check's exception in call order, or None."""
+        if self._launched is None:
+            return None
+        items, words = self._launched
+        self._launched = None
+        failed: set = set()
+        for indices, host, done in words:
+            done.synchronize()
+            word = int(host[0])
+            failed.update(index for bit, index in enumerate(indices) if word >> bit & 1)
         for index, (_, _, exc_type, message) in enumerate(items):
             if index in failed:
                 return exc_type(message)
         return None
+
+    def first_failure(self):
+        """Evaluates the queued checks; returns the first failing one's exception, or None."""
+        self.launch()
+        return self.resolve()
+
+    def check(self) -> None:
+        """Raises the first failing launched check (see deferred_value_checks(pending=True))."""
+        failure = self.resolve()
+        if failure is not None:
+            raise failure
 
 
 _active = threading.local()
 
 
 @contextlib.contextmanager
-def deferred_value_checks():
-    """Queue the value checks made inside the block and evaluate them with one host read."""
+def deferred_value_checks(pending: bool = False):
+    """Queue the value checks made inside the block and evaluate them with one host read.
+
+    With ``pending=True`` the checks are only launched when the block ends; the
+    caller enqueues its device work and then calls ``check()`` on the yielded
+    object, which waits for the checks alone and raises the first failure, so
+    the device does not idle on the read. Callers resolve before anything
+    depends on the inputs being valid on the host (allocations sized from
+    device counts, consuming a context).
+    """
     checks = _ValueChecks()
     previous = getattr(_active, "checks", None)
     _active.checks = checks
@@ -90,6 +129,9 @@ def deferred_value_checks():
             raise earlier from None
         raise
     _active.checks = previous
+    if pending:
+        checks.launch()
+        return
     failure = checks.first_failure()
     if failure is not None:
         raise failure

@@ -62,17 +62,32 @@ __global__ void __launch_bounds__(256) voxel_fwd_kernel(const Rec3D<S>* __restri
     const uint32_t rem = key - tz * g.tiles_x * g.tiles_y;
     const uint32_t ty = rem / g.tiles_x, tx = rem - ty * g.tiles_x;
     const uint32_t t = threadIdx.x;
+    constexpr bool kRowShared = PPT == 4 && !kBeta && std::is_same<S, float>::value;
 
     S px[PPT], py[PPT], pz[PPT], acc[PPT], accv[PPT];
     size_t vid[PPT];
     bool inside[PPT];
+    // PPT = 4: a thread owns 4 consecutive voxels of one row (same y, z), so
+    // the Gaussian terms in d2 and d3 alone are computed once per record.
+    const uint32_t segs = (T + 3u) / 4u;
+    const uint32_t row = PPT == 4 ? t / segs : 0u;
+    const uint32_t seg = PPT == 4 ? t - row * segs : 0u;
 #pragma unroll
     for (int k = 0; k < PPT; ++k) {
-        const uint32_t p = t + uint32_t(k) * nthreads;
         uint32_t lz, ly, lx;
-        tile_voxel(p, T, lz, ly, lx);
+        bool in_tile;
+        if (PPT == 4) {
+            lz = row / T;
+            ly = row - lz * T;
+            lx = 4u * seg + uint32_t(k);
+            in_tile = row < T * T && lx < T;
+        } else {
+            const uint32_t p = t + uint32_t(k) * nthreads;
+            tile_voxel(p, T, lz, ly, lx);
+            in_tile = p < T * T * T;
+        }
         const uint32_t i = tz * T + lz, j = ty * T + ly, kk = tx * T + lx;
-        inside[k] = p < T * T * T && i < g.dim0 && j < g.dim1 && kk < g.dim2;
+        inside[k] = in_tile && i < g.dim0 && j < g.dim1 && kk < g.dim2;
         px[k] = static_cast<S>(kk) + static_cast<S>(0.5);
         py[k] = static_cast<S>(j) + static_cast<S>(0.5);
         pz[k] = static_cast<S>(i) + static_cast<S>(0.5);
@@ -101,6 +116,29 @@ __global__ void __launch_bounds__(256) voxel_fwd_kernel(const Rec3D<S>* __restri
         const int32_t batch = min(int32_t(nthreads), count - b * int32_t(nthreads));
         for (int32_t s = 0; s < batch; ++s) {
             const Rec3D<S> r = buf[s];
+            if constexpr (kRowShared) {
+                // The reference's sigma with its contraction made explicit
+                // (nvcc -O3 --use_fast_math fuses the first product of each
+                // sum): S3 = fma(c22 d3, d3, fma(c00 d1, d1, (c11 d2) d2)),
+                // sigma = fma(c12 d2, d3, fma(c02 d1, d3, fma(1/2, S3,
+                // (c01 d1) d2))). The d2/d3 factors are shared by the row.
+                const float d2 = py[0] - r.y, d3 = pz[0] - r.z;
+                const float b2 = __fmul_rn(__fmul_rn(r.c11, d2), d2);
+                const float c22d3 = __fmul_rn(r.c22, d3), c12d2 = __fmul_rn(r.c12, d2);
+#pragma unroll
+                for (int k = 0; k < PPT; ++k) {
+                    const float d1 = px[k] - r.x;
+                    const float s3 = __fmaf_rn(c22d3, d3, __fmaf_rn(__fmul_rn(r.c00, d1), d1, b2));
+                    const float la = __fmaf_rn(0.5f, s3, __fmul_rn(__fmul_rn(r.c01, d1), d2));
+                    const float sigma = __fmaf_rn(c12d2, d3, __fmaf_rn(__fmul_rn(r.c02, d1), d3, la));
+                    const float alpha = r.o * exp(-sigma);
+                    if (!(sigma < 0.f || fabs(alpha) < 1e-6f)) {
+                        acc[k] += alpha;
+                        if (kVar) accv[k] += r.q * alpha * alpha;
+                    }
+                }
+                continue;
+            }
 #pragma unroll
             for (int k = 0; k < PPT; ++k) {
                 if (!kBeta) {
@@ -560,7 +598,8 @@ int launch_vfwd_p(const VoxelGeom& g, const Rec3D<S>* rec, const int32_t* offset
         const unsigned nt = (voxels + 31) / 32 * 32;
         return launch_vfwd_t<S, kBeta, kVar, 1>(g, rec, offsets, ids, vol, vol_var, nt, stream);
     }
-    const unsigned nt = ((voxels + 3) / 4 + 31) / 32 * 32;
+    // Four consecutive voxels of a row per thread: T^2 rows of ceil(T / 4) segments.
+    const unsigned nt = (g.T * g.T * ((g.T + 3) / 4) + 31) / 32 * 32;
     return launch_vfwd_t<S, kBeta, kVar, 4>(g, rec, offsets, ids, vol, vol_var, nt, stream);
 }
 

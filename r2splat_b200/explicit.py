@@ -16,6 +16,7 @@ summation order in the reference).
 
 from __future__ import annotations
 
+import contextlib
 from dataclasses import dataclass
 from typing import Optional, Sequence, Union
 
@@ -53,6 +54,22 @@ class _Context:
     backward_mode: str
     detach_variance: bool
     used: bool = False
+
+
+@contextlib.contextmanager
+def _resolving(checks):
+    """Resolves pending input checks after the block's device work is enqueued.
+
+    A failing check is raised in preference to an error of the block itself.
+    """
+    try:
+        yield
+    except BaseException:
+        failure = checks.resolve()
+        if failure is not None:
+            raise failure from None
+        raise
+    checks.check()
 
 
 def _mode(value):
@@ -184,7 +201,7 @@ def _rasterize_fwd(means, quats, scales, densities, viewmats, Ks, image_size, be
         ("means", "quats", "scales", "densities", "viewmats", "Ks", "beta", "uncertainty"),
         (means, quats, scales, densities, viewmats, Ks, beta, uncertainty),
     ))
-    with deferred_value_checks():
+    with deferred_value_checks(pending=True) as checks:
         height, width = _shape("image_size", image_size, 2)
         primitives = _primitives(means, quats, scales, densities, beta, uncertainty)
         means, quats, scales, densities, beta, uncertainty = primitives
@@ -213,6 +230,7 @@ def _rasterize_fwd(means, quats, scales, densities, viewmats, Ks, image_size, be
     buffers = {"viewmats": viewmats, "Ks": Ks}
     loss_out = None
     if means.shape[0] == 0:
+        checks.check()
         image = means.new_zeros(shape)
         output = image if uncertainty is None else (image, image.clone())
         if image_loss is not None:
@@ -226,8 +244,10 @@ def _rasterize_fwd(means, quats, scales, densities, viewmats, Ks, image_size, be
                                                     means.device)
     else:
         with torch.cuda.device(means.device):
+            # The input checks resolve just before the intersection count is read.
             result = _fused.raster_forward(means, quats, scales, densities, viewmats, Ks, width, height, beta,
-                                           uncertainty, eps, radius_clip, image_loss=image_loss)
+                                           uncertainty, eps, radius_clip, image_loss=image_loss,
+                                           before_count=checks.check)
         output, state = result[0], result[1]
         if image_loss is not None:
             loss_out = result[2]
@@ -251,13 +271,16 @@ def rasterize_bwd(context: _Context, v_image: Optional[Tensor], v_variance: Opti
     means, quats, scales, densities, beta, uncertainty = context.primitives
     if v_variance is not None and uncertainty is None:
         raise ValueError("v_variance requires uncertainty in the forward call")
-    with deferred_value_checks():
+    with deferred_value_checks(pending=True) as checks:
         v_image = _adjoint("v_image", v_image, context)
         v_variance = _adjoint("v_variance", v_variance, context)
     if means.shape[0] == 0 or (v_image is None and v_variance is None):
+        checks.check()
         return _consume(context, _zero_gradients(context))
     b = context.buffers
-    with torch.cuda.device(means.device):
+    # The VJP is enqueued before the adjoint checks resolve; on a failure its
+    # result is dropped and the context stays unconsumed.
+    with _resolving(checks), torch.cuda.device(means.device):
         grads = _fused.raster_backward(b["state"], means, quats, scales, densities, beta, uncertainty,
                                        b["viewmats"], b["Ks"], context.eps, v_image, v_variance,
                                        context.detach_variance)
@@ -290,7 +313,7 @@ def voxelize_fwd(
         ("means", "quats", "scales", "densities", "volume_extent", "volume_center", "beta", "uncertainty"),
         (means, quats, scales, densities, volume_extent, volume_center, beta, uncertainty),
     ))
-    with deferred_value_checks():
+    with deferred_value_checks(pending=True) as checks:
         depth, height, width = _shape("volume_shape", volume_shape, 3)
         if max(height, width) > 8 * 65535:
             raise ValueError("volume_shape exceeds CUDA grid limits")
@@ -307,12 +330,13 @@ def voxelize_fwd(
     shape = (depth, height, width)
     buffers = {"extent": extent, "center": center}
     if means.shape[0] == 0:
+        checks.check()
         volume = means.new_zeros(shape)
         output = volume if uncertainty is None else (volume, volume.clone())
     else:
         with torch.cuda.device(means.device):
             output, state = _fused.voxel_forward(means, quats, scales, densities, shape, extent, center, beta,
-                                                 uncertainty, eps, radius_clip)
+                                                 uncertainty, eps, radius_clip, before_count=checks.check)
         buffers.update(state=state, covars=state.covars, records=state.records, offsets=state.offsets,
                        isect_ids=state.isect_ids, flatten_ids=state.flatten_ids)
     context = _context("voxelize", shape, primitives, buffers, originals, eps, mode, detach_variance)
@@ -327,13 +351,14 @@ def voxelize_bwd(context: _Context, v_volume: Optional[Tensor], v_variance: Opti
     means, quats, scales, densities, beta, uncertainty = context.primitives
     if v_variance is not None and uncertainty is None:
         raise ValueError("v_variance requires uncertainty in the forward call")
-    with deferred_value_checks():
+    with deferred_value_checks(pending=True) as checks:
         v_volume = _adjoint("v_volume", v_volume, context)
         v_variance = _adjoint("v_variance", v_variance, context)
     if means.shape[0] == 0 or (v_volume is None and v_variance is None):
+        checks.check()
         return _consume(context, _zero_gradients(context))
     b = context.buffers
-    with torch.cuda.device(means.device):
+    with _resolving(checks), torch.cuda.device(means.device):
         grads = _fused.voxel_backward(b["state"], means, quats, scales, beta, uncertainty, b["extent"],
                                       b["center"], context.eps, v_volume, v_variance, context.detach_variance)
     return _consume(context, ParameterGradients(*grads))
