@@ -56,7 +56,7 @@ FLOPS_PER_EVAL = {
 }
 # DRAM bytes (read + write) of one record-parallel raster VJP launch at the CT
 # workload, from ncu (dram__bytes_read.sum + dram__bytes_write.sum, one pass).
-RASTER_VJP_TRAFFIC_BYTES = 569.6e6 + 371.2e6
+RASTER_VJP_TRAFFIC_BYTES = 536.2e6 + 367.7e6
 
 
 # --------------------------------------------------------------------------- utilities
@@ -85,7 +85,13 @@ def job_rate(units_per_rank_step: float, ranks: int, ms_per_step: float) -> floa
 
 
 class ClockSampler:
-    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+    """Samples nvidia-smi clocks and throttle reasons during the timed region.
+
+    The polling process is started before the warm-up, so its start-up does not
+    compete with the timed steps; ``mark(True)`` / ``mark(False)`` bracket the
+    timed region and the summary keeps the samples taken inside it (or the one
+    nearest to it when the region is shorter than the polling interval).
+    """
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -93,9 +99,13 @@ class ClockSampler:
 
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
-        self.samples: list[list[str]] = []
+        self.samples: list[tuple[float, list[str]]] = []
+        self.window = [None, None]
         self._proc = None
         self._thread = None
+
+    def mark(self, start: bool):
+        self.window[0 if start else 1] = time.monotonic()
 
     def __enter__(self):
         try:
@@ -104,6 +114,10 @@ class ClockSampler:
                  "-i", str(self.gpu)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self._thread = threading.Thread(target=self._read, daemon=True)
             self._thread.start()
+            # Let nvidia-smi finish starting up (first sample in) before any step runs.
+            deadline = time.monotonic() + 3.0
+            while not self.samples and time.monotonic() < deadline and self._proc.poll() is None:
+                time.sleep(0.01)
         except (OSError, ValueError):
             self._proc = None
         return self
@@ -112,7 +126,17 @@ class ClockSampler:
         for line in self._proc.stdout:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) >= 9:
-                self.samples.append(parts)
+                self.samples.append((time.monotonic(), parts))
+
+    def _timed_samples(self) -> list:
+        start, end = self.window
+        if start is None or end is None or not self.samples:
+            return [parts for _, parts in self.samples]
+        inside = [parts for t, parts in self.samples if start <= t <= end]
+        if inside:
+            return inside
+        nearest = min(self.samples, key=lambda item: min(abs(item[0] - start), abs(item[0] - end)))
+        return [nearest[1]]
 
     def __exit__(self, *exc):
         if self._proc is not None:
@@ -128,7 +152,7 @@ class ClockSampler:
     def summary(self) -> dict:
         clocks, maxes, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for s in self.samples:
+        for s in self._timed_samples():
             try:
                 clocks.append(float(s[1]))
                 maxes.append(float(s[2]))
@@ -339,7 +363,7 @@ def cpu_baseline(budget_s: float = 15.0) -> dict:
             "extrapolation": "not measured: dense evaluations of one full CT fit step divided by the measured rate"}
 
 
-def timed_run(step, scene, steps, warmup, device, flush_buf):
+def timed_run(step, scene, steps, warmup, device, flush_buf, clocks=None):
     """Device-resident inputs; per-step CUDA events with an L2 flush between steps."""
     from r2splat_b200 import _fused
 
@@ -347,6 +371,8 @@ def timed_run(step, scene, steps, warmup, device, flush_buf):
     for _ in range(warmup):
         step(*prims)
     torch.cuda.synchronize()
+    if clocks is not None:
+        clocks.mark(True)
     timer = _fused.StageTimer()
     total_ms = 0.0
     launches = 0
@@ -363,6 +389,8 @@ def timed_run(step, scene, steps, warmup, device, flush_buf):
         end.synchronize()
         total_ms += start.elapsed_time(end)
     torch.cuda.synchronize()
+    if clocks is not None:
+        clocks.mark(False)
     return total_ms, timer.totals_ms(), launches
 
 
@@ -560,7 +588,7 @@ def main(argv=None) -> int:
         dist.barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clocks:
-        total_ms, stages, own_launches = timed_run(step, scene, args.steps, args.warmup, device, flush_buf)
+        total_ms, stages, own_launches = timed_run(step, scene, args.steps, args.warmup, device, flush_buf, clocks)
     ranks = world if args.impl == "ours" else 1
     total_ms = max_over_ranks(total_ms, ranks, device)
     ms_per_step = total_ms / args.steps
