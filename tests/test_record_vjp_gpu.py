@@ -88,3 +88,55 @@ def test_record_vjp_matches_float64_with_degenerate_records(device, seed, dtype)
     scale = want.abs().amax(0).clamp(min=1e-12)
     err = ((got.double() - want).abs() / scale).amax(0)
     assert (err < 1e-4).all(), err.tolist()
+
+
+def _expected_beta_var(rec, q, v, vv):
+    """float64 Beta adjoints with the variance branch (q = 0 for a detached branch)."""
+    r = rec.double()
+    x, y, a, b, c, o, mu, beta = [r[:, i, None, None] for i in range(8)]
+    qq = q.double()[:, None, None]
+    py, px = torch.meshgrid(torch.arange(H, device=rec.device, dtype=torch.float64) + 0.5,
+                            torch.arange(W, device=rec.device, dtype=torch.float64) + 0.5, indexing="ij")
+    dx, dy = x - px, y - py
+    d2 = a * dx * dx + 2 * b * dx * dy + c * dy * dy
+    support = (d2 >= 0) & (d2 < 1)
+    h = torch.where(support, 1 - d2, torch.ones_like(d2))
+    vis = h ** beta
+    alpha = o * mu * vis
+    keep = support & (alpha.abs() >= 1e-5)
+    g, gv = v.double()[None], vv.double()[None]
+    v_eff = torch.where(keep, g + 2 * qq * alpha * gv, torch.zeros_like(d2))
+    w = -o * mu * beta * h ** (beta - 1) * v_eff
+    k = torch.where(keep, torch.ones_like(d2), torch.zeros_like(d2))
+    s = [(w * dx).sum((1, 2)), (w * dy).sum((1, 2)), (w * dx * dx).sum((1, 2)), (w * dx * dy).sum((1, 2)),
+         (w * dy * dy).sum((1, 2)), (v_eff * vis * k).sum((1, 2)), (v_eff * alpha * torch.log(h) * k).sum((1, 2)),
+         (gv * alpha * alpha * k).sum((1, 2))]
+    a, b, c, o, mu = [r[:, i] for i in range(2, 7)]
+    grads = torch.stack([2 * (a * s[0] + b * s[1]), 2 * (b * s[0] + c * s[1]), s[2], 2 * s[3], s[4], mu * s[5],
+                         o * s[5], s[6]], 1)
+    return grads, s[7]
+
+
+@pytest.mark.parametrize("detach", [False, True])
+def test_record_vjp_beta_variance_matches_float64(device, detach):
+    n = 96
+    rec = _records(device, n=n, seed=3)
+    gen = torch.Generator(device="cpu").manual_seed(13)
+    rec[:, 7] = (torch.rand(n, generator=gen) * 3.5 + 0.5).to(device)  # beta
+    rec[:, 2:5] *= 0.25  # Beta supports of a few pixels: d^2 < 1
+    q = (torch.rand(n, generator=gen) * 0.1).to(device)
+    v = torch.randn((H, W), generator=gen).to(device)
+    vv = (0.1 * torch.randn((H, W), generator=gen)).to(device)
+    rects = torch.tensor([0, 0, (W + T - 1) // T, (H + T - 1) // T], dtype=torch.int16, device=device).repeat(n, 1)
+    grads = torch.full((n, 8), float("nan"), device=device)
+    v_unc = torch.zeros(n, device=device)
+    _backend.call("r2s_raster_record_bwd", 0, rec.data_ptr(), rects.data_ptr(), q.data_ptr(), 1, int(detach),
+                  v.data_ptr(), vv.data_ptr(), 1, n, W, H, T, grads.data_ptr(), None, v_unc.data_ptr(),
+                  torch.cuda.current_stream(device).cuda_stream)
+    want, want_unc = _expected_beta_var(rec, torch.zeros_like(q) if detach else q, v, vv)
+    assert torch.isfinite(grads).all() and torch.isfinite(v_unc).all()
+    scale = want.abs().amax(0).clamp(min=1e-12)
+    err = ((grads.double() - want).abs() / scale).amax(0)
+    assert (err < 1e-4).all(), err.tolist()
+    unc_scale = want_unc.abs().max().clamp(min=1e-12)
+    assert ((v_unc.double() - want_unc).abs().max() / unc_scale).item() < 1e-4
