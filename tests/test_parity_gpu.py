@@ -453,3 +453,27 @@ def test_ct_scale_tile_lists_and_images_match_reference_build(device):
     vst = vctx.buffers["state"]
     assert torch.equal(vst.isect_ids, vsaved["isect_ids"]) and torch.equal(vst.flatten_ids, vsaved["flatten_ids"])
     torch.testing.assert_close(vol, ref_vol, atol=1e-6, rtol=1e-5)
+
+
+@needs_ref
+def test_ct_scale_gradients_match_reference_build(device):
+    """Full CT-scale fit-step gradients (record-parallel VJPs) against the reference build."""
+    sc = scenes.ct_scene().to(device)
+    img, ctx = r2s.rasterize_fwd(*sc.primitives, sc.viewmats, sc.Ks, sc.image_size)
+    _, saved = ref_ops.explicit_rasterize_fwd(*sc.primitives, sc.viewmats, sc.Ks, sc.image_size)
+    gen = torch.Generator().manual_seed(21)
+    v = (torch.randn(img.shape, generator=gen) / img.numel()).to(device)
+    g = r2s.rasterize_bwd(ctx, v)
+    r1 = ref_ops.explicit_rasterize_bwd(saved, sc.means, sc.quats, sc.scales, None, None, v)
+    r2 = ref_ops.explicit_rasterize_bwd(saved, sc.means, sc.quats, sc.scales, None, None, v)
+    for a, b, c in zip((g.means, g.quats, g.scales, g.densities), r1, r2):
+        _reference_gradients_close(a, b, c)
+    del ctx, saved, r1, r2
+    vol, vctx = r2s.voxelize_fwd(*sc.primitives, sc.volume_shape, volume_extent=(1, 1, 1))
+    _, vsaved = ref_ops.explicit_voxelize_fwd(*sc.primitives, sc.volume_shape, volume_extent=(1, 1, 1))
+    w = low.volume_loss_bwd(vol.unsqueeze(0), torch.ones(1, device=device), 0.05)[0]
+    g = r2s.voxelize_bwd(vctx, w)
+    r1 = ref_ops.explicit_voxelize_bwd(vsaved, sc.means, sc.quats, sc.scales, sc.densities, None, None, w)
+    r2 = ref_ops.explicit_voxelize_bwd(vsaved, sc.means, sc.quats, sc.scales, sc.densities, None, None, w)
+    for a, b, c in zip((g.means, g.quats, g.scales, g.densities), r1, r2):
+        _reference_gradients_close(a, b, c)
