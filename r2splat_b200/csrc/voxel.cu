@@ -283,7 +283,7 @@ __global__ void __launch_bounds__(kVoxBwdThreads) voxel_bwd_kernel(
     // The tile's adjoints are stored by rows of T voxels at a stride of T + 1,
     // so the lanes of a warp (one box row each) read distinct banks.
     const uint32_t RS = T + 1u;
-    const uint32_t tile_slots = T * T * RS;
+    const uint32_t tile_slots = T * T * RS + RS;  // + one zero row read by idle lanes
     Rec3D<S>* s_rec = reinterpret_cast<Rec3D<S>*>(smem);                          // [2][threads]
     VoxelBox* s_box = reinterpret_cast<VoxelBox*>(s_rec + 2 * kVoxBwdThreads);     // [threads]
     S* s_v = reinterpret_cast<S*>(s_box + kVoxBwdThreads);                         // [T^2][T+1] adjoint
@@ -317,6 +317,10 @@ __global__ void __launch_bounds__(kVoxBwdThreads) voxel_bwd_kernel(
         s_v[slot] = (ok && v_volume != nullptr) ? v_volume[vid] : S(0);
         if (kVar) s_vv[slot] = ok ? v_volume_var[vid] : S(0);
     }
+    // Row pads (x = T) and one zero row after the tile: the packed row walk
+    // reads them without a bounds test.
+    for (uint32_t p = t; p < T * T + RS; p += kVoxBwdThreads)
+        s_v[p < T * T ? p * RS + T : T * T * RS + (p - T * T)] = S(0);
 
     const int32_t n_batches = (count + kVoxBwdThreads - 1) / kVoxBwdThreads;
     auto load = [&](int32_t b, uint32_t stage) {
@@ -394,9 +398,14 @@ __global__ void __launch_bounds__(kVoxBwdThreads) voxel_bwd_kernel(
                     const float2 qk = splat2(K * kVoxNegLog2e), two = splat2(2.f);
                     float2 d1 = make_float2(px0 - r.x, px0 + 1.f - r.x);
                     float2 a1 = splat2(0.f), a2 = a1, a3 = a1;
+                    // Idle lanes read the zero row. With an odd width the second
+                    // sample of the last step is the next voxel of the row (or
+                    // the zero pad at x = T): it lies outside the record's box,
+                    // so its contribution test fails like the reference's.
+                    const uint32_t pz = valid ? p0 : T * T * RS;
                     for (uint32_t i = 0; i < w; i += 2u) {
-                        const float ga = valid ? s_v[p0 + i] : 0.f;
-                        const float gb = (valid && i + 1u < w) ? s_v[p0 + i + 1u] : 0.f;
+                        const float ga = s_v[pz + i];
+                        const float gb = s_v[pz + i + 1u];
                         const float2 e = fma2(fma2(qa, d1, ql), d1, qk);
                         const float2 vis = make_float2(exp2f(e.x), exp2f(e.y));
                         const bool ka = !(e.x > 0.f || e.x < e_min);
@@ -618,7 +627,7 @@ int launch_vfwd(const VoxelGeom& g, const Rec3D<S>* rec, bool beta, const int32_
 template <typename S, bool kBeta, bool kVar>
 int launch_vbwd_p(const VoxelGeom& g, const Rec3D<S>* rec, bool chain_var, const int32_t* offsets,
                   const int32_t* ids, const S* v_vol, const S* v_vol_var, Rec3D<S>* grads, cudaStream_t stream) {
-    const size_t tile_slots = size_t(g.T) * g.T * (g.T + 1);
+    const size_t tile_slots = size_t(g.T) * g.T * (g.T + 1) + (g.T + 1);
     const size_t smem = 2 * size_t(kVoxBwdThreads) * (sizeof(Rec3D<S>) + sizeof(int32_t)) +
                         size_t(kVoxBwdThreads) * sizeof(VoxelBox) + 2 * tile_slots * sizeof(S);
     R2S_TRY(allow_dynamic_smem(voxel_bwd_kernel<S, kBeta, kVar>, smem));
