@@ -54,6 +54,20 @@ FLOPS_PER_EVAL = {
     # + conic adjoints 11 + density / mu adjoints 6 -> 44.
     "raster_render": 16, "raster_render_bwd": 44,
 }
+# SFU operations per sample of the Beta raster VJP in the reference's form.
+BETA_VJP_MUFU_PER_EVAL = 5
+# Metric and workload description of each single-scene workload.
+WORKLOAD_TEXT = {
+    "ct": ("fwd+bwd Gaussian-sample evals/s (CT fit step: raster 64x512^2 + voxel 256^3 + TV)",
+           "ct-plain-gaussian: N=200000, C=64 views R=3, 512x512 f=600, volume 256^3, TV lambda 0.05"),
+    "ct4": ("fwd+bwd Gaussian-sample evals/s (CT fit step, 4 of the 64 views)",
+            "ct4: the CT scene with every 16th view (4 views), 512x512, volume 256^3, TV lambda 0.05"),
+    "small": ("fwd+bwd Gaussian-sample evals/s (small fit step: raster 4x64^2 + voxel 32^3 + TV)",
+              "small: N=2000, C=4, 64x64, volume 32^3, TV lambda 0.05"),
+    "beta": ("fwd+bwd Beta-sample evals/s (raster 128x768^2 + voxel 384^3, mean and variance outputs)",
+             "beta-uncertainty: N=500000, beta ~ U[0.5, 4], q ~ U[0, 0.1], C=128 views R=3, 768x768 f=900, "
+             "volume 384^3, adjoints v ~ N(0, 1) and v_var ~ N(0, 0.1), variance branch attached"),
+}
 # DRAM bytes (read + write) of one record-parallel raster VJP launch at the CT
 # workload, from ncu (dram__bytes_read.sum + dram__bytes_write.sum, one pass).
 RASTER_VJP_TRAFFIC_BYTES = 536.2e6 + 367.7e6
@@ -273,6 +287,79 @@ class ReferenceStep:
         return raster, voxel, r["isect_ids"].numel(), v["isect_ids"].numel()
 
 
+class _BetaAdjoints:
+    """Fixed seeded adjoints of the Beta workload: v ~ N(0, 1) for the mean outputs and N(0, 0.1) for the
+    variances, for the [C, H, W] images and the [D, H, W] volume."""
+
+    def __init__(self, scene):
+        device = scene.means.device
+        gen = torch.Generator(device="cpu").manual_seed(1)
+        c, (h, w) = scene.viewmats.shape[0], scene.image_size
+        self.v_image = torch.randn((c, h, w), generator=gen).to(device)
+        self.v_image_var = (0.1 * torch.randn((c, h, w), generator=gen)).to(device)
+        self.v_volume = torch.randn(scene.volume_shape, generator=gen).to(device)
+        self.v_volume_var = (0.1 * torch.randn(scene.volume_shape, generator=gen)).to(device)
+
+
+class OursBetaStep(_BetaAdjoints):
+    """Beta primitives with uncertainty through this package's explicit operators: rasterize and voxelize,
+    mean and variance outputs, variance branch attached."""
+
+    def __init__(self, scene, target=None):
+        import r2splat_b200 as r2s
+
+        super().__init__(scene)
+        self.r2s, self.scene, self.last = r2s, scene, {}
+
+    def __call__(self, means, quats, scales, densities, beta, uncertainty):
+        sc = self.scene
+        _, ctx = self.r2s.rasterize_fwd(means, quats, scales, densities, sc.viewmats, sc.Ks, sc.image_size, beta=beta,
+                                        uncertainty=uncertainty)
+        self.last["raster_state"] = ctx.buffers["state"]
+        g = self.r2s.rasterize_bwd(ctx, self.v_image, self.v_image_var)
+        _, vctx = self.r2s.voxelize_fwd(means, quats, scales, densities, sc.volume_shape,
+                                        volume_extent=sc.volume_extent, beta=beta, uncertainty=uncertainty)
+        self.last["voxel_state"] = vctx.buffers["state"]
+        gv = self.r2s.voxelize_bwd(vctx, self.v_volume, self.v_volume_var)
+        grads = tuple(a + b for a, b in zip((g.means, g.quats, g.scales, g.densities, g.beta, g.uncertainty),
+                                            (gv.means, gv.quats, gv.scales, gv.densities, gv.beta, gv.uncertainty)))
+        return grads[3].sum(), grads
+
+    eval_counts = OursStep.eval_counts
+
+
+class ReferenceBetaStep(_BetaAdjoints):
+    """The same Beta step on the reference's own CUDA kernels (oracle/_ref)."""
+
+    def __init__(self, scene, target=None):
+        from oracle import ref_ops
+
+        super().__init__(scene)
+        self.ref_ops, self.scene, self.last = ref_ops, scene, {}
+
+    def __call__(self, means, quats, scales, densities, beta, uncertainty):
+        sc, ro = self.scene, self.ref_ops
+        _, saved = ro.explicit_rasterize_fwd(means, quats, scales, densities, sc.viewmats, sc.Ks, sc.image_size,
+                                             beta=beta, uncertainty=uncertainty)
+        self.last["raster"] = saved
+        g = ro.explicit_rasterize_bwd(saved, means, quats, scales, beta, uncertainty, self.v_image,
+                                      self.v_image_var)
+        _, vsaved = ro.explicit_voxelize_fwd(means, quats, scales, densities, sc.volume_shape,
+                                             volume_extent=sc.volume_extent, beta=beta, uncertainty=uncertainty)
+        self.last["voxel"] = vsaved
+        gv = ro.explicit_voxelize_bwd(vsaved, means, quats, scales, densities, beta, uncertainty, self.v_volume,
+                                      self.v_volume_var)
+        grads = tuple(a + b for a, b in zip(g, gv) if a is not None and b is not None)
+        return grads[3].sum(), grads
+
+    eval_counts = ReferenceStep.eval_counts
+
+
+def step_inputs(scene) -> tuple:
+    """The per-step inputs of a workload: the primitives, plus beta and uncertainty when the scene has them."""
+    return tuple(t for t in (*scene.primitives, scene.beta, scene.uncertainty) if t is not None)
+
+
 def build_workload(device, workload: str):
     from r2splat_b200 import scenes
 
@@ -284,6 +371,9 @@ def build_workload(device, workload: str):
         scene.viewmats, scene.Ks = scene.viewmats[::16].contiguous(), scene.Ks[::16].contiguous()
     elif workload == "small":
         scene = scenes.small_scene()
+    elif workload == "beta":
+        # Beta primitives with uncertainty: N=500k, C=128 views, 768x768 (f=900), volume 384^3.
+        return scenes.beta_scene().to(device), None
     else:
         raise SystemExit(f"unknown workload {workload}")
     scene = scene.to(device)
@@ -367,7 +457,7 @@ def timed_run(step, scene, steps, warmup, device, flush_buf, clocks=None):
     """Device-resident inputs; per-step CUDA events with an L2 flush between steps."""
     from r2splat_b200 import _fused
 
-    prims = scene.primitives
+    prims = step_inputs(scene)
     for _ in range(warmup):
         step(*prims)
     torch.cuda.synchronize()
@@ -403,7 +493,7 @@ def library_launches() -> int:
 
 def e2e_run(step, scene, steps, warmup, device):
     """Public API with pinned host inputs copied in and gradients copied out each step."""
-    host = [t.detach().cpu().pin_memory() for t in scene.primitives]
+    host = [t.detach().cpu().pin_memory() for t in step_inputs(scene)]
     outs = None
     h2d = sum(t.numel() * t.element_size() for t in host)
     d2h = 0
@@ -429,7 +519,7 @@ def count_launches(step, scene, prefix: str) -> int:
     from torch.profiler import ProfilerActivity, profile
 
     with profile(activities=[ProfilerActivity.CUDA]) as prof:
-        step(*scene.primitives)
+        step(*step_inputs(scene))
         torch.cuda.synchronize()
     return sum(e.count for e in prof.key_averages() if prefix in e.key)
 
@@ -531,7 +621,7 @@ def main(argv=None) -> int:
     parser.add_argument("--steps", type=int, default=20)
     parser.add_argument("--warmup", type=int, default=3)
     parser.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    parser.add_argument("--workload", choices=("ct", "ct4", "small", "batched", "serve"), default="ct",
+    parser.add_argument("--workload", choices=("ct", "ct4", "small", "beta", "batched", "serve"), default="ct",
                         help="ct: the CT fit step (default); batched / serve: the multi-reconstruction forms")
     parser.add_argument("--scenes", type=int, default=32, help="reconstructions for --workload batched/serve")
     parser.add_argument("--requests", type=int, default=400, help="requests for --workload serve")
@@ -576,10 +666,13 @@ def main(argv=None) -> int:
             return 0
 
     scene, target = build_workload(device, args.workload)
-    step = OursStep(scene, target) if args.impl == "ours" else ReferenceStep(scene, target)
+    if args.workload == "beta":
+        step = OursBetaStep(scene) if args.impl == "ours" else ReferenceBetaStep(scene)
+    else:
+        step = OursStep(scene, target) if args.impl == "ours" else ReferenceStep(scene, target)
     if args.profile_only:
         for _ in range(args.warmup):
-            step(*scene.primitives)
+            step(*step_inputs(scene))
         torch.cuda.synchronize()
         return 0
     flush_buf = torch.zeros(L2_FLUSH_BYTES // 4, device=device)
@@ -606,7 +699,7 @@ def main(argv=None) -> int:
 
     peaks = measured_peaks()
     result = {
-        "metric": "fwd+bwd Gaussian-sample evals/s (CT fit step: raster 64x512^2 + voxel 256^3 + TV)",
+        "metric": WORKLOAD_TEXT[args.workload][0],
         "value": value,
         "unit": "evals/s",
         "n_gpus": world,
@@ -620,8 +713,7 @@ def main(argv=None) -> int:
         "dtype": "f32",
         "data": "synthetic (seeded scene generator, r2splat_b200/scenes.py)",
         "config": {
-            "workload": "ct-plain-gaussian: N=200000, C=64 views R=3, 512x512 f=600, volume 256^3, TV lambda 0.05"
-            if args.workload == "ct" else "small: N=2000, C=4, 64x64, volume 32^3",
+            "workload": WORKLOAD_TEXT[args.workload][1],
             "raster_isects": m2, "voxel_isects": m3,
             "raster_evals_per_pass": raster_evals, "voxel_evals_per_pass": voxel_evals,
             "l2": "flushed (512 MiB write) between timed steps",
@@ -640,6 +732,20 @@ def main(argv=None) -> int:
             "sample": "the reference's own CUDA kernels (compiled unmodified from its sources for sm_100a) on the "
                       "same B200, driven by its explicit.py call sequence; the reference has no CPU implementation "
                       "of these operators",
+        }
+    elif args.workload == "beta":
+        # Beta VJP samples are SFU-bound: the reference's per-sample form takes h^beta (lg2 + ex2),
+        # h^(beta - 1) (lg2 + ex2) and log h (lg2).
+        kernel_ms = stages.get("raster_render_bwd", 0.0) / args.steps
+        peak = sfu_peak_gops(device)
+        achieved = BETA_VJP_MUFU_PER_EVAL * raster_evals / (kernel_ms * 1e-3) / 1e9 if kernel_ms else None
+        result["roofline"] = {
+            "kernel": "raster_record_bwd_kernel (record-parallel raster VJP, Beta with the variance branch)",
+            "bound": "sfu",
+            "work": "algorithmic: 5 MUFU operations x the reference's tile samples of one raster VJP pass",
+            "achieved": achieved, "peak": peak, "unit": "G MUFU/s",
+            "frac": achieved / peak if achieved else None, "traffic": None,
+            "peak_source": "measured in-bench: SFU ex2 probe r2s_sfu_peak_probe",
         }
     else:
         kernel = "raster_render_bwd"
