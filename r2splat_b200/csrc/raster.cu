@@ -348,8 +348,12 @@ __device__ __forceinline__ void vjp_sample(const Rec2D<S>& r, S om, S q, S px, S
         const S d2 = r.a * dx * dx + static_cast<S>(2) * r.b * dx * dy + r.c * dy * dy;
         const S h_raw = static_cast<S>(1) - d2;
         const bool in_support = valid && !(d2 < static_cast<S>(0) || h_raw <= static_cast<S>(0));
-        const S h = in_support ? h_raw : S(1);  // keeps pow/log finite on skipped samples
-        const S vis_raw = pow(h, r.beta);
+        const S h = in_support ? h_raw : S(1);  // keeps the logarithm finite on skipped samples
+        // h^beta = 2^(beta log2 h) for h in (0, 1]; log2 h also gives ln h and, with one
+        // division, h^(beta - 1) = h^beta / h: three special-function operations a sample
+        // instead of the five of pow(h, beta), pow(h, beta - 1) and log(h).
+        const S lg = log2(h);
+        const S vis_raw = exp2(r.beta * lg);
         const S alpha_raw = om * vis_raw;
         const bool keep = in_support && !(fabs(alpha_raw) < static_cast<S>(1e-5));
         const S vis = keep ? vis_raw : S(0);
@@ -359,7 +363,7 @@ __device__ __forceinline__ void vjp_sample(const Rec2D<S>& r, S om, S q, S px, S
             part[7] += vv * alpha * alpha;
             v += static_cast<S>(2) * q * alpha * vv;
         }
-        const S w = -om * r.beta * pow(h, r.beta - static_cast<S>(1)) * v;
+        const S w = -om * r.beta * (vis_raw / h) * v;
         const S wx = w * dx, wy = w * dy;
         part[0] += wx;
         part[1] += wy;
@@ -367,7 +371,7 @@ __device__ __forceinline__ void vjp_sample(const Rec2D<S>& r, S om, S q, S px, S
         part[3] += wx * dy;
         part[4] += wy * dy;
         part[5] += v * vis;
-        part[6] += v * alpha * log(h);
+        part[6] += v * alpha * (lg * static_cast<S>(0.6931471805599453));  // ln h = ln 2 log2 h
         if (kAbs) {
             g_ax += fabs(static_cast<S>(2) * (r.a * wx + r.b * wy));
             g_ay += fabs(static_cast<S>(2) * (r.b * wx + r.c * wy));

@@ -450,8 +450,11 @@ __global__ void __launch_bounds__(kVoxBwdThreads) voxel_bwd_kernel(
                         const S qf = a * d1 * d1 + L * d1 + K;
                         const S h_raw = static_cast<S>(1) - qf;
                         const bool in_support = valid && !(qf < static_cast<S>(0) || h_raw <= static_cast<S>(0));
-                        const S hh = in_support ? h_raw : S(1);  // keeps pow/log finite on skipped samples
-                        const S vis_raw = pow(hh, r.beta);
+                        const S hh = in_support ? h_raw : S(1);  // keeps the logarithm finite on skipped samples
+                        // hh^beta = 2^(beta log2 hh); log2 hh also gives ln hh and, with one
+                        // division, hh^(beta - 1) = hh^beta / hh.
+                        const S lg = log2(hh);
+                        const S vis_raw = exp2(r.beta * lg);
                         const S alpha_raw = opac * vis_raw;
                         const bool keep = in_support && !(fabs(alpha_raw) < static_cast<S>(1e-5));
                         const S vis = keep ? vis_raw : S(0);
@@ -461,9 +464,9 @@ __global__ void __launch_bounds__(kVoxBwdThreads) voxel_bwd_kernel(
                             A4 += vv * alpha * alpha;
                             v += static_cast<S>(2) * uq * alpha * vv;
                         }
-                        wgt = -opac * r.beta * pow(hh, r.beta - static_cast<S>(1)) * v;
+                        wgt = -opac * r.beta * (vis_raw / hh) * v;
                         A3 += v * vis;
-                        A5 += v * alpha * log(hh);
+                        A5 += v * alpha * (lg * static_cast<S>(0.6931471805599453));  // ln hh = ln 2 log2 hh
                     }
                     const S wd = wgt * d1;
                     A0 += wgt;
