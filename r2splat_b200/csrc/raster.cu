@@ -576,7 +576,7 @@ constexpr float kNegLog2e = -1.4426950408889634f;
 // With w = -g alpha = -(o mu) g vis, the walk sums g vis and its moments and
 // scales them by -(o mu) once: part[0..4] are S0..S4 and part[5] = S5 of
 // vjp_sample.
-__device__ __forceinline__ void record_walk_packed(const Rec2D<float>& r, float om, const float* vimg,
+__device__ __forceinline__ void record_walk_packed(const Rec2D<float>& r, float om, float e_min, const float* vimg,
                                                    uint32_t bx0, uint32_t by0, uint32_t bw, uint32_t barea,
                                                    uint32_t magic, uint32_t width, float (&part)[8]) {
     const uint32_t lane = threadIdx.x & 31u;
@@ -596,7 +596,6 @@ __device__ __forceinline__ void record_walk_packed(const Rec2D<float>& r, float 
     const float2 nx = splat2(-r.x), ny = splat2(-r.y);
     const float2 qa = splat2(0.5f * r.a * kNegLog2e), qb = splat2(r.b * kNegLog2e);
     const float2 qc = splat2(0.5f * r.c * kNegLog2e);
-    const float e_min = log2f(1e-5f / fabsf(om));
     float2 acc0 = splat2(0.f), acc1 = acc0, acc2 = acc0, acc3 = acc0, acc4 = acc0, acc5 = acc0;
     const uint32_t iters = (barea + 63u) >> 6;
     uint32_t k = lane;
@@ -641,6 +640,17 @@ __device__ __forceinline__ void record_walk_packed(const Rec2D<float>& r, float 
     part[7] = 0.f;
 }
 
+// A record's walk constants, set up by the lane that loaded the record and
+// read by the whole warp from shared memory (broadcast loads).
+template <typename S>
+struct alignas(16) RecordStage {
+    Rec2D<S> r;
+    uint32_t x0, y0, w, area;
+    uint32_t magic, cam;
+    S q;
+    float e_min;
+};
+
 template <typename S, bool kBeta, bool kVar, bool kAbs>
 __global__ void __launch_bounds__(kRecBwdThreads) raster_record_bwd_kernel(
     const Rec2D<S>* __restrict__ records, const ushort4* __restrict__ rects, const S* __restrict__ var_q,
@@ -657,8 +667,11 @@ __global__ void __launch_bounds__(kRecBwdThreads) raster_record_bwd_kernel(
     const bool packed = kPacked && v_render != nullptr && uint64_t(width) * height < (uint64_t(1) << 22);
     // Each warp takes 32 consecutive records at a time. Lane-parallel set-up:
     // lane L loads record base + L (coalesced) and computes its pixel box and
-    // stepping constants; the warp then walks the 32 records one by one,
-    // broadcasting each record's constants with shuffles.
+    // stepping constants into the warp's shared-memory stage; the warp then
+    // walks the 32 records one by one, reading each record's constants with
+    // broadcast loads.
+    __shared__ RecordStage<S> s_stage[kRecBwdThreads];
+    RecordStage<S>* stage = s_stage + (threadIdx.x & ~31u);
     for (size_t base = (size_t(blockIdx.x) * warps_per_block + (threadIdx.x >> 5)) * 32u; base < total;
          base += group_stride) {
         const size_t my_rid = base + lane;
@@ -695,37 +708,41 @@ __global__ void __launch_bounds__(kRecBwdThreads) raster_record_bwd_kernel(
             }
         }
         uint32_t pending = __ballot_sync(0xffffffffu, area != 0u);
+        __syncwarp();  // the previous group's constants have been read
+        if (area != 0u) {
+            RecordStage<S> st;
+            st.r = mine;
+            st.x0 = x0;
+            st.y0 = y0;
+            st.w = w;
+            st.area = area;
+            st.magic = magic;
+            st.cam = my_cam;
+            st.q = my_q;
+            st.e_min = kPacked ? log2f(1e-5f / fabsf(float(mine.o * mine.mu))) : 0.f;
+            stage[lane] = st;
+        }
+        __syncwarp();
         while (pending != 0u) {
             const uint32_t j = __ffs(pending) - 1u;
             pending &= pending - 1u;
-            Rec2D<S> r;
-            r.x = __shfl_sync(0xffffffffu, mine.x, j);
-            r.y = __shfl_sync(0xffffffffu, mine.y, j);
-            r.a = __shfl_sync(0xffffffffu, mine.a, j);
-            r.b = __shfl_sync(0xffffffffu, mine.b, j);
-            r.c = __shfl_sync(0xffffffffu, mine.c, j);
-            r.o = __shfl_sync(0xffffffffu, mine.o, j);
-            r.mu = __shfl_sync(0xffffffffu, mine.mu, j);
-            r.beta = kBeta ? __shfl_sync(0xffffffffu, mine.beta, j) : S(0);
-            const uint32_t bx0 = __shfl_sync(0xffffffffu, x0, j);
-            const uint32_t by0 = __shfl_sync(0xffffffffu, y0, j);
-            const uint32_t bw = __shfl_sync(0xffffffffu, w, j);
-            const uint32_t barea = __shfl_sync(0xffffffffu, area, j);
+            const RecordStage<S> st = stage[j];
+            const Rec2D<S>& r = st.r;
+            const uint32_t bx0 = st.x0, by0 = st.y0, bw = st.w, barea = st.area;
             const size_t rid = base + j;
-            const uint32_t cam = __shfl_sync(0xffffffffu, my_cam, j);
+            const uint32_t cam = st.cam;
             const uint32_t n = uint32_t(rid) - cam * N;
             const size_t cam_base = size_t(cam) * height * width;
             const S* vimg = v_render != nullptr ? v_render + cam_base : nullptr;
             const S* vvar = kVar ? v_render_var + cam_base : nullptr;
-            const S q = chain_var ? __shfl_sync(0xffffffffu, my_q, j) : S(0);
+            const S q = chain_var ? st.q : S(0);
             const S om = r.o * r.mu;
             S part[8];
             S g_ax = S(0), g_ay = S(0);
             bool walked = false;
             if constexpr (kPacked) {
                 if (packed) {
-                    const uint32_t bmagic = __shfl_sync(0xffffffffu, magic, j);
-                    record_walk_packed(r, om, vimg, bx0, by0, bw, barea, bmagic, width, part);
+                    record_walk_packed(r, om, st.e_min, vimg, bx0, by0, bw, barea, st.magic, width, part);
                     walked = true;
                 }
             }
