@@ -61,6 +61,8 @@ def _resolving(checks):
     """Resolves pending input checks after the block's device work is enqueued.
 
     A failing check is raised in preference to an error of the block itself.
+    Checks already resolved inside the block (before a host read) are not
+    evaluated again.
     """
     try:
         yield
@@ -243,7 +245,7 @@ def _rasterize_fwd(means, quats, scales, densities, viewmats, Ks, image_size, be
                                                     image_loss[0], image_loss[1], image_loss[2], image, None,
                                                     means.device)
     else:
-        with torch.cuda.device(means.device):
+        with _resolving(checks), torch.cuda.device(means.device):
             # The input checks resolve just before the intersection count is read.
             result = _fused.raster_forward(means, quats, scales, densities, viewmats, Ks, width, height, beta,
                                            uncertainty, eps, radius_clip, image_loss=image_loss,
@@ -334,7 +336,7 @@ def voxelize_fwd(
         volume = means.new_zeros(shape)
         output = volume if uncertainty is None else (volume, volume.clone())
     else:
-        with torch.cuda.device(means.device):
+        with _resolving(checks), torch.cuda.device(means.device):
             output, state = _fused.voxel_forward(means, quats, scales, densities, shape, extent, center, beta,
                                                  uncertainty, eps, radius_clip, before_count=checks.check)
         buffers.update(state=state, covars=state.covars, records=state.records, offsets=state.offsets,
