@@ -54,8 +54,11 @@ FLOPS_PER_EVAL = {
     # + conic adjoints 11 + density / mu adjoints 6 -> 44.
     "raster_render": 16, "raster_render_bwd": 44,
 }
-# SFU operations per sample of the Beta raster VJP in the reference's form.
-BETA_VJP_MUFU_PER_EVAL = 5
+# FP32 operations per sample of the Beta raster VJP with the variance branch in the reference's form
+# (RasterizeToPixelsBwd.cu:817-1046), multiplies and adds counted separately: offsets 2, d^2 9, h 1,
+# pow argument 1, alpha 1, variance terms 7, w with h^(beta - 1) 6, w dx and w dy 2, their moments 8,
+# g vis 2, g alpha ln h 4.
+BETA_VAR_VJP_FLOPS_PER_EVAL = 43
 # Metric and workload description of each single-scene workload.
 WORKLOAD_TEXT = {
     "ct": ("fwd+bwd Gaussian-sample evals/s (CT fit step: raster 64x512^2 + voxel 256^3 + TV)",
@@ -64,6 +67,8 @@ WORKLOAD_TEXT = {
             "ct4: the CT scene with every 16th view (4 views), 512x512, volume 256^3, TV lambda 0.05"),
     "small": ("fwd+bwd Gaussian-sample evals/s (small fit step: raster 4x64^2 + voxel 32^3 + TV)",
               "small: N=2000, C=4, 64x64, volume 32^3, TV lambda 0.05"),
+    "beta8": ("fwd+bwd Beta-sample evals/s (Beta workload, 8 of the 128 views)",
+              "beta8: the Beta workload with every 16th view (8 views), 768x768, volume 384^3"),
     "beta": ("fwd+bwd Beta-sample evals/s (raster 128x768^2 + voxel 384^3, mean and variance outputs)",
              "beta-uncertainty: N=500000, beta ~ U[0.5, 4], q ~ U[0, 0.1], C=128 views R=3, 768x768 f=900, "
              "volume 384^3, adjoints v ~ N(0, 1) and v_var ~ N(0, 0.1), variance branch attached"),
@@ -371,9 +376,13 @@ def build_workload(device, workload: str):
         scene.viewmats, scene.Ks = scene.viewmats[::16].contiguous(), scene.Ks[::16].contiguous()
     elif workload == "small":
         scene = scenes.small_scene()
-    elif workload == "beta":
-        # Beta primitives with uncertainty: N=500k, C=128 views, 768x768 (f=900), volume 384^3.
-        return scenes.beta_scene().to(device), None
+    elif workload in ("beta", "beta8"):
+        # Beta primitives with uncertainty: N=500k, C=128 views, 768x768 (f=900), volume 384^3;
+        # beta8 is the profiling case with every 16th view (8 views).
+        scene = scenes.beta_scene()
+        if workload == "beta8":
+            scene.viewmats, scene.Ks = scene.viewmats[::16].contiguous(), scene.Ks[::16].contiguous()
+        return scene.to(device), None
     else:
         raise SystemExit(f"unknown workload {workload}")
     scene = scene.to(device)
@@ -621,7 +630,7 @@ def main(argv=None) -> int:
     parser.add_argument("--steps", type=int, default=20)
     parser.add_argument("--warmup", type=int, default=3)
     parser.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    parser.add_argument("--workload", choices=("ct", "ct4", "small", "beta", "batched", "serve"), default="ct",
+    parser.add_argument("--workload", choices=("ct", "ct4", "small", "beta", "beta8", "batched", "serve"), default="ct",
                         help="ct: the CT fit step (default); batched / serve: the multi-reconstruction forms")
     parser.add_argument("--scenes", type=int, default=32, help="reconstructions for --workload batched/serve")
     parser.add_argument("--requests", type=int, default=400, help="requests for --workload serve")
@@ -666,7 +675,7 @@ def main(argv=None) -> int:
             return 0
 
     scene, target = build_workload(device, args.workload)
-    if args.workload == "beta":
+    if args.workload in ("beta", "beta8"):
         step = OursBetaStep(scene) if args.impl == "ours" else ReferenceBetaStep(scene)
     else:
         step = OursStep(scene, target) if args.impl == "ours" else ReferenceStep(scene, target)
@@ -733,19 +742,21 @@ def main(argv=None) -> int:
                       "same B200, driven by its explicit.py call sequence; the reference has no CPU implementation "
                       "of these operators",
         }
-    elif args.workload == "beta":
-        # Beta VJP samples are SFU-bound: the reference's per-sample form takes h^beta (lg2 + ex2),
-        # h^(beta - 1) (lg2 + ex2) and log h (lg2).
+    elif args.workload in ("beta", "beta8"):
+        # The Beta VJP with the variance branch is bound by instruction issue (ncu: XU 15 %, issue 74 %);
+        # its roofline counts the FP32 operations of the reference's per-sample form.
         kernel_ms = stages.get("raster_render_bwd", 0.0) / args.steps
-        peak = sfu_peak_gops(device)
-        achieved = BETA_VJP_MUFU_PER_EVAL * raster_evals / (kernel_ms * 1e-3) / 1e9 if kernel_ms else None
+        peak = fp32_peak_tflops(device)
+        achieved = BETA_VAR_VJP_FLOPS_PER_EVAL * raster_evals / (kernel_ms * 1e-3) / 1e12 if kernel_ms else None
         result["roofline"] = {
             "kernel": "raster_record_bwd_kernel (record-parallel raster VJP, Beta with the variance branch)",
-            "bound": "sfu",
-            "work": "algorithmic: 5 MUFU operations x the reference's tile samples of one raster VJP pass",
-            "achieved": achieved, "peak": peak, "unit": "G MUFU/s",
+            "bound": "fp32",
+            "work": f"algorithmic: {BETA_VAR_VJP_FLOPS_PER_EVAL} FP32 ops (and 5 MUFU) x the reference's tile samples "
+                    "of one raster VJP pass; the kernel evaluates only the samples inside each record's box",
+            "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
             "frac": achieved / peak if achieved else None, "traffic": None,
-            "peak_source": "measured in-bench: SFU ex2 probe r2s_sfu_peak_probe",
+            "peak_source": "measured in-bench: FP32 FMA probe r2s_fp32_peak_probe",
+            "sfu_peak_gex2_s_measured": sfu_peak_gops(device),
         }
     else:
         kernel = "raster_render_bwd"
