@@ -160,10 +160,10 @@ __global__ void __launch_bounds__(kMaxThreads) raster_fwd_kernel(
     uint32_t C, uint32_t width, uint32_t height, uint32_t T, uint32_t tiles_x, uint32_t n_tiles,
     S* __restrict__ render, S* __restrict__ render_var, uint32_t B, ImageLossEpilogue<S> loss) {
     extern __shared__ __align__(16) unsigned char smem[];  // B = records staged per batch (<= blockDim.x)
-    Rec2D<S>* s_rec = reinterpret_cast<Rec2D<S>*>(smem);          // [2][B]
-    S* s_q = reinterpret_cast<S*>(s_rec + 2 * B);                   // [2][B]
-    uint2* s_mask = reinterpret_cast<uint2*>(s_q + 2 * B);          // [B] (column, row) masks
-    uint16_t* s_hits = reinterpret_cast<uint16_t*>(s_mask + B);     // [warps][32] hit lists
+    Rec2D<S>* s_rec = reinterpret_cast<Rec2D<S>*>(smem);          // [3][B]
+    S* s_q = reinterpret_cast<S*>(s_rec + 3 * B);                   // [3][B]
+    uint2* s_mask = reinterpret_cast<uint2*>(s_q + 3 * B);          // [2][B] (column, row) masks
+    uint16_t* s_hits = reinterpret_cast<uint16_t*>(s_mask + 2 * B); // [warps][32] hit lists
 
     const uint32_t tile = blockIdx.x, cam = blockIdx.y;
     const uint32_t key = cam * n_tiles + tile;
@@ -205,20 +205,21 @@ __global__ void __launch_bounds__(kMaxThreads) raster_fwd_kernel(
     if (n_batches > 0) load(0, 0);
     for (int32_t bi = 0; bi < n_batches; ++bi) {
         if (bi + 1 < n_batches) {
-            load(bi + 1, uint32_t(bi + 1) & 1u);
+            load(bi + 1, uint32_t(bi + 1) % 3u);
             cp_async_wait<1>();
         } else {
             cp_async_wait<0>();
         }
         __syncthreads();
-        const uint32_t stage = uint32_t(bi) & 1u;
+        const uint32_t stage = uint32_t(bi) % 3u;
         const Rec2D<S>* buf = s_rec + stage * B;
         const S* qbuf = s_q + stage * B;
+        uint2* masks = s_mask + (uint32_t(bi) & 1u) * B;
         const int32_t batch = min(int32_t(B), count - bi * int32_t(B));
         if (int32_t(t) < batch) {
             Rec2D<S>& rec = s_rec[stage * B + t];
             const TileBox box = record_box<S, kBeta>(rec, ox, oy, vx, vy);
-            s_mask[t] = make_uint2(box.cols, box.rows);
+            masks[t] = make_uint2(box.cols, box.rows);
             rec.o = rec.o * rec.mu;  // o mu, once per record (the samples use only the product)
         }
         __syncthreads();
@@ -226,7 +227,7 @@ __global__ void __launch_bounds__(kMaxThreads) raster_fwd_kernel(
             for (int32_t base = 0; base < batch; base += 32) {
                 bool hit = false;
                 if (base + int32_t(lane) < batch) {
-                    const uint2 m = s_mask[base + int32_t(lane)];
+                    const uint2 m = masks[base + int32_t(lane)];
                     hit = (m.x & warp_cols) != 0u && (m.y & warp_rows) != 0u;
                 }
                 // The warp's hits, compacted in lane (= list) order.
@@ -267,7 +268,10 @@ __global__ void __launch_bounds__(kMaxThreads) raster_fwd_kernel(
                 __syncwarp();  // the list is rewritten for the next 32 records
             }
         }
-        __syncthreads();
+        // No barrier here. The next iteration's load goes to the third record
+        // buffer, which no warp can still be reading: its batch was evaluated
+        // before the previous iteration's first barrier. The masks alternate
+        // between two buffers.
     }
     const size_t pid = size_t(cam) * height * width + size_t(oy + ly) * width + (ox + lx);
     if (inside) {
@@ -477,7 +481,7 @@ __global__ void __launch_bounds__(kBwdThreads) raster_bwd_kernel(
     load(0, 0);
     for (int32_t bi = 0; bi < n_batches; ++bi) {
         if (bi + 1 < n_batches) {
-            load(bi + 1, uint32_t(bi + 1) & 1u);
+            load(bi + 1, uint32_t(bi + 1) % 3u);
             cp_async_wait<1>();
         } else {
             cp_async_wait<0>();
@@ -878,7 +882,7 @@ int launch_fwd_p(const RasterGeom& g, const Rec2D<S>* rec, const S* unc, const i
     unsigned batch = g.stage_batch < kFwdBatch ? g.stage_batch : kFwdBatch;
     if (batch > nthreads) batch = nthreads;
     if (batch < 1) batch = 1;
-    const size_t smem = 2 * size_t(batch) * (sizeof(Rec2D<S>) + sizeof(S)) + size_t(batch) * sizeof(uint2) +
+    const size_t smem = 3 * size_t(batch) * (sizeof(Rec2D<S>) + sizeof(S)) + 2 * size_t(batch) * sizeof(uint2) +
                         size_t(nthreads) * sizeof(uint16_t);
     dim3 grid(g.tiles_x * g.tiles_y, g.C);
     if (nthreads <= 256) {

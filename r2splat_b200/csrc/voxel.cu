@@ -51,7 +51,7 @@ __global__ void __launch_bounds__(256) voxel_fwd_kernel(const Rec3D<S>* __restri
                                                         S* __restrict__ volume, S* __restrict__ volume_var) {
     extern __shared__ __align__(16) unsigned char smem[];
     const uint32_t nthreads = blockDim.x;
-    Rec3D<S>* s_rec = reinterpret_cast<Rec3D<S>*>(smem);  // [2][nthreads]
+    Rec3D<S>* s_rec = reinterpret_cast<Rec3D<S>*>(smem);  // [3][nthreads]
     const uint32_t T = g.T;
     const uint32_t n_tiles = g.tiles_x * g.tiles_y * g.tiles_z;
     const uint32_t key = blockIdx.x;
@@ -106,13 +106,13 @@ __global__ void __launch_bounds__(256) voxel_fwd_kernel(const Rec3D<S>* __restri
     if (n_batches > 0) load(0, 0);
     for (int32_t b = 0; b < n_batches; ++b) {
         if (b + 1 < n_batches) {
-            load(b + 1, (b + 1) & 1);
+            load(b + 1, (b + 1) % 3);
             cp_async_wait<1>();
         } else {
             cp_async_wait<0>();
         }
         __syncthreads();
-        const Rec3D<S>* buf = s_rec + (b & 1) * nthreads;
+        const Rec3D<S>* buf = s_rec + (b % 3) * nthreads;
         const int32_t batch = min(int32_t(nthreads), count - b * int32_t(nthreads));
         for (int32_t s = 0; s < batch; ++s) {
             const Rec3D<S> r = buf[s];
@@ -166,7 +166,8 @@ __global__ void __launch_bounds__(256) voxel_fwd_kernel(const Rec3D<S>* __restri
                 }
             }
         }
-        __syncthreads();
+        // No barrier here: the next load goes to the third buffer, whose batch
+        // every thread finished before this iteration's barrier.
     }
 #pragma unroll
     for (int k = 0; k < PPT; ++k) {
@@ -593,7 +594,7 @@ inline int check_vgeom(const VoxelGeom& g) {
 template <typename S, bool kBeta, bool kVar, int PPT>
 int launch_vfwd_t(const VoxelGeom& g, const Rec3D<S>* rec, const int32_t* offsets, const int32_t* ids, S* vol,
                   S* vol_var, unsigned nthreads, cudaStream_t stream) {
-    const size_t smem = 2 * nthreads * sizeof(Rec3D<S>);
+    const size_t smem = 3 * nthreads * sizeof(Rec3D<S>);
     if (smem > 48 * 1024)
         cudaFuncSetAttribute(voxel_fwd_kernel<S, kBeta, kVar, PPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              int(smem));
