@@ -121,20 +121,30 @@ __global__ void __launch_bounds__(256) voxel_fwd_kernel(const Rec3D<S>* __restri
                 // (nvcc -O3 --use_fast_math fuses the first product of each
                 // sum): S3 = fma(c22 d3, d3, fma(c00 d1, d1, (c11 d2) d2)),
                 // sigma = fma(c12 d2, d3, fma(c02 d1, d3, fma(1/2, S3,
-                // (c01 d1) d2))). The d2/d3 factors are shared by the row.
+                // (c01 d1) d2))). The d2/d3 factors are shared by the row, and the
+                // four voxels go two at a time through packed FP32x2 operations,
+                // each component rounding as the scalar operation does.
                 const float d2 = py[0] - r.y, d3 = pz[0] - r.z;
                 const float b2 = __fmul_rn(__fmul_rn(r.c11, d2), d2);
                 const float c22d3 = __fmul_rn(r.c22, d3), c12d2 = __fmul_rn(r.c12, d2);
+                const float2 nx = splat2(-r.x), c00 = splat2(r.c00), c01 = splat2(r.c01), c02 = splat2(r.c02);
+                const float2 b22 = splat2(b2), c22d32 = splat2(c22d3), c12d22 = splat2(c12d2);
+                const float2 d22 = splat2(d2), d32 = splat2(d3), half = splat2(0.5f);
 #pragma unroll
-                for (int k = 0; k < PPT; ++k) {
-                    const float d1 = px[k] - r.x;
-                    const float s3 = __fmaf_rn(c22d3, d3, __fmaf_rn(__fmul_rn(r.c00, d1), d1, b2));
-                    const float la = __fmaf_rn(0.5f, s3, __fmul_rn(__fmul_rn(r.c01, d1), d2));
-                    const float sigma = __fmaf_rn(c12d2, d3, __fmaf_rn(__fmul_rn(r.c02, d1), d3, la));
-                    const float alpha = r.o * exp(-sigma);
-                    if (!(sigma < 0.f || fabs(alpha) < 1e-6f)) {
-                        acc[k] += alpha;
-                        if (kVar) accv[k] += r.q * alpha * alpha;
+                for (int k = 0; k < PPT; k += 2) {
+                    const float2 d1 = add2(make_float2(px[k], px[k + 1]), nx);
+                    const float2 s3 = fma2(c22d32, d32, fma2(mul2(c00, d1), d1, b22));
+                    const float2 la = fma2(half, s3, mul2(mul2(c01, d1), d22));
+                    const float2 sigma = fma2(c12d22, d32, fma2(mul2(c02, d1), d32, la));
+                    const float alpha0 = r.o * exp(-sigma.x);
+                    const float alpha1 = r.o * exp(-sigma.y);
+                    if (!(sigma.x < 0.f || fabs(alpha0) < 1e-6f)) {
+                        acc[k] += alpha0;
+                        if (kVar) accv[k] += r.q * alpha0 * alpha0;
+                    }
+                    if (!(sigma.y < 0.f || fabs(alpha1) < 1e-6f)) {
+                        acc[k + 1] += alpha1;
+                        if (kVar) accv[k + 1] += r.q * alpha1 * alpha1;
                     }
                 }
                 continue;
