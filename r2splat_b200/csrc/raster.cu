@@ -310,6 +310,148 @@ __global__ void __launch_bounds__(kMaxThreads) raster_fwd_kernel(
     }
 }
 
+// Gaussian forward (fp32, no variance branch) with two pixels per lane: lane
+// (x, y) of a warp's 8x8 pixel block owns pixels (x, y) and (x, y + 4), which
+// share dx, so a x dx and b dx are computed once per record and the two
+// samples go through packed FP32x2 operations. The reference's sigma is
+// written with the contraction nvcc applies to its source expression there,
+// fma(b dx, dy, 1/2 fma(a dx, dx, (c dy) dy)); each packed component rounds as
+// that scalar operation does, so the images stay bit-exact. Staging, culling,
+// list order and the image-loss epilogue are those of raster_fwd_kernel.
+template <int kMaxThreads>
+__global__ void __launch_bounds__(kMaxThreads) raster_fwd_pair_kernel(
+    const Rec2D<float>* __restrict__ records, const int32_t* __restrict__ offsets,
+    const int32_t* __restrict__ flatten_ids, int32_t n_isects, const int64_t* __restrict__ n_dev, uint32_t C,
+    uint32_t width, uint32_t height, uint32_t T, uint32_t tiles_x, uint32_t n_tiles, float* __restrict__ render,
+    uint32_t B, ImageLossEpilogue<float> loss) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    Rec2D<float>* s_rec = reinterpret_cast<Rec2D<float>*>(smem);   // [3][B]
+    uint2* s_mask = reinterpret_cast<uint2*>(s_rec + 3 * B);        // [2][B] (column, row) masks
+    uint16_t* s_hits = reinterpret_cast<uint16_t*>(s_mask + 2 * B); // [warps][32] hit lists
+
+    const uint32_t tile = blockIdx.x, cam = blockIdx.y;
+    const uint32_t key = cam * n_tiles + tile;
+    const uint32_t ty = tile / tiles_x, tx = tile - ty * tiles_x;
+    const uint32_t ox = tx * T, oy = ty * T;
+    if (ox >= width || oy >= height) {
+        if (loss.target != nullptr && threadIdx.x == 0) loss.partials[key] = 0.0;
+        return;
+    }
+    const uint32_t vx = min(T, width - ox), vy = min(T, height - oy);
+    const int32_t start = offsets[key];
+    const int32_t n_total = n_dev != nullptr ? int32_t(*n_dev) : n_isects;
+    const int32_t end = (key + 1 == C * n_tiles) ? n_total : offsets[key + 1];
+    const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5, nthreads = blockDim.x;
+
+    const uint32_t blocks_x = (T + 7u) / 8u;
+    const uint32_t bx0 = (warp % blocks_x) * 8u, by0 = (warp / blocks_x) * 8u;
+    const uint32_t lx = bx0 + (lane & 7u), ly = by0 + (lane >> 3);
+    const bool inside0 = lx < vx && ly < vy, inside1 = lx < vx && ly + 4u < vy;
+    const uint32_t warp_cols = bx0 < 32u ? ((0xffu << bx0) & low_bits(vx)) : 0u;
+    const uint32_t warp_rows = by0 < 32u ? ((0xffu << by0) & low_bits(vy)) : 0u;
+    const bool warp_active = warp_cols != 0u && warp_rows != 0u;
+    const float px = static_cast<float>(ox + lx) + 0.5f;
+    const float2 py = make_float2(static_cast<float>(oy + ly) + 0.5f, static_cast<float>(oy + ly + 4u) + 0.5f);
+    float acc0 = 0.f, acc1 = 0.f;
+
+    const int32_t count = end - start;
+    const int32_t n_batches = count > 0 ? (count + int32_t(B) - 1) / int32_t(B) : 0;
+    auto load = [&](int32_t bi, uint32_t stage) {
+        for (uint32_t i = t; i < B; i += nthreads) {
+            const int32_t idx = start + bi * int32_t(B) + int32_t(i);
+            if (idx < end) gather_record(s_rec + stage * B + i, records + flatten_ids[idx]);
+        }
+        cp_async_commit();
+    };
+    if (n_batches > 0) load(0, 0);
+    for (int32_t bi = 0; bi < n_batches; ++bi) {
+        if (bi + 1 < n_batches) {
+            load(bi + 1, uint32_t(bi + 1) % 3u);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const uint32_t stage = uint32_t(bi) % 3u;
+        const Rec2D<float>* buf = s_rec + stage * B;
+        uint2* masks = s_mask + (uint32_t(bi) & 1u) * B;
+        const int32_t batch = min(int32_t(B), count - bi * int32_t(B));
+        for (int32_t i = int32_t(t); i < batch; i += int32_t(nthreads)) {
+            Rec2D<float>& rec = s_rec[stage * B + uint32_t(i)];
+            const TileBox box = record_box<float, false>(rec, ox, oy, vx, vy);
+            masks[i] = make_uint2(box.cols, box.rows);
+            rec.o = rec.o * rec.mu;  // o mu, once per record
+        }
+        __syncthreads();
+        if (warp_active) {
+            for (int32_t base = 0; base < batch; base += 32) {
+                bool hit = false;
+                if (base + int32_t(lane) < batch) {
+                    const uint2 m = masks[base + int32_t(lane)];
+                    hit = (m.x & warp_cols) != 0u && (m.y & warp_rows) != 0u;
+                }
+                const uint32_t hits = __ballot_sync(0xffffffffu, hit);
+                uint16_t* my_hits = s_hits + warp * 32u;
+                if (hit) my_hits[__popc(hits & ((1u << lane) - 1u))] = uint16_t(base + int32_t(lane));
+                __syncwarp();
+                const int32_t n_hits = __popc(hits);
+                for (int32_t e = 0; e < n_hits; ++e) {
+                    const Rec2D<float>& r = buf[my_hits[e]];
+                    const float dx = px - r.x;
+                    const float adx = __fmul_rn(r.a, dx), bdx = __fmul_rn(r.b, dx);
+                    const float2 dy = add2(py, splat2(-r.y));
+                    const float2 in = fma2(splat2(adx), splat2(dx), mul2(mul2(splat2(r.c), dy), dy));
+                    const float2 sigma = fma2(splat2(bdx), dy, mul2(splat2(0.5f), in));
+                    const float alpha0 = r.o * exp(-sigma.x);
+                    const float alpha1 = r.o * exp(-sigma.y);
+                    if (!(sigma.x < 0.f || fabs(alpha0) < 1e-5f)) acc0 += alpha0;
+                    if (!(sigma.y < 0.f || fabs(alpha1) < 1e-5f)) acc1 += alpha1;
+                }
+                __syncwarp();  // the list is rewritten for the next 32 records
+            }
+        }
+        // No barrier here (see raster_fwd_kernel): three record buffers, two mask buffers.
+    }
+    const size_t pid0 = size_t(cam) * height * width + size_t(oy + ly) * width + (ox + lx);
+    const size_t pid1 = pid0 + 4u * size_t(width);
+    if (inside0) render[pid0] = acc0;
+    if (inside1) render[pid1] = acc1;
+    if (loss.target != nullptr) {
+        double term = 0.0;
+        const float accs[2] = {acc0, acc1};
+        const size_t pids[2] = {pid0, pid1};
+        const bool ins[2] = {inside0, inside1};
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            if (!ins[k]) continue;
+            const float diff = accs[k] - loss.target[pids[k]];
+            float v;
+            if (loss.l1) {
+                const float sgn = diff > 0.f ? 1.f : (diff < 0.f ? -1.f : 0.f);
+                v = loss.scale * sgn / loss.numel;
+                term += fabs(static_cast<double>(diff));
+            } else {
+                v = diff * loss.scale;
+                term += static_cast<double>(diff) * static_cast<double>(diff);
+            }
+            loss.v_render[pids[k]] = v;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) term += __shfl_xor_sync(0xffffffffu, term, o);
+        double* s_sum = reinterpret_cast<double*>(s_hits);  // hit lists are no longer read
+        const uint32_t n_warps = blockDim.x >> 5;
+        __syncthreads();
+        if (lane == 0) s_sum[warp] = term;
+        __syncthreads();
+        if (warp == 0) {
+            double w = lane < n_warps ? s_sum[lane] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+            if (lane == 0) loss.partials[key] = w;
+        }
+    }
+}
+
 // --------------------------------------------------------------------------
 // Backward
 // --------------------------------------------------------------------------
@@ -876,6 +1018,28 @@ inline int check_geom(const RasterGeom& g) {
 template <typename S, bool kBeta, bool kVar>
 int launch_fwd_p(const RasterGeom& g, const Rec2D<S>* rec, const S* unc, const int32_t* offsets,
                  const int32_t* ids, S* out, S* out_var, const ImageLossEpilogue<S>& loss, cudaStream_t stream) {
+    if constexpr (std::is_same<S, float>::value && !kBeta && !kVar) {
+        // Two pixels per lane: warps of 8x8 pixels.
+        const uint32_t blocks = ((g.T + 7) / 8) * ((g.T + 7) / 8);
+        const unsigned nthreads = 32u * blocks;
+        unsigned batch = g.stage_batch < kFwdBatch ? g.stage_batch : kFwdBatch;
+        if (batch < 1) batch = 1;
+        const size_t smem = 3 * size_t(batch) * sizeof(Rec2D<S>) + 2 * size_t(batch) * sizeof(uint2) +
+                            size_t(nthreads) * sizeof(uint16_t) + 64;
+        dim3 grid(g.tiles_x * g.tiles_y, g.C);
+        if (nthreads <= 128) {
+            R2S_TRY(allow_dynamic_smem(raster_fwd_pair_kernel<128>, smem));
+            raster_fwd_pair_kernel<128><<<grid, nthreads, smem, stream>>>(
+                rec, offsets, ids, int32_t(g.n_isects), g.n_dev, g.C, g.width, g.height, g.T, g.tiles_x,
+                g.tiles_x * g.tiles_y, out, batch, loss);
+        } else {
+            R2S_TRY(allow_dynamic_smem(raster_fwd_pair_kernel<512>, smem));
+            raster_fwd_pair_kernel<512><<<grid, nthreads, smem, stream>>>(
+                rec, offsets, ids, int32_t(g.n_isects), g.n_dev, g.C, g.width, g.height, g.T, g.tiles_x,
+                g.tiles_x * g.tiles_y, out, batch, loss);
+        }
+        return check_launch("rasterize_to_pixels_fwd");
+    }
     // One warp per 8x4 block of the tile: at most 4 x 8 warps for 32x32 tiles.
     const uint32_t blocks = ((g.T + kBlockW - 1) / kBlockW) * ((g.T + kBlockH - 1) / kBlockH);
     const unsigned nthreads = 32u * blocks;
