@@ -310,23 +310,29 @@ __global__ void __launch_bounds__(kMaxThreads) raster_fwd_kernel(
     }
 }
 
-// Gaussian forward (fp32, no variance branch) with two pixels per lane: lane
-// (x, y) of a warp's 8x8 pixel block owns pixels (x, y) and (x, y + 4), which
-// share dx, so a x dx and b dx are computed once per record and the two
-// samples go through packed FP32x2 operations. The reference's sigma is
-// written with the contraction nvcc applies to its source expression there,
-// fma(b dx, dy, 1/2 fma(a dx, dx, (c dy) dy)); each packed component rounds as
-// that scalar operation does, so the images stay bit-exact. Staging, culling,
-// list order and the image-loss epilogue are those of raster_fwd_kernel.
-template <int kMaxThreads>
+// Forward in fp32 with two pixels per lane: lane (x, y) of a warp's 8x8 pixel
+// block owns pixels (x, y) and (x, y + 4), which share dx, so the record's
+// dx terms are computed once and the two samples go through packed FP32x2
+// operations. The reference's expressions are written with the contraction
+// nvcc applies to its source in this kernel, so each packed component rounds
+// as that scalar operation does and the images stay bit-exact:
+//   Gaussian: sigma = fma(b dx, dy, 1/2 fma(a dx, dx, (c dy) dy));
+//   Beta:     d^2 = fma(c dy, dy, fma(a dx, dx, ((2 b) dx) dy)), with dx and dy
+//             taken mean - pixel as the reference does;
+//   variance: accv = fma(q alpha, alpha, accv).
+// Staging, culling, list order and the image-loss epilogue are those of
+// raster_fwd_kernel.
+template <bool kBeta, bool kVar, int kMaxThreads>
 __global__ void __launch_bounds__(kMaxThreads) raster_fwd_pair_kernel(
-    const Rec2D<float>* __restrict__ records, const int32_t* __restrict__ offsets,
-    const int32_t* __restrict__ flatten_ids, int32_t n_isects, const int64_t* __restrict__ n_dev, uint32_t C,
-    uint32_t width, uint32_t height, uint32_t T, uint32_t tiles_x, uint32_t n_tiles, float* __restrict__ render,
-    uint32_t B, ImageLossEpilogue<float> loss) {
+    const Rec2D<float>* __restrict__ records, const float* __restrict__ uncertainties, uint32_t N,
+    const int32_t* __restrict__ offsets, const int32_t* __restrict__ flatten_ids, int32_t n_isects,
+    const int64_t* __restrict__ n_dev, uint32_t C, uint32_t width, uint32_t height, uint32_t T, uint32_t tiles_x,
+    uint32_t n_tiles, float* __restrict__ render, float* __restrict__ render_var, uint32_t B,
+    ImageLossEpilogue<float> loss) {
     extern __shared__ __align__(16) unsigned char smem[];
     Rec2D<float>* s_rec = reinterpret_cast<Rec2D<float>*>(smem);   // [3][B]
-    uint2* s_mask = reinterpret_cast<uint2*>(s_rec + 3 * B);        // [2][B] (column, row) masks
+    float* s_q = reinterpret_cast<float*>(s_rec + 3 * B);           // [3][B] uncertainties
+    uint2* s_mask = reinterpret_cast<uint2*>(s_q + 3 * B);          // [2][B] (column, row) masks
     uint16_t* s_hits = reinterpret_cast<uint16_t*>(s_mask + 2 * B); // [warps][32] hit lists
 
     const uint32_t tile = blockIdx.x, cam = blockIdx.y;
@@ -352,14 +358,18 @@ __global__ void __launch_bounds__(kMaxThreads) raster_fwd_pair_kernel(
     const bool warp_active = warp_cols != 0u && warp_rows != 0u;
     const float px = static_cast<float>(ox + lx) + 0.5f;
     const float2 py = make_float2(static_cast<float>(oy + ly) + 0.5f, static_cast<float>(oy + ly + 4u) + 0.5f);
-    float acc0 = 0.f, acc1 = 0.f;
+    float acc0 = 0.f, acc1 = 0.f, accv0 = 0.f, accv1 = 0.f;
 
     const int32_t count = end - start;
     const int32_t n_batches = count > 0 ? (count + int32_t(B) - 1) / int32_t(B) : 0;
     auto load = [&](int32_t bi, uint32_t stage) {
         for (uint32_t i = t; i < B; i += nthreads) {
             const int32_t idx = start + bi * int32_t(B) + int32_t(i);
-            if (idx < end) gather_record(s_rec + stage * B + i, records + flatten_ids[idx]);
+            if (idx < end) {
+                const int32_t g = flatten_ids[idx];
+                gather_record(s_rec + stage * B + i, records + g);
+                if (kVar) s_q[stage * B + i] = uncertainties[uint32_t(g) % N];
+            }
         }
         cp_async_commit();
     };
@@ -374,11 +384,12 @@ __global__ void __launch_bounds__(kMaxThreads) raster_fwd_pair_kernel(
         __syncthreads();
         const uint32_t stage = uint32_t(bi) % 3u;
         const Rec2D<float>* buf = s_rec + stage * B;
+        const float* qbuf = s_q + stage * B;
         uint2* masks = s_mask + (uint32_t(bi) & 1u) * B;
         const int32_t batch = min(int32_t(B), count - bi * int32_t(B));
         for (int32_t i = int32_t(t); i < batch; i += int32_t(nthreads)) {
             Rec2D<float>& rec = s_rec[stage * B + uint32_t(i)];
-            const TileBox box = record_box<float, false>(rec, ox, oy, vx, vy);
+            const TileBox box = record_box<float, kBeta>(rec, ox, oy, vx, vy);
             masks[i] = make_uint2(box.cols, box.rows);
             rec.o = rec.o * rec.mu;  // o mu, once per record
         }
@@ -396,16 +407,41 @@ __global__ void __launch_bounds__(kMaxThreads) raster_fwd_pair_kernel(
                 __syncwarp();
                 const int32_t n_hits = __popc(hits);
                 for (int32_t e = 0; e < n_hits; ++e) {
-                    const Rec2D<float>& r = buf[my_hits[e]];
-                    const float dx = px - r.x;
-                    const float adx = __fmul_rn(r.a, dx), bdx = __fmul_rn(r.b, dx);
-                    const float2 dy = add2(py, splat2(-r.y));
-                    const float2 in = fma2(splat2(adx), splat2(dx), mul2(mul2(splat2(r.c), dy), dy));
-                    const float2 sigma = fma2(splat2(bdx), dy, mul2(splat2(0.5f), in));
-                    const float alpha0 = r.o * exp(-sigma.x);
-                    const float alpha1 = r.o * exp(-sigma.y);
-                    if (!(sigma.x < 0.f || fabs(alpha0) < 1e-5f)) acc0 += alpha0;
-                    if (!(sigma.y < 0.f || fabs(alpha1) < 1e-5f)) acc1 += alpha1;
+                    const int32_t s = my_hits[e];
+                    const Rec2D<float>& r = buf[s];
+                    float alpha0, alpha1;
+                    bool k0, k1;
+                    if (!kBeta) {
+                        const float dx = px - r.x;
+                        const float adx = __fmul_rn(r.a, dx), bdx = __fmul_rn(r.b, dx);
+                        const float2 dy = add2(py, splat2(-r.y));
+                        const float2 in = fma2(splat2(adx), splat2(dx), mul2(mul2(splat2(r.c), dy), dy));
+                        const float2 sigma = fma2(splat2(bdx), dy, mul2(splat2(0.5f), in));
+                        alpha0 = r.o * exp(-sigma.x);
+                        alpha1 = r.o * exp(-sigma.y);
+                        k0 = !(sigma.x < 0.f || fabs(alpha0) < 1e-5f);
+                        k1 = !(sigma.y < 0.f || fabs(alpha1) < 1e-5f);
+                    } else {
+                        const float dx = r.x - px;
+                        const float adx = __fmul_rn(r.a, dx), b2dx = __fmul_rn(__fmul_rn(2.f, r.b), dx);
+                        const float2 dy = add2(splat2(r.y), make_float2(-py.x, -py.y));
+                        const float2 d2 = fma2(mul2(splat2(r.c), dy), dy,
+                                               fma2(splat2(adx), splat2(dx), mul2(splat2(b2dx), dy)));
+                        const bool s0 = !(d2.x < 0.f || d2.x >= 1.f), s1 = !(d2.y < 0.f || d2.y >= 1.f);
+                        const float2 h = add2(splat2(1.f), make_float2(-d2.x, -d2.y));
+                        alpha0 = s0 ? r.o * pow(h.x, r.beta) : 0.f;
+                        alpha1 = s1 ? r.o * pow(h.y, r.beta) : 0.f;
+                        k0 = s0 && !(fabs(alpha0) < 1e-5f);
+                        k1 = s1 && !(fabs(alpha1) < 1e-5f);
+                    }
+                    if (k0) {
+                        acc0 += alpha0;
+                        if (kVar) accv0 = __fmaf_rn(__fmul_rn(qbuf[s], alpha0), alpha0, accv0);
+                    }
+                    if (k1) {
+                        acc1 += alpha1;
+                        if (kVar) accv1 = __fmaf_rn(__fmul_rn(qbuf[s], alpha1), alpha1, accv1);
+                    }
                 }
                 __syncwarp();  // the list is rewritten for the next 32 records
             }
@@ -414,8 +450,14 @@ __global__ void __launch_bounds__(kMaxThreads) raster_fwd_pair_kernel(
     }
     const size_t pid0 = size_t(cam) * height * width + size_t(oy + ly) * width + (ox + lx);
     const size_t pid1 = pid0 + 4u * size_t(width);
-    if (inside0) render[pid0] = acc0;
-    if (inside1) render[pid1] = acc1;
+    if (inside0) {
+        render[pid0] = acc0;
+        if (kVar) render_var[pid0] = accv0;
+    }
+    if (inside1) {
+        render[pid1] = acc1;
+        if (kVar) render_var[pid1] = accv1;
+    }
     if (loss.target != nullptr) {
         double term = 0.0;
         const float accs[2] = {acc0, acc1};
@@ -1018,25 +1060,25 @@ inline int check_geom(const RasterGeom& g) {
 template <typename S, bool kBeta, bool kVar>
 int launch_fwd_p(const RasterGeom& g, const Rec2D<S>* rec, const S* unc, const int32_t* offsets,
                  const int32_t* ids, S* out, S* out_var, const ImageLossEpilogue<S>& loss, cudaStream_t stream) {
-    if constexpr (std::is_same<S, float>::value && !kBeta && !kVar) {
+    if constexpr (std::is_same<S, float>::value) {
         // Two pixels per lane: warps of 8x8 pixels.
         const uint32_t blocks = ((g.T + 7) / 8) * ((g.T + 7) / 8);
         const unsigned nthreads = 32u * blocks;
         unsigned batch = g.stage_batch < kFwdBatch ? g.stage_batch : kFwdBatch;
         if (batch < 1) batch = 1;
-        const size_t smem = 3 * size_t(batch) * sizeof(Rec2D<S>) + 2 * size_t(batch) * sizeof(uint2) +
+        const size_t smem = 3 * size_t(batch) * (sizeof(Rec2D<S>) + sizeof(S)) + 2 * size_t(batch) * sizeof(uint2) +
                             size_t(nthreads) * sizeof(uint16_t) + 64;
         dim3 grid(g.tiles_x * g.tiles_y, g.C);
         if (nthreads <= 128) {
-            R2S_TRY(allow_dynamic_smem(raster_fwd_pair_kernel<128>, smem));
-            raster_fwd_pair_kernel<128><<<grid, nthreads, smem, stream>>>(
-                rec, offsets, ids, int32_t(g.n_isects), g.n_dev, g.C, g.width, g.height, g.T, g.tiles_x,
-                g.tiles_x * g.tiles_y, out, batch, loss);
+            R2S_TRY(allow_dynamic_smem(raster_fwd_pair_kernel<kBeta, kVar, 128>, smem));
+            raster_fwd_pair_kernel<kBeta, kVar, 128><<<grid, nthreads, smem, stream>>>(
+                rec, unc, g.N, offsets, ids, int32_t(g.n_isects), g.n_dev, g.C, g.width, g.height, g.T, g.tiles_x,
+                g.tiles_x * g.tiles_y, out, out_var, batch, loss);
         } else {
-            R2S_TRY(allow_dynamic_smem(raster_fwd_pair_kernel<512>, smem));
-            raster_fwd_pair_kernel<512><<<grid, nthreads, smem, stream>>>(
-                rec, offsets, ids, int32_t(g.n_isects), g.n_dev, g.C, g.width, g.height, g.T, g.tiles_x,
-                g.tiles_x * g.tiles_y, out, batch, loss);
+            R2S_TRY(allow_dynamic_smem(raster_fwd_pair_kernel<kBeta, kVar, 512>, smem));
+            raster_fwd_pair_kernel<kBeta, kVar, 512><<<grid, nthreads, smem, stream>>>(
+                rec, unc, g.N, offsets, ids, int32_t(g.n_isects), g.n_dev, g.C, g.width, g.height, g.T, g.tiles_x,
+                g.tiles_x * g.tiles_y, out, out_var, batch, loss);
         }
         return check_launch("rasterize_to_pixels_fwd");
     }
