@@ -75,7 +75,7 @@ WORKLOAD_TEXT = {
 }
 # DRAM bytes (read + write) of one record-parallel raster VJP launch at the CT
 # workload, from ncu (dram__bytes_read.sum + dram__bytes_write.sum, one pass).
-RASTER_VJP_TRAFFIC_BYTES = 536.0e6 + 367.2e6
+RASTER_VJP_TRAFFIC_BYTES = 535.5e6 + 366.9e6
 
 
 # --------------------------------------------------------------------------- utilities
