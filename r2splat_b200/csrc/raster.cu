@@ -331,8 +331,8 @@ __global__ void __launch_bounds__(kMaxThreads) raster_fwd_pair_kernel(
     ImageLossEpilogue<float> loss) {
     extern __shared__ __align__(16) unsigned char smem[];
     Rec2D<float>* s_rec = reinterpret_cast<Rec2D<float>*>(smem);   // [3][B]
-    float* s_q = reinterpret_cast<float*>(s_rec + 3 * B);           // [3][B] uncertainties
-    uint2* s_mask = reinterpret_cast<uint2*>(s_q + 3 * B);          // [2][B] (column, row) masks
+    float* s_q = reinterpret_cast<float*>(s_rec + 3 * B);           // [3][B] uncertainties (variance only)
+    uint2* s_mask = reinterpret_cast<uint2*>(s_q + (kVar ? 3 * B : 0u));  // [2][B] (column, row) masks
     uint16_t* s_hits = reinterpret_cast<uint16_t*>(s_mask + 2 * B); // [warps][32] hit lists
 
     const uint32_t tile = blockIdx.x, cam = blockIdx.y;
@@ -1066,8 +1066,8 @@ int launch_fwd_p(const RasterGeom& g, const Rec2D<S>* rec, const S* unc, const i
         const unsigned nthreads = 32u * blocks;
         unsigned batch = g.stage_batch < kFwdBatch ? g.stage_batch : kFwdBatch;
         if (batch < 1) batch = 1;
-        const size_t smem = 3 * size_t(batch) * (sizeof(Rec2D<S>) + sizeof(S)) + 2 * size_t(batch) * sizeof(uint2) +
-                            size_t(nthreads) * sizeof(uint16_t) + 64;
+        const size_t smem = 3 * size_t(batch) * (sizeof(Rec2D<S>) + (kVar ? sizeof(S) : 0)) +
+                            2 * size_t(batch) * sizeof(uint2) + size_t(nthreads) * sizeof(uint16_t) + 64;
         dim3 grid(g.tiles_x * g.tiles_y, g.C);
         if (nthreads <= 128) {
             R2S_TRY(allow_dynamic_smem(raster_fwd_pair_kernel<kBeta, kVar, 128>, smem));
@@ -1081,29 +1081,30 @@ int launch_fwd_p(const RasterGeom& g, const Rec2D<S>* rec, const S* unc, const i
                 g.tiles_x * g.tiles_y, out, out_var, batch, loss);
         }
         return check_launch("rasterize_to_pixels_fwd");
-    }
-    // One warp per 8x4 block of the tile: at most 4 x 8 warps for 32x32 tiles.
-    const uint32_t blocks = ((g.T + kBlockW - 1) / kBlockW) * ((g.T + kBlockH - 1) / kBlockH);
-    const unsigned nthreads = 32u * blocks;
-    unsigned batch = g.stage_batch < kFwdBatch ? g.stage_batch : kFwdBatch;
-    if (batch > nthreads) batch = nthreads;
-    if (batch < 1) batch = 1;
-    const size_t smem = 3 * size_t(batch) * (sizeof(Rec2D<S>) + sizeof(S)) + 2 * size_t(batch) * sizeof(uint2) +
-                        size_t(nthreads) * sizeof(uint16_t);
-    dim3 grid(g.tiles_x * g.tiles_y, g.C);
-    if (nthreads <= 256) {
-        // Tiles up to 16x16: a register budget sized for 256-thread CTAs.
-        R2S_TRY(allow_dynamic_smem(raster_fwd_kernel<S, kBeta, kVar, 256>, smem));
-        raster_fwd_kernel<S, kBeta, kVar, 256><<<grid, nthreads, smem, stream>>>(
-            rec, unc, g.N, offsets, ids, int32_t(g.n_isects), g.n_dev, g.C, g.width, g.height, g.T, g.tiles_x,
-            g.tiles_x * g.tiles_y, out, out_var, batch, loss);
     } else {
-        R2S_TRY(allow_dynamic_smem(raster_fwd_kernel<S, kBeta, kVar, 1024>, smem));
-        raster_fwd_kernel<S, kBeta, kVar, 1024><<<grid, nthreads, smem, stream>>>(
-            rec, unc, g.N, offsets, ids, int32_t(g.n_isects), g.n_dev, g.C, g.width, g.height, g.T, g.tiles_x,
-            g.tiles_x * g.tiles_y, out, out_var, batch, loss);
+        // fp64: one warp per 8x4 block of the tile, at most 4 x 8 warps for 32x32 tiles.
+        const uint32_t blocks = ((g.T + kBlockW - 1) / kBlockW) * ((g.T + kBlockH - 1) / kBlockH);
+        const unsigned nthreads = 32u * blocks;
+        unsigned batch = g.stage_batch < kFwdBatch ? g.stage_batch : kFwdBatch;
+        if (batch > nthreads) batch = nthreads;
+        if (batch < 1) batch = 1;
+        const size_t smem = 3 * size_t(batch) * (sizeof(Rec2D<S>) + sizeof(S)) + 2 * size_t(batch) * sizeof(uint2) +
+                            size_t(nthreads) * sizeof(uint16_t);
+        dim3 grid(g.tiles_x * g.tiles_y, g.C);
+        if (nthreads <= 256) {
+            // Tiles up to 16x16: a register budget sized for 256-thread CTAs.
+            R2S_TRY(allow_dynamic_smem(raster_fwd_kernel<S, kBeta, kVar, 256>, smem));
+            raster_fwd_kernel<S, kBeta, kVar, 256><<<grid, nthreads, smem, stream>>>(
+                rec, unc, g.N, offsets, ids, int32_t(g.n_isects), g.n_dev, g.C, g.width, g.height, g.T, g.tiles_x,
+                g.tiles_x * g.tiles_y, out, out_var, batch, loss);
+        } else {
+            R2S_TRY(allow_dynamic_smem(raster_fwd_kernel<S, kBeta, kVar, 1024>, smem));
+            raster_fwd_kernel<S, kBeta, kVar, 1024><<<grid, nthreads, smem, stream>>>(
+                rec, unc, g.N, offsets, ids, int32_t(g.n_isects), g.n_dev, g.C, g.width, g.height, g.T, g.tiles_x,
+                g.tiles_x * g.tiles_y, out, out_var, batch, loss);
+        }
+        return check_launch("rasterize_to_pixels_fwd");
     }
-    return check_launch("rasterize_to_pixels_fwd");
 }
 
 template <typename S>
