@@ -140,32 +140,34 @@ __device__ __forceinline__ S warp_sum(S v) {
     return v;
 }
 
-// Warp sum of eight per-lane values by recursive halving: each exchange step
-// sends half of the lane's values to its partner and keeps the other half, so
-// the whole reduction costs 4 + 2 + 2 * 3 shuffles instead of 8 * 5. On
-// return every lane of group G = lane / 8 holds the warp totals of values
-// 2G and 2G + 1 in (out0, out1).
-template <typename S>
+// Sum of eight per-lane values over each group of kLanes lanes (32: the warp;
+// 16: each half of it) by recursive halving: each exchange step sends half of
+// the lane's values to its partner and keeps the other half, so a warp-wide
+// reduction costs 4 + 2 + 2 * 3 shuffles instead of 8 * 5. On return every
+// lane of subgroup G = (lane % kLanes) / (kLanes / 4) holds its group's totals
+// of values 2G and 2G + 1 in (out0, out1).
+template <uint32_t kLanes = 32u, typename S>
 __device__ __forceinline__ void warp_sum8_pairs(const S (&v)[8], S& out0, S& out1) {
+    static_assert(kLanes == 32u || kLanes == 16u, "groups of 32 or 16 lanes");
     const uint32_t lane = threadIdx.x & 31u;
-    const bool hi16 = (lane & 16u) != 0;
+    const bool upper = (lane & (kLanes / 2u)) != 0;
     S w[4];
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-        const S send = hi16 ? v[i] : v[i + 4];
-        const S keep = hi16 ? v[i + 4] : v[i];
-        w[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+        const S send = upper ? v[i] : v[i + 4];
+        const S keep = upper ? v[i + 4] : v[i];
+        w[i] = keep + __shfl_xor_sync(0xffffffffu, send, kLanes / 2u);
     }
-    const bool hi8 = (lane & 8u) != 0;
+    const bool upper2 = (lane & (kLanes / 4u)) != 0;
     S u[2];
 #pragma unroll
     for (int i = 0; i < 2; ++i) {
-        const S send = hi8 ? w[i] : w[i + 2];
-        const S keep = hi8 ? w[i + 2] : w[i];
-        u[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+        const S send = upper2 ? w[i] : w[i + 2];
+        const S keep = upper2 ? w[i + 2] : w[i];
+        u[i] = keep + __shfl_xor_sync(0xffffffffu, send, kLanes / 4u);
     }
 #pragma unroll
-    for (int offset = 4; offset > 0; offset >>= 1) {
+    for (int offset = kLanes / 8u; offset > 0; offset >>= 1) {
         u[0] += __shfl_xor_sync(0xffffffffu, u[0], offset);
         u[1] += __shfl_xor_sync(0xffffffffu, u[1], offset);
     }

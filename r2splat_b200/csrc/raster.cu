@@ -567,8 +567,8 @@ __device__ __forceinline__ void vjp_sample(const Rec2D<S>& r, S om, S q, S px, S
     }
 }
 
-// The record-slot adjoints held by lane group grp (= lane / 8) after
-// warp_sum8_pairs reduced the partial sums to (lo, hi): group 0 gives
+// The record-slot adjoints held by lane subgroup grp (lane / 8 in a whole warp,
+// (lane / 4) % 4 in a half warp) after warp_sum8_pairs reduced the partial sums to (lo, hi): group 0 gives
 // (x, y), group 1 (a, b), group 2 (c, o) and mu (in e2), group 3 beta (in e0).
 template <typename S, bool kBeta>
 __device__ __forceinline__ void record_adjoints(const Rec2D<S>& r, uint32_t grp, S lo, S hi, S& e0, S& e1, S& e2) {
@@ -828,6 +828,71 @@ __device__ __forceinline__ void record_walk_packed(const Rec2D<float>& r, float 
     part[7] = 0.f;
 }
 
+// The scalar walk of one record by kLanes lanes (a full warp, or one half of
+// it): lane l = lane % kLanes starts at box position k = l (row-major, width
+// bw) and steps by kLanes positions, i.e. dq rows and dr columns plus one wrap
+// when the column overflows. iters is uniform over the warp; lanes past the
+// box end evaluate nothing (valid = false) and load nothing. part and the
+// absgrad sums are vjp_sample's.
+template <typename S, bool kBeta, bool kVar, bool kAbs, uint32_t kLanes>
+__device__ __forceinline__ void record_walk_scalar(const Rec2D<S>& r, S om, S q, const S* vimg, const S* vvar,
+                                                   uint32_t bx0, uint32_t by0, uint32_t bw, uint32_t barea,
+                                                   uint32_t iters, uint32_t width, S (&part)[8], S& g_ax, S& g_ay) {
+    const uint32_t l = threadIdx.x & (kLanes - 1u);
+    uint32_t dq = 0u, dr = kLanes, row = 0u, col = l;
+    if (bw < kLanes) {
+        const uint32_t m = c_div_magic[bw];
+        dq = (kLanes * m) >> 16;
+        dr = kLanes - dq * bw;
+        row = (l * m) >> 16;
+        col = l - row * bw;
+    }
+    uint32_t off = (by0 + row) * width + bx0 + col;
+    const uint32_t step = dq * width + dr, wrap_step = width - bw;
+    S px = static_cast<S>(bx0 + col) + static_cast<S>(0.5);
+    S py = static_cast<S>(by0 + row) + static_cast<S>(0.5);
+    const S x_end = static_cast<S>(bx0 + bw);  // a centre past the row is >= x0 + w + 0.5
+    const S step_x = static_cast<S>(dr), step_y = static_cast<S>(dq), wrap_x = static_cast<S>(bw);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) part[i] = S(0);
+    uint32_t k = l;
+    for (uint32_t it = 0; it < iters; ++it, k += kLanes) {
+        const bool valid = k < barea;
+        const S v = (valid && vimg != nullptr) ? vimg[off] : S(0);
+        const S vv = (kVar && valid) ? vvar[off] : S(0);
+        vjp_sample<S, kBeta, kVar, kAbs>(r, om, q, px, py, v, vv, valid, part, g_ax, g_ay);
+        px += step_x;
+        py += step_y;
+        off += step;
+        const bool wrap = px > x_end;
+        px = wrap ? px - wrap_x : px;
+        py = wrap ? py + static_cast<S>(1) : py;
+        off = wrap ? off + wrap_step : off;
+    }
+}
+
+// Boxes of at most this many pixels are walked by half warps, two records at a
+// time: a small box fills a 16-lane step about as well as a 32-lane one, and
+// the pair shares one pass of the per-record set-up and reduction.
+constexpr uint32_t kHalfWarpArea = 128u;
+
+// Writes the slot adjoints of record subgroup grp (0..3) from its pair of
+// reduced sums (see record_adjoints) and adds the uncertainty adjoint.
+template <typename S, bool kBeta, bool kVar>
+__device__ __forceinline__ void store_record_adjoints(const Rec2D<S>& r, uint32_t grp, S lo, S hi, Rec2D<S>* slot,
+                                                      S* v_unc, uint32_t n) {
+    S* dst = reinterpret_cast<S*>(slot);
+    S e0, e1, e2;
+    record_adjoints<S, kBeta>(r, grp, lo, hi, e0, e1, e2);
+    if (grp < 3u) {
+        dst[2 * grp] = e0;
+        dst[2 * grp + 1] = e1;
+    }
+    if (grp == 2u) dst[6] = e2;
+    if (grp == 3u) dst[7] = e0;
+    if (kVar && grp == 3u && v_unc != nullptr) red_add(v_unc + n, hi);
+}
+
 // A record's walk constants, set up by the lane that loaded the record and
 // read by the whole warp from shared memory (broadcast loads).
 template <typename S>
@@ -895,7 +960,11 @@ __global__ void __launch_bounds__(kRecBwdThreads) raster_record_bwd_kernel(
                 }
             }
         }
-        uint32_t pending = __ballot_sync(0xffffffffu, area != 0u);
+        // Boxes of the scalar walk with at most kHalfWarpArea pixels go to the
+        // half-warp pairs; the rest are walked one by one by the whole warp.
+        // (The plain Gaussian instantiation, which takes the packed walk, has no pairs.)
+        uint32_t pairs = kPacked ? 0u : __ballot_sync(0xffffffffu, area != 0u && area <= kHalfWarpArea);
+        uint32_t pending = __ballot_sync(0xffffffffu, area != 0u) & ~pairs;
         __syncwarp();  // the previous group's constants have been read
         if (area != 0u) {
             RecordStage<S> st;
@@ -934,44 +1003,9 @@ __global__ void __launch_bounds__(kRecBwdThreads) raster_record_bwd_kernel(
                     walked = true;
                 }
             }
-            if (!walked) {
-                // Lane k of the box (row-major, width bw) starts at k = lane and
-                // steps by 32: dq rows and dr columns, plus one wrap when the
-                // column overflows.
-                uint32_t dq = 0u, dr = 32u, row = 0u, col = lane;
-                if (bw < 32u) {
-                    const uint32_t m = c_div_magic[bw];
-                    dq = (32u * m) >> 16;
-                    dr = 32u - dq * bw;
-                    row = (lane * m) >> 16;
-                    col = lane - row * bw;
-                }
-                uint32_t off = (by0 + row) * width + bx0 + col;
-                const uint32_t step = dq * width + dr, wrap_step = width - bw;
-                S px = static_cast<S>(bx0 + col) + static_cast<S>(0.5);
-                S py = static_cast<S>(by0 + row) + static_cast<S>(0.5);
-                const S x_end = static_cast<S>(bx0 + bw);  // a centre past the row is >= x0 + w + 0.5
-                const S step_x = static_cast<S>(dr), step_y = static_cast<S>(dq), wrap_x = static_cast<S>(bw);
-                const uint32_t iters = (barea + 31u) >> 5;
-#pragma unroll
-                for (int i = 0; i < 8; ++i) part[i] = S(0);
-                // A warp-uniform trip count; lanes past the box end in the last step
-                // evaluate nothing (valid = false) and load nothing.
-                uint32_t k = lane;
-                for (uint32_t it = 0; it < iters; ++it, k += 32u) {
-                    const bool valid = k < barea;
-                    const S v = (valid && vimg != nullptr) ? vimg[off] : S(0);
-                    const S vv = (kVar && valid) ? vvar[off] : S(0);
-                    vjp_sample<S, kBeta, kVar, kAbs>(r, om, q, px, py, v, vv, valid, part, g_ax, g_ay);
-                    px += step_x;
-                    py += step_y;
-                    off += step;
-                    const bool wrap = px > x_end;
-                    px = wrap ? px - wrap_x : px;
-                    py = wrap ? py + static_cast<S>(1) : py;
-                    off = wrap ? off + wrap_step : off;
-                }
-            }
+            if (!walked)
+                record_walk_scalar<S, kBeta, kVar, kAbs, 32u>(r, om, q, vimg, vvar, bx0, by0, bw, barea,
+                                                              (barea + 31u) >> 5, width, part, g_ax, g_ay);
             S lo, hi;
             warp_sum8_pairs(part, lo, hi);
             const uint32_t grp = lane >> 3;
@@ -991,6 +1025,50 @@ __global__ void __launch_bounds__(kRecBwdThreads) raster_record_bwd_kernel(
                 g_ax = warp_sum(g_ax);
                 g_ay = warp_sum(g_ay);
                 if (lane == 0u) {
+                    v_abs[2 * rid] = g_ax;
+                    v_abs[2 * rid + 1] = g_ay;
+                }
+            }
+        }
+        // The small boxes, two records per step: the lower half warp walks
+        // record j0, the upper one j1 (none for an odd count: that half walks
+        // nothing and stores nothing).
+        if constexpr (!kPacked) while (pairs != 0u) {
+            const uint32_t j0 = __ffs(pairs) - 1u;
+            pairs &= pairs - 1u;
+            const uint32_t j1 = pairs != 0u ? __ffs(pairs) - 1u : 32u;
+            pairs &= pairs - 1u;
+            const uint32_t jh = (lane & 16u) != 0u ? j1 : j0;
+            const bool active = jh < 32u;
+            const uint32_t j = active ? jh : j0;
+            const RecordStage<S> st = stage[j];
+            const Rec2D<S>& r = st.r;
+            const uint32_t barea = active ? st.area : 0u;
+            const uint32_t span = (barea + 15u) >> 4;
+            const uint32_t iters = max(span, __shfl_xor_sync(0xffffffffu, span, 16));
+            const size_t rid = base + j;
+            const uint32_t cam = st.cam;
+            const uint32_t n = uint32_t(rid) - cam * N;
+            const size_t cam_base = size_t(cam) * height * width;
+            const S* vimg = v_render != nullptr ? v_render + cam_base : nullptr;
+            const S* vvar = kVar ? v_render_var + cam_base : nullptr;
+            const S q = chain_var ? st.q : S(0);
+            const S om = r.o * r.mu;
+            S part[8];
+            S g_ax = S(0), g_ay = S(0);
+            record_walk_scalar<S, kBeta, kVar, kAbs, 16u>(r, om, q, vimg, vvar, st.x0, st.y0, st.w, barea, iters,
+                                                          width, part, g_ax, g_ay);
+            S lo, hi;
+            warp_sum8_pairs<16u>(part, lo, hi);
+            if (active && (lane & 3u) == 0u)
+                store_record_adjoints<S, kBeta, kVar>(r, (lane >> 2) & 3u, lo, hi, grads + rid, v_unc, n);
+            if (kAbs) {
+#pragma unroll
+                for (int offset = 8; offset > 0; offset >>= 1) {
+                    g_ax += __shfl_xor_sync(0xffffffffu, g_ax, offset);
+                    g_ay += __shfl_xor_sync(0xffffffffu, g_ay, offset);
+                }
+                if (active && (lane & 15u) == 0u) {
                     v_abs[2 * rid] = g_ax;
                     v_abs[2 * rid + 1] = g_ay;
                 }

@@ -114,7 +114,10 @@ def _expected_beta_var(rec, q, v, vv):
     a, b, c, o, mu = [r[:, i] for i in range(2, 7)]
     grads = torch.stack([2 * (a * s[0] + b * s[1]), 2 * (b * s[0] + c * s[1]), s[2], 2 * s[3], s[4], mu * s[5],
                          o * s[5], s[6]], 1)
-    return grads, s[7]
+    a, b, c = [r[:, i, None, None] for i in range(2, 5)]
+    absgrad = torch.stack([(2 * (a * w * dx + b * w * dy)).abs().sum((1, 2)),
+                           (2 * (b * w * dx + c * w * dy)).abs().sum((1, 2))], 1)
+    return grads, s[7], absgrad
 
 
 @pytest.mark.parametrize("detach", [False, True])
@@ -133,10 +136,50 @@ def test_record_vjp_beta_variance_matches_float64(device, detach):
     _backend.call("r2s_raster_record_bwd", 0, rec.data_ptr(), rects.data_ptr(), q.data_ptr(), 1, int(detach),
                   v.data_ptr(), vv.data_ptr(), 1, n, W, H, T, grads.data_ptr(), None, v_unc.data_ptr(),
                   torch.cuda.current_stream(device).cuda_stream)
-    want, want_unc = _expected_beta_var(rec, torch.zeros_like(q) if detach else q, v, vv)
+    want, want_unc, _ = _expected_beta_var(rec, torch.zeros_like(q) if detach else q, v, vv)
     assert torch.isfinite(grads).all() and torch.isfinite(v_unc).all()
     scale = want.abs().amax(0).clamp(min=1e-12)
     err = ((grads.double() - want).abs() / scale).amax(0)
     assert (err < 1e-4).all(), err.tolist()
     unc_scale = want_unc.abs().max().clamp(min=1e-12)
     assert ((v_unc.double() - want_unc).abs().max() / unc_scale).item() < 1e-4
+
+
+@pytest.mark.parametrize("var,absgrad", [(True, False), (False, True), (True, True)])
+def test_record_vjp_beta_mixed_box_sizes(device, var, absgrad):
+    """Boxes from a few pixels to the whole image and an odd record count: boxes of at
+    most 128 pixels are walked two records at a time by half warps, larger ones by the
+    whole warp, and an unpaired small record leaves one half idle."""
+    n = 77
+    rec = _records(device, n=n, seed=5)
+    gen = torch.Generator(device="cpu").manual_seed(21)
+    rec[:, 7] = (torch.rand(n, generator=gen) * 3.5 + 0.5).to(device)  # beta
+    rec[:, 2:5] *= torch.exp(torch.rand(n, 1, generator=gen) * 5 - 2.5).to(device)
+    r = rec.double()
+    det = r[:, 2] * r[:, 4] - r[:, 3] ** 2
+    hx = torch.sqrt((r[:, 4] / det).clamp(min=0)) + 0.01
+    hy = torch.sqrt((r[:, 2] / det).clamp(min=0)) + 0.01
+    area = (2 * hx + 1) * (2 * hy + 1)
+    assert int((area < 100).sum()) > 10 and int((area > 160).sum()) > 10  # both walks are taken
+    q = (torch.rand(n, generator=gen) * 0.1).to(device)
+    v = torch.randn((H, W), generator=gen).to(device)
+    vv = (0.1 * torch.randn((H, W), generator=gen)).to(device) if var else torch.zeros((H, W), device=device)
+    rects = torch.tensor([0, 0, (W + T - 1) // T, (H + T - 1) // T], dtype=torch.int16, device=device).repeat(n, 1)
+    grads = torch.full((n, 8), float("nan"), device=device)
+    v_unc = torch.zeros(n, device=device)
+    v_abs = torch.full((n, 2), float("nan"), device=device)
+    _backend.call("r2s_raster_record_bwd", 0, rec.data_ptr(), rects.data_ptr(), q.data_ptr(), 1, 0,
+                  v.data_ptr(), vv.data_ptr() if var else None, 1, n, W, H, T, grads.data_ptr(),
+                  v_abs.data_ptr() if absgrad else None, v_unc.data_ptr() if var else None,
+                  torch.cuda.current_stream(device).cuda_stream)
+    want, want_unc, want_abs = _expected_beta_var(rec, q, v, vv)
+    assert torch.isfinite(grads).all()
+    scale = want.abs().amax(0).clamp(min=1e-12)
+    err = ((grads.double() - want).abs() / scale).amax(0)
+    assert (err < 1e-4).all(), err.tolist()
+    if var:
+        unc_scale = want_unc.abs().max().clamp(min=1e-12)
+        assert ((v_unc.double() - want_unc).abs().max() / unc_scale).item() < 1e-4
+    if absgrad:
+        abs_scale = want_abs.abs().amax(0).clamp(min=1e-12)
+        assert (((v_abs.double() - want_abs).abs() / abs_scale).amax(0) < 1e-4).all()
