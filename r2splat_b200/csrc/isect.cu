@@ -136,11 +136,18 @@ constexpr int kMaxDigitBits = 10;
 template <typename Digit>
 __device__ __forceinline__ void block_histogram(const uint32_t* __restrict__ keys, int64_t begin, int64_t end,
                                                 Digit digit, uint32_t bins, uint32_t* s_hist) {
-    for (uint32_t d = threadIdx.x; d < bins; d += kSortThreads) s_hist[d] = 0;
-    __syncthreads();
+    uint32_t k_key[kSortItems];
+#pragma unroll
     for (int k = 0; k < kSortItems; ++k) {
         const int64_t i = begin + int64_t(k) * kSortThreads + threadIdx.x;
-        if (i < end) atomicAdd(&s_hist[digit(keys[i])], 1u);
+        k_key[k] = i < end ? keys[i] : 0u;
+    }
+    for (uint32_t d = threadIdx.x; d < bins; d += kSortThreads) s_hist[d] = 0;
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kSortItems; ++k) {
+        const int64_t i = begin + int64_t(k) * kSortThreads + threadIdx.x;
+        if (i < end) atomicAdd(&s_hist[digit(k_key[k])], 1u);
     }
     __syncthreads();
 }
@@ -184,15 +191,21 @@ __device__ __forceinline__ void block_scatter(const uint32_t* __restrict__ keys,
     uint32_t* my_cnt = s_cnt + warp * bins;
     const uint32_t lt_mask = (1u << lane) - 1u;
     const int64_t base = block_base + int64_t(warp) * (kSortTile / kSortWarps);
-    uint32_t k_key[kSortItems], k_val[kSortItems], k_rank[kSortItems];
+    uint32_t k_key[kSortItems], k_rank[kSortItems];
+    // The keys are loaded first: the ranking loop below orders its
+    // shared-memory updates with __syncwarp, which would otherwise hold each
+    // load back until the previous item was ranked. The values are loaded
+    // where they are staged.
+#pragma unroll
+    for (int k = 0; k < kSortItems; ++k) {
+        const int64_t i = base + int64_t(k) * 32 + lane;
+        k_key[k] = i < end ? keys[i] : 0u;
+    }
 #pragma unroll
     for (int k = 0; k < kSortItems; ++k) {
         const int64_t i = base + int64_t(k) * 32 + lane;
         const bool valid = i < end;
-        const uint32_t key = valid ? keys[i] : 0u;
-        k_key[k] = key;
-        k_val[k] = valid ? vals[i] : 0u;
-        const uint32_t d = valid ? digit(key) : bins;
+        const uint32_t d = valid ? digit(k_key[k]) : bins;
         const uint32_t peers = __match_any_sync(0xffffffffu, d);
         const uint32_t leader = __ffs(peers) - 1;
         uint32_t count = 0;
@@ -240,7 +253,7 @@ __device__ __forceinline__ void block_scatter(const uint32_t* __restrict__ keys,
             const uint32_t d = digit(k_key[k]);
             const uint32_t slot = s_local[d] + my_cnt[d] + k_rank[k];
             s_key[slot] = k_key[k];
-            s_val[slot] = k_val[k];
+            s_val[slot] = vals[i];
         }
     }
     __syncthreads();
@@ -255,8 +268,11 @@ __device__ __forceinline__ void block_scatter(const uint32_t* __restrict__ keys,
     }
 }
 
+// The scatter kernels are bounded to three resident blocks per SM (at most 85
+// registers a thread): left to itself ptxas gives them 128 registers and two
+// blocks, and the sort runs latency-bound.
 template <typename KeyOut, typename ValOut>
-__global__ void __launch_bounds__(kSortThreads) radix_downsweep_kernel(
+__global__ void __launch_bounds__(kSortThreads, 3) radix_downsweep_kernel(
     const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals, int64_t n, const int64_t* __restrict__ n_dev,
     int shift, uint32_t mask, const uint32_t* __restrict__ offsets, KeyOut* __restrict__ keys_out,
     ValOut* __restrict__ vals_out) {
@@ -273,12 +289,13 @@ __global__ void __launch_bounds__(kSortThreads) radix_downsweep_kernel(
 // ------------------------------------------------ camera-segmented 2D sort
 //
 // 2D keys are cam * n_tiles + tile and emission is camera-major, so the key
-// array is already ordered by camera: one stable pass on the tile digit
-// inside each camera's segment sorts it completely. Each sort block takes
-// kSortTile elements of one camera. The histogram of camera c, tile d, block
-// j (of nb_c) sits at n_tiles * first_block_c + d * nb_c + j, so one
-// exclusive scan over all of them gives every block's output position per
-// tile directly (cameras before c, then tiles before d, then earlier blocks).
+// array is already ordered by camera: stable passes on the tile index inside
+// each camera's segment sort it completely, and the camera never needs a
+// digit of its own. Each sort block takes kSortTile elements of one camera.
+// The histogram of camera c, digit d, block j (of nb_c) sits at
+// bins * first_block_c + d * nb_c + j, so one exclusive scan over all of them
+// gives every block's output position per digit directly (cameras before c,
+// then digits before d, then earlier blocks).
 
 struct CamSegment {
     int64_t begin, end;    // elements of the camera
@@ -318,32 +335,40 @@ __device__ __forceinline__ uint32_t block_camera(const CamSegment* seg, uint32_t
     return lo;
 }
 
+// The digit of a segmented pass: bits [shift, shift + bits(mask)) of the tile
+// index key - key0.
+struct SegDigit {
+    uint32_t key0, shift, mask;
+    __device__ __forceinline__ uint32_t operator()(uint32_t key) const { return ((key - key0) >> shift) & mask; }
+};
+
 __global__ void __launch_bounds__(kSortThreads) segmented_upsweep_kernel(
     const uint32_t* __restrict__ keys, const CamSegment* __restrict__ seg, uint32_t C, uint32_t n_tiles,
-    const uint32_t* __restrict__ total_blocks, uint32_t* __restrict__ hist) {
+    uint32_t shift, uint32_t mask, uint32_t bins, const uint32_t* __restrict__ total_blocks,
+    uint32_t* __restrict__ hist) {
     extern __shared__ uint32_t s_hist[];
     const uint32_t b = blockIdx.x, used = *total_blocks;
     if (b >= used) {
-        // Zero the histogram tail that no camera uses (gridDim.x - used blocks of n_tiles).
-        uint32_t* tail = hist + size_t(n_tiles) * used + size_t(b - used) * n_tiles;
-        for (uint32_t d = threadIdx.x; d < n_tiles; d += kSortThreads) tail[d] = 0;
+        // Zero the histogram tail that no camera uses (gridDim.x - used blocks of bins).
+        uint32_t* tail = hist + size_t(bins) * used + size_t(b - used) * bins;
+        for (uint32_t d = threadIdx.x; d < bins; d += kSortThreads) tail[d] = 0;
         return;
     }
     const uint32_t c = block_camera(seg, C, b);
     const CamSegment sg = seg[c];
     const uint32_t j = b - sg.first_block;
     const int64_t begin = sg.begin + int64_t(j) * kSortTile;
-    const uint32_t key0 = c * n_tiles;
-    block_histogram(keys, begin, min(sg.end, begin + kSortTile), [=](uint32_t key) { return key - key0; }, n_tiles,
-                    s_hist);
-    uint32_t* out = hist + size_t(n_tiles) * sg.first_block + j;
-    for (uint32_t d = threadIdx.x; d < n_tiles; d += kSortThreads) out[size_t(d) * sg.n_blocks] = s_hist[d];
+    block_histogram(keys, begin, min(sg.end, begin + kSortTile), SegDigit{c * n_tiles, shift, mask}, bins, s_hist);
+    uint32_t* out = hist + size_t(bins) * sg.first_block + j;
+    for (uint32_t d = threadIdx.x; d < bins; d += kSortThreads) out[size_t(d) * sg.n_blocks] = s_hist[d];
 }
 
-__global__ void __launch_bounds__(kSortThreads) segmented_downsweep_kernel(
+template <typename KeyOut, typename ValOut>
+__global__ void __launch_bounds__(kSortThreads, 3) segmented_downsweep_kernel(
     const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals, const CamSegment* __restrict__ seg,
-    uint32_t C, uint32_t n_tiles, const uint32_t* __restrict__ total_blocks, const uint32_t* __restrict__ offsets,
-    int64_t* __restrict__ keys_out, int32_t* __restrict__ vals_out) {
+    uint32_t C, uint32_t n_tiles, uint32_t shift, uint32_t mask, uint32_t bins,
+    const uint32_t* __restrict__ total_blocks, const uint32_t* __restrict__ offsets, KeyOut* __restrict__ keys_out,
+    ValOut* __restrict__ vals_out) {
     extern __shared__ uint32_t s_cnt[];
     const uint32_t b = blockIdx.x;
     if (b >= *total_blocks) return;
@@ -351,11 +376,10 @@ __global__ void __launch_bounds__(kSortThreads) segmented_downsweep_kernel(
     const CamSegment sg = seg[c];
     const uint32_t j = b - sg.first_block;
     const int64_t begin = sg.begin + int64_t(j) * kSortTile;
-    const uint32_t key0 = c * n_tiles;
-    const uint32_t* base = offsets + size_t(n_tiles) * sg.first_block + j;
+    const uint32_t* base = offsets + size_t(bins) * sg.first_block + j;
     const uint32_t nb = sg.n_blocks;
-    block_scatter(keys, vals, begin, min(sg.end, begin + kSortTile), [=](uint32_t key) { return key - key0; },
-                  n_tiles, [=](uint32_t d) { return base[size_t(d) * nb]; }, keys_out, vals_out, s_cnt);
+    block_scatter(keys, vals, begin, min(sg.end, begin + kSortTile), SegDigit{c * n_tiles, shift, mask}, bins,
+                  [=](uint32_t d) { return base[size_t(d) * nb]; }, keys_out, vals_out, s_cnt);
 }
 
 __global__ void widen_kernel(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals, int64_t n,
@@ -420,15 +444,34 @@ inline SortPlan plan_sort(int64_t n, uint64_t n_keys) {
 }
 
 // Camera layout of 2D keys (cam * n_tiles + tile, emitted camera-major) for
-// the one-pass segmented sort; cum is the inclusive tile-count prefix over the
+// the camera-segmented sort; cum is the inclusive tile-count prefix over the
 // C * N (camera, element) pairs.
 struct CamLayout {
     const int64_t* cum;
     uint32_t C, N, n_tiles;
 };
 
-constexpr uint32_t kMaxSegmentedTiles = 1024;  // digit bins of the segmented pass
 constexpr uint32_t kMaxCameras = 65535;
+// The segmented sort takes the tile index in one pass of n_tiles bins up to
+// kSegmentedOnePass tiles, and beyond that in passes of at most
+// kSegmentedDigitBits bits (least significant first): few bins keep the
+// histogram L2-resident and each block's output runs long enough to coalesce.
+constexpr uint32_t kSegmentedOnePass = 1024;
+constexpr int kSegmentedDigitBits = 6;
+constexpr uint32_t kMaxSegmentedTiles = 1u << 24;
+
+struct SegPlan {
+    int passes, digit_bits;
+    uint32_t bins;  // per pass
+};
+
+inline SegPlan plan_segmented(uint32_t n_tiles) {
+    if (n_tiles <= kSegmentedOnePass) return SegPlan{1, 0, n_tiles};
+    const int bits = bits_for(n_tiles - 1);
+    const int passes = (bits + kSegmentedDigitBits - 1) / kSegmentedDigitBits;
+    const int digit_bits = (bits + passes - 1) / passes;
+    return SegPlan{passes, digit_bits, 1u << digit_bits};
+}
 
 inline size_t emit_workspace(int64_t n, uint64_t n_keys) {
     const SortPlan p = plan_sort(n, n_keys);
@@ -439,8 +482,10 @@ inline size_t emit_workspace(int64_t n, uint64_t n_keys) {
     a.take<uint32_t>(size_t(n));  // vals B
     const size_t blocks = size_t(p.blocks > 0 ? p.blocks : 1);
     const size_t hist_generic = size_t(1u << (p.digit_bits > 0 ? p.digit_bits : 1)) * blocks;
-    // Segmented: n_tiles * (blocks + C) <= kMaxSegmentedTiles * blocks + n_keys.
-    const size_t hist_segmented = size_t(kMaxSegmentedTiles) * blocks + size_t(n_keys);
+    // Segmented: bins * (blocks + C) with bins <= kSegmentedOnePass, and
+    // bins * C <= n_tiles * C = n_keys (bins = n_tiles in one pass, below it
+    // otherwise).
+    const size_t hist_segmented = size_t(kSegmentedOnePass) * blocks + size_t(n_keys);
     const size_t hist = hist_generic > hist_segmented ? hist_generic : hist_segmented;
     a.take<CamSegment>(size_t(n_keys < kMaxCameras ? n_keys : kMaxCameras));
     a.take<uint32_t>(1);
@@ -449,37 +494,58 @@ inline size_t emit_workspace(int64_t n, uint64_t n_keys) {
     return a.bytes();
 }
 
-// One stable pass on the tile digit inside each camera's segment, writing the
-// widened result to isect_ids/flatten_ids.
-inline int segmented_sort(const uint32_t* keys, const uint32_t* vals, int64_t n, const CamLayout& cams,
-                          Arena& arena, int64_t* isect_ids, int32_t* flatten_ids, cudaStream_t stream,
-                          const int64_t* n_dev) {
+// Stable passes on the tile index inside each camera's segment (one pass up to
+// kSegmentedOnePass tiles), the last writing the widened result to
+// isect_ids/flatten_ids. keys and vals are kept intact for a single pass and
+// serve as ping-pong buffers otherwise.
+inline int segmented_sort(uint32_t* keys, uint32_t* vals, int64_t n, const CamLayout& cams, Arena& arena,
+                          int64_t* isect_ids, int32_t* flatten_ids, cudaStream_t stream, const int64_t* n_dev) {
+    const SegPlan plan = plan_segmented(cams.n_tiles);
     const int64_t max_blocks = (n + kSortTile - 1) / kSortTile + int64_t(cams.C);
     R2S_REQUIRE(max_blocks < (int64_t(1) << 31), R2S_ERR_UNSUPPORTED, "too many intersections");
+    uint32_t* keys_b = plan.passes > 1 ? arena.take<uint32_t>(size_t(n)) : nullptr;
+    uint32_t* vals_b = plan.passes > 1 ? arena.take<uint32_t>(size_t(n)) : nullptr;
     CamSegment* seg = arena.take<CamSegment>(cams.C);
     uint32_t* total_blocks = arena.take<uint32_t>(1);
-    const int64_t hist_len = int64_t(cams.n_tiles) * max_blocks;
+    const int64_t hist_len = int64_t(plan.bins) * max_blocks;
     uint32_t* hist = arena.take<uint32_t>(size_t(hist_len));
-    R2S_REQUIRE(seg && total_blocks && hist, R2S_ERR_WORKSPACE, "intersection workspace too small");
+    R2S_REQUIRE(seg && total_blocks && hist && (plan.passes == 1 || (keys_b && vals_b)), R2S_ERR_WORKSPACE,
+                "intersection workspace too small");
     void* scan_ws = arena.base + arena.used;
     const size_t scan_bytes = arena.size - arena.used;
     cam_segments_kernel<<<1, 32, 0, stream>>>(cams.cum, cams.C, cams.N, n, n_dev, seg, total_blocks);
     R2S_TRY(check_launch("cam_segments"));
-    segmented_upsweep_kernel<<<unsigned(max_blocks), kSortThreads, cams.n_tiles * sizeof(uint32_t), stream>>>(
-        keys, seg, cams.C, cams.n_tiles, total_blocks, hist);
-    R2S_TRY(check_launch("segmented_upsweep"));
-    R2S_TRY((device_scan<uint32_t, uint32_t, false>(hist, hist, hist_len, scan_ws, scan_bytes, stream)));
-    const size_t down_smem = (size_t(cams.n_tiles) * (kSortWarps + 2) + 2 * size_t(kSortTile)) * sizeof(uint32_t);
-    R2S_TRY(allow_dynamic_smem(segmented_downsweep_kernel, down_smem));
-    segmented_downsweep_kernel<<<unsigned(max_blocks), kSortThreads, down_smem, stream>>>(
-        keys, vals, seg, cams.C, cams.n_tiles, total_blocks, hist, isect_ids, flatten_ids);
-    return check_launch("segmented_downsweep");
+    const size_t down_smem = (size_t(plan.bins) * (kSortWarps + 2) + 2 * size_t(kSortTile)) * sizeof(uint32_t);
+    R2S_TRY(allow_dynamic_smem(segmented_downsweep_kernel<int64_t, int32_t>, down_smem));
+    if (plan.passes > 1) R2S_TRY(allow_dynamic_smem(segmented_downsweep_kernel<uint32_t, uint32_t>, down_smem));
+    uint32_t *src_k = keys, *src_v = vals, *dst_k = keys_b, *dst_v = vals_b;
+    for (int pass = 0; pass < plan.passes; ++pass) {
+        const uint32_t shift = uint32_t(pass * plan.digit_bits);
+        const uint32_t mask = plan.passes == 1 ? 0xffffffffu : plan.bins - 1u;
+        segmented_upsweep_kernel<<<unsigned(max_blocks), kSortThreads, plan.bins * sizeof(uint32_t), stream>>>(
+            src_k, seg, cams.C, cams.n_tiles, shift, mask, plan.bins, total_blocks, hist);
+        R2S_TRY(check_launch("segmented_upsweep"));
+        R2S_TRY((device_scan<uint32_t, uint32_t, false>(hist, hist, hist_len, scan_ws, scan_bytes, stream)));
+        if (pass == plan.passes - 1) {
+            segmented_downsweep_kernel<int64_t, int32_t><<<unsigned(max_blocks), kSortThreads, down_smem, stream>>>(
+                src_k, src_v, seg, cams.C, cams.n_tiles, shift, mask, plan.bins, total_blocks, hist, isect_ids,
+                flatten_ids);
+        } else {
+            segmented_downsweep_kernel<uint32_t, uint32_t><<<unsigned(max_blocks), kSortThreads, down_smem,
+                                                             stream>>>(
+                src_k, src_v, seg, cams.C, cams.n_tiles, shift, mask, plan.bins, total_blocks, hist, dst_k, dst_v);
+        }
+        R2S_TRY(check_launch("segmented_downsweep"));
+        uint32_t* t = src_k; src_k = dst_k; dst_k = t;
+        t = src_v; src_v = dst_v; dst_v = t;
+    }
+    return R2S_OK;
 }
 
 // Sorts (keys, vals) of length n by key bits [0, bits(n_keys-1)), writing
 // the widened result to isect_ids/flatten_ids, then fills offsets. With a
-// camera layout of at most kMaxSegmentedTiles tiles per camera the sort is
-// the one-pass segmented one.
+// camera layout (at most kMaxSegmentedTiles tiles per camera) the sort is the
+// camera-segmented one, which needs no passes over the camera bits.
 inline int sort_and_finish(uint32_t* keys, uint32_t* vals, int64_t n, uint64_t n_keys, Arena& arena,
                            int64_t* isect_ids, int32_t* flatten_ids, int32_t* offsets, cudaStream_t stream,
                            const int64_t* n_dev = nullptr, const CamLayout* cams = nullptr) {

@@ -206,6 +206,24 @@ def test_tile_lists_match_numpy_oracle_bit_exact(device, tile, dtype):
                           tiles.offset_encode(i3, t3 ** 3))
 
 
+@pytest.mark.parametrize("tiles_xy", [(40, 52), (48, 48), (64, 64), (100, 100)])
+def test_tile_lists_with_many_tiles_per_camera_bit_exact(device, tiles_xy):
+    """More than 1024 tiles per camera (1-pixel tiles): the camera-segmented sort takes
+    the tile index in two or three passes of a few bits each."""
+    sc = scenes.small_scene().to(device)
+    covars, _ = low.parameter_transform_fwd(sc.quats, sc.scales)
+    m2, _, radii = low.world_to_image_projection_fwd(sc.means, covars, sc.viewmats, sc.Ks, 64, 64, 1e-8, 3.0)
+    tx, ty = tiles_xy
+    counts, ids, fids = low.isect_tiles(m2, radii, 1, tx, ty)
+    c2, i2, f2 = tiles.isect_tiles_2d(m2.cpu().numpy(), radii.cpu().numpy(), 1, tx, ty)
+    assert ids.numel() > 100_000
+    assert np.array_equal(counts.cpu().numpy(), c2)
+    assert np.array_equal(ids.cpu().numpy(), i2)
+    assert np.array_equal(fids.cpu().numpy(), f2)
+    offsets = low.isect_offset_encode(ids, 4, tx, ty)
+    assert np.array_equal(offsets.cpu().numpy().reshape(-1), tiles.offset_encode(i2, 4 * tx * ty))
+
+
 def test_3d_tile_bound_golden_cases(device):
     import json
 
