@@ -141,14 +141,14 @@ __device__ __forceinline__ S warp_sum(S v) {
 }
 
 // Sum of eight per-lane values over each group of kLanes lanes (32: the warp;
-// 16: each half of it) by recursive halving: each exchange step sends half of
+// 16 or 8: each half or quarter of it) by recursive halving: each exchange step sends half of
 // the lane's values to its partner and keeps the other half, so a warp-wide
 // reduction costs 4 + 2 + 2 * 3 shuffles instead of 8 * 5. On return every
 // lane of subgroup G = (lane % kLanes) / (kLanes / 4) holds its group's totals
 // of values 2G and 2G + 1 in (out0, out1).
 template <uint32_t kLanes = 32u, typename S>
 __device__ __forceinline__ void warp_sum8_pairs(const S (&v)[8], S& out0, S& out1) {
-    static_assert(kLanes == 32u || kLanes == 16u, "groups of 32 or 16 lanes");
+    static_assert(kLanes == 32u || kLanes == 16u || kLanes == 8u, "groups of 32, 16 or 8 lanes");
     const uint32_t lane = threadIdx.x & 31u;
     const bool upper = (lane & (kLanes / 2u)) != 0;
     S w[4];

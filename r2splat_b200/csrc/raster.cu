@@ -871,10 +871,12 @@ __device__ __forceinline__ void record_walk_scalar(const Rec2D<S>& r, S om, S q,
     }
 }
 
-// Boxes of at most this many pixels are walked by half warps, two records at a
-// time: a small box fills a 16-lane step about as well as a 32-lane one, and
-// the pair shares one pass of the per-record set-up and reduction.
+// Boxes of at most kHalfWarpArea pixels are walked by half warps, two records
+// at a time, and boxes of at most kQuarterWarpArea by quarter warps, four at a
+// time: a small box fills a narrow step about as well as a 32-lane one, and
+// the group shares one pass of the per-record set-up and reduction.
 constexpr uint32_t kHalfWarpArea = 128u;
+constexpr uint32_t kQuarterWarpArea = 64u;
 
 // Writes the slot adjoints of record subgroup grp (0..3) from its pair of
 // reduced sums (see record_adjoints) and adds the uncertainty adjoint.
@@ -903,6 +905,68 @@ struct alignas(16) RecordStage {
     S q;
     float e_min;
 };
+
+// Walks the staged records of `mask` in groups of 32 / kLanes, one record per
+// kLanes-lane group of the warp (a group without a record walks nothing and
+// stores nothing), with the scalar walk, a group-wide reduction and the
+// record's stores. base is the warp's first record; var_q is null without the
+// variance chain term.
+template <typename S, bool kBeta, bool kVar, bool kAbs, uint32_t kLanes>
+__device__ __forceinline__ void walk_record_groups(uint32_t mask, const RecordStage<S>* stage, size_t base, uint32_t N,
+                                                   uint32_t width, uint32_t height, const S* v_render,
+                                                   const S* v_render_var, const S* var_q, Rec2D<S>* grads,
+                                                   S* v_abs, S* v_unc) {
+    constexpr uint32_t kGroups = 32u / kLanes;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t group = lane / kLanes;
+    while (mask != 0u) {
+        const uint32_t j0 = __ffs(mask) - 1u;
+        uint32_t jg = 32u;
+#pragma unroll
+        for (uint32_t g = 0; g < kGroups; ++g) {
+            const uint32_t jn = mask != 0u ? __ffs(mask) - 1u : 32u;
+            mask &= mask - 1u;
+            if (group == g) jg = jn;
+        }
+        const bool active = jg < 32u;
+        const uint32_t j = active ? jg : j0;
+        const RecordStage<S> st = stage[j];
+        const Rec2D<S>& r = st.r;
+        const uint32_t barea = active ? st.area : 0u;
+        uint32_t iters = (barea + kLanes - 1u) / kLanes;
+#pragma unroll
+        for (uint32_t offset = kLanes; offset < 32u; offset <<= 1)
+            iters = max(iters, __shfl_xor_sync(0xffffffffu, iters, offset));
+        const size_t rid = base + j;
+        const uint32_t cam = st.cam;
+        const uint32_t n = uint32_t(rid) - cam * N;
+        const size_t cam_base = size_t(cam) * height * width;
+        const S* vimg = v_render != nullptr ? v_render + cam_base : nullptr;
+        const S* vvar = kVar ? v_render_var + cam_base : nullptr;
+        const S q = var_q != nullptr ? st.q : S(0);
+        const S om = r.o * r.mu;
+        S part[8];
+        S g_ax = S(0), g_ay = S(0);
+        record_walk_scalar<S, kBeta, kVar, kAbs, kLanes>(r, om, q, vimg, vvar, st.x0, st.y0, st.w, barea, iters,
+                                                         width, part, g_ax, g_ay);
+        S lo, hi;
+        warp_sum8_pairs<kLanes>(part, lo, hi);
+        constexpr uint32_t kSub = kLanes / 4u;  // lanes per reduced pair
+        if (active && (lane & (kSub - 1u)) == 0u)
+            store_record_adjoints<S, kBeta, kVar>(r, (lane % kLanes) / kSub, lo, hi, grads + rid, v_unc, n);
+        if (kAbs) {
+#pragma unroll
+            for (uint32_t offset = kLanes / 2u; offset > 0u; offset >>= 1) {
+                g_ax += __shfl_xor_sync(0xffffffffu, g_ax, offset);
+                g_ay += __shfl_xor_sync(0xffffffffu, g_ay, offset);
+            }
+            if (active && (lane % kLanes) == 0u) {
+                v_abs[2 * rid] = g_ax;
+                v_abs[2 * rid + 1] = g_ay;
+            }
+        }
+    }
+}
 
 template <typename S, bool kBeta, bool kVar, bool kAbs>
 __global__ void __launch_bounds__(kRecBwdThreads) raster_record_bwd_kernel(
@@ -960,11 +1024,14 @@ __global__ void __launch_bounds__(kRecBwdThreads) raster_record_bwd_kernel(
                 }
             }
         }
-        // Boxes of the scalar walk with at most kHalfWarpArea pixels go to the
-        // half-warp pairs; the rest are walked one by one by the whole warp.
-        // (The plain Gaussian instantiation, which takes the packed walk, has no pairs.)
-        uint32_t pairs = kPacked ? 0u : __ballot_sync(0xffffffffu, area != 0u && area <= kHalfWarpArea);
-        uint32_t pending = __ballot_sync(0xffffffffu, area != 0u) & ~pairs;
+        // Boxes of the scalar walk with at most kQuarterWarpArea pixels go to
+        // quarter-warp groups, up to kHalfWarpArea to half-warp pairs; the rest
+        // are walked one by one by the whole warp. (The plain Gaussian
+        // instantiation, which takes the packed walk, has no groups.)
+        uint32_t quads = kPacked ? 0u : __ballot_sync(0xffffffffu, area != 0u && area <= kQuarterWarpArea);
+        uint32_t pairs =
+            kPacked ? 0u : __ballot_sync(0xffffffffu, area > kQuarterWarpArea && area <= kHalfWarpArea);
+        uint32_t pending = __ballot_sync(0xffffffffu, area != 0u) & ~(pairs | quads);
         __syncwarp();  // the previous group's constants have been read
         if (area != 0u) {
             RecordStage<S> st;
@@ -1030,49 +1097,13 @@ __global__ void __launch_bounds__(kRecBwdThreads) raster_record_bwd_kernel(
                 }
             }
         }
-        // The small boxes, two records per step: the lower half warp walks
-        // record j0, the upper one j1 (none for an odd count: that half walks
-        // nothing and stores nothing).
-        if constexpr (!kPacked) while (pairs != 0u) {
-            const uint32_t j0 = __ffs(pairs) - 1u;
-            pairs &= pairs - 1u;
-            const uint32_t j1 = pairs != 0u ? __ffs(pairs) - 1u : 32u;
-            pairs &= pairs - 1u;
-            const uint32_t jh = (lane & 16u) != 0u ? j1 : j0;
-            const bool active = jh < 32u;
-            const uint32_t j = active ? jh : j0;
-            const RecordStage<S> st = stage[j];
-            const Rec2D<S>& r = st.r;
-            const uint32_t barea = active ? st.area : 0u;
-            const uint32_t span = (barea + 15u) >> 4;
-            const uint32_t iters = max(span, __shfl_xor_sync(0xffffffffu, span, 16));
-            const size_t rid = base + j;
-            const uint32_t cam = st.cam;
-            const uint32_t n = uint32_t(rid) - cam * N;
-            const size_t cam_base = size_t(cam) * height * width;
-            const S* vimg = v_render != nullptr ? v_render + cam_base : nullptr;
-            const S* vvar = kVar ? v_render_var + cam_base : nullptr;
-            const S q = chain_var ? st.q : S(0);
-            const S om = r.o * r.mu;
-            S part[8];
-            S g_ax = S(0), g_ay = S(0);
-            record_walk_scalar<S, kBeta, kVar, kAbs, 16u>(r, om, q, vimg, vvar, st.x0, st.y0, st.w, barea, iters,
-                                                          width, part, g_ax, g_ay);
-            S lo, hi;
-            warp_sum8_pairs<16u>(part, lo, hi);
-            if (active && (lane & 3u) == 0u)
-                store_record_adjoints<S, kBeta, kVar>(r, (lane >> 2) & 3u, lo, hi, grads + rid, v_unc, n);
-            if (kAbs) {
-#pragma unroll
-                for (int offset = 8; offset > 0; offset >>= 1) {
-                    g_ax += __shfl_xor_sync(0xffffffffu, g_ax, offset);
-                    g_ay += __shfl_xor_sync(0xffffffffu, g_ay, offset);
-                }
-                if (active && (lane & 15u) == 0u) {
-                    v_abs[2 * rid] = g_ax;
-                    v_abs[2 * rid + 1] = g_ay;
-                }
-            }
+        // The small boxes, four or two records per warp step.
+        if constexpr (!kPacked) {
+            walk_record_groups<S, kBeta, kVar, kAbs, 8u>(quads, stage, base, N, width, height, v_render, v_render_var,
+                                                         chain_var ? var_q : nullptr, grads, v_abs, v_unc);
+            walk_record_groups<S, kBeta, kVar, kAbs, 16u>(pairs, stage, base, N, width, height, v_render,
+                                                          v_render_var, chain_var ? var_q : nullptr, grads, v_abs,
+                                                          v_unc);
         }
     }
 }

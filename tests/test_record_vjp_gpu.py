@@ -148,8 +148,9 @@ def test_record_vjp_beta_variance_matches_float64(device, detach):
 @pytest.mark.parametrize("var,absgrad", [(True, False), (False, True), (True, True)])
 def test_record_vjp_beta_mixed_box_sizes(device, var, absgrad):
     """Boxes from a few pixels to the whole image and an odd record count: boxes of at
-    most 128 pixels are walked two records at a time by half warps, larger ones by the
-    whole warp, and an unpaired small record leaves one half idle."""
+    most 64 pixels are walked four records at a time by quarter warps, up to 128 pixels
+    two at a time by half warps, larger ones by the whole warp; a group short of records
+    leaves lanes idle."""
     n = 77
     rec = _records(device, n=n, seed=5)
     gen = torch.Generator(device="cpu").manual_seed(21)
@@ -160,7 +161,8 @@ def test_record_vjp_beta_mixed_box_sizes(device, var, absgrad):
     hx = torch.sqrt((r[:, 4] / det).clamp(min=0)) + 0.01
     hy = torch.sqrt((r[:, 2] / det).clamp(min=0)) + 0.01
     area = (2 * hx + 1) * (2 * hy + 1)
-    assert int((area < 100).sum()) > 10 and int((area > 160).sum()) > 10  # both walks are taken
+    assert int((area < 50).sum()) > 10 and int(((area > 66) & (area < 120)).sum()) > 4  # quarter and half groups
+    assert int((area > 160).sum()) > 10  # and the whole-warp walk
     q = (torch.rand(n, generator=gen) * 0.1).to(device)
     v = torch.randn((H, W), generator=gen).to(device)
     vv = (0.1 * torch.randn((H, W), generator=gen)).to(device) if var else torch.zeros((H, W), device=device)
