@@ -190,3 +190,32 @@ def test_check_kernel_flags_each_kind(device):
                   torch.cuda.current_stream(device).cuda_stream)
     word = int(flags.item()) & 0xFFFFFFFF
     assert word == ((1 << 14) - 1) & ~((1 << 7) - 1)
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+def test_finite_check_vector_path_positions(device, dtype):
+    # Large finiteness checks read 16-byte vectors, four in flight per thread, then the
+    # remaining vectors, then a scalar tail; unaligned data takes the element loop.
+    # A single non-finite value in each region, and in an unaligned view, sets its bit.
+    from r2splat_b200._validation import FINITE, _ValueCheck
+    n = 1184 * 256 * 4 * 4 * 3 + 1184 * 256 * 2 + 3  # unrolled strides, single vectors and a scalar tail
+    per = 16 // torch.tensor([], dtype=dtype).element_size()
+    base = torch.ones(n, dtype=dtype, device=device)
+    positions = {"unrolled": 12345, "vectors": (n // per) * per - per - 7, "tail": n - 1}
+    tensors, bits = [base], []
+    for pos in positions.values():
+        t = base.clone()
+        t[pos] = math.nan
+        tensors.append(t)
+    unaligned = base.clone()
+    unaligned[n // 2] = -math.inf
+    views = [(t, t.numel()) for t in tensors] + [(unaligned[1:], n - 1)]
+    table = (_ValueCheck * len(views))()
+    for bit, (t, count) in enumerate(views):
+        assert t.data_ptr() % 16 == (0 if bit < len(tensors) else t.element_size())
+        table[bit] = _ValueCheck(t.data_ptr(), count, FINITE, bit)
+    flags = torch.full((1,), -1, dtype=torch.int32, device=device)
+    _backend.call("r2s_check_values", 0 if dtype == torch.float32 else 1, table, len(views), flags.data_ptr(),
+                  torch.cuda.current_stream(device).cuda_stream)
+    word = int(flags.item()) & 0xFFFFFFFF
+    assert word == (1 << len(views)) - 2  # every bit but the all-finite tensor's
