@@ -871,12 +871,14 @@ __device__ __forceinline__ void record_walk_scalar(const Rec2D<S>& r, S om, S q,
     }
 }
 
-// Boxes of at most kHalfWarpArea pixels are walked by half warps, two records
-// at a time, and boxes of at most kQuarterWarpArea by quarter warps, four at a
-// time: a small box fills a narrow step about as well as a 32-lane one, and
-// the group shares one pass of the per-record set-up and reduction.
-constexpr uint32_t kHalfWarpArea = 128u;
-constexpr uint32_t kQuarterWarpArea = 64u;
+// In the scalar walk, boxes of at most kHalfWarpArea pixels are walked by half
+// warps, two records at a time, and boxes of at most kQuarterWarpArea by
+// quarter warps, four at a time: a small box fills a narrow step about as well
+// as a 32-lane one, and the group shares one pass of the per-record set-up and
+// reduction. The warp's records are sorted by box size first, so a group's
+// boxes take about the same number of steps.
+constexpr uint32_t kHalfWarpArea = 1024u;
+constexpr uint32_t kQuarterWarpArea = 256u;
 
 // Writes the slot adjoints of record subgroup grp (0..3) from its pair of
 // reduced sums (see record_adjoints) and adds the uncertainty adjoint.
@@ -906,28 +908,43 @@ struct alignas(16) RecordStage {
     float e_min;
 };
 
-// Walks the staged records of `mask` in groups of 32 / kLanes, one record per
-// kLanes-lane group of the warp (a group without a record walks nothing and
-// stores nothing), with the scalar walk, a group-wide reduction and the
-// record's stores. base is the warp's first record; var_q is null without the
-// variance chain term.
+// Ascending sort of one 32-bit key per lane across the warp (bitonic network,
+// 15 compare-exchange stages through shuffles); keys must be distinct.
+__device__ __forceinline__ uint32_t warp_sort_ascending(uint32_t key) {
+    const uint32_t lane = threadIdx.x & 31u;
+#pragma unroll
+    for (uint32_t k = 2u; k <= 32u; k <<= 1) {
+#pragma unroll
+        for (uint32_t j = k >> 1; j > 0u; j >>= 1) {
+            const uint32_t other = __shfl_xor_sync(0xffffffffu, key, j);
+            const bool ascending = (lane & k) == 0u;
+            const bool lower = (lane & j) == 0u;
+            key = lower == ascending ? min(key, other) : max(key, other);
+        }
+    }
+    return key;
+}
+
+// Walks the staged records at sorted positions [p, p_end) in groups of
+// 32 / kLanes, one record per kLanes-lane group of the warp (a group without
+// a record walks nothing and stores nothing), with the scalar walk, a
+// group-wide reduction and the record's stores. Lane L of `sorted` holds the
+// L-th smallest (area << 5 | record lane) of the warp's records, so a step's
+// records have boxes of about one size. base is the warp's first record;
+// var_q is null without the variance chain term.
 template <typename S, bool kBeta, bool kVar, bool kAbs, uint32_t kLanes>
-__device__ __forceinline__ void walk_record_groups(uint32_t mask, const RecordStage<S>* stage, size_t base, uint32_t N,
+__device__ __forceinline__ void walk_record_groups(uint32_t sorted, uint32_t p, uint32_t p_end,
+                                                   const RecordStage<S>* stage, size_t base, uint32_t N,
                                                    uint32_t width, uint32_t height, const S* v_render,
                                                    const S* v_render_var, const S* var_q, Rec2D<S>* grads,
                                                    S* v_abs, S* v_unc) {
     constexpr uint32_t kGroups = 32u / kLanes;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t group = lane / kLanes;
-    while (mask != 0u) {
-        const uint32_t j0 = __ffs(mask) - 1u;
-        uint32_t jg = 32u;
-#pragma unroll
-        for (uint32_t g = 0; g < kGroups; ++g) {
-            const uint32_t jn = mask != 0u ? __ffs(mask) - 1u : 32u;
-            mask &= mask - 1u;
-            if (group == g) jg = jn;
-        }
+    for (; p < p_end; p += kGroups) {
+        const uint32_t j0 = __shfl_sync(0xffffffffu, sorted, p) & 31u;
+        const uint32_t mine = __shfl_sync(0xffffffffu, sorted, min(p + group, 31u)) & 31u;
+        const uint32_t jg = p + group < p_end ? mine : 32u;
         const bool active = jg < 32u;
         const uint32_t j = active ? jg : j0;
         const RecordStage<S> st = stage[j];
@@ -1028,10 +1045,8 @@ __global__ void __launch_bounds__(kRecBwdThreads) raster_record_bwd_kernel(
         // quarter-warp groups, up to kHalfWarpArea to half-warp pairs; the rest
         // are walked one by one by the whole warp. (The plain Gaussian
         // instantiation, which takes the packed walk, has no groups.)
-        uint32_t quads = kPacked ? 0u : __ballot_sync(0xffffffffu, area != 0u && area <= kQuarterWarpArea);
-        uint32_t pairs =
-            kPacked ? 0u : __ballot_sync(0xffffffffu, area > kQuarterWarpArea && area <= kHalfWarpArea);
-        uint32_t pending = __ballot_sync(0xffffffffu, area != 0u) & ~(pairs | quads);
+        const bool grouped = !kPacked && area != 0u && area <= kHalfWarpArea;
+        uint32_t pending = __ballot_sync(0xffffffffu, area != 0u && !grouped);
         __syncwarp();  // the previous group's constants have been read
         if (area != 0u) {
             RecordStage<S> st;
@@ -1097,13 +1112,21 @@ __global__ void __launch_bounds__(kRecBwdThreads) raster_record_bwd_kernel(
                 }
             }
         }
-        // The small boxes, four or two records per warp step.
+        // The small boxes, four or two records per warp step, taken in order of
+        // box size: sorted positions [0, n_quad) hold the quarter-warp records,
+        // [n_quad, n_group) the half-warp ones, and the other lanes sort last.
         if constexpr (!kPacked) {
-            walk_record_groups<S, kBeta, kVar, kAbs, 8u>(quads, stage, base, N, width, height, v_render, v_render_var,
-                                                         chain_var ? var_q : nullptr, grads, v_abs, v_unc);
-            walk_record_groups<S, kBeta, kVar, kAbs, 16u>(pairs, stage, base, N, width, height, v_render,
-                                                          v_render_var, chain_var ? var_q : nullptr, grads, v_abs,
-                                                          v_unc);
+            const uint32_t n_group = __popc(__ballot_sync(0xffffffffu, grouped));
+            const uint32_t n_quad = __popc(__ballot_sync(0xffffffffu, grouped && area <= kQuarterWarpArea));
+            if (n_group != 0u) {
+                const uint32_t sorted = warp_sort_ascending(grouped ? (area << 5) | lane : 0xffffffe0u | lane);
+                walk_record_groups<S, kBeta, kVar, kAbs, 8u>(sorted, 0u, n_quad, stage, base, N, width, height,
+                                                             v_render, v_render_var, chain_var ? var_q : nullptr,
+                                                             grads, v_abs, v_unc);
+                walk_record_groups<S, kBeta, kVar, kAbs, 16u>(sorted, n_quad, n_group, stage, base, N, width,
+                                                              height, v_render, v_render_var,
+                                                              chain_var ? var_q : nullptr, grads, v_abs, v_unc);
+            }
         }
     }
 }
