@@ -751,9 +751,11 @@ __constant__ uint32_t c_div_magic[33] = {
 // -(log2 e): exp(-s) = 2^(-s log2 e).
 constexpr float kNegLog2e = -1.4426950408889634f;
 
-// The walk of one Gaussian record (no variance branch, no absgrad) in packed
-// FP32x2 form: each lane evaluates two samples per step, k and k + 32 of the
-// row-major box order (k = lane + 64 it), so one FADD2/FMUL2/FFMA2 serves both.
+// The walk of one Gaussian record (no variance branch, no absgrad) by kLanes
+// lanes (the warp, or a half or quarter of it) in packed FP32x2 form: lane
+// l = lane % kLanes evaluates two samples per step, k and k + kLanes of the
+// row-major box order (k = l + 2 kLanes it), so one FADD2/FMUL2/FFMA2 serves
+// both. iters is uniform over the warp.
 // Pixel centres are stepped exactly in float (integers + 0.5); the pixel's
 // element offset py * width + px - (width + 1) / 2 is formed exactly in float
 // as well and read out through the 2^23 bias (valid while width * height <
@@ -764,14 +766,15 @@ constexpr float kNegLog2e = -1.4426950408889634f;
 // With w = -g alpha = -(o mu) g vis, the walk sums g vis and its moments and
 // scales them by -(o mu) once: part[0..4] are S0..S4 and part[5] = S5 of
 // vjp_sample.
+template <uint32_t kLanes = 32u>
 __device__ __forceinline__ void record_walk_packed(const Rec2D<float>& r, float om, float e_min, const float* vimg,
                                                    uint32_t bx0, uint32_t by0, uint32_t bw, uint32_t barea,
-                                                   uint32_t magic, uint32_t width, float (&part)[8]) {
-    const uint32_t lane = threadIdx.x & 31u;
+                                                   uint32_t magic, uint32_t width, uint32_t iters, float (&part)[8]) {
+    const uint32_t lane = threadIdx.x & (kLanes - 1u);
     // (k * magic) >> 16 == k / bw for k <= 64 (magic = ceil(2^16 / bw)).
-    const uint32_t dq = (64u * magic) >> 16, dr = 64u - dq * bw;
-    const uint32_t ra = (lane * magic) >> 16, rb = ((lane + 32u) * magic) >> 16;
-    const uint32_t ca = lane - ra * bw, cb = lane + 32u - rb * bw;
+    const uint32_t dq = (2u * kLanes * magic) >> 16, dr = 2u * kLanes - dq * bw;
+    const uint32_t ra = (lane * magic) >> 16, rb = ((lane + kLanes) * magic) >> 16;
+    const uint32_t ca = lane - ra * bw, cb = lane + kLanes - rb * bw;
     float2 px = make_float2(static_cast<float>(bx0 + ca) + 0.5f, static_cast<float>(bx0 + cb) + 0.5f);
     float2 py = make_float2(static_cast<float>(by0 + ra) + 0.5f, static_cast<float>(by0 + rb) + 0.5f);
     const float x_end = static_cast<float>(bx0 + bw);
@@ -785,14 +788,13 @@ __device__ __forceinline__ void record_walk_packed(const Rec2D<float>& r, float 
     const float2 qa = splat2(0.5f * r.a * kNegLog2e), qb = splat2(r.b * kNegLog2e);
     const float2 qc = splat2(0.5f * r.c * kNegLog2e);
     float2 acc0 = splat2(0.f), acc1 = acc0, acc2 = acc0, acc3 = acc0, acc4 = acc0, acc5 = acc0;
-    const uint32_t iters = (barea + 63u) >> 6;
     uint32_t k = lane;
-    for (uint32_t it = 0; it < iters; ++it, k += 64u) {
+    for (uint32_t it = 0; it < iters; ++it, k += 2u * kLanes) {
         const float2 offb = add2(fma2(py, fw, px), bias);
         const float* pa = reinterpret_cast<const float*>(vbase + uint64_t(__float_as_uint(offb.x)) * sizeof(float));
         const float* pb = reinterpret_cast<const float*>(vbase + uint64_t(__float_as_uint(offb.y)) * sizeof(float));
         const float ga = k < barea ? __ldg(pa) : 0.f;
-        const float gb = k + 32u < barea ? __ldg(pb) : 0.f;
+        const float gb = k + kLanes < barea ? __ldg(pb) : 0.f;
         const float2 dx = add2(px, nx), dy = add2(py, ny);
         const float2 t = fma2(qa, dx, mul2(qb, dy));
         const float2 e = fma2(dx, t, mul2(mul2(qc, dy), dy));
@@ -871,14 +873,16 @@ __device__ __forceinline__ void record_walk_scalar(const Rec2D<S>& r, S om, S q,
     }
 }
 
-// In the scalar walk, boxes of at most kHalfWarpArea pixels are walked by half
-// warps, two records at a time, and boxes of at most kQuarterWarpArea by
-// quarter warps, four at a time: a small box fills a narrow step about as well
-// as a 32-lane one, and the group shares one pass of the per-record set-up and
-// reduction. The warp's records are sorted by box size first, so a group's
-// boxes take about the same number of steps.
+// Boxes of at most kHalfWarpArea pixels are walked by half warps, two records
+// at a time, and boxes of at most kQuarterWarpArea by quarter warps, four at a
+// time (kPacked*: the same for the packed walk): a small box fills a narrow
+// step about as well as a 32-lane one, and the group shares one pass of the
+// per-record set-up and reduction. The warp's records are sorted by box size
+// first, so a group's boxes take about the same number of steps.
 constexpr uint32_t kHalfWarpArea = 1024u;
 constexpr uint32_t kQuarterWarpArea = 256u;
+constexpr uint32_t kPackedHalfWarpArea = 1024u;
+constexpr uint32_t kPackedQuarterWarpArea = 256u;
 
 // Writes the slot adjoints of record subgroup grp (0..3) from its pair of
 // reduced sums (see record_adjoints) and adds the uncertainty adjoint.
@@ -927,12 +931,13 @@ __device__ __forceinline__ uint32_t warp_sort_ascending(uint32_t key) {
 
 // Walks the staged records at sorted positions [p, p_end) in groups of
 // 32 / kLanes, one record per kLanes-lane group of the warp (a group without
-// a record walks nothing and stores nothing), with the scalar walk, a
-// group-wide reduction and the record's stores. Lane L of `sorted` holds the
+// a record walks nothing and stores nothing), with the packed walk
+// (kPackedWalk) or the scalar one, a group-wide reduction and the record's
+// stores. Lane L of `sorted` holds the
 // L-th smallest (area << 5 | record lane) of the warp's records, so a step's
 // records have boxes of about one size. base is the warp's first record;
 // var_q is null without the variance chain term.
-template <typename S, bool kBeta, bool kVar, bool kAbs, uint32_t kLanes>
+template <typename S, bool kBeta, bool kVar, bool kAbs, uint32_t kLanes, bool kPackedWalk>
 __device__ __forceinline__ void walk_record_groups(uint32_t sorted, uint32_t p, uint32_t p_end,
                                                    const RecordStage<S>* stage, size_t base, uint32_t N,
                                                    uint32_t width, uint32_t height, const S* v_render,
@@ -950,7 +955,8 @@ __device__ __forceinline__ void walk_record_groups(uint32_t sorted, uint32_t p, 
         const RecordStage<S> st = stage[j];
         const Rec2D<S>& r = st.r;
         const uint32_t barea = active ? st.area : 0u;
-        uint32_t iters = (barea + kLanes - 1u) / kLanes;
+        constexpr uint32_t kPerStep = kPackedWalk ? 2u * kLanes : kLanes;
+        uint32_t iters = (barea + kPerStep - 1u) / kPerStep;
 #pragma unroll
         for (uint32_t offset = kLanes; offset < 32u; offset <<= 1)
             iters = max(iters, __shfl_xor_sync(0xffffffffu, iters, offset));
@@ -964,8 +970,12 @@ __device__ __forceinline__ void walk_record_groups(uint32_t sorted, uint32_t p, 
         const S om = r.o * r.mu;
         S part[8];
         S g_ax = S(0), g_ay = S(0);
-        record_walk_scalar<S, kBeta, kVar, kAbs, kLanes>(r, om, q, vimg, vvar, st.x0, st.y0, st.w, barea, iters,
-                                                         width, part, g_ax, g_ay);
+        if constexpr (kPackedWalk)
+            record_walk_packed<kLanes>(r, om, st.e_min, vimg, st.x0, st.y0, st.w, barea, st.magic, width, iters,
+                                       part);
+        else
+            record_walk_scalar<S, kBeta, kVar, kAbs, kLanes>(r, om, q, vimg, vvar, st.x0, st.y0, st.w, barea,
+                                                             iters, width, part, g_ax, g_ay);
         S lo, hi;
         warp_sum8_pairs<kLanes>(part, lo, hi);
         constexpr uint32_t kSub = kLanes / 4u;  // lanes per reduced pair
@@ -1041,11 +1051,13 @@ __global__ void __launch_bounds__(kRecBwdThreads) raster_record_bwd_kernel(
                 }
             }
         }
-        // Boxes of the scalar walk with at most kQuarterWarpArea pixels go to
-        // quarter-warp groups, up to kHalfWarpArea to half-warp pairs; the rest
-        // are walked one by one by the whole warp. (The plain Gaussian
-        // instantiation, which takes the packed walk, has no groups.)
-        const bool grouped = !kPacked && area != 0u && area <= kHalfWarpArea;
+        // Boxes with at most the quarter-warp area go to quarter-warp groups,
+        // up to the half-warp area to half-warp pairs; the rest are walked one
+        // by one by the whole warp. (A plain Gaussian record that cannot take
+        // the packed walk is not grouped.)
+        const bool grouped =
+            area != 0u && (kPacked ? packed && area <= kPackedHalfWarpArea : area <= kHalfWarpArea);
+        const uint32_t quarter_area = kPacked ? kPackedQuarterWarpArea : kQuarterWarpArea;
         uint32_t pending = __ballot_sync(0xffffffffu, area != 0u && !grouped);
         __syncwarp();  // the previous group's constants have been read
         if (area != 0u) {
@@ -1081,7 +1093,8 @@ __global__ void __launch_bounds__(kRecBwdThreads) raster_record_bwd_kernel(
             bool walked = false;
             if constexpr (kPacked) {
                 if (packed) {
-                    record_walk_packed(r, om, st.e_min, vimg, bx0, by0, bw, barea, st.magic, width, part);
+                    record_walk_packed(r, om, st.e_min, vimg, bx0, by0, bw, barea, st.magic, width,
+                                       (barea + 63u) >> 6, part);
                     walked = true;
                 }
             }
@@ -1115,15 +1128,15 @@ __global__ void __launch_bounds__(kRecBwdThreads) raster_record_bwd_kernel(
         // The small boxes, four or two records per warp step, taken in order of
         // box size: sorted positions [0, n_quad) hold the quarter-warp records,
         // [n_quad, n_group) the half-warp ones, and the other lanes sort last.
-        if constexpr (!kPacked) {
+        {
             const uint32_t n_group = __popc(__ballot_sync(0xffffffffu, grouped));
-            const uint32_t n_quad = __popc(__ballot_sync(0xffffffffu, grouped && area <= kQuarterWarpArea));
+            const uint32_t n_quad = __popc(__ballot_sync(0xffffffffu, grouped && area <= quarter_area));
             if (n_group != 0u) {
                 const uint32_t sorted = warp_sort_ascending(grouped ? (area << 5) | lane : 0xffffffe0u | lane);
-                walk_record_groups<S, kBeta, kVar, kAbs, 8u>(sorted, 0u, n_quad, stage, base, N, width, height,
+                walk_record_groups<S, kBeta, kVar, kAbs, 8u, kPacked>(sorted, 0u, n_quad, stage, base, N, width, height,
                                                              v_render, v_render_var, chain_var ? var_q : nullptr,
                                                              grads, v_abs, v_unc);
-                walk_record_groups<S, kBeta, kVar, kAbs, 16u>(sorted, n_quad, n_group, stage, base, N, width,
+                walk_record_groups<S, kBeta, kVar, kAbs, 16u, kPacked>(sorted, n_quad, n_group, stage, base, N, width,
                                                               height, v_render, v_render_var,
                                                               chain_var ? var_q : nullptr, grads, v_abs, v_unc);
             }
