@@ -933,10 +933,10 @@ __device__ __forceinline__ uint32_t warp_sort_ascending(uint32_t key) {
 // 32 / kLanes, one record per kLanes-lane group of the warp (a group without
 // a record walks nothing and stores nothing), with the packed walk
 // (kPackedWalk) or the scalar one, a group-wide reduction and the record's
-// stores. Lane L of `sorted` holds the
-// L-th smallest (area << 5 | record lane) of the warp's records, so a step's
-// records have boxes of about one size. base is the warp's first record;
-// var_q is null without the variance chain term.
+// stores. Lane L of `sorted` holds the L-th smallest (area << 5 | record lane)
+// of the warp's records, so a step's records have boxes of about one size.
+// base is the warp's first record; var_q is null without the variance chain
+// term.
 template <typename S, bool kBeta, bool kVar, bool kAbs, uint32_t kLanes, bool kPackedWalk>
 __device__ __forceinline__ void walk_record_groups(uint32_t sorted, uint32_t p, uint32_t p_end,
                                                    const RecordStage<S>* stage, size_t base, uint32_t N,
