@@ -17,9 +17,15 @@ and voxel forward and backward passes of a step.
 Arms:
   --impl ours       this package (device-resident inputs for ``value``; the
                     public API with pinned host buffers for ``e2e``)
-  --impl reference  the reference's own CUDA build (oracle/_ref, compiled
-                    unmodified from the reference sources) driven through a
-                    restatement of the reference's explicit.py call sequence
+  --impl reference  the reference's own code: its unmodified Python package
+                    (explicit.py, _validation.py, _beta.py, cuda/_wrapper.py,
+                    staged under oracle/_ref/py) on its own CUDA kernels
+                    (oracle/_ref, compiled unmodified from the reference
+                    sources). This process loads none of this package's native
+                    code: the line lists the shared objects it mapped.
+
+Both arms print a stage table of CUDA-event times around each public call
+(``api_stages_ms_per_step``); this package's arm adds its kernel stages.
 
 Under torchrun each rank runs its own replica of the workload (weak scaling,
 no data-path collective); the timing is the max over ranks.
@@ -44,20 +50,39 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 L2_FLUSH_BYTES = 512 << 20
-FLOPS_PER_EVAL = {
-    # FP32 operations per (primitive, pixel) sample of the Gaussian kernels,
-    # counted from the reference formulas (RasterizeToPixelsFwd.cu:160-177,
-    # RasterizeToPixelsBwd.cu:417-468), an FMA counting as two:
-    # forward: offsets 2, quadratic form 8, exp argument 1 (+1 MUFU), alpha 1,
-    # two threshold compares, accumulate 1 -> 16;
-    # backward: forward part 14 + v_sigma 1 + mean adjoint 8 + 2 accumulates
-    # + conic adjoints 11 + density / mu adjoints 6 -> 44.
-    "raster_render": 16, "raster_render_bwd": 44,
+# FP32 operations per algorithmic sample in the reference's source form of each per-sample body:
+# every add, subtract, multiply and compare counts one (no FMA contraction assumed); exp counts its
+# argument multiply here and one MUFU ex2 besides.
+SOURCE_FORM_OPS = {
+    # RasterizeToPixelsFwd.cu:160-177: offsets 2, sigma 9, exp argument 1, alpha o mu vis 2, two
+    # threshold compares 2, accumulate 1.
+    "raster_render": 17,
+    # RasterizeToPixelsBwd.cu:429-463: the forward part without its accumulate 16, v_sigma 1, mean
+    # adjoints 8 and their accumulates 2, conic adjoints 11, density and mu adjoints 6.
+    "raster_render_bwd": 44,
+    # VoxelizeToVoxelsFwd.cu:180-215: offsets 3, sigma 18, exp argument 1, alpha 1, compares 2,
+    # accumulate 1.
+    "voxel_render": 26,
+    # VoxelizeToVoxelsBwd.cu:398-432: the forward part without its accumulate 25, v_sigma 2, o vis 1,
+    # density adjoint 2, conic adjoints 21, mean adjoints 22.
+    "voxel_render_bwd": 73,
+}
+# The same bodies with FMA contraction (a multiply feeding an add counts once): 11 per raster forward and
+# 30 per raster backward sample; in 3D the quadratic form has six terms, giving 21 per forward (offsets 3,
+# sigma 13, exp 1, alpha 1, compares 2, accumulate 1) and 48 per backward sample (the forward part 20,
+# v_sigma 1, density adjoint 1, conic adjoints 13, mean adjoints 13). The headline roofline fraction uses
+# these, the lower of the two counts.
+CONTRACTED_OPS = {"raster_render": 11, "raster_render_bwd": 30, "voxel_render": 21, "voxel_render_bwd": 48}
+ACCUMULATE_KERNELS = {
+    "raster_render": "raster_fwd_pair_kernel (tile forward, two pixels per lane)",
+    "raster_render_bwd": "raster_record_bwd_kernel (record-parallel raster VJP)",
+    "voxel_render": "voxel_fwd_kernel (tile forward, four voxels per thread)",
+    "voxel_render_bwd": "voxel_bwd_kernel (row-wise voxel VJP)",
 }
 # FP32 operations per sample of the Beta raster VJP with the variance branch in the reference's form
-# (RasterizeToPixelsBwd.cu:817-1046), multiplies and adds counted separately: offsets 2, d^2 9, h 1,
-# pow argument 1, alpha 1, variance terms 7, w with h^(beta - 1) 6, w dx and w dy 2, their moments 8,
-# g vis 2, g alpha ln h 4.
+# (RasterizeToPixelsBwd.cu:817-1046), counted by the same rule: offsets 2, d^2 9, h 1, pow argument 1,
+# alpha 1, variance terms 7, w with h^(beta - 1) 6, w dx and w dy 2, their moments 8, g vis 2,
+# g alpha ln h 4.
 BETA_VAR_VJP_FLOPS_PER_EVAL = 43
 # Metric and workload description of each single-scene workload.
 WORKLOAD_TEXT = {
@@ -73,9 +98,10 @@ WORKLOAD_TEXT = {
              "beta-uncertainty: N=500000, beta ~ U[0.5, 4], q ~ U[0, 0.1], C=128 views R=3, 768x768 f=900, "
              "volume 384^3, adjoints v ~ N(0, 1) and v_var ~ N(0, 0.1), variance branch attached"),
 }
-# DRAM bytes (read + write) of one record-parallel raster VJP launch at the CT
-# workload, from ncu (dram__bytes_read.sum + dram__bytes_write.sum, one pass).
-RASTER_VJP_TRAFFIC_BYTES = 535.5e6 + 366.9e6
+# DRAM bytes (read + write) of one record-parallel raster VJP launch, from ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum, one pass, one full-size launch of the
+# shipped kernel): 536.03 MB read, 369.60 MB written at the CT workload.
+RASTER_VJP_TRAFFIC_BYTES = {"ct": 536.03e6 + 369.60e6}
 
 
 # --------------------------------------------------------------------------- utilities
@@ -197,6 +223,64 @@ def flush_l2(buf: torch.Tensor):
     buf.add_(1.0)
 
 
+class ApiStages:
+    """CUDA-event times around each public call of a step, summed per call name.
+
+    Recording only while ``active``; the events go on the current stream, so
+    host time a call spends before its kernels (validation, synchronising reads
+    of counts, allocation) shows up as device idle time inside its stage.
+    """
+
+    def __init__(self):
+        self.active = False
+        self.records: list = []
+
+    def __call__(self, name: str):
+        return _ApiStage(self, name)
+
+    def totals_ms(self) -> dict:
+        out: dict = {}
+        for name, start, end in self.records:
+            out[name] = out.get(name, 0.0) + start.elapsed_time(end)
+        return out
+
+
+class _ApiStage:
+    def __init__(self, owner: ApiStages, name: str):
+        self.owner, self.name, self.start = owner, name, None
+
+    def __enter__(self):
+        if self.owner.active:
+            self.start = torch.cuda.Event(enable_timing=True)
+            self.start.record()
+        return self
+
+    def __exit__(self, *exc):
+        if self.start is not None:
+            end = torch.cuda.Event(enable_timing=True)
+            end.record()
+            self.owner.records.append((self.name, self.start, end))
+        return False
+
+
+def mapped_native_libs() -> list:
+    """Shared objects under this repository that this process has mapped (from /proc/self/maps)."""
+    found = set()
+    try:
+        with open("/proc/self/maps") as maps:
+            for line in maps:
+                path = line.split()[-1] if len(line.split()) >= 6 else ""
+                if path.endswith(".so") or ".so." in path or ".cpython-" in path:
+                    p = Path(path)
+                    try:
+                        found.add(str(p.relative_to(ROOT)))
+                    except ValueError:
+                        continue
+    except OSError:
+        return []
+    return sorted(found)
+
+
 def count_evals_2d(offsets: torch.Tensor, n_isects: int, height: int, width: int, tile: int) -> int:
     """Sum over intersections of the in-bounds pixels of their tile."""
     c, ty, tx = offsets.shape
@@ -233,21 +317,29 @@ class OursStep:
         self.scene, self.target, self.lam = scene, target, lambda_tv
         self.ones = torch.ones(1, device=scene.means.device)
         self.last = {}
+        self.stages = ApiStages()
 
     def __call__(self, means, quats, scales, densities):
-        sc = self.scene
-        image, ctx = self.r2s.rasterize_fwd(means, quats, scales, densities, sc.viewmats, sc.Ks, sc.image_size)
+        sc, st = self.scene, self.stages
+        with st("rasterize_fwd"):
+            image, ctx = self.r2s.rasterize_fwd(means, quats, scales, densities, sc.viewmats, sc.Ks, sc.image_size)
         self.last["raster_state"] = ctx.buffers["state"]
-        v_image = 2 * (image - self.target) / image.numel()
-        g = self.r2s.rasterize_bwd(ctx, v_image)
-        volume, vctx = self.r2s.voxelize_fwd(means, quats, scales, densities, sc.volume_shape,
-                                             volume_extent=sc.volume_extent)
+        with st("image_loss_grad"):
+            v_image = 2 * (image - self.target) / image.numel()
+        with st("rasterize_bwd"):
+            g = self.r2s.rasterize_bwd(ctx, v_image)
+        with st("voxelize_fwd"):
+            volume, vctx = self.r2s.voxelize_fwd(means, quats, scales, densities, sc.volume_shape,
+                                                 volume_extent=sc.volume_extent)
         self.last["voxel_state"] = vctx.buffers["state"]
-        vol4 = volume.unsqueeze(0)
-        loss, _, _ = self.low.volume_loss_fwd(vol4, self.lam)
-        g_vol = self.low.volume_loss_bwd(vol4, self.ones, self.lam)[0]
-        gv = self.r2s.voxelize_bwd(vctx, g_vol)
-        return loss, (g.means + gv.means, g.quats + gv.quats, g.scales + gv.scales, g.densities + gv.densities)
+        with st("volume_loss_fwd_bwd"):
+            # One pass: the TV term's upstream gradient (one) is known before its forward.
+            loss, _, g_vol = self.low.volume_loss_fwd_bwd(volume.unsqueeze(0), self.ones, self.lam)
+        with st("voxelize_bwd"):
+            gv = self.r2s.voxelize_bwd(vctx, g_vol[0])
+        with st("gradient_sum"):
+            grads = (g.means + gv.means, g.quats + gv.quats, g.scales + gv.scales, g.densities + gv.densities)
+        return loss, grads
 
     def eval_counts(self):
         rs, vs = self.last["raster_state"], self.last["voxel_state"]
@@ -258,38 +350,51 @@ class OursStep:
 
 
 class ReferenceStep:
-    """The same fit step on the reference's own CUDA kernels (oracle/_ref)."""
+    """The same fit step through the reference's own package (explicit.py) on its own kernels."""
 
     def __init__(self, scene, target, lambda_tv=0.05):
         from oracle import ref_ops
 
-        self.ref_ops = ref_ops
-        self.ref = ref_ops.load()
+        self.ref = ref_ops.load_package()
         self.scene, self.target, self.lam = scene, target, lambda_tv
         self.ones = torch.ones(1, device=scene.means.device)
         self.last = {}
+        self.stages = ApiStages()
+
+    def _keep(self, key, ctx):
+        # The reference's backward clears the context's buffers; keep what the eval count reads.
+        self.last[key] = {"offsets": ctx.buffers["offsets"], "n_isects": ctx.buffers["isect_ids"].numel()}
 
     def __call__(self, means, quats, scales, densities):
-        sc, ro = self.scene, self.ref_ops
-        image, saved = ro.explicit_rasterize_fwd(means, quats, scales, densities, sc.viewmats, sc.Ks, sc.image_size)
-        self.last["raster"] = saved
-        v_image = 2 * (image - self.target) / image.numel()
-        g = ro.explicit_rasterize_bwd(saved, means, quats, scales, None, None, v_image)
-        volume, vsaved = ro.explicit_voxelize_fwd(means, quats, scales, densities, sc.volume_shape,
-                                                  volume_extent=sc.volume_extent)
-        self.last["voxel"] = vsaved
+        sc, r, st = self.scene, self.ref, self.stages
+        with st("rasterize_fwd"):
+            image, ctx = r.rasterize_fwd(means, quats, scales, densities, sc.viewmats, sc.Ks, sc.image_size)
+        self._keep("raster", ctx)
+        with st("image_loss_grad"):
+            v_image = 2 * (image - self.target) / image.numel()
+        with st("rasterize_bwd"):
+            g = r.rasterize_bwd(ctx, v_image)
+        with st("voxelize_fwd"):
+            volume, vctx = r.voxelize_fwd(means, quats, scales, densities, sc.volume_shape,
+                                          volume_extent=sc.volume_extent)
+        self._keep("voxel", vctx)
         vol4 = volume.unsqueeze(0)
-        loss, _, _ = self.ref.volume_loss_fwd(vol4, self.lam)
-        g_vol = self.ref.volume_loss_bwd(vol4, self.ones, self.lam)[0]
-        gv = ro.explicit_voxelize_bwd(vsaved, means, quats, scales, densities, None, None, g_vol)
-        return loss, tuple(a + b for a, b in zip(g[:4], gv[:4]))
+        with st("volume_loss_fwd_bwd"):
+            loss, _, _ = r.cuda.volume_loss_fwd(vol4, self.lam)
+            g_vol = r.cuda.volume_loss_bwd(vol4, self.ones, self.lam)[0]
+        with st("voxelize_bwd"):
+            gv = r.voxelize_bwd(vctx, g_vol)
+        with st("gradient_sum"):
+            grads = (g.means + gv.means, g.quats + gv.quats, g.scales + gv.scales, g.densities + gv.densities)
+        return loss, grads
 
     def eval_counts(self):
         r, v = self.last["raster"], self.last["voxel"]
         h, w = self.scene.image_size
-        raster = count_evals_2d(r["offsets"], r["isect_ids"].numel(), h, w, 16)
-        voxel = count_evals_3d(v["offsets"], v["isect_ids"].numel(), v["shape"], 8)
-        return raster, voxel, r["isect_ids"].numel(), v["isect_ids"].numel()
+        d, hh, ww = self.scene.volume_shape
+        raster = count_evals_2d(r["offsets"], r["n_isects"], h, w, 16)
+        voxel = count_evals_3d(v["offsets"], v["n_isects"], (d, hh, ww), 8)
+        return raster, voxel, r["n_isects"], v["n_isects"]
 
 
 class _BetaAdjoints:
@@ -315,46 +420,61 @@ class OursBetaStep(_BetaAdjoints):
 
         super().__init__(scene)
         self.r2s, self.scene, self.last = r2s, scene, {}
+        self.stages = ApiStages()
 
     def __call__(self, means, quats, scales, densities, beta, uncertainty):
-        sc = self.scene
-        _, ctx = self.r2s.rasterize_fwd(means, quats, scales, densities, sc.viewmats, sc.Ks, sc.image_size, beta=beta,
-                                        uncertainty=uncertainty)
+        sc, st = self.scene, self.stages
+        with st("rasterize_fwd"):
+            _, ctx = self.r2s.rasterize_fwd(means, quats, scales, densities, sc.viewmats, sc.Ks, sc.image_size,
+                                            beta=beta, uncertainty=uncertainty)
         self.last["raster_state"] = ctx.buffers["state"]
-        g = self.r2s.rasterize_bwd(ctx, self.v_image, self.v_image_var)
-        _, vctx = self.r2s.voxelize_fwd(means, quats, scales, densities, sc.volume_shape,
-                                        volume_extent=sc.volume_extent, beta=beta, uncertainty=uncertainty)
+        with st("rasterize_bwd"):
+            g = self.r2s.rasterize_bwd(ctx, self.v_image, self.v_image_var)
+        with st("voxelize_fwd"):
+            _, vctx = self.r2s.voxelize_fwd(means, quats, scales, densities, sc.volume_shape,
+                                            volume_extent=sc.volume_extent, beta=beta, uncertainty=uncertainty)
         self.last["voxel_state"] = vctx.buffers["state"]
-        gv = self.r2s.voxelize_bwd(vctx, self.v_volume, self.v_volume_var)
-        grads = tuple(a + b for a, b in zip((g.means, g.quats, g.scales, g.densities, g.beta, g.uncertainty),
-                                            (gv.means, gv.quats, gv.scales, gv.densities, gv.beta, gv.uncertainty)))
+        with st("voxelize_bwd"):
+            gv = self.r2s.voxelize_bwd(vctx, self.v_volume, self.v_volume_var)
+        with st("gradient_sum"):
+            grads = tuple(a + b for a, b in zip(
+                (g.means, g.quats, g.scales, g.densities, g.beta, g.uncertainty),
+                (gv.means, gv.quats, gv.scales, gv.densities, gv.beta, gv.uncertainty)))
         return grads[3].sum(), grads
 
     eval_counts = OursStep.eval_counts
 
 
 class ReferenceBetaStep(_BetaAdjoints):
-    """The same Beta step on the reference's own CUDA kernels (oracle/_ref)."""
+    """The same Beta step through the reference's own package on its own kernels."""
 
     def __init__(self, scene, target=None):
         from oracle import ref_ops
 
         super().__init__(scene)
-        self.ref_ops, self.scene, self.last = ref_ops, scene, {}
+        self.ref, self.scene, self.last = ref_ops.load_package(), scene, {}
+        self.stages = ApiStages()
+
+    _keep = ReferenceStep._keep
 
     def __call__(self, means, quats, scales, densities, beta, uncertainty):
-        sc, ro = self.scene, self.ref_ops
-        _, saved = ro.explicit_rasterize_fwd(means, quats, scales, densities, sc.viewmats, sc.Ks, sc.image_size,
-                                             beta=beta, uncertainty=uncertainty)
-        self.last["raster"] = saved
-        g = ro.explicit_rasterize_bwd(saved, means, quats, scales, beta, uncertainty, self.v_image,
-                                      self.v_image_var)
-        _, vsaved = ro.explicit_voxelize_fwd(means, quats, scales, densities, sc.volume_shape,
-                                             volume_extent=sc.volume_extent, beta=beta, uncertainty=uncertainty)
-        self.last["voxel"] = vsaved
-        gv = ro.explicit_voxelize_bwd(vsaved, means, quats, scales, densities, beta, uncertainty, self.v_volume,
-                                      self.v_volume_var)
-        grads = tuple(a + b for a, b in zip(g, gv) if a is not None and b is not None)
+        sc, r, st = self.scene, self.ref, self.stages
+        with st("rasterize_fwd"):
+            _, ctx = r.rasterize_fwd(means, quats, scales, densities, sc.viewmats, sc.Ks, sc.image_size,
+                                     beta=beta, uncertainty=uncertainty)
+        self._keep("raster", ctx)
+        with st("rasterize_bwd"):
+            g = r.rasterize_bwd(ctx, self.v_image, self.v_image_var)
+        with st("voxelize_fwd"):
+            _, vctx = r.voxelize_fwd(means, quats, scales, densities, sc.volume_shape,
+                                     volume_extent=sc.volume_extent, beta=beta, uncertainty=uncertainty)
+        self._keep("voxel", vctx)
+        with st("voxelize_bwd"):
+            gv = r.voxelize_bwd(vctx, self.v_volume, self.v_volume_var)
+        with st("gradient_sum"):
+            grads = tuple(a + b for a, b in zip(
+                (g.means, g.quats, g.scales, g.densities, g.beta, g.uncertainty),
+                (gv.means, gv.quats, gv.scales, gv.densities, gv.beta, gv.uncertainty)))
         return grads[3].sum(), grads
 
     eval_counts = ReferenceStep.eval_counts
@@ -365,7 +485,12 @@ def step_inputs(scene) -> tuple:
     return tuple(t for t in (*scene.primitives, scene.beta, scene.uncertainty) if t is not None)
 
 
-def build_workload(device, workload: str):
+def build_workload(device, workload: str, impl: str = "ours"):
+    """The workload's scene on ``device`` and, for the fit-step workloads, its target images.
+
+    The target is rendered by the arm's own implementation, so the reference
+    arm runs no code of this package's library.
+    """
     from r2splat_b200 import scenes
 
     if workload == "ct":
@@ -388,9 +513,13 @@ def build_workload(device, workload: str):
     scene = scene.to(device)
     target_scene = scene.to(device)
     target_scene.means = scenes.perturbed_means(scene.means)
-    import r2splat_b200 as r2s
+    if impl == "reference":
+        from oracle import ref_ops
 
-    target, _ = r2s.rasterize_fwd(*target_scene.primitives, target_scene.viewmats, target_scene.Ks,
+        api = ref_ops.load_package()
+    else:
+        import r2splat_b200 as api
+    target, _ = api.rasterize_fwd(*target_scene.primitives, target_scene.viewmats, target_scene.Ks,
                                   target_scene.image_size)
     return scene, target
 
@@ -427,70 +556,122 @@ def sfu_peak_gops(device) -> float:
     return _probe_rate("r2s_sfu_peak_probe", device, 128.0, 512) / 1e9
 
 
-def cpu_baseline(budget_s: float = 15.0) -> dict:
-    """fp64 dense oracle on the host cores: raster fwd+bwd evaluations per second on a bounded sample."""
-    from oracle import dense
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as info:
+            for line in info:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def _config1_fit_step_cpu(sc, v_image, lam):
+    """One float64 fit step of the small configuration with the dense oracle: raster fwd + bwd against
+    ``v_image``, voxel fwd, TV fwd/bwd, voxel bwd with the TV gradient as its adjoint."""
+    from oracle import dense, losses
+
+    prims = [t.clone().requires_grad_(True) for t in sc.primitives]
+    img = dense.rasterize_dense(*prims, sc.viewmats, sc.Ks, sc.image_size, eps=1e-8, chunk=1000)
+    raster_grads = torch.autograd.grad((img * v_image).sum(), prims)
+    prims = [t.detach().clone().requires_grad_(True) for t in sc.primitives]
+    vol = dense.voxelize_dense(*prims, sc.volume_shape, volume_extent=sc.volume_extent, eps=1e-8, chunk=1000)
+    vol_np = vol.detach().unsqueeze(0).numpy()
+    losses.tv_forward(vol_np, lam)
+    g_vol = torch.from_numpy(losses.tv_backward(vol_np, 1.0, lam)[0])
+    voxel_grads = torch.autograd.grad((vol * g_vol).sum(), prims)
+    return [a + b for a, b in zip(raster_grads, voxel_grads)]
+
+
+def cpu_baseline(device, budget_s: float = 15.0) -> dict:
+    """The float64 dense oracle on the host cores, run on the small configuration in full.
+
+    Small configuration: N=2,000, C=4 views at 64x64, volume 32^3, v_image ~
+    N(0, 1) (seed 1), TV lambda 0.05. ``value`` is that step's algorithmic
+    evaluations (the tile samples the reference's kernels evaluate, counted on
+    the GPU path) per second of host time; the oracle itself evaluates every
+    (primitive, sample) pair, and ``dense_evals_per_s`` counts those.
+    """
+    import r2splat_b200 as r2s
     from r2splat_b200 import scenes
 
     threads = os.cpu_count() or 1
     torch.set_num_threads(threads)
-    sc = scenes.ct_scene(dtype=torch.float64)
-    view = slice(0, 1)
-    n = 64
-    prims = [t[:n].clone().requires_grad_(True) for t in sc.primitives]
-    evals = 0
+    small = scenes.small_scene()
+    # Algorithmic evaluations of the small step, from the GPU path's own tile lists.
+    dev = small.to(device)
+    _, ctx = r2s.rasterize_fwd(*dev.primitives, dev.viewmats, dev.Ks, dev.image_size)
+    _, vctx = r2s.voxelize_fwd(*dev.primitives, dev.volume_shape, volume_extent=dev.volume_extent)
+    rs, vs = ctx.buffers["state"], vctx.buffers["state"]
+    raster = count_evals_2d(rs.offsets, rs.n_isects, *dev.image_size, rs.tile_size)
+    voxel = count_evals_3d(vs.offsets, vs.n_isects, vs.shape, vs.tile_size)
+    algorithmic = 2 * raster + 2 * voxel
+    sc = scenes.small_scene(dtype=torch.float64)
+    c, (h, w) = sc.viewmats.shape[0], sc.image_size
+    v_image = torch.randn((c, h, w), generator=torch.Generator().manual_seed(1), dtype=torch.float64)
+    n = sc.means.shape[0]
+    dense_per_step = 2 * n * (c * h * w + math.prod(sc.volume_shape))
+    steps = 0
     t0 = time.perf_counter()
-    reps = 0
     while True:
-        img = dense.rasterize_dense(*prims, sc.viewmats[view], sc.Ks[view], sc.image_size, eps=1e-8, chunk=16)
-        grads = torch.autograd.grad(img.sum(), prims)
-        evals += 2 * n * sc.image_size[0] * sc.image_size[1]
-        reps += 1
+        _config1_fit_step_cpu(sc, v_image, 0.05)
+        steps += 1
         if time.perf_counter() - t0 > budget_s:
             break
     elapsed = time.perf_counter() - t0
-    del grads
-    rate = evals / elapsed
-    # The dense oracle evaluates every (primitive, pixel) and (primitive, voxel) pair: a whole CT fit step
-    # (200k primitives, 64 views x 512^2, 256^3 volume, forward + backward) is this many dense evaluations.
-    full = sc.means.shape[0]
-    dense_per_step = 2 * full * (sc.viewmats.shape[0] * sc.image_size[0] * sc.image_size[1] + 256 ** 3)
-    return {"value": rate, "unit": "evals/s", "cores": threads, "kind": "port",
-            "sample": f"float64 dense oracle (oracle/dense.py): {n} Gaussians x 1 view x 512x512, raster fwd+bwd "
-                      f"(autograd), {reps} repetitions in {elapsed:.1f}s; dense evals counted",
-            "extrapolated_ct_fit_step_s": dense_per_step / rate,
-            "extrapolation": "not measured: dense evaluations of one full CT fit step divided by the measured rate"}
+    return {"value": algorithmic * steps / elapsed, "unit": "evals/s", "cores": threads, "kind": "port",
+            "cpu_model": cpu_model(), "torch_threads": torch.get_num_threads(),
+            "sample": f"small configuration in full (N=2000, 4 views at 64x64, volume 32^3, TV): {steps} float64 "
+                      f"fit steps of the dense oracle (oracle/dense.py, autograd VJPs) in {elapsed:.1f} s",
+            "seconds_per_fit_step": elapsed / steps,
+            "algorithmic_evals_per_step": algorithmic,
+            "dense_evals_per_s": dense_per_step * steps / elapsed}
 
 
-def timed_run(step, scene, steps, warmup, device, flush_buf, clocks=None):
-    """Device-resident inputs; per-step CUDA events with an L2 flush between steps."""
-    from r2splat_b200 import _fused
+def timed_run(step, scene, steps, warmup, device, flush_buf, clocks=None, ours=True):
+    """Device-resident inputs; per-step CUDA events with an L2 flush between steps.
 
+    Returns (total ms, kernel-stage ms, public-call-stage ms, launches). The
+    kernel stages and this library's launch counter exist only in this
+    package's arm (``ours``); the reference arm never touches the library.
+    """
     prims = step_inputs(scene)
     for _ in range(warmup):
         step(*prims)
     torch.cuda.synchronize()
     if clocks is not None:
         clocks.mark(True)
-    timer = _fused.StageTimer()
+    timer = None
+    if ours:
+        from r2splat_b200 import _fused
+
+        timer = _fused.StageTimer()
     total_ms = 0.0
     launches = 0
+    per_step: list = []
+    step.stages.active = True
     for _ in range(steps):
         flush_l2(flush_buf)
         start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        _fused.StageTimer.active = timer
-        before = library_launches()
+        if ours:
+            _fused.StageTimer.active = timer
+            before = library_launches()
         start.record()
         step(*prims)
         end.record()
-        launches += library_launches() - before
-        _fused.StageTimer.active = None
+        if ours:
+            launches += library_launches() - before
+            _fused.StageTimer.active = None
         end.synchronize()
-        total_ms += start.elapsed_time(end)
+        per_step.append(start.elapsed_time(end))
+        total_ms += per_step[-1]
+    step.stages.active = False
+    timed_run.per_step_ms = per_step
     torch.cuda.synchronize()
     if clocks is not None:
         clocks.mark(False)
-    return total_ms, timer.totals_ms(), launches
+    return total_ms, (timer.totals_ms() if timer else {}), step.stages.totals_ms(), launches
 
 
 def library_launches() -> int:
@@ -524,13 +705,17 @@ def e2e_run(step, scene, steps, warmup, device):
     return start.elapsed_time(end), h2d, d2h
 
 
-def count_launches(step, scene, prefix: str) -> int:
+def count_launches(step, scene) -> dict:
+    """Kernels one step launches, from the torch profiler: all of them, and those outside torch's own."""
     from torch.profiler import ProfilerActivity, profile
 
     with profile(activities=[ProfilerActivity.CUDA]) as prof:
         step(*step_inputs(scene))
         torch.cuda.synchronize()
-    return sum(e.count for e in prof.key_averages() if prefix in e.key)
+    kernels = [e for e in prof.events() if e.device_type == torch.autograd.DeviceType.CUDA]
+    own = [e for e in kernels if not any(tag in e.name for tag in ("at::", "at_cuda_detail", "Memset", "Memcpy",
+                                                                    "cub::", "void at::"))]
+    return {"all": len(kernels), "operator_kernels": len(own)}
 
 
 def _mixed_scene_specs(count: int, small: bool):
@@ -552,7 +737,7 @@ def _mixed_scene_specs(count: int, small: bool):
     return specs
 
 
-def mixed_workload(args, device) -> dict:
+def mixed_workload(args, device, autotune: bool = True) -> dict:
     """Aggregate fit-steps/s of the batched (one CUDA graph) or served form vs the plain drop-in run
     scene by scene (explicit API + the same update), on many uneven reconstructions."""
     from r2splat_b200 import batched, serve
@@ -567,8 +752,11 @@ def mixed_workload(args, device) -> dict:
             return batched.make_synthetic_scene(spec["n"], spec["cameras"], spec["side"], spec["volume"],
                                                 beta=spec["beta"], seed=spec["seed"], tile=tile,
                                                 stage_batch=stage_batch, device=device)
-        tile, stage = tuner.choose(make, spec["n"], spec["cameras"], (spec["side"], spec["side"]),
-                                   "beta" if spec["beta"] else "gaussian")
+        if autotune:
+            tile, stage = tuner.choose(make, spec["n"], spec["cameras"], (spec["side"], spec["side"]),
+                                       "beta" if spec["beta"] else "gaussian")
+        else:
+            tile, stage = 16, 256
         spec["tile"] = tile
         makers.append(lambda make=make, tile=tile, stage=stage: make(tile, stage))
     server = None
@@ -611,9 +799,29 @@ def mixed_workload(args, device) -> dict:
         torch.cuda.synchronize(device)
         fit.step()  # one checked step: overflow handling stays exercised
         ms = start_ev.elapsed_time(end_ev) / args.steps
+        recaptures = fit.recaptures
+        del fit
+        # Device work of each scene's step alone (its own one-scene graph, CUDA events): batching
+        # removes host time and overlaps scenes, but cannot remove this work.
+        device_ms = []
+        for scene in scenes:
+            one = batched.BatchedFit([scene])
+            one.capture(warm=False)
+            one.step(check=False)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(2):
+                one.step(check=False)
+            b.record()
+            torch.cuda.synchronize(device)
+            device_ms.append(a.elapsed_time(b) / 2)
+            del one
         result.update({"value": len(scenes) * 1e3 / ms, "ms_per_batched_step": ms, "steps": args.steps,
-                       "warmup": args.warmup, "recaptures": fit.recaptures,
-                       "vs_plain": len(scenes) * 1e3 / ms / result["plain_fit_steps_per_s"]})
+                       "warmup": args.warmup, "recaptures": recaptures,
+                       "vs_plain": len(scenes) * 1e3 / ms / result["plain_fit_steps_per_s"],
+                       "plain_ms_per_round": plain_s * 1e3,
+                       "sum_device_ms_per_round": sum(device_ms),
+                       "host_free_bound_vs_plain": plain_s * 1e3 / sum(device_ms)})
         return result
     requests = serve.poisson_requests(list(server.recons), args.rate, args.requests, seed=1)
     served = server.serve(requests)
@@ -624,13 +832,151 @@ def mixed_workload(args, device) -> dict:
     return result
 
 
+def _estimated_full_bytes(spec: dict) -> float:
+    """Rough device footprint of a fully allocated FitScene (step buffers, lists with slack, slots)."""
+    n, c, side, vol = spec["n"], spec["cameras"], spec["side"], spec["volume"]
+    sigma_vox = 0.01 * vol
+    m2 = 4.0 * c * n
+    m3 = n * (6 * sigma_vox / 8 + 1) ** 3
+    return (c * n * 84 + 3 * 4 * c * side * side + n * 160 + 8 * vol ** 3 + 1.3 * (12 * m2 + 60 * m3))
+
+
+def serving_at_scale(args, device) -> dict:
+    """The serving loop on the large mix: 200 reconstructions drawn from the 32-scene distribution (N
+    log-uniform in [10k, 400k], 16-128 views, 256-1024^2, 128-384^3, Gaussian or Beta), three of them
+    with N = 2,000,000 and a 1024^3 volume; a 150 GB HBM budget; reconstructions that do not fit graphed
+    run lean with recompute-in-backward. Measures the saturated throughput first, then serves Poisson
+    arrivals at 80 % of it and at the requested rate, against the plain drop-in run serially on the same
+    requests."""
+    from r2splat_b200 import batched, serve
+
+    specs = _mixed_scene_specs(args.scenes, small=False)
+    for spec in specs[:3]:
+        spec.update(n=2_000_000, volume=1024)
+    server = serve.FitServer(budget_bytes=150 << 30, slots=8, device=device, lean_recompute=True)
+    built_lean = 0
+    t0 = time.perf_counter()
+    for i, spec in enumerate(specs):
+        lean = _estimated_full_bytes(spec) > (16 << 30)
+        built_lean += int(lean)
+
+        def make(spec=spec, lean=lean):
+            return batched.make_synthetic_scene(spec["n"], spec["cameras"], spec["side"], spec["volume"],
+                                                beta=spec["beta"], seed=spec["seed"], device=device, lean=lean)
+        server.admit(i, make)
+    admit_s = time.perf_counter() - t0
+    keys = sorted(server.recons)
+    # Saturated: every request arrives at once.
+    burst = [(0.0, key) for _, key in serve.poisson_requests(keys, 1.0, args.requests, seed=4)]
+    saturated = server.serve(burst)
+    rate_ok = 0.8 * saturated.steps_per_s
+    runs = {}
+    for label, rate in (("sustained", rate_ok), ("offered", args.rate)):
+        requests = serve.poisson_requests(keys, rate, args.requests, seed=5)
+        runs[label] = {"offered_rate_per_s": rate, "served": server.serve(requests).summary()}
+    serial_requests = serve.poisson_requests(keys, rate_ok, args.requests, seed=5)
+    serial = serve.serve_serially({k: server.recons[k].scene for k in keys}, serial_requests)
+    return {"metric": "served fit-steps/s and p50/p99 step latency at scale", "unit": "fit-steps/s",
+            "value": runs["sustained"]["served"]["fit_steps_per_s"], "higher_is_better": True, "n_gpus": 1,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{len(specs)} reconstructions (3 with N=2M, 1024^3), 150 GB budget",
+                       "admitted": len(keys), "waiting": len(server.waiting), "built_lean": built_lean,
+                       "graphed": sum(server.recons[k].graphed for k in keys), "admission_s": admit_s,
+                       "budget_used_gb": server.used / 2**30},
+            "saturated": saturated.summary(), **runs,
+            "serial_at_sustained_rate": serial.summary(),
+            "vs_serial": runs["sustained"]["served"]["fit_steps_per_s"] / serial.steps_per_s
+            if serial.steps_per_s else None}
+
+
+def bounded_mix(device, kind: str) -> dict:
+    """A bounded run of the batched or served form for the default bench line.
+
+    batched: the first 8 reconstructions of the 32-scene mix (N log-uniform in [10k, 400k], 16-128
+    views, 256-1024^2, 128-384^3, Gaussian or Beta), raster tile 16 (``--workload batched`` runs all
+    32 with the autotuner); served: 16 small reconstructions, 200 Poisson requests at 400/s.
+    """
+    ns = argparse.Namespace(workload=kind, scenes=8 if kind == "batched" else 16, steps=4, warmup=3,
+                            requests=200, rate=400.0)
+    out = mixed_workload(ns, device, autotune=False)
+    out.pop("config", None)
+    out["scenes"] = ns.scenes
+    return out
+
+
+def accumulate_rooflines(workload, stages, steps, raster_evals, voxel_evals, fp32_peak) -> dict:
+    """Per accumulate kernel: its mean CUDA-event time per launch, and the FP32 rate its algorithmic work
+    (the reference's tile samples times the per-sample operation count) represents, against the
+    FP32 issue peak measured in the same run. The kernels evaluate only the samples inside each record's
+    conservative box, so this is a work-equivalent rate."""
+    out = {}
+    beta = workload in ("beta", "beta8")
+    for stage, kernel in ACCUMULATE_KERNELS.items():
+        if stage not in stages or not stages[stage]:
+            continue
+        ms = stages[stage] / steps
+        evals = raster_evals if stage.startswith("raster") else voxel_evals
+        entry = {"kernel": kernel, "ms": ms, "samples": evals}
+        if beta:
+            if stage == "raster_render_bwd":
+                entry["ops_per_sample"] = BETA_VAR_VJP_FLOPS_PER_EVAL
+                entry["achieved_tflops"] = BETA_VAR_VJP_FLOPS_PER_EVAL * evals / (ms * 1e-3) / 1e12
+                entry["frac"] = entry["achieved_tflops"] / fp32_peak
+        else:
+            ops = SOURCE_FORM_OPS[stage]
+            entry["ops_per_sample_source_form"] = ops
+            entry["achieved_tflops_source_form"] = ops * evals / (ms * 1e-3) / 1e12
+            entry["frac_source_form"] = entry["achieved_tflops_source_form"] / fp32_peak
+            if stage in CONTRACTED_OPS:
+                entry["ops_per_sample_contracted"] = CONTRACTED_OPS[stage]
+                entry["achieved_tflops_contracted"] = CONTRACTED_OPS[stage] * evals / (ms * 1e-3) / 1e12
+                entry["frac_contracted"] = entry["achieved_tflops_contracted"] / fp32_peak
+        out[stage] = entry
+    return out
+
+
+def dominant_roofline(workload, rooflines, fp32_peak, sfu_peak, hbm_peak) -> dict:
+    """The roofline object of the step's dominant kernel, the record-parallel raster VJP."""
+    entry = rooflines.get("raster_render_bwd", {})
+    beta = workload in ("beta", "beta8")
+    if beta:
+        achieved, ops, frac = entry.get("achieved_tflops"), BETA_VAR_VJP_FLOPS_PER_EVAL, entry.get("frac")
+        work = (f"algorithmic: {ops} FP32 ops (and 5 MUFU) x the reference's tile samples of one raster VJP pass "
+                "(Beta with the variance branch); the kernel evaluates only the samples inside each record's box")
+    else:
+        achieved, frac = entry.get("achieved_tflops_contracted"), entry.get("frac_contracted")
+        ops = CONTRACTED_OPS["raster_render_bwd"]
+        work = (f"algorithmic: {ops} FP32 ops (FMA contracted; {SOURCE_FORM_OPS['raster_render_bwd']} in the "
+                "reference's source form) x the reference's tile samples of one raster VJP pass; the kernel "
+                "evaluates only the samples inside each record's conservative box")
+    traffic = RASTER_VJP_TRAFFIC_BYTES.get(workload)
+    return {
+        "kernel": ACCUMULATE_KERNELS["raster_render_bwd"],
+        "bound": "fp32",
+        "work": work,
+        "achieved": achieved,
+        "peak": fp32_peak,
+        "unit": "TFLOP/s",
+        "frac": frac,
+        "frac_source_form": entry.get("frac_source_form"),
+        "kernel_ms": entry.get("ms"),
+        "traffic": traffic,
+        "traffic_unit": "DRAM bytes read + written per launch (ncu)",
+        "peak_source": "measured in-bench: FP32 FMA issue probe r2s_fp32_peak_probe (MEASURED_PEAKS.json has no "
+                       "FP32 figure)",
+        "hbm_peak_gbs_measured": hbm_peak,
+        "sfu_peak_gex2_s_measured": sfu_peak,
+    }
+
+
 def main(argv=None) -> int:
     parser = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     parser.add_argument("--gpus", type=int, default=1)
     parser.add_argument("--steps", type=int, default=20)
     parser.add_argument("--warmup", type=int, default=3)
     parser.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    parser.add_argument("--workload", choices=("ct", "ct4", "small", "beta", "beta8", "batched", "serve"), default="ct",
+    parser.add_argument("--workload", choices=("ct", "ct4", "small", "beta", "beta8", "batched", "serve", "serve5"),
+                        default="ct",
                         help="ct: the CT fit step (default); batched / serve: the multi-reconstruction forms")
     parser.add_argument("--scenes", type=int, default=32, help="reconstructions for --workload batched/serve")
     parser.add_argument("--requests", type=int, default=400, help="requests for --workload serve")
@@ -639,6 +985,8 @@ def main(argv=None) -> int:
                         help="run the warm-up steps of the workload and exit (profiling driver, no timing)")
     parser.add_argument("--cpu-budget", type=float, default=15.0)
     parser.add_argument("--no-cpu-baseline", action="store_true")
+    parser.add_argument("--no-mix", action="store_true",
+                        help="skip the bounded batched / served runs that the default CT line carries")
     args = parser.parse_args(argv)
     if args.warmup < 3:
         parser.error("--warmup must be at least 3")
@@ -652,9 +1000,10 @@ def main(argv=None) -> int:
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
-    if args.workload in ("batched", "serve"):
+    if args.workload in ("batched", "serve", "serve5"):
         if rank == 0:
-            print(json.dumps(mixed_workload(args, device)))
+            out = serving_at_scale(args, device) if args.workload == "serve5" else mixed_workload(args, device)
+            print(json.dumps(out))
         if world > 1:
             dist.destroy_process_group()
         return 0
@@ -667,18 +1016,20 @@ def main(argv=None) -> int:
             dist.barrier()
             dist.destroy_process_group()
             return 0
-        if not ref_ops.available():
-            print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref missing"}))
+        if not ref_ops.package_available():
+            print(json.dumps({"impl": "reference",
+                              "unavailable": "reference build or staged package (oracle/_ref) missing"}))
             if world > 1:
                 dist.barrier()
                 dist.destroy_process_group()
             return 0
 
-    scene, target = build_workload(device, args.workload)
+    ours = args.impl == "ours"
+    scene, target = build_workload(device, args.workload, args.impl)
     if args.workload in ("beta", "beta8"):
-        step = OursBetaStep(scene) if args.impl == "ours" else ReferenceBetaStep(scene)
+        step = OursBetaStep(scene) if ours else ReferenceBetaStep(scene)
     else:
-        step = OursStep(scene, target) if args.impl == "ours" else ReferenceStep(scene, target)
+        step = OursStep(scene, target) if ours else ReferenceStep(scene, target)
     if args.profile_only:
         for _ in range(args.warmup):
             step(*step_inputs(scene))
@@ -686,12 +1037,13 @@ def main(argv=None) -> int:
         return 0
     flush_buf = torch.zeros(L2_FLUSH_BYTES // 4, device=device)
 
-    if world > 1 and args.impl == "ours":
+    if world > 1 and ours:
         dist.barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clocks:
-        total_ms, stages, own_launches = timed_run(step, scene, args.steps, args.warmup, device, flush_buf, clocks)
-    ranks = world if args.impl == "ours" else 1
+        total_ms, stages, api_stages, own_launches = timed_run(step, scene, args.steps, args.warmup, device,
+                                                               flush_buf, clocks, ours=ours)
+    ranks = world if ours else 1
     total_ms = max_over_ranks(total_ms, ranks, device)
     ms_per_step = total_ms / args.steps
     raster_evals, voxel_evals, m2, m3 = step.eval_counts()
@@ -701,10 +1053,10 @@ def main(argv=None) -> int:
     e2e_ms, h2d, d2h = e2e_run(step, scene, args.steps, args.warmup, device)
     e2e_ms = max_over_ranks(e2e_ms, ranks, device)
     e2e_value = job_rate(evals_per_step, ranks, e2e_ms / args.steps)
-    if args.impl == "ours":
-        launches = own_launches
-    else:
-        launches = count_launches(step, scene, "r2splat::") * args.steps
+    per_step = sorted(getattr(timed_run, "per_step_ms", []))
+    api_ms = {k: v / args.steps for k, v in api_stages.items()}
+    api_ms["sum_of_stages"] = sum(api_ms.values())
+    api_ms["outside_stages"] = ms_per_step - api_ms["sum_of_stages"]
 
     peaks = measured_peaks()
     result = {
@@ -715,7 +1067,7 @@ def main(argv=None) -> int:
         "steps": args.steps,
         "warmup": args.warmup,
         "ms_per_step": ms_per_step,
-        "fit_steps_per_s": (world if args.impl == "ours" else 1) * 1e3 / ms_per_step,
+        "fit_steps_per_s": ranks * 1e3 / ms_per_step,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
@@ -730,57 +1082,43 @@ def main(argv=None) -> int:
         },
         "clocks": clocks.summary(),
         "e2e": {"value": e2e_value, "unit": "evals/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "gpu_launches": launches,
-        "stages_ms_per_step": {k: v / args.steps for k, v in stages.items()},
+        "api_stages_ms_per_step": api_ms,
+        "step_ms_distribution": ({"min": per_step[0], "median": statistics.median(per_step), "max": per_step[-1]}
+                                 if per_step else None),
     }
-    if args.impl == "reference":
-        result["impl"] = "reference"
-        result["e2e"] = {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
-        result["cpu_baseline"] = {
-            "value": value, "unit": "evals/s", "cores": 0, "kind": "reference",
-            "sample": "the reference's own CUDA kernels (compiled unmodified from its sources for sm_100a) on the "
-                      "same B200, driven by its explicit.py call sequence; the reference has no CPU implementation "
-                      "of these operators",
-        }
-    elif args.workload in ("beta", "beta8"):
-        # The Beta VJP with the variance branch is bound by instruction issue (ncu: XU 15 %, issue 74 %);
-        # its roofline counts the FP32 operations of the reference's per-sample form.
-        kernel_ms = stages.get("raster_render_bwd", 0.0) / args.steps
-        peak = fp32_peak_tflops(device)
-        achieved = BETA_VAR_VJP_FLOPS_PER_EVAL * raster_evals / (kernel_ms * 1e-3) / 1e12 if kernel_ms else None
-        result["roofline"] = {
-            "kernel": "raster_record_bwd_kernel (record-parallel raster VJP, Beta with the variance branch)",
-            "bound": "fp32",
-            "work": f"algorithmic: {BETA_VAR_VJP_FLOPS_PER_EVAL} FP32 ops (and 5 MUFU) x the reference's tile samples "
-                    "of one raster VJP pass; the kernel evaluates only the samples inside each record's box",
-            "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-            "frac": achieved / peak if achieved else None, "traffic": None,
-            "peak_source": "measured in-bench: FP32 FMA probe r2s_fp32_peak_probe",
-            "sfu_peak_gex2_s_measured": sfu_peak_gops(device),
-        }
+    if not ours:
+        launches = count_launches(step, scene)
+        result.update({
+            "impl": "reference",
+            "gpu_launches": launches["all"] * args.steps,
+            "launches_per_step": launches,
+            "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "cpu_baseline": {
+                "value": value, "unit": "evals/s", "cores": 1, "kind": "reference",
+                "sample": "the reference's own package (explicit.py and its low-level wrapper, unmodified) on its "
+                          "own CUDA kernels (compiled unmodified for sm_100a), driven by one host thread on the "
+                          "same B200; the reference has no CPU implementation of these operators",
+            },
+        })
     else:
-        kernel = "raster_render_bwd"
-        kernel_ms = stages.get(kernel, 0.0) / args.steps
-        achieved = FLOPS_PER_EVAL[kernel] * raster_evals / (kernel_ms * 1e-3) / 1e12 if kernel_ms else None
-        peak = fp32_peak_tflops(device)
-        result["roofline"] = {
-            "kernel": "raster_record_bwd_kernel (record-parallel raster VJP)",
-            "bound": "fp32",
-            "work": "algorithmic: 44 FP32 ops x the reference's tile samples of one raster VJP pass; the kernel "
-                    "itself evaluates only the samples inside each record's conservative box",
-            "achieved": achieved,
-            "peak": peak,
-            "unit": "TFLOP/s",
-            "frac": achieved / peak if achieved else None,
-            "traffic": RASTER_VJP_TRAFFIC_BYTES if args.workload == "ct" else None,
-            "traffic_unit": "bytes per launch (ncu)",
-            "peak_source": "measured in-bench: FP32 FMA probe r2s_fp32_peak_probe (MEASURED_PEAKS.json has no "
-                           "FP32 figure)",
-            "hbm_peak_gbs_measured": peaks.get("hbm_gbs"),
-            "sfu_peak_gex2_s_measured": sfu_peak_gops(device),
-        }
-        if rank == 0 and not args.no_cpu_baseline:
-            result["cpu_baseline"] = cpu_baseline(args.cpu_budget)
+        result["gpu_launches"] = own_launches
+        result["stages_ms_per_step"] = {k: v / args.steps for k, v in stages.items()}
+        fp32_peak = fp32_peak_tflops(device)
+        sfu_peak = sfu_peak_gops(device)
+        result["rooflines"] = accumulate_rooflines(args.workload, stages, args.steps, raster_evals, voxel_evals,
+                                                   fp32_peak)
+        result["roofline"] = dominant_roofline(args.workload, result["rooflines"], fp32_peak, sfu_peak,
+                                               peaks.get("hbm_gbs"))
+        if rank == 0 and not args.no_cpu_baseline and args.workload in ("ct", "small"):
+            result["cpu_baseline"] = cpu_baseline(device, args.cpu_budget)
+        if args.workload == "ct" and not args.no_mix and rank == 0:
+            # Bounded runs of the multi-reconstruction forms, so the default line records them too.
+            del step, scene, target, flush_buf
+            torch.cuda.empty_cache()
+            result["batched"] = bounded_mix(device, "batched")
+            torch.cuda.empty_cache()
+            result["served"] = bounded_mix(device, "serve")
+    result["native_libs"] = mapped_native_libs()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

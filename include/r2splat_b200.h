@@ -294,6 +294,16 @@ int r2s_volume_loss_bwd(int dtype, const void* volume, const void* grad_output, 
                         uint32_t D, uint32_t H, uint32_t W, float lambda_tv, void* grad_volume,
                         void* stream);
 
+/* Ops.h:37-44 volume_loss_fwd followed by volume_loss_bwd, as one pass over the volume, for
+ * callers that know the upstream gradient grad_output [1] (device) before the forward, as a fit
+ * step does. -> loss [1], tv [1], tv_map [B,D,H,W] (optional, null to skip), grad_volume
+ * [B,D,H,W]. tv_map and grad_volume equal the two calls' bit for bit. Workspace:
+ * r2s_volume_loss_workspace(numel). */
+int r2s_volume_loss_fwd_bwd(int dtype, const void* volume, const void* grad_output, uint32_t B,
+                            uint32_t D, uint32_t H, uint32_t W, float lambda_tv, void* loss,
+                            void* tv, void* tv_map, void* grad_volume, void* workspace,
+                            size_t workspace_bytes, void* stream);
+
 /* Ops.h:15-18 image_loss_fwd / Ops.h:26-29 image_loss_l1_fwd (mean L1 over [B,H,W]).
  * -> loss [1], l1 [1], l1_map [B,H,W]. Workspace: r2s_volume_loss_workspace(numel). */
 int r2s_image_loss_l1_fwd(int dtype, const void* prediction, const void* target, uint32_t B,
@@ -443,6 +453,48 @@ int r2s_voxel_render_bwd_capacity(int dtype, const void* records, int beta, int 
                                   uint32_t dim1, uint32_t dim0, uint32_t tile_size, uint32_t tiles_x,
                                   uint32_t tiles_y, uint32_t tiles_z, void* grads, void* stream);
 
+/* Deterministic form of r2s_voxel_render_bwd (the explicit path's voxel VJP; the
+ * reference's K30/K32, VoxelizeToVoxelsBwd.cu:322-514, add every (tile, primitive)
+ * pair's sums into the primitive's adjoints with atomics). Each pair writes its 12
+ * sums to slot tile_cum[n - 1] + (the tile's index in primitive n's 3D tile box,
+ * z then y then x), and a second pass adds each primitive's slots in order into
+ * grads [N] (written, not accumulated): the same result on every run. means_v [N,3]
+ * and radii [N,3] are r2s_voxel_project's, tile_cum [N] int64 the inclusive scan of
+ * its tile counts; slots [slot_capacity, 12] is caller scratch. Capacity-bounded
+ * form: n_used (device count) instead of n_isects; slots past slot_capacity are
+ * neither written nor read (such a step overflowed and is discarded). */
+int r2s_voxel_render_bwd_slots(int dtype, const void* records, int beta, int detach_variance,
+                               const int32_t* tile_offsets, const int32_t* flatten_ids, uint64_t n_isects,
+                               const int64_t* n_used, const void* means_v, const int32_t* radii,
+                               const int64_t* tile_cum, const void* v_volume, const void* v_volume_var, uint32_t N,
+                               uint32_t dim2, uint32_t dim1, uint32_t dim0, uint32_t tile_size, uint32_t tiles_x,
+                               uint32_t tiles_y, uint32_t tiles_z, void* slots, uint64_t slot_capacity, void* grads,
+                               void* stream);
+
+/* Record-parallel voxel VJP, for a backward that keeps no intersection lists
+ * (recompute-in-backward under a memory budget), replacing the tile-parallel
+ * per-primitive VJP with atomics (VoxelizeToVoxelsBwd.cu:322-514, K30/K32, for
+ * the path explicit.py:331-350 drives). A work item is one primitive and one
+ * z-layer of its 3D tile box (IsectTiles3DKernel.cu:38-112); it needs no sorted
+ * lists. r2s_voxel_layer_counts writes each primitive's layer count [N] int32
+ * from the voxel-space means and radii of r2s_voxel_project; its inclusive
+ * scan (r2s_scan_tile_counts) is layer_cum [N] int64 and its total n_items.
+ * r2s_voxel_record_bwd walks every item into partials [n_items] (64-byte
+ * records) and sums each primitive's slots in layer order into grads [N]
+ * (packed as r2s_voxel_render_bwd's, written, not accumulated): deterministic.
+ * Capacity-bounded form: n_items is the capacity of partials and n_items_dev
+ * the device-side total (layer_cum's last entry); a total above the capacity
+ * sets *overflow (may be null) and the result is to be discarded. */
+int r2s_voxel_layer_counts(int dtype, const void* means_v, const int32_t* radii, uint32_t N, uint32_t dim2,
+                           uint32_t dim1, uint32_t dim0, uint32_t tile_size, uint32_t tiles_x, uint32_t tiles_y,
+                           uint32_t tiles_z, int32_t* layers, void* stream);
+int r2s_voxel_record_bwd(int dtype, const void* records, const void* means_v, const int32_t* radii,
+                         const int64_t* layer_cum, uint64_t n_items, const int64_t* n_items_dev, int beta,
+                         int detach_variance, const void* v_volume, const void* v_volume_var, uint32_t N,
+                         uint32_t dim2, uint32_t dim1, uint32_t dim0, uint32_t tile_size, uint32_t tiles_x,
+                         uint32_t tiles_y, uint32_t tiles_z, void* partials, void* grads, uint32_t* overflow,
+                         void* stream);
+
 /* ------------------------------------------ forward with fused image loss
  * Replaces, in a fit step, the separate image-loss pass after
  * rasterize_to_pixels_fwd (caller-side in examples/optimize.py; the L1 form is
@@ -492,7 +544,9 @@ int r2s_adam_activation_step(int dtype, uint32_t N, void* means, void* quats, vo
  * R2S_ERR_UNSUPPORTED with nothing launched. Calls on one device share the
  * scratch: calls that overlap in time race and must be serialised by the
  * caller. The first call on a device resolves the scratch address and should
- * come before any stream capture on that device. */
+ * come before any stream capture on that device. The address stays cached for
+ * the process, so a device must not be reset (cudaDeviceReset) after this
+ * entry point has been called on it. */
 uint64_t r2s_scan_tile_counts_noalloc_max(void);
 int r2s_scan_tile_counts_noalloc(const int32_t* counts, uint64_t n, int64_t* cum, void* stream);
 

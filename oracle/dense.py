@@ -146,6 +146,55 @@ def rasterize_dense(means, quats, scales, densities, viewmats, Ks, image_size, *
     return mean_total if uncertainty is None else (mean_total, var_total)
 
 
+def absgrad_dense(means2d, conics, opacities, mus, v_image, *, betas=None, tile_mask=None):
+    """Per (camera, primitive) sum over pixels of |d loss / d means2d| of each pixel's term, float64.
+
+    The densification statistic the reference's raster VJPs return in their
+    first slot when ``absgrad`` is set: each pixel's mean-position adjoint is
+    taken in absolute value per component before the sum
+    (``RasterizeToPixelsBwd.cu:216-221`` pixel mode, ``:459-462`` per-primitive
+    mode; the reference's test oracle ``tests/test_beta_low_level_numeric.py:113-149``).
+    Inputs are the low-level 2D operands: ``means2d [C,N,2]``, ``conics
+    [C,N,3]`` (a, b, c), ``opacities [C,N]``, ``mus [C,N]``, ``v_image [C,H,W]``,
+    and for Beta primitives the exponents ``betas [C,N]``. Gaussian samples
+    count when sigma >= 0 and |alpha| >= 1e-5; Beta samples when 0 <= d^2 < 1
+    and |alpha| >= 1e-5. ``tile_mask`` (bool [C,N,H,W]) restricts each pair to
+    the pixels of its listed tiles.
+    """
+    cams, height, width = v_image.shape
+    yy, xx = torch.meshgrid(torch.arange(height, dtype=means2d.dtype) + 0.5,
+                            torch.arange(width, dtype=means2d.dtype) + 0.5, indexing="ij")
+    dx = xx[None, None] - means2d[..., 0, None, None]
+    dy = yy[None, None] - means2d[..., 1, None, None]
+    a, b, c = (conics[..., i, None, None] for i in range(3))
+    om = (opacities * mus)[..., None, None]
+    v = v_image[:, None]
+    if betas is None:
+        sigma = 0.5 * (a * dx * dx + c * dy * dy) + b * dx * dy
+        alpha = om * torch.exp(-sigma)
+        valid = (sigma >= 0) & (alpha.abs() >= 1e-5)
+        v_sigma = -v * alpha
+        vx = -v_sigma * (a * dx + b * dy)
+        vy = -v_sigma * (c * dy + b * dx)
+    else:
+        ex, ey = -dx, -dy  # the Beta form measures from the pixel to the centre
+        d2 = a * ex * ex + 2.0 * b * ex * ey + c * ey * ey
+        h = 1.0 - d2
+        inside = (d2 >= 0) & (h > 0)
+        hp = h.clamp_min(0)
+        beta = betas[..., None, None]
+        alpha = torch.where(inside, om * hp.pow(beta), torch.zeros_like(h))
+        valid = inside & (alpha.abs() >= 1e-5)
+        v_d2 = -om * beta * torch.where(inside, hp.pow(beta - 1.0), torch.zeros_like(h)) * v
+        vx = 2.0 * v_d2 * (a * ex + b * ey)
+        vy = 2.0 * v_d2 * (b * ex + c * ey)
+    if tile_mask is not None:
+        valid = valid & tile_mask
+    zero = torch.zeros_like(vx)
+    return torch.stack((torch.where(valid, vx.abs(), zero).sum((-2, -1)),
+                        torch.where(valid, vy.abs(), zero).sum((-2, -1))), dim=-1)
+
+
 def tile_mask_2d(flatten_ids, offsets, n_primitives, cameras, height, width, tile_size):
     """bool [C,N,H,W]: pixel belongs to a tile that lists the (camera, primitive) pair."""
     import numpy as np
@@ -164,4 +213,5 @@ def tile_mask_2d(flatten_ids, offsets, n_primitives, cameras, height, width, til
     return torch.from_numpy(mask)
 
 
-__all__ = ["covariance_matrix", "rasterize_dense", "rotation_matrix", "tile_mask_2d", "voxelize_dense"]
+__all__ = ["absgrad_dense", "covariance_matrix", "rasterize_dense", "rotation_matrix", "tile_mask_2d",
+           "voxelize_dense"]

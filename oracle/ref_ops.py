@@ -6,14 +6,18 @@ pybind names of ``ext.cpp:8-183``). ``load()`` imports that module;
 ``explicit_rasterize_fwd/bwd`` and ``explicit_voxelize_fwd/bwd`` restate the
 call sequence of the reference's ``explicit.py`` (:160-183, :204-241,
 :286-307, :331-350) on top of it, so parity tests and the reference bench arm
-run the reference kernels exactly as the reference's public API does (the
-reference's Python package itself is not available on the GPU host).
+run the reference kernels exactly as the reference's public API does and can
+read the intermediate buffers. ``load_package()`` imports the reference's own
+Python package as staged by ``oracle/build_ref.py`` (``oracle/_ref/py``) with
+``r2splat.csrc`` bound to the compiled module, so the reference bench arm runs
+the reference's unmodified ``explicit.py`` on the reference's kernels.
 """
 
 from __future__ import annotations
 
 import importlib.machinery
 import importlib.util
+import sys
 from pathlib import Path
 
 import torch
@@ -40,6 +44,32 @@ def load():
     loader.exec_module(module)
     _module = module
     return module
+
+
+def package_available() -> bool:
+    return available() and (_REF_DIR / "py" / "r2splat" / "explicit.py").is_file()
+
+
+def load_package():
+    """The reference's own ``r2splat`` package with its extension bound to ``load()``'s module.
+
+    The reference resolves its kernels with ``importlib.import_module("r2splat.csrc")``
+    (``r2splat/cuda/_backend.py:29``); registering the compiled module under that
+    name beforehand makes that import return it. Raises FileNotFoundError when
+    either the build or the staged package is missing.
+    """
+    root = _REF_DIR / "py"
+    if not (root / "r2splat" / "explicit.py").is_file():
+        raise FileNotFoundError(f"no staged reference package under {root}; run python oracle/build_ref.py")
+    module = load()
+    sys.modules.setdefault("r2splat.csrc", module)
+    if str(root) not in sys.path:
+        sys.path.insert(0, str(root))
+    import r2splat
+
+    if not r2splat.cuda.is_cuda_extension_available():
+        raise RuntimeError("the reference package did not bind its CUDA extension")
+    return r2splat
 
 
 def _ratio(beta):
@@ -185,5 +215,5 @@ def explicit_voxelize_bwd(saved, means, quats, scales, densities, beta, uncertai
     return v_means, v_quats, v_scales, v_dens, v_beta, v_unc
 
 
-__all__ = ["available", "explicit_rasterize_bwd", "explicit_rasterize_fwd", "explicit_voxelize_bwd",
+__all__ = ["available", "load_package", "package_available", "explicit_rasterize_bwd", "explicit_rasterize_fwd", "explicit_voxelize_bwd",
            "explicit_voxelize_fwd", "load"]

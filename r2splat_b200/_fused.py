@@ -11,7 +11,12 @@ Rasterize (the reference's explicit.py:160-183 and :204-241):
   factor, parameter-transform VJP); neither uses atomics.
 
 Voxelize (explicit.py:286-307, :331-350): the same structure in 3D with
-64-byte records [N,16].
+64-byte records [N,16]. Its VJP is tile-parallel over the sorted lists, but
+deterministic: each (tile, primitive) pair writes its sums to a slot of its
+own and one pass adds each primitive's slots in a fixed order, so the voxel
+gradients, like the raster ones, are the same on every run. A backward that
+keeps no lists (recompute under a memory budget) walks each primitive's tile
+box layer by layer instead (record-parallel, also deterministic).
 
 All arrays are allocated through the torch caching allocator and passed to the
 C ABI; nothing here computes on the CPU.
@@ -32,6 +37,9 @@ from .cuda import _wrapper as low
 Tensor = torch.Tensor
 RASTER_TILE = 16
 VOXEL_TILE = 8
+# Largest scratch the deterministic voxel VJP takes for its per-intersection slots (12 values each);
+# past it the VJP walks the primitives' tile boxes instead (one slot per primitive and z-layer).
+VOXEL_SLOT_BUDGET_BYTES = 8 << 30
 
 
 def _ptr(t: Optional[Tensor]):
@@ -71,11 +79,15 @@ class StageTimer:
 
 
 class _stage:
+    """A named pipeline stage: an NVTX range (visible to nsys / ncu --nvtx) and, while a StageTimer is
+    active, a CUDA-event pair."""
+
     def __init__(self, name: str):
         self.name = name
         self.start = None
 
     def __enter__(self):
+        torch.cuda.nvtx.range_push("r2s:" + self.name)
         if StageTimer.active is not None:
             self.start = torch.cuda.Event(enable_timing=True)
             self.start.record()
@@ -86,6 +98,7 @@ class _stage:
             end = torch.cuda.Event(enable_timing=True)
             end.record()
             StageTimer.active.records.append((self.name, self.start, end))
+        torch.cuda.nvtx.range_pop()
         return False
 
 
@@ -108,14 +121,23 @@ class RasterState:
 
 @dataclass
 class VoxelState:
+    """Device buffers of a voxelize forward. The VJP reads the records, the voxel-space
+    means and radii (its tile boxes) and the inclusive scan of the per-primitive layer
+    counts; the sorted lists serve the forward (and callers that inspect them)."""
+
     covars: Tensor
     records: Tensor
-    offsets: Tensor
-    isect_ids: Tensor
-    flatten_ids: Tensor
+    offsets: Optional[Tensor]
+    isect_ids: Optional[Tensor]
+    flatten_ids: Optional[Tensor]
     n_isects: int
     shape: tuple
     tile_size: int = VOXEL_TILE
+    means_v: Optional[Tensor] = None
+    radii: Optional[Tensor] = None
+    tile_cum: Optional[Tensor] = None
+    layer_cum: Optional[Tensor] = None
+    n_items: int = 0
 
 
 def raster_intersections(means, covars, densities, beta, ratio, viewmats, Ks, width, height, eps, radius_clip,
@@ -239,11 +261,15 @@ def raster_vjp_state(means, quats, scales, densities, viewmats, Ks, width, heigh
 
 def voxel_vjp_state(means, quats, scales, densities, shape, extent, center, beta, uncertainty, eps, radius_clip,
                     tile_size=VOXEL_TILE):
-    """What the voxel VJP reads (covariances, records, sorted tile lists), rebuilt without the volume."""
+    """What the voxel VJP reads (covariances, records, voxel-space means and radii, layer scan),
+    rebuilt without the volume: the projection and the layer counts, no intersection lists or sort."""
     covars, _ = low.parameter_transform_fwd(quats, scales)
-    records, offsets, isect_ids, flatten_ids, m = voxel_intersections(
-        means, covars, densities, beta, uncertainty, extent, center, shape, eps, radius_clip, tile_size)
-    return VoxelState(covars, records, offsets, isect_ids, flatten_ids, m, tuple(shape), tile_size)
+    records, means_v, radii, _, _ = _voxel_project(means, covars, densities, beta, uncertainty, extent, center,
+                                                   shape, eps, radius_clip, tile_size)
+    layer_cum = _layer_scan(means_v, radii, shape, tile_size)
+    n_items = int(layer_cum[-1].item()) if layer_cum.numel() else 0
+    return VoxelState(covars, records, None, None, None, 0, tuple(shape), tile_size, means_v, radii, None,
+                      layer_cum, n_items)
 
 
 def raster_backward(state: RasterState, means, quats, scales, densities, beta, uncertainty, viewmats, Ks, eps,
@@ -275,14 +301,18 @@ def raster_backward(state: RasterState, means, quats, scales, densities, beta, u
     return v_means, v_quats, v_scales, v_dens, v_beta, v_unc
 
 
-def voxel_intersections(means, covars, densities, beta, uncertainty, extent, center, shape, eps, radius_clip,
-                        tile_size=VOXEL_TILE, before_count=None):
+def _voxel_tiles(shape, tile_size):
+    depth, height, width = shape
+    return (width + tile_size - 1) // tile_size, (height + tile_size - 1) // tile_size, \
+        (depth + tile_size - 1) // tile_size
+
+
+def _voxel_project(means, covars, densities, beta, uncertainty, extent, center, shape, eps, radius_clip, tile_size):
+    """Records [N,16], voxel-space means, radii, tile counts and their inclusive scan."""
     device = means.device
     depth, height, width = shape
     n = means.shape[0]
-    tx = (width + tile_size - 1) // tile_size
-    ty = (height + tile_size - 1) // tile_size
-    tz = (depth + tile_size - 1) // tile_size
+    tx, ty, tz = _voxel_tiles(shape, tile_size)
     stream = _stream(device)
     lib = _backend.library()
     records = means.new_empty((n, 16))
@@ -296,6 +326,38 @@ def voxel_intersections(means, covars, densities, beta, uncertainty, extent, cen
     cum = torch.empty((n,), dtype=torch.int64, device=device)
     ws = _ws(lib.r2s_isect_count_workspace(n), device)
     _backend.call("r2s_scan_tile_counts", _ptr(counts), n, _ptr(cum), _ptr(ws), ws.numel(), stream)
+    return records, means_v, radii, counts, cum
+
+
+def _layer_scan(means_v, radii, shape, tile_size):
+    """Inclusive scan of the per-primitive z-layer counts of the 3D tile boxes (the VJP's work items)."""
+    device = means_v.device
+    depth, height, width = shape
+    n = means_v.shape[0]
+    tx, ty, tz = _voxel_tiles(shape, tile_size)
+    stream = _stream(device)
+    layers = torch.empty((n,), dtype=torch.int32, device=device)
+    _backend.call("r2s_voxel_layer_counts", _dtype(means_v), _ptr(means_v), _ptr(radii), n, width, height, depth,
+                  tile_size, tx, ty, tz, _ptr(layers), stream)
+    layer_cum = torch.empty((n,), dtype=torch.int64, device=device)
+    ws = _ws(_backend.library().r2s_isect_count_workspace(n), device)
+    _backend.call("r2s_scan_tile_counts", _ptr(layers), n, _ptr(layer_cum), _ptr(ws), ws.numel(), stream)
+    return layer_cum
+
+
+def voxel_intersections(means, covars, densities, beta, uncertainty, extent, center, shape, eps, radius_clip,
+                        tile_size=VOXEL_TILE, before_count=None):
+    """Projection and sorted 3D tile lists.
+
+    Returns (records, offsets, isect_ids, flatten_ids, M, means_v, radii, tile_cum); tile_cum is the
+    inclusive scan of the per-primitive tile counts, which the VJP's slots are numbered by.
+    """
+    device = means.device
+    tx, ty, tz = _voxel_tiles(shape, tile_size)
+    stream = _stream(device)
+    lib = _backend.library()
+    records, means_v, radii, _, cum = _voxel_project(means, covars, densities, beta, uncertainty, extent, center,
+                                                     shape, eps, radius_clip, tile_size)
     if before_count is not None:
         before_count()
     m = int(cum[-1].item())
@@ -304,10 +366,19 @@ def voxel_intersections(means, covars, densities, beta, uncertainty, extent, cen
     offsets = torch.empty((tz, ty, tx), dtype=torch.int32, device=device)
     ws = _ws(lib.r2s_isect_emit_workspace(m, tx * ty * tz), device)
     with _stage("voxel_sort"):
-        _backend.call("r2s_isect_tiles_3d_emit", _dtype(means), _ptr(means_v), _ptr(radii), n, tile_size, tx, ty,
-                      tz, _ptr(cum), m, _ptr(isect_ids), _ptr(flatten_ids), _ptr(offsets), _ptr(ws), ws.numel(),
-                      stream)
-    return records, offsets, isect_ids, flatten_ids, m
+        _backend.call("r2s_isect_tiles_3d_emit", _dtype(means), _ptr(means_v), _ptr(radii), means.shape[0],
+                      tile_size, tx, ty, tz, _ptr(cum), m, _ptr(isect_ids), _ptr(flatten_ids), _ptr(offsets),
+                      _ptr(ws), ws.numel(), stream)
+    return records, offsets, isect_ids, flatten_ids, m, means_v, radii, cum
+
+
+def release_lists(state):
+    """Drops a forward state's intersection lists (raster or voxel): neither VJP needs them (the raster VJP
+    walks tile rectangles; the voxel VJP then takes its list-free form), so a caller short of memory can
+    free them between forward and backward. Returns the tensors dropped."""
+    dropped = [t for t in (state.isect_ids, state.flatten_ids, state.offsets) if t is not None]
+    state.isect_ids = state.flatten_ids = state.offsets = None
+    return dropped
 
 
 def voxel_forward(means, quats, scales, densities, shape, extent, center, beta, uncertainty, eps, radius_clip,
@@ -315,7 +386,7 @@ def voxel_forward(means, quats, scales, densities, shape, extent, center, beta, 
     device = means.device
     depth, height, width = shape
     covars, _ = low.parameter_transform_fwd(quats, scales)
-    records, offsets, isect_ids, flatten_ids, m = voxel_intersections(
+    records, offsets, isect_ids, flatten_ids, m, means_v, radii, tile_cum = voxel_intersections(
         means, covars, densities, beta, uncertainty, extent, center, shape, eps, radius_clip, tile_size,
         before_count)
     volume = means.new_empty(shape)
@@ -327,25 +398,44 @@ def voxel_forward(means, quats, scales, densities, shape, extent, center, beta, 
         _backend.call("r2s_voxel_render", _dtype(means), _ptr(records), int(beta is not None), _ptr(offsets),
                       _ptr(flatten_ids), means.shape[0], m, width, height, depth, tile_size, tx, ty, tz,
                       _ptr(volume), _ptr(variance), _stream(device))
-    state = VoxelState(covars, records, offsets, isect_ids, flatten_ids, m, tuple(shape), tile_size)
+    state = VoxelState(covars, records, offsets, isect_ids, flatten_ids, m, tuple(shape), tile_size, means_v, radii,
+                       tile_cum)
     return (volume if uncertainty is None else (volume, variance)), state
 
 
 def voxel_backward(state: VoxelState, means, quats, scales, beta, uncertainty, extent, center, eps, v_volume,
                    v_variance, detach_variance):
+    """Explicit voxel VJP -> (v_means, v_quats, v_scales, v_densities, v_beta, v_uncertainty)."""
     device = means.device
     n = means.shape[0]
     depth, height, width = state.shape
     tile = state.tile_size
-    tx = (width + tile - 1) // tile
-    ty = (height + tile - 1) // tile
-    tz = (depth + tile - 1) // tile
+    tx, ty, tz = _voxel_tiles(state.shape, tile)
     stream = _stream(device)
-    grads = means.new_zeros((n, 16))
+    grads = means.new_empty((n, 16))  # every primitive's entry is written
+    # The list-free form when no lists were kept, or when per-intersection slots would take more memory
+    # than the budget (it needs one slot per primitive and tile-box z-layer instead).
+    slot_bytes = state.n_isects * 12 * means.element_size()
+    list_free = state.offsets is None or slot_bytes > VOXEL_SLOT_BUDGET_BYTES
+    if list_free and state.layer_cum is None:
+        state.layer_cum = _layer_scan(state.means_v, state.radii, state.shape, state.tile_size)
+        state.n_items = int(state.layer_cum[-1].item()) if n else 0
     with _stage("voxel_render_bwd"):
-        _backend.call("r2s_voxel_render_bwd", _dtype(means), _ptr(state.records), int(beta is not None),
-                      int(bool(detach_variance)), _ptr(state.offsets), _ptr(state.flatten_ids), _ptr(v_volume),
-                      _ptr(v_variance), n, state.n_isects, width, height, depth, tile, tx, ty, tz, _ptr(grads), stream)
+        if not list_free:
+            # Tile-parallel over the forward's sorted lists, one slot per (tile, primitive) pair.
+            slots = means.new_empty((max(state.n_isects, 1), 12))
+            _backend.call("r2s_voxel_render_bwd_slots", _dtype(means), _ptr(state.records), int(beta is not None),
+                          int(bool(detach_variance)), _ptr(state.offsets), _ptr(state.flatten_ids), state.n_isects,
+                          None, _ptr(state.means_v), _ptr(state.radii), _ptr(state.tile_cum), _ptr(v_volume),
+                          _ptr(v_variance), n, width, height, depth, tile, tx, ty, tz, _ptr(slots), slots.shape[0],
+                          _ptr(grads), stream)
+        else:
+            # No lists kept: record-parallel over the primitives' tile-box layers.
+            partials = means.new_empty((max(state.n_items, 1), 16))
+            _backend.call("r2s_voxel_record_bwd", _dtype(means), _ptr(state.records), _ptr(state.means_v),
+                          _ptr(state.radii), _ptr(state.layer_cum), state.n_items, None, int(beta is not None),
+                          int(bool(detach_variance)), _ptr(v_volume), _ptr(v_variance), n, width, height, depth,
+                          tile, tx, ty, tz, _ptr(partials), _ptr(grads), None, stream)
     v_means = means.new_empty((n, 3))
     v_quats = means.new_empty((n, 4))
     v_scales = means.new_empty((n, 3))

@@ -11,11 +11,13 @@ backward rebuilds what the VJP reads:
 * rasterize: the parameter transform and the projection (packed records and
   tile rectangles). The record-parallel VJP walks each record's tile
   rectangle, so the intersection lists are neither stored nor rebuilt.
-* voxelize: the parameter transform, the voxel mapping and the sorted
-  per-tile intersection lists.
+* voxelize: the parameter transform, the voxel mapping and the scan of the
+  per-primitive tile-box layer counts. The record-parallel voxel VJP walks
+  each primitive's tile box, so here too the intersection lists are neither
+  stored nor rebuilt.
 
-That trades a projection (and, for voxelize, a sort) for the memory of the
-saved lists and records between forward and backward. Without ``recompute``
+That trades a projection for the memory of the saved lists and records
+between forward and backward. Without ``recompute``
 the explicit context from the forward is kept and consumed by the first
 backward; a second backward (``retain_graph=True``) rebuilds it.
 """

@@ -14,13 +14,14 @@ synchronisation:
 * the MSE image loss and its gradient ``2 (image - target) / numel``, written by
   the forward's tile kernel (fused epilogue);
 * the record-parallel raster VJP and its chain rule;
-* voxel forward, TV loss forward and backward, the voxel VJP and its chain rule;
+* voxel forward, TV loss forward and backward in one pass, the voxel VJP and its chain rule;
 * the fused activation-chain + Adam update.
 
-The intersection count stays on the device (``r2s_*_capacity`` entry points).
-When it exceeds the scene's list capacity, the step is flagged and the update
-is skipped; ``BatchedFit`` then grows that capacity, re-captures and the next
-replay redoes the step.
+The intersection counts stay on the device (``r2s_*_capacity`` entry points,
+and the capacity-bounded form of the deterministic voxel VJP, whose slots are
+the 3D intersections). When a count exceeds the scene's capacity, the step is
+flagged and the update is skipped; ``BatchedFit`` then grows that capacity,
+re-captures and the next replay redoes the step.
 
 ``BatchedFit`` captures the steps of all its scenes into one CUDA graph, each
 scene on its own stream branch so that small scenes' kernels overlap, and
@@ -80,8 +81,13 @@ class FitScene:
     """One reconstruction's parameters, Adam state and fit-step buffers on the device."""
 
     def __init__(self, means: Tensor, quats: Tensor, scales: Tensor, densities: Tensor, viewmats: Tensor,
-                 Ks: Tensor, target: Tensor, config: SceneConfig, beta: Optional[Tensor] = None):
+                 Ks: Tensor, target: Tensor, config: SceneConfig, beta: Optional[Tensor] = None,
+                 lean: bool = False):
+        """``lean``: keep only what a fit continues from (parameters, activations, Adam state, cameras,
+        target); the step buffers are not allocated and the scene is stepped through the explicit API
+        (``serve.lean_step``), never by ``enqueue``."""
         self.cfg = config
+        self.is_lean = bool(lean)
         self.device = means.device
         dev, dt = self.device, means.dtype
         n, c = means.shape[0], viewmats.shape[0]
@@ -109,9 +115,12 @@ class FitScene:
         self.center = torch.tensor(config.volume_center, dtype=dt, device=dev)
         self.overflow = torch.zeros(1, dtype=torch.int32, device=dev)
         self.loss = torch.zeros(1, dtype=dt, device=dev)
-        self._allocate_fixed()
+        self.ones = torch.ones(1, dtype=dt, device=dev)
         self.capacity_2d = 0
         self.capacity_3d = 0
+        if self.is_lean:
+            return
+        self._allocate_fixed()
         self.set_capacity(*self.measure_counts())
 
     # ------------------------------------------------------------------ buffers
@@ -164,12 +173,14 @@ class FitScene:
                         torch.empty((n,), dtype=dt, device=dev) if self.raw_beta is not None else None]
 
     def set_capacity(self, m2: int, m3: int):
-        """(Re)allocates the intersection lists for m2 2D and m3 3D intersections plus slack."""
+        """(Re)allocates the intersection lists (and the voxel VJP's per-intersection slots) for m2 2D and
+        m3 3D intersections plus slack."""
         dev = self.device
         lib = _backend.library()
         slack = self.cfg.capacity_slack
         self.capacity_2d = max(1024, int(math.ceil(m2 * slack)))
         self.capacity_3d = max(1024, int(math.ceil(m3 * slack)))
+        self.slots3 = torch.empty((self.capacity_3d, 12), dtype=self.means.dtype, device=dev)
         self.isect_ids = torch.empty((self.capacity_2d,), dtype=torch.int64, device=dev)
         self.flatten_ids = torch.empty((self.capacity_2d,), dtype=torch.int32, device=dev)
         self.emit_ws = _ws(lib.r2s_isect_emit_workspace(self.capacity_2d, self.c * self.tx * self.ty), dev)
@@ -178,12 +189,15 @@ class FitScene:
         self.emit3_ws = _ws(lib.r2s_isect_emit_workspace(self.capacity_3d, self.vtx * self.vty * self.vtz), dev)
 
     def measure_counts(self) -> tuple[int, int]:
-        """Intersection counts of the current parameters (host read; used outside capture)."""
+        """2D and 3D intersection counts of the current parameters (host read; used outside capture)."""
         stream = torch.cuda.current_stream(self.device).cuda_stream
         self._project(stream)
         self._project3(stream)
         torch.cuda.current_stream(self.device).synchronize()
-        return int(self.cum[-1].item()) if self.cum.numel() else 0, int(self.cum3[-1].item()) if self.n else 0
+        if not self.n:
+            return 0, 0
+        m2, m3 = torch.stack((self.cum[-1], self.cum3[-1])).tolist()
+        return int(m2), int(m3)
 
     def needs_capacity(self) -> tuple[int, int]:
         """(m2, m3) of the current parameters; call after a flagged overflow."""
@@ -247,15 +261,15 @@ class FitScene:
             _backend.call("r2s_voxel_render_capacity", d, _p(self.records3), beta_flag, _p(self.offsets3),
                           _p(self.flatten3_ids), _p(self.n_used3), self.n, self.vwidth, self.vheight, self.depth,
                           self.cfg.voxel_tile, self.vtx, self.vty, self.vtz, _p(self.volume), None, s)
-            _backend.call("r2s_volume_loss_fwd", d, _p(self.volume), 1, self.depth, self.vheight, self.vwidth,
-                          float(self.cfg.lambda_tv), _p(self.tv_loss), _p(self.tv_value), None, _p(self.tv_ws),
-                          self.tv_ws.numel(), s)
-            _backend.call("r2s_volume_loss_bwd", d, _p(self.volume), _p(self.ones), 1, self.depth, self.vheight,
-                          self.vwidth, float(self.cfg.lambda_tv), _p(self.g_volume), s)
-            self.grads3d.zero_()
-            _backend.call("r2s_voxel_render_bwd_capacity", d, _p(self.records3), beta_flag, 1, _p(self.offsets3),
-                          _p(self.flatten3_ids), _p(self.n_used3), _p(self.g_volume), None, self.n, self.vwidth,
-                          self.vheight, self.depth, self.cfg.voxel_tile, self.vtx, self.vty, self.vtz,
+            # TV forward and backward in one pass (the TV term enters the loss with weight one).
+            _backend.call("r2s_volume_loss_fwd_bwd", d, _p(self.volume), _p(self.ones), 1, self.depth, self.vheight,
+                          self.vwidth, float(self.cfg.lambda_tv), _p(self.tv_loss), _p(self.tv_value), None,
+                          _p(self.g_volume), _p(self.tv_ws), self.tv_ws.numel(), s)
+            # Deterministic tile VJP: one slot per 3D intersection, summed per primitive in a fixed order.
+            _backend.call("r2s_voxel_render_bwd_slots", d, _p(self.records3), beta_flag, 1, _p(self.offsets3),
+                          _p(self.flatten3_ids), 0, _p(self.n_used3), _p(self.means_v), _p(self.radii3),
+                          _p(self.cum3), _p(self.g_volume), None, self.n, self.vwidth, self.vheight, self.depth,
+                          self.cfg.voxel_tile, self.vtx, self.vty, self.vtz, _p(self.slots3), self.capacity_3d,
                           _p(self.grads3d), s)
             v = self.g_voxel
             _backend.call("r2s_voxel_chain_bwd", d, _p(self.means), _p(self.quats), _p(self.scales), _p(self.covars),
@@ -280,6 +294,32 @@ class FitScene:
             if int(self.overflow.item()) == 0:
                 return
             self.set_capacity(*self.needs_capacity())
+
+    # ------------------------------------------------------------------ snapshot / restore
+    STATE_KEYS = ("means", "quats", "raw_scales", "raw_densities", "raw_beta", "scales", "densities", "beta",
+                  "adam_m", "adam_v", "step_count")
+
+    def state_dict(self) -> dict:
+        """Host copies of everything a fit continues from: the raw parameters, their activations (as the
+        update kernel wrote them, so a restore needs no recomputation that could round differently), the
+        Adam moments and the step counter."""
+        torch.cuda.current_stream(self.device).synchronize()
+        return {k: None if getattr(self, k) is None else getattr(self, k).detach().cpu().clone()
+                for k in self.STATE_KEYS}
+
+    def load_state_dict(self, state: dict):
+        """Copies a ``state_dict`` back in place (the buffers keep their addresses, so a captured graph of
+        this scene stays valid). The scene must have the same primitive count and kind."""
+        for k in self.STATE_KEYS:
+            dst, src = getattr(self, k), state[k]
+            if (dst is None) != (src is None):
+                raise ValueError(f"state {k!r} does not match this scene (Gaussian vs Beta)")
+            if dst is None:
+                continue
+            if tuple(dst.shape) != tuple(src.shape) or dst.dtype != src.dtype:
+                raise ValueError(f"state {k!r} has shape {tuple(src.shape)} {src.dtype}, this scene "
+                                 f"{tuple(dst.shape)} {dst.dtype}")
+            dst.copy_(src, non_blocking=False)
 
 
 class BatchedFit:
@@ -374,7 +414,7 @@ class Autotuner:
 
 def make_synthetic_scene(n: int, cameras: int, side: int, volume: int, *, beta: bool = False, seed: int = 0,
                          tile: int = 16, stage_batch: int = 256, lr: float = 1e-3, device="cuda",
-                         dtype=torch.float32) -> FitScene:
+                         dtype=torch.float32, lean: bool = False) -> FitScene:
     """A seeded reconstruction in the CT benchmark's distributions.
 
     Primitives: scales exp(N(log 0.01, 0.4)). Cameras: an orbit of radius 3 with focal length
@@ -391,7 +431,7 @@ def make_synthetic_scene(n: int, cameras: int, side: int, volume: int, *, beta: 
     target, _ = explicit.rasterize_fwd(shifted, quats, scales, densities, viewmats, Ks, (side, side), beta=b)
     config = SceneConfig(image_size=(side, side), volume_shape=(volume, volume, volume), tile=tile,
                          stage_batch=stage_batch, lr=lr)
-    return FitScene(means, quats, scales, densities, viewmats, Ks, target, config, beta=b)
+    return FitScene(means, quats, scales, densities, viewmats, Ks, target, config, beta=b, lean=lean)
 
 
 __all__ = ["Autotuner", "BatchedFit", "FitScene", "SceneConfig", "make_synthetic_scene"]

@@ -183,6 +183,17 @@ __device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a
 __device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 
+// Scalar multiply that the compiler may not contract into a following add:
+// the per-sample expressions below spell out which products round on their own.
+template <typename S>
+__device__ __forceinline__ S mul_rn(S a, S b) {
+    if constexpr (sizeof(S) == 4) {
+        return __fmul_rn(a, b);
+    } else {
+        return __dmul_rn(a, b);
+    }
+}
+
 // 1.0f when a > b, else 0.0f (also 0.0f when either is NaN), as one PTX set.
 __device__ __forceinline__ float gt_mask(float a, float b) {
     float m;

@@ -9,6 +9,17 @@
 // the same pass (the reference applies lambda in a second torch pass,
 // Loss.cpp:187), keeping the reference's rounding order: the sign sum times
 // g/edges, then times lambda.
+//
+// When the upstream gradient is known before the forward (a fit step: the TV
+// term enters the loss with weight one), tv_fused_kernel does forward and
+// backward in one pass: each thread owns one (y, x) column of a 32 x 8 tile
+// and marches down a chunk of depth slices, keeping the previous, current and
+// next slice's values in registers, taking its x neighbours from the adjacent
+// lanes by shuffle and its y neighbours from the adjacent warps' rows (L1/L2).
+// Each voxel is read from DRAM once; the gradient (and the map, if requested)
+// is written once. The map and gradient values are the two kernels' above bit
+// for bit (same operation order); the loss sums the same fp32 terms in fp64 in
+// another fixed order.
 #include "common.cuh"
 
 namespace r2s {
@@ -76,6 +87,69 @@ __global__ void __launch_bounds__(kLossThreads) tv_fwd_kernel(const S* __restric
             if (x + 1 < W) tv += abs_diff(vol[idx + 1] - val);
             if (tv_map != nullptr) tv_map[idx] = tv;
             sum += static_cast<double>(tv);
+        }
+    }
+    const double total_sum = block_sum(sum);
+    if (threadIdx.x == 0) partials[blockIdx.x] = total_sum;
+}
+
+constexpr uint32_t kTvTileX = 32, kTvTileY = kLossThreads / 32, kTvChunk = 32;
+
+template <typename S, bool kMap>
+__global__ void __launch_bounds__(kLossThreads) tv_fused_kernel(
+    const S* __restrict__ vol, uint32_t D, uint32_t H, uint32_t W, uint32_t tiles_x, uint32_t tiles_y,
+    uint32_t chunks, uint64_t n_tiles, const S* __restrict__ grad_output, int64_t edges, float lambda,
+    S* __restrict__ tv_map, S* __restrict__ grad, double* __restrict__ partials) {
+    const S grad_out = grad_output[0] / static_cast<S>(edges);
+    const S lam = static_cast<S>(lambda);
+    const uint64_t HW = uint64_t(H) * W;
+    const uint32_t lx = threadIdx.x & 31u, ly = threadIdx.x >> 5;
+    double sum = 0;
+    for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+        uint64_t t = tile;
+        const uint32_t tx = uint32_t(t % tiles_x);
+        t /= tiles_x;
+        const uint32_t ty = uint32_t(t % tiles_y);
+        t /= tiles_y;
+        const uint32_t chunk = uint32_t(t % chunks);
+        const uint64_t b = t / chunks;
+        const uint32_t x = tx * kTvTileX + lx, y = ty * kTvTileY + ly;
+        const uint32_t d0 = chunk * kTvChunk, d1 = min(D, d0 + kTvChunk);
+        const bool active = x < W && y < H;
+        const uint64_t column = b * D * HW + uint64_t(y) * W + x;
+        S prev = S(0), cur = S(0), next = S(0);
+        if (active) {
+            cur = vol[column + uint64_t(d0) * HW];
+            if (d0 > 0) prev = vol[column + uint64_t(d0 - 1) * HW];
+        }
+        for (uint32_t d = d0; d < d1; ++d) {
+            const uint64_t idx = column + uint64_t(d) * HW;
+            if (active && d + 1 < D) next = vol[idx + HW];
+            // Inactive lanes hold 0; a lane reads a neighbour's value only when that neighbour is inside.
+            S xp = __shfl_down_sync(0xffffffffu, cur, 1);
+            S xm = __shfl_up_sync(0xffffffffu, cur, 1);
+            if (active) {
+                if (lx == 31u && x + 1 < W) xp = vol[idx + 1];
+                if (lx == 0u && x > 0) xm = vol[idx - 1];
+                const S yp = y + 1 < H ? vol[idx + W] : S(0);
+                const S ym = y > 0 ? vol[idx - W] : S(0);
+                S tv = 0;
+                if (d + 1 < D) tv += abs_diff(next - cur);
+                if (y + 1 < H) tv += abs_diff(yp - cur);
+                if (x + 1 < W) tv += abs_diff(xp - cur);
+                S g = 0;
+                if (d + 1 < D) g -= sign_of(next - cur);
+                if (d > 0) g += sign_of(cur - prev);
+                if (y + 1 < H) g -= sign_of(yp - cur);
+                if (y > 0) g += sign_of(cur - ym);
+                if (x + 1 < W) g -= sign_of(xp - cur);
+                if (x > 0) g += sign_of(cur - xm);
+                if (kMap) tv_map[idx] = tv;
+                grad[idx] = (g * grad_out) * lam;
+                sum += static_cast<double>(tv);
+            }
+            prev = cur;
+            cur = next;
         }
     }
     const double total_sum = block_sum(sum);
@@ -219,6 +293,45 @@ int r2s_volume_loss_bwd(int dtype, const void* volume, const void* grad_output, 
             static_cast<const S*>(volume), static_cast<const S*>(grad_output), D, H, W, rows, edges, lambda_tv,
             static_cast<S*>(grad_volume));
         return check_launch("volume_loss_bwd");
+    });
+}
+
+int r2s_volume_loss_fwd_bwd(int dtype, const void* volume, const void* grad_output, uint32_t B, uint32_t D,
+                            uint32_t H, uint32_t W, float lambda_tv, void* loss, void* tv, void* tv_map,
+                            void* grad_volume, void* workspace, size_t workspace_bytes, void* stream) {
+    const int64_t total = int64_t(B) * D * H * W;
+    const int64_t edges_raw = int64_t(B) * ((int64_t(D) - 1) * H * W + int64_t(D) * (H - 1) * W +
+                                            int64_t(D) * H * (int64_t(W) - 1));
+    const int64_t edges = edges_raw > 1 ? edges_raw : 1;
+    R2S_REQUIRE(grad_output != nullptr && grad_volume != nullptr, R2S_ERR_ARGUMENT,
+                "grad_output and grad_volume must be non-null");
+    const uint32_t tiles_x = (W + kTvTileX - 1) / kTvTileX, tiles_y = (H + kTvTileY - 1) / kTvTileY;
+    const uint32_t chunks = (D + kTvChunk - 1) / kTvChunk;
+    const uint64_t n_tiles = uint64_t(B) * chunks * tiles_y * tiles_x;
+    const unsigned blocks = unsigned(n_tiles < uint64_t(kLossMaxBlocks) ? (n_tiles > 0 ? n_tiles : 1)
+                                                                        : uint64_t(kLossMaxBlocks));
+    Arena arena(workspace, workspace_bytes);
+    double* partials = arena.take<double>(blocks);
+    R2S_REQUIRE(partials, R2S_ERR_WORKSPACE, "loss workspace too small");
+    cudaStream_t st = as_stream(stream);
+    R2S_DISPATCH(dtype, {
+        if (total > 0) {
+            if (tv_map != nullptr) {
+                tv_fused_kernel<S, true><<<blocks, kLossThreads, 0, st>>>(
+                    static_cast<const S*>(volume), D, H, W, tiles_x, tiles_y, chunks, n_tiles,
+                    static_cast<const S*>(grad_output), edges, lambda_tv, static_cast<S*>(tv_map),
+                    static_cast<S*>(grad_volume), partials);
+            } else {
+                tv_fused_kernel<S, false><<<blocks, kLossThreads, 0, st>>>(
+                    static_cast<const S*>(volume), D, H, W, tiles_x, tiles_y, chunks, n_tiles,
+                    static_cast<const S*>(grad_output), edges, lambda_tv, nullptr, static_cast<S*>(grad_volume),
+                    partials);
+            }
+            R2S_TRY(check_launch("volume_loss_fwd_bwd"));
+        }
+        finish_mean_kernel<S><<<1, kLossThreads, 0, st>>>(partials, total > 0 ? int(blocks) : 0, edges, lambda_tv,
+                                                         static_cast<S*>(loss), static_cast<S*>(tv));
+        return check_launch("volume_loss_finish");
     });
 }
 

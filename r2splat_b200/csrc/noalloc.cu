@@ -13,7 +13,11 @@
 // calls that overlap in time (on different streams or host threads) race on it
 // and must be serialised by the caller. The first call on a device resolves the
 // array's address with cudaGetSymbolAddress (which may load the module); make
-// that first call before any stream capture on the device.
+// that first call before any stream capture on the device. The address is
+// cached per device ordinal for the life of the process: after a
+// cudaDeviceReset (or any other teardown of the device's primary context) the
+// cached address would be stale, so this entry point does not support a reset
+// of a device it has already been called on.
 #include <mutex>
 
 #include "scan.cuh"

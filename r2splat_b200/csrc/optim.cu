@@ -6,8 +6,19 @@
 // multiplied by the activation derivatives, then torch.optim.Adam). Here one
 // thread per primitive does all of it: sums the two VJPs, applies the
 // activation derivatives (exp for scales and beta, sigmoid for densities), runs
-// the Adam update in torch.optim.Adam's order of operations (no weight decay,
-// no amsgrad), and writes the activated physical parameters for the next step.
+// the Adam update (no weight decay, no amsgrad), and writes the activated
+// physical parameters for the next step.
+//
+// The update follows the operations torch.optim.Adam issues per element:
+// m.lerp_(g, 1 - beta1), i.e. m + (1 - beta1) (g - m) for a weight below 1/2;
+// v.mul_(beta2).addcmul_(g, g, 1 - beta2); the bias corrections, step size and
+// sqrt of the second correction in double precision on the host side of torch
+// (here in double in the kernel), then rounded to the parameter type;
+// denom = sqrt(v) / sqrt(bias2) + eps; p.addcdiv_(m, denom, -step_size).
+// Division and square root are the correctly rounded ones, as in torch's
+// kernels, although this library otherwise builds with fast math. The
+// activation derivatives (exp, sigmoid) use the fast-math functions, so the
+// result agrees with torch to rounding, not bit for bit.
 // The step counter lives on the device so the update can be captured in a
 // CUDA graph; a nonzero skip flag (an intersection-capacity overflow of this
 // step) turns the whole update, counter included, into a no-op.
@@ -43,15 +54,36 @@ __device__ __forceinline__ S sigmoid(S x) {
 }
 
 template <typename S>
-__global__ void adam_kernel(AdamParams<S> p, uint32_t N, S lr, S beta1, S beta2, S eps,
+__device__ __forceinline__ S div_rn(S a, S b) {
+    if constexpr (sizeof(S) == 4) {
+        return __fdiv_rn(a, b);
+    } else {
+        return __ddiv_rn(a, b);
+    }
+}
+
+template <typename S>
+__device__ __forceinline__ S sqrt_rn(S a) {
+    if constexpr (sizeof(S) == 4) {
+        return __fsqrt_rn(a);
+    } else {
+        return __dsqrt_rn(a);
+    }
+}
+
+template <typename S>
+__global__ void adam_kernel(AdamParams<S> p, uint32_t N, double lr, double beta1, double beta2, double eps,
                             const int32_t* __restrict__ step, const uint32_t* __restrict__ skip) {
     const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= N) return;
     if (skip != nullptr && *skip != 0u) return;
-    const int32_t t = *step + 1;
-    const S bias1 = S(1) - pow(beta1, static_cast<S>(t));
-    const S bias2_sqrt = sqrt(S(1) - pow(beta2, static_cast<S>(t)));
-    const S step_size = lr / bias1;
+    const double t = static_cast<double>(*step + 1);
+    const S step_size = static_cast<S>(lr / (1.0 - pow(beta1, t)));
+    const S bias2_sqrt = static_cast<S>(sqrt(1.0 - pow(beta2, t)));
+    const S w1 = static_cast<S>(1.0 - beta1);
+    const S w2 = static_cast<S>(1.0 - beta2);
+    const S b2 = static_cast<S>(beta2);
+    const S e = static_cast<S>(eps);
     const bool has_beta = p.raw_beta != nullptr;
 
     S* raw[12];
@@ -85,12 +117,13 @@ __global__ void adam_kernel(AdamParams<S> p, uint32_t N, S lr, S beta1, S beta2,
     for (int i = 0; i < k; ++i) {
         const size_t mi = 12 * size_t(n) + i;
         const S g = grad[i];
-        const S m = p.m[mi] * beta1 + g * (S(1) - beta1);
-        const S v = p.v[mi] * beta2 + g * g * (S(1) - beta2);
+        const S m_old = p.m[mi];
+        const S m = fma(w1, g - m_old, m_old);
+        const S v = fma(w2 * g, g, p.v[mi] * b2);
         p.m[mi] = m;
         p.v[mi] = v;
-        const S denom = sqrt(v) / bias2_sqrt + eps;
-        *raw[i] -= step_size * (m / denom);
+        const S denom = div_rn(sqrt_rn(v), bias2_sqrt) + e;
+        *raw[i] = fma(-step_size, div_rn(m, denom), *raw[i]);
     }
     for (int c = 0; c < 3; ++c) p.scales[3 * size_t(n) + c] = exp(p.raw_scales[3 * size_t(n) + c]);
     p.densities[n] = softplus(p.raw_densities[n]);
@@ -131,7 +164,7 @@ int r2s_adam_activation_step(int dtype, uint32_t N, void* means, void* quats, vo
                 p.g1[i] = static_cast<const S*>(grads_a[i]);
                 p.g2[i] = grads_b != nullptr ? static_cast<const S*>(grads_b[i]) : nullptr;
             }
-            adam_kernel<S><<<blocks_for(N, 256), 256, 0, st>>>(p, N, S(lr), S(beta1), S(beta2), S(eps), step, skip);
+            adam_kernel<S><<<blocks_for(N, 256), 256, 0, st>>>(p, N, lr, beta1, beta2, eps, step, skip);
         });
         R2S_TRY(check_launch("adam_activation_step"));
     }

@@ -664,8 +664,10 @@ __global__ void __launch_bounds__(kBwdThreads) raster_bwd_kernel(
     };
     load(0, 0);
     for (int32_t bi = 0; bi < n_batches; ++bi) {
+        // Double-buffered: batch bi + 1 loads into the stage that batch bi - 1 used, which every warp
+        // finished before the barrier that ended the previous iteration.
         if (bi + 1 < n_batches) {
-            load(bi + 1, uint32_t(bi + 1) % 3u);
+            load(bi + 1, uint32_t(bi + 1) & 1u);
             cp_async_wait<1>();
         } else {
             cp_async_wait<0>();

@@ -16,6 +16,7 @@
 #include <type_traits>
 
 #include "common.cuh"
+#include "geometry.cuh"
 
 namespace r2s {
 
@@ -117,13 +118,14 @@ __global__ void __launch_bounds__(256) voxel_fwd_kernel(const Rec3D<S>* __restri
         for (int32_t s = 0; s < batch; ++s) {
             const Rec3D<S> r = buf[s];
             if constexpr (kRowShared) {
-                // The reference's sigma with its contraction made explicit
-                // (nvcc -O3 --use_fast_math fuses the first product of each
-                // sum): S3 = fma(c22 d3, d3, fma(c00 d1, d1, (c11 d2) d2)),
-                // sigma = fma(c12 d2, d3, fma(c02 d1, d3, fma(1/2, S3,
-                // (c01 d1) d2))). The d2/d3 factors are shared by the row, and the
-                // four voxels go two at a time through packed FP32x2 operations,
-                // each component rounding as the scalar operation does.
+                // The reference's sigma with its contraction made explicit, as
+                // nvcc -O3 --use_fast_math compiles the reference's kernel
+                // (VoxelizeToVoxelsFwd.cu:200-205): S3 = fma(c22 d3, d3,
+                // fma(c00 d1, d1, (c11 d2) d2)), then sigma = fma(c12 d2, d3,
+                // fma(c02 d1, d3, fma(c01 d1, d2, S3 / 2))). The d2/d3 factors are
+                // shared by the row, and the four voxels go two at a time through
+                // packed FP32x2 operations, each component rounding as the scalar
+                // operation does.
                 const float d2 = py[0] - r.y, d3 = pz[0] - r.z;
                 const float b2 = __fmul_rn(__fmul_rn(r.c11, d2), d2);
                 const float c22d3 = __fmul_rn(r.c22, d3), c12d2 = __fmul_rn(r.c12, d2);
@@ -134,17 +136,17 @@ __global__ void __launch_bounds__(256) voxel_fwd_kernel(const Rec3D<S>* __restri
                 for (int k = 0; k < PPT; k += 2) {
                     const float2 d1 = add2(make_float2(px[k], px[k + 1]), nx);
                     const float2 s3 = fma2(c22d32, d32, fma2(mul2(c00, d1), d1, b22));
-                    const float2 la = fma2(half, s3, mul2(mul2(c01, d1), d22));
+                    const float2 la = fma2(mul2(c01, d1), d22, mul2(half, s3));
                     const float2 sigma = fma2(c12d22, d32, fma2(mul2(c02, d1), d32, la));
                     const float alpha0 = r.o * exp(-sigma.x);
                     const float alpha1 = r.o * exp(-sigma.y);
                     if (!(sigma.x < 0.f || fabs(alpha0) < 1e-6f)) {
                         acc[k] += alpha0;
-                        if (kVar) accv[k] += r.q * alpha0 * alpha0;
+                        if (kVar) accv[k] = fmaf(__fmul_rn(r.q, alpha0), alpha0, accv[k]);
                     }
                     if (!(sigma.y < 0.f || fabs(alpha1) < 1e-6f)) {
                         acc[k + 1] += alpha1;
-                        if (kVar) accv[k + 1] += r.q * alpha1 * alpha1;
+                        if (kVar) accv[k + 1] = fmaf(__fmul_rn(r.q, alpha1), alpha1, accv[k + 1]);
                     }
                 }
                 continue;
@@ -152,25 +154,32 @@ __global__ void __launch_bounds__(256) voxel_fwd_kernel(const Rec3D<S>* __restri
 #pragma unroll
             for (int k = 0; k < PPT; ++k) {
                 if (!kBeta) {
+                    // Same contraction as above (VoxelizeToVoxelsFwd.cu:200-205, :390-396).
                     const S d1 = px[k] - r.x, d2 = py[k] - r.y, d3 = pz[k] - r.z;
-                    const S sigma = static_cast<S>(0.5) * (r.c00 * d1 * d1 + r.c11 * d2 * d2 + r.c22 * d3 * d3) +
-                                    r.c01 * d1 * d2 + r.c02 * d1 * d3 + r.c12 * d2 * d3;
+                    const S s3 = fma(mul_rn(r.c22, d3), d3, fma(mul_rn(r.c00, d1), d1, mul_rn(mul_rn(r.c11, d2), d2)));
+                    const S sigma = fma(mul_rn(r.c12, d2), d3,
+                                        fma(mul_rn(r.c02, d1), d3,
+                                            fma(mul_rn(r.c01, d1), d2, mul_rn(static_cast<S>(0.5), s3))));
                     const S alpha = r.o * exp(-sigma);
                     if (!(sigma < static_cast<S>(0) || fabs(alpha) < static_cast<S>(1e-6))) {
                         acc[k] += alpha;
-                        if (kVar) accv[k] += r.q * alpha * alpha;
+                        if (kVar) accv[k] = fma(mul_rn(r.q, alpha), alpha, accv[k]);
                     }
                 } else {
+                    // The reference's d^T Q d (VoxelizeToVoxelsFwd.cu:563-567) with its contraction
+                    // explicit: s = fma(c d3, d3, fma(a d1, d1, (bb d2) d2)), then
+                    // q = fma((2 r) d2, d3, fma((2 q) d1, d3, fma((2 p) d1, d2, s))).
                     const S d1 = r.x - px[k], d2 = r.y - py[k], d3 = r.z - pz[k];
-                    const S qf = r.c00 * d1 * d1 + r.c11 * d2 * d2 + r.c22 * d3 * d3 +
-                                 static_cast<S>(2) * r.c01 * d1 * d2 + static_cast<S>(2) * r.c02 * d1 * d3 +
-                                 static_cast<S>(2) * r.c12 * d2 * d3;
+                    const S two = static_cast<S>(2);
+                    const S sq = fma(mul_rn(r.c22, d3), d3, fma(mul_rn(r.c00, d1), d1, mul_rn(mul_rn(r.c11, d2), d2)));
+                    const S qf = fma(mul_rn(mul_rn(two, r.c12), d2), d3,
+                                     fma(mul_rn(mul_rn(two, r.c02), d1), d3, fma(mul_rn(mul_rn(two, r.c01), d1), d2, sq)));
                     if (!(qf < static_cast<S>(0) || qf >= static_cast<S>(1))) {
                         const S h = static_cast<S>(1) - qf;
                         const S alpha = r.o * pow(h, r.beta);
                         if (!(fabs(alpha) < static_cast<S>(1e-5))) {
                             acc[k] += alpha;
-                            if (kVar) accv[k] += r.q * alpha * alpha;
+                            if (kVar) accv[k] = fma(mul_rn(r.q, alpha), alpha, accv[k]);
                         }
                     }
                 }
@@ -210,11 +219,13 @@ struct alignas(16) VoxelBox {
 // 1.001. Half-widths are widened by 0.1 % + 0.01 voxel and by 1e-6 of the
 // coordinates' magnitude; any other case takes the whole tile.
 template <typename S, bool kBeta>
-__device__ __forceinline__ VoxelBox voxel_box(const Rec3D<S>& r, uint32_t ox, uint32_t oy, uint32_t oz, uint32_t vx,
-                                              uint32_t vy, uint32_t vz) {
-    uint32_t lo[3] = {0u, 0u, 0u};
-    uint32_t hi[3] = {vx - 1, vy - 1, vz - 1};
-    const VoxelBox empty{0u, 0u, 1u, 0u};
+__device__ __forceinline__ bool voxel_box_bounds(const Rec3D<S>& r, uint32_t ox, uint32_t oy, uint32_t oz,
+                                                 uint32_t vx, uint32_t vy, uint32_t vz, uint32_t* lo,
+                                                 uint32_t* hi) {
+    lo[0] = lo[1] = lo[2] = 0u;
+    hi[0] = vx - 1;
+    hi[1] = vy - 1;
+    hi[2] = vz - 1;
     const S a = r.c00, p = r.c01, q = r.c02, bb = r.c11, rr = r.c12, c = r.c22;
     const S adj0 = bb * c - rr * rr;
     const S adj1 = a * c - q * q;
@@ -227,7 +238,7 @@ __device__ __forceinline__ VoxelBox voxel_box(const Rec3D<S>& r, uint32_t ox, ui
     if (!kBeta) {
         S s = log(fabs(r.o)) + S(13.815510557964274);  // ln(1e6)
         s = s + S(1e-3) * fabs(s) + S(1e-3);
-        if (bounded && isfinite(s) && s < S(0)) return empty;
+        if (bounded && isfinite(s) && s < S(0)) return false;
         bounded = bounded && isfinite(s);
         reach = S(2) * s;
     }
@@ -242,12 +253,20 @@ __device__ __forceinline__ VoxelBox voxel_box(const Rec3D<S>& r, uint32_t ox, ui
             const S m = S(1e-6) * (fabs(centre[axis]) + h + static_cast<S>(origin[axis]));
             const S l = ceil(cc - h - m), u = floor(cc + h + m);
             if (!(isfinite(l) && isfinite(u))) continue;
-            if (u < S(0) || l > static_cast<S>(hi[axis])) return empty;
+            if (u < S(0) || l > static_cast<S>(hi[axis])) return false;
             if (l > S(0)) lo[axis] = static_cast<uint32_t>(l);
             if (u < static_cast<S>(hi[axis])) hi[axis] = static_cast<uint32_t>(u);
-            if (lo[axis] > hi[axis]) return empty;
+            if (lo[axis] > hi[axis]) return false;
         }
     }
+    return true;
+}
+
+template <typename S, bool kBeta>
+__device__ __forceinline__ VoxelBox voxel_box(const Rec3D<S>& r, uint32_t ox, uint32_t oy, uint32_t oz, uint32_t vx,
+                                              uint32_t vy, uint32_t vz) {
+    uint32_t lo[3], hi[3];
+    if (!voxel_box_bounds<S, kBeta>(r, ox, oy, oz, vx, vy, vz, lo, hi)) return VoxelBox{0u, 0u, 1u, 0u};
     const uint32_t w = hi[0] - lo[0] + 1, h = hi[1] - lo[1] + 1, d = hi[2] - lo[2] + 1;
     VoxelBox box;
     box.origin = lo[0] | (lo[1] << 8) | (lo[2] << 16);
@@ -256,6 +275,38 @@ __device__ __forceinline__ VoxelBox voxel_box(const Rec3D<S>& r, uint32_t ox, ui
     box.unused = 0u;
     return box;
 }
+
+// A primitive's 3D tile box as the intersection lists enumerate it (the tile
+// span of IsectTiles3DKernel.cu:38-112 on the voxel-space mean and radii):
+// [lo, hi) per axis; false when it has no tiles.
+template <typename S>
+__device__ __forceinline__ bool tile_box_3d(const S* means_v, const int32_t* radii, uint32_t n, uint32_t T,
+                                            uint32_t tiles_x, uint32_t tiles_y, uint32_t tiles_z, uint32_t* lo,
+                                            uint32_t* hi) {
+    const int32_t rx = radii[3 * size_t(n)], ry = radii[3 * size_t(n) + 1], rz = radii[3 * size_t(n) + 2];
+    if (rx <= 0 || ry <= 0 || rz <= 0) return false;
+    tile_span(means_v[3 * size_t(n)], static_cast<S>(rx), T, tiles_x, lo[0], hi[0]);
+    tile_span(means_v[3 * size_t(n) + 1], static_cast<S>(ry), T, tiles_y, lo[1], hi[1]);
+    tile_span(means_v[3 * size_t(n) + 2], static_cast<S>(rz), T, tiles_z, lo[2], hi[2]);
+    return hi[0] > lo[0] && hi[1] > lo[1] && hi[2] > lo[2];
+}
+
+// Deterministic output of the tile VJP: instead of adding a (tile, primitive)
+// pair's 12 sums into the primitive's adjoints with atomics, the pair writes
+// them to a slot of its own, slot = cum[n - 1] + the tile's index in the
+// primitive's tile box (z, then y, then x), and voxel_slot_reduce_kernel adds
+// each primitive's slots in that order. cum is the inclusive scan of the
+// per-primitive tile counts, so the slots of the primitives are consecutive;
+// slots past `capacity` (an overflowing capacity-bounded step, which is
+// discarded) are not written.
+template <typename S>
+struct VoxelSlots {
+    const S* means_v = nullptr;
+    const int32_t* radii = nullptr;
+    const int64_t* cum = nullptr;
+    S* slots = nullptr;  // [capacity][12]; null: accumulate into grads with atomics
+    uint64_t capacity = 0;
+};
 
 // Null-pointer conventions as in the rasterizer VJP: v_volume null = zero
 // adjoint; v_volume_var null = no variance branch; chain_var false =
@@ -287,7 +338,7 @@ template <typename S, bool kBeta, bool kVar>
 __global__ void __launch_bounds__(kVoxBwdThreads) voxel_bwd_kernel(
     const Rec3D<S>* __restrict__ records, bool chain_var, const int32_t* __restrict__ offsets,
     const int32_t* __restrict__ flatten_ids, VoxelGeom g, const S* __restrict__ v_volume,
-    const S* __restrict__ v_volume_var, Rec3D<S>* __restrict__ grads) {
+    const S* __restrict__ v_volume_var, Rec3D<S>* __restrict__ grads, VoxelSlots<S> sl) {
     extern __shared__ __align__(16) unsigned char smem[];
     const uint32_t T = g.T;
     const uint32_t tile_voxels = T * T * T;
@@ -300,6 +351,7 @@ __global__ void __launch_bounds__(kVoxBwdThreads) voxel_bwd_kernel(
     S* s_v = reinterpret_cast<S*>(s_box + kVoxBwdThreads);                         // [T^2][T+1] adjoint
     S* s_vv = s_v + tile_slots;                                                    // [T^2][T+1] variance adjoint
     int32_t* s_id = reinterpret_cast<int32_t*>(s_vv + tile_slots);                 // [2][threads]
+    uint32_t* s_slot = reinterpret_cast<uint32_t*>(s_id + 2 * kVoxBwdThreads);    // [2][threads] (slot output)
 
     const uint32_t n_tiles = g.tiles_x * g.tiles_y * g.tiles_z;
     const uint32_t key = blockIdx.x;
@@ -340,6 +392,18 @@ __global__ void __launch_bounds__(kVoxBwdThreads) voxel_bwd_kernel(
             const int32_t gid = flatten_ids[idx];
             gather_record3(s_rec + stage * kVoxBwdThreads + t, records + gid);
             s_id[stage * kVoxBwdThreads + t] = gid;
+            if (sl.slots != nullptr) {
+                // The pair's slot, found while the previous batch is walked (slots fit 31 bits).
+                uint32_t slot = 0xffffffffu;
+                uint32_t blo[3], bhi[3];
+                if (tile_box_3d(sl.means_v, sl.radii, uint32_t(gid), T, g.tiles_x, g.tiles_y, g.tiles_z, blo, bhi)) {
+                    const uint64_t local = (uint64_t(tz - blo[2]) * (bhi[1] - blo[1]) + (ty - blo[1])) *
+                                               (bhi[0] - blo[0]) + (tx - blo[0]);
+                    const uint64_t j = (gid > 0 ? uint64_t(sl.cum[gid - 1]) : 0u) + local;
+                    if (j < sl.capacity) slot = uint32_t(j);
+                }
+                s_slot[stage * kVoxBwdThreads + t] = slot;
+            }
         }
         cp_async_commit();
     };
@@ -360,10 +424,18 @@ __global__ void __launch_bounds__(kVoxBwdThreads) voxel_bwd_kernel(
             const VoxelBox box = s_box[s];
             const uint32_t w = box.extent & 0xffu, h = (box.extent >> 8) & 0xffu, d = (box.extent >> 16) & 0xffu;
             const uint32_t rows = h * d;
-            if (rows * w == 0u) continue;
+            const int32_t gid = s_id[stage * kVoxBwdThreads + s];
+            // This pair's slot (deterministic output), written by the leaders of lane groups 0..2.
+            const uint32_t slot = sl.slots != nullptr ? s_slot[stage * kVoxBwdThreads + s] : 0xffffffffu;
+            if (rows * w == 0u) {
+                if (slot != 0xffffffffu && (lane & 7u) == 0u && (lane >> 3) < 3u) {
+                    S* out = sl.slots + size_t(slot) * 12u + 4u * (lane >> 3);
+                    out[0] = out[1] = out[2] = out[3] = S(0);
+                }
+                continue;
+            }
             const uint32_t x0 = box.origin & 0xffu, y0 = (box.origin >> 8) & 0xffu, z0 = (box.origin >> 16) & 0xffu;
             const Rec3D<S> r = s_rec[stage * kVoxBwdThreads + s];
-            const int32_t gid = s_id[stage * kVoxBwdThreads + s];
             const S a = r.c00, p = r.c01, q = r.c02, bb = r.c11, rr = r.c12, c = r.c22;
             const S opac = r.o;
             const S uq = chain_var ? r.q : S(0);
@@ -543,11 +615,392 @@ __global__ void __launch_bounds__(kVoxBwdThreads) voxel_bwd_kernel(
                     e2 = w4[2];
                     e3 = w4[3];
                 }
-                red_add_v4(reinterpret_cast<S*>(grads + gid) + 4 * grp, e0, e1, e2, e3);
+                if (sl.slots == nullptr) {
+                    red_add_v4(reinterpret_cast<S*>(grads + gid) + 4 * grp, e0, e1, e2, e3);
+                } else if (slot != 0xffffffffu && grp < 3u) {
+                    S* out = sl.slots + size_t(slot) * 12u + 4u * grp;
+                    out[0] = e0;
+                    out[1] = e1;
+                    out[2] = e2;
+                    out[3] = e3;
+                }
             }
         }
         __syncthreads();
     }
+}
+
+// grads[n] = the sum of primitive n's slots in order (12 sums), zero pads.
+template <typename S>
+__global__ void voxel_slot_reduce_kernel(const S* __restrict__ slots, const int64_t* __restrict__ cum, uint32_t N,
+                                         int64_t capacity, Rec3D<S>* __restrict__ grads) {
+    const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    const int64_t first = n == 0u ? 0 : min(cum[n - 1], capacity), last = min(cum[n], capacity);
+    S acc[12];
+#pragma unroll
+    for (int i = 0; i < 12; ++i) acc[i] = S(0);
+    for (int64_t j = first; j < last; ++j) {
+        if constexpr (sizeof(S) == 4) {
+            // A slot is 48 bytes, 16-byte aligned: three vector loads.
+            const float4* p = reinterpret_cast<const float4*>(slots + size_t(j) * 12u);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const float4 v = __ldg(p + k);
+                acc[4 * k] += v.x;
+                acc[4 * k + 1] += v.y;
+                acc[4 * k + 2] += v.z;
+                acc[4 * k + 3] += v.w;
+            }
+        } else {
+            const S* p = slots + size_t(j) * 12u;
+#pragma unroll
+            for (int i = 0; i < 12; ++i) acc[i] += p[i];
+        }
+    }
+    S* out = reinterpret_cast<S*>(grads + n);
+#pragma unroll
+    for (int i = 0; i < 12; ++i) out[i] = acc[i];
+#pragma unroll
+    for (int i = 12; i < 16; ++i) out[i] = S(0);
+}
+
+// ---------------------------------------------------------------------------
+// Record-parallel voxel VJP (the explicit path).
+//
+// The reference's VJP is tile-parallel with atomics (VoxelizeToVoxelsBwd.cu:
+// 322-514): every (tile, primitive) pair of the sorted lists adds its sums into
+// the primitive's adjoints. Here the work is split by primitive instead: a
+// work item is one primitive and one z-layer of its tile box (the box of
+// tiles its list entries cover: the tile span of IsectTiles3DKernel.cu:38-112,
+// one layer = tile_size voxel slices), and one warp walks the item's voxels of
+// the primitive's conservative box, reading the volume adjoint from global
+// memory (L2). Items of a primitive are numbered consecutively (an inclusive
+// scan of the per-primitive layer counts), each writes its 12 sums to its own
+// slot, and voxel_record_reduce_kernel adds a primitive's slots in layer
+// order. No atomics, no sorted lists, and the result is the same bit for bit
+// on every run and in every batch. The evaluated samples are the reference's:
+// the union of a primitive's tiles is its tile box, and every sample outside
+// the conservative box fails the contribution test.
+// ---------------------------------------------------------------------------
+
+struct VoxelRecordGeom {
+    uint32_t N, dim2, dim1, dim0, T, tiles_x, tiles_y, tiles_z;
+    uint64_t n_items;                 // item count, or the capacity when n_items_dev is set
+    const int64_t* n_items_dev;       // device-side item count (capacity-bounded launches), or null
+};
+
+// Layers of a primitive's 3D tile box (0 when it has no tiles).
+template <typename S>
+__device__ __forceinline__ uint32_t record_tile_box(const S* means_v, const int32_t* radii, uint32_t n,
+                                                    const VoxelRecordGeom& g, uint32_t* lo, uint32_t* hi) {
+    const int32_t rx = radii[3 * size_t(n)], ry = radii[3 * size_t(n) + 1], rz = radii[3 * size_t(n) + 2];
+    if (rx <= 0 || ry <= 0 || rz <= 0) return 0u;
+    tile_span(means_v[3 * size_t(n)], static_cast<S>(rx), g.T, g.tiles_x, lo[0], hi[0]);
+    tile_span(means_v[3 * size_t(n) + 1], static_cast<S>(ry), g.T, g.tiles_y, lo[1], hi[1]);
+    tile_span(means_v[3 * size_t(n) + 2], static_cast<S>(rz), g.T, g.tiles_z, lo[2], hi[2]);
+    if (!(hi[0] > lo[0] && hi[1] > lo[1] && hi[2] > lo[2])) return 0u;
+    return hi[2] - lo[2];
+}
+
+template <typename S>
+__global__ void voxel_layer_count_kernel(const S* __restrict__ means_v, const int32_t* __restrict__ radii,
+                                         VoxelRecordGeom g, int32_t* __restrict__ layers) {
+    const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= g.N) return;
+    uint32_t lo[3], hi[3];
+    layers[n] = static_cast<int32_t>(record_tile_box(means_v, radii, n, g, lo, hi));
+}
+
+// Rows of an item are walked 32 at a time (one per lane) in chunks of up to 32
+// voxels along x. Each chunk's adjoints are first copied by the warp from
+// global memory into a per-warp shared tile [32 rows][33] with coalesced loads
+// (one row's chunk per load instruction), then each lane walks its row from
+// shared memory as the tile kernel does. Unloaded slots (past the chunk, idle
+// rows) hold zero adjoints.
+constexpr uint32_t kRecChunk = 32u, kRecStride = kRecChunk + 1u;
+
+template <typename S, bool kBeta, bool kVar>
+__global__ void __launch_bounds__(kVoxBwdThreads) voxel_record_bwd_kernel(
+    const Rec3D<S>* __restrict__ records, const S* __restrict__ means_v, const int32_t* __restrict__ radii,
+    const int64_t* __restrict__ item_cum, bool chain_var, VoxelRecordGeom g, const S* __restrict__ v_volume,
+    const S* __restrict__ v_volume_var, Rec3D<S>* __restrict__ partials) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    S* s_v = reinterpret_cast<S*>(smem) + size_t(warp) * 32u * kRecStride * (kVar ? 2u : 1u);
+    S* s_vv = s_v + 32u * kRecStride;  // used with the variance branch only
+    uint64_t n_items = g.n_items;
+    if (g.n_items_dev != nullptr) {
+        const uint64_t used = uint64_t(*g.n_items_dev);
+        n_items = used < n_items ? used : n_items;  // past the capacity the step is flagged and skipped
+    }
+    // Each warp takes a contiguous run of items, so it finds its first primitive once by binary search
+    // and then steps through the primitives in order.
+    const uint64_t warps = uint64_t(gridDim.x) * kVoxBwdWarps;
+    const uint64_t gw = uint64_t(blockIdx.x) * kVoxBwdWarps + warp;
+    const uint64_t per = (n_items + warps - 1) / warps;
+    const uint64_t i0 = gw * per, i1 = min(n_items, i0 + per);
+    if (i0 >= i1) return;
+    uint32_t n;
+    {
+        uint32_t lo_n = 0u, hi_n = g.N;
+        while (lo_n < hi_n) {
+            const uint32_t mid = (lo_n + hi_n) >> 1;
+            if (uint64_t(item_cum[mid]) > i0) hi_n = mid; else lo_n = mid + 1u;
+        }
+        n = lo_n;
+    }
+    constexpr bool kPackedRow = std::is_same<S, float>::value && !kBeta && !kVar;
+    const uint32_t T = g.T;
+    const bool has_v = v_volume != nullptr;
+    for (uint64_t item = i0; item < i1; ++item) {
+        while (n < g.N && uint64_t(item_cum[n]) <= item) ++n;  // warp-uniform
+        if (n >= g.N) break;                                    // cannot happen while n_items <= item_cum[N - 1]
+        S part[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) part[i] = S(0);
+        const Rec3D<S> r = records[n];
+        uint32_t tlo[3], thi[3];
+        const uint32_t layers = record_tile_box(means_v, radii, n, g, tlo, thi);
+        const uint64_t first = n == 0u ? 0u : uint64_t(item_cum[n - 1]);
+        uint32_t blo[3], bhi[3];
+        bool any = layers > 0u && item - first < layers;
+        uint32_t ox = 0u, oy = 0u, oz = 0u;
+        if (any) {
+            const uint32_t layer = tlo[2] + uint32_t(item - first);
+            ox = tlo[0] * T;
+            oy = tlo[1] * T;
+            oz = layer * T;
+            const uint32_t vx = min(thi[0] * T, g.dim2) - ox;
+            const uint32_t vy = min(thi[1] * T, g.dim1) - oy;
+            const uint32_t vz = min(oz + T, g.dim0) - oz;
+            any = voxel_box_bounds<S, kBeta>(r, ox, oy, oz, vx, vy, vz, blo, bhi);
+        }
+        if (any) {
+            const uint32_t x0 = blo[0], y0 = blo[1], z0 = blo[2];
+            const uint32_t w = bhi[0] - x0 + 1u, h = bhi[1] - y0 + 1u, d = bhi[2] - z0 + 1u;
+            const uint32_t rows = h * d;
+            const S a = r.c00, p = r.c01, q = r.c02, bb = r.c11, rr = r.c12, c = r.c22;
+            const S opac = r.o;
+            const S uq = chain_var ? r.q : S(0);
+            const S half_a = static_cast<S>(0.5) * a;
+            float e_min = 0.f;
+            if constexpr (kPackedRow) e_min = log2f(1e-6f / fabsf(opac));
+            const size_t item_base = (size_t(oz + z0) * g.dim1 + (oy + y0)) * g.dim2 + (ox + x0);
+            const uint32_t plane = g.dim1 * g.dim2;
+            for (uint32_t r0 = 0; r0 < rows; r0 += 32u) {
+                const uint32_t row = r0 + lane;
+                const bool valid = row < rows;
+                const uint32_t zz = valid ? row / h : 0u;
+                const uint32_t yy = valid ? row - zz * h : 0u;
+                // Offset of this lane's row from the item's first voxel (fits 32 bits: z < tile_size).
+                const uint32_t row_off = valid ? zz * plane + yy * g.dim2 : 0xffffffffu;
+                const uint32_t n_rows = min(32u, rows - r0);
+                const S py = static_cast<S>(oy + y0 + yy) + static_cast<S>(0.5);
+                const S pz = static_cast<S>(oz + z0 + zz) + static_cast<S>(0.5);
+                S d2, d3, K, L;
+                if (!kBeta) {
+                    d2 = py - r.y;
+                    d3 = pz - r.z;
+                    K = static_cast<S>(0.5) * (bb * d2 * d2 + c * d3 * d3) + rr * d2 * d3;
+                    L = p * d2 + q * d3;
+                } else {
+                    d2 = r.y - py;
+                    d3 = r.z - pz;
+                    K = bb * d2 * d2 + c * d3 * d3 + static_cast<S>(2) * rr * d2 * d3;
+                    L = static_cast<S>(2) * (p * d2 + q * d3);
+                }
+                S A0 = S(0), A1 = S(0), A2 = S(0), A3 = S(0), A4 = S(0), A5 = S(0);
+                float2 a1 = splat2(0.f), a2 = a1, a3 = a1;
+                for (uint32_t xs = 0; xs < w; xs += kRecChunk) {
+                    const uint32_t cols = min(kRecChunk, w - xs);
+                    // Stage: lane = column; one row of the chunk per iteration.
+                    __syncwarp();
+                    for (uint32_t k = 0; k < 32u; ++k) {
+                        const uint32_t off = __shfl_sync(0xffffffffu, row_off, int(k));
+                        const bool load = k < n_rows && lane < cols;
+                        const size_t gi = item_base + off + xs + lane;
+                        s_v[k * kRecStride + lane] = (load && has_v) ? v_volume[gi] : S(0);
+                        if (kVar) s_vv[k * kRecStride + lane] = load ? v_volume_var[gi] : S(0);
+                    }
+                    if (lane == 0u) {
+                        for (uint32_t k = 0; k < 32u; ++k) {
+                            s_v[k * kRecStride + kRecChunk] = S(0);
+                            if (kVar) s_vv[k * kRecStride + kRecChunk] = S(0);
+                        }
+                    }
+                    __syncwarp();
+                    const S* vrow = s_v + lane * kRecStride;
+                    const S px0 = static_cast<S>(ox + x0 + xs) + static_cast<S>(0.5);
+                    if constexpr (kPackedRow) {
+                        // Two voxels of the row per step in packed FP32x2 form, as in the tile kernel:
+                        // e = -sigma log2(e) by Horner in d1 from prescaled coefficients, vis = 2^e.
+                        const float2 qa = splat2(half_a * kVoxNegLog2e), ql = splat2(L * kVoxNegLog2e);
+                        const float2 qk = splat2(K * kVoxNegLog2e), two = splat2(2.f);
+                        float2 d1 = make_float2(px0 - r.x, px0 + 1.f - r.x);
+                        for (uint32_t i = 0; i < cols; i += 2u) {
+                            // Slots past the chunk are zero: the odd tail's second sample adds nothing.
+                            const float ga = vrow[i];
+                            const float gb = vrow[i + 1u];
+                            const float2 e = fma2(fma2(qa, d1, ql), d1, qk);
+                            const float2 vis = make_float2(exp2f(e.x), exp2f(e.y));
+                            const bool ka = !(e.x > 0.f || e.x < e_min);
+                            const bool kb = !(e.y > 0.f || e.y < e_min);
+                            const float2 gvr = mul2(make_float2(ga, gb), vis);
+                            const float2 gv = make_float2(ka ? gvr.x : 0.f, kb ? gvr.y : 0.f);
+                            a3 = add2(a3, gv);
+                            const float2 gvd = mul2(gv, d1);
+                            a1 = add2(a1, gvd);
+                            a2 = fma2(gvd, d1, a2);
+                            d1 = add2(d1, two);
+                        }
+                    } else {
+                        S px = px0;
+                        for (uint32_t i = 0; i < cols; ++i, px += S(1)) {
+                            S v = vrow[i];
+                            const S vv = kVar ? s_vv[lane * kRecStride + i] : S(0);
+                            S wgt, d1;
+                            if (!kBeta) {
+                                d1 = px - r.x;
+                                const S sigma = half_a * d1 * d1 + L * d1 + K;
+                                const S vis_raw = exp(-sigma);
+                                const S alpha_raw = opac * vis_raw;
+                                const bool keep = valid &&
+                                                  !(sigma < static_cast<S>(0) || fabs(alpha_raw) < static_cast<S>(1e-6));
+                                const S vis = keep ? vis_raw : S(0);
+                                const S alpha = keep ? alpha_raw : S(0);
+                                if (kVar) {
+                                    A4 += vv * alpha * alpha;
+                                    v += static_cast<S>(2) * uq * alpha * vv;
+                                }
+                                wgt = -v * alpha;
+                                A3 += v * vis;
+                            } else {
+                                d1 = r.x - px;
+                                const S qf = a * d1 * d1 + L * d1 + K;
+                                const S h_raw = static_cast<S>(1) - qf;
+                                const bool in_support =
+                                    valid && !(qf < static_cast<S>(0) || h_raw <= static_cast<S>(0));
+                                const S hh = in_support ? h_raw : S(1);
+                                const S lg = log2(hh);
+                                const S vis_raw = exp2(r.beta * lg);
+                                const S alpha_raw = opac * vis_raw;
+                                const bool keep = in_support && !(fabs(alpha_raw) < static_cast<S>(1e-5));
+                                const S vis = keep ? vis_raw : S(0);
+                                const S alpha = keep ? alpha_raw : S(0);
+                                v = keep ? v : S(0);
+                                if (kVar) {
+                                    A4 += vv * alpha * alpha;
+                                    v += static_cast<S>(2) * uq * alpha * vv;
+                                }
+                                wgt = -opac * r.beta * (vis_raw / hh) * v;
+                                A3 += v * vis;
+                                A5 += v * alpha * (lg * static_cast<S>(0.6931471805599453));
+                            }
+                            const S wd = wgt * d1;
+                            A0 += wgt;
+                            A1 += wd;
+                            A2 += wd * d1;
+                        }
+                    }
+                }
+                if constexpr (kPackedRow) {
+                    A3 = a3.x + a3.y;
+                    A0 = -opac * A3;
+                    A1 = -opac * (a1.x + a1.y);
+                    A2 = -opac * (a2.x + a2.y);
+                }
+                part[0] += A1;
+                part[1] += d2 * A0;
+                part[2] += d3 * A0;
+                part[3] += A3;
+                part[4] += A2;
+                part[5] += d2 * A1;
+                part[6] += d3 * A1;
+                part[7] += d2 * d2 * A0;
+                part[8] += d2 * d3 * A0;
+                part[9] += d3 * d3 * A0;
+                part[10] += A5;
+                part[11] += A4;
+            }
+        }
+        // Recursive halving as in the tile kernel; lane group G = lane / 8 ends with the warp totals of
+        // part[4G .. 4G+3].
+        const bool hi16 = (lane & 16u) != 0, hi8 = (lane & 8u) != 0;
+        S w8[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const S send = hi16 ? part[i] : part[i + 8];
+            const S keep = hi16 ? part[i + 8] : part[i];
+            w8[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+        }
+        S w4[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const S send = hi8 ? w8[i] : w8[i + 4];
+            const S keep = hi8 ? w8[i + 4] : w8[i];
+            w4[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+        }
+#pragma unroll
+        for (int offset = 4; offset > 0; offset >>= 1) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) w4[i] += __shfl_xor_sync(0xffffffffu, w4[i], offset);
+        }
+        const uint32_t grp = lane >> 3;
+        if ((lane & 7u) == 0u) {
+            const S a = r.c00, p = r.c01, q = r.c02, bb = r.c11, rr = r.c12, c = r.c22;
+            const S two = static_cast<S>(2), half = static_cast<S>(0.5);
+            S e0 = S(0), e1 = S(0), e2 = S(0), e3 = S(0);
+            if (grp == 0u) {
+                const S sx = a * w4[0] + p * w4[1] + q * w4[2];
+                const S sy = bb * w4[1] + p * w4[0] + rr * w4[2];
+                const S sz = c * w4[2] + q * w4[0] + rr * w4[1];
+                e0 = kBeta ? two * sx : -sx;
+                e1 = kBeta ? two * sy : -sy;
+                e2 = kBeta ? two * sz : -sz;
+                e3 = w4[3];
+            } else if (grp == 1u) {
+                e0 = kBeta ? w4[0] : half * w4[0];
+                e1 = kBeta ? two * w4[1] : w4[1];
+                e2 = kBeta ? two * w4[2] : w4[2];
+                e3 = kBeta ? w4[3] : half * w4[3];
+            } else if (grp == 2u) {
+                e0 = kBeta ? two * w4[0] : w4[0];
+                e1 = kBeta ? w4[1] : half * w4[1];
+                e2 = w4[2];
+                e3 = w4[3];
+            }
+            S* out = reinterpret_cast<S*>(partials + item) + 4 * grp;
+            out[0] = e0;
+            out[1] = e1;
+            out[2] = e2;
+            out[3] = e3;
+        }
+    }
+}
+
+// grads[n] = sum of the primitive's item slots, in layer order.
+template <typename S>
+__global__ void voxel_record_reduce_kernel(const Rec3D<S>* __restrict__ partials,
+                                           const int64_t* __restrict__ item_cum, uint32_t N, int64_t capacity,
+                                           Rec3D<S>* __restrict__ grads) {
+    const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    // Slots past the capacity were not computed (that step is flagged); they are never read.
+    const int64_t first = n == 0u ? 0 : min(item_cum[n - 1], capacity), last = min(item_cum[n], capacity);
+    S acc[12];
+#pragma unroll
+    for (int i = 0; i < 12; ++i) acc[i] = S(0);
+    for (int64_t item = first; item < last; ++item) {
+        const S* p = reinterpret_cast<const S*>(partials + item);
+#pragma unroll
+        for (int i = 0; i < 12; ++i) acc[i] += p[i];
+    }
+    S* out = reinterpret_cast<S*>(grads + n);
+#pragma unroll
+    for (int i = 0; i < 12; ++i) out[i] = acc[i];
+#pragma unroll
+    for (int i = 12; i < 16; ++i) out[i] = S(0);
 }
 
 template <typename S>
@@ -640,28 +1093,87 @@ int launch_vfwd(const VoxelGeom& g, const Rec3D<S>* rec, bool beta, const int32_
 
 template <typename S, bool kBeta, bool kVar>
 int launch_vbwd_p(const VoxelGeom& g, const Rec3D<S>* rec, bool chain_var, const int32_t* offsets,
-                  const int32_t* ids, const S* v_vol, const S* v_vol_var, Rec3D<S>* grads, cudaStream_t stream) {
+                  const int32_t* ids, const S* v_vol, const S* v_vol_var, Rec3D<S>* grads, cudaStream_t stream,
+                  const VoxelSlots<S>& sl) {
     const size_t tile_slots = size_t(g.T) * g.T * (g.T + 1) + (g.T + 1);
-    const size_t smem = 2 * size_t(kVoxBwdThreads) * (sizeof(Rec3D<S>) + sizeof(int32_t)) +
+    const size_t smem = 2 * size_t(kVoxBwdThreads) * (sizeof(Rec3D<S>) + 2 * sizeof(int32_t)) +
                         size_t(kVoxBwdThreads) * sizeof(VoxelBox) + 2 * tile_slots * sizeof(S);
     R2S_TRY(allow_dynamic_smem(voxel_bwd_kernel<S, kBeta, kVar>, smem));
     const unsigned grid = g.tiles_x * g.tiles_y * g.tiles_z;
     voxel_bwd_kernel<S, kBeta, kVar><<<grid, kVoxBwdThreads, smem, stream>>>(rec, chain_var, offsets, ids, g, v_vol,
-                                                                           v_vol_var, grads);
+                                                                           v_vol_var, grads, sl);
     return check_launch("voxelize_to_voxels_bwd");
 }
 
 template <typename S>
 int launch_vbwd(const VoxelGeom& g, const Rec3D<S>* rec, bool beta, bool chain_var, const int32_t* offsets,
-                const int32_t* ids, const S* v_vol, const S* v_vol_var, Rec3D<S>* grads, cudaStream_t stream) {
+                const int32_t* ids, const S* v_vol, const S* v_vol_var, Rec3D<S>* grads, cudaStream_t stream,
+                const VoxelSlots<S>& sl = VoxelSlots<S>{}) {
     R2S_TRY(check_vgeom(g));
     if (g.n_isects == 0 || uint64_t(g.tiles_x) * g.tiles_y * g.tiles_z == 0) return R2S_OK;
     const bool var = v_vol_var != nullptr;
     if (beta)
-        return var ? launch_vbwd_p<S, true, true>(g, rec, chain_var, offsets, ids, v_vol, v_vol_var, grads, stream)
-                   : launch_vbwd_p<S, true, false>(g, rec, chain_var, offsets, ids, v_vol, v_vol_var, grads, stream);
-    return var ? launch_vbwd_p<S, false, true>(g, rec, chain_var, offsets, ids, v_vol, v_vol_var, grads, stream)
-               : launch_vbwd_p<S, false, false>(g, rec, chain_var, offsets, ids, v_vol, v_vol_var, grads, stream);
+        return var ? launch_vbwd_p<S, true, true>(g, rec, chain_var, offsets, ids, v_vol, v_vol_var, grads, stream, sl)
+                   : launch_vbwd_p<S, true, false>(g, rec, chain_var, offsets, ids, v_vol, v_vol_var, grads, stream,
+                                                   sl);
+    return var ? launch_vbwd_p<S, false, true>(g, rec, chain_var, offsets, ids, v_vol, v_vol_var, grads, stream, sl)
+               : launch_vbwd_p<S, false, false>(g, rec, chain_var, offsets, ids, v_vol, v_vol_var, grads, stream, sl);
+}
+
+// Tile VJP into slots, then the in-order per-primitive sum into grads (written, not accumulated).
+template <typename S>
+int launch_vbwd_slots(const VoxelGeom& g, const Rec3D<S>* rec, bool beta, bool chain_var, const int32_t* offsets,
+                      const int32_t* ids, const S* v_vol, const S* v_vol_var, const VoxelSlots<S>& sl,
+                      Rec3D<S>* grads, cudaStream_t stream) {
+    if (g.N == 0) return R2S_OK;
+    R2S_TRY(launch_vbwd<S>(g, rec, beta, chain_var, offsets, ids, v_vol, v_vol_var, grads, stream, sl));
+    voxel_slot_reduce_kernel<S><<<blocks_for(g.N, 256), 256, 0, stream>>>(sl.slots, sl.cum, g.N,
+                                                                         int64_t(sl.capacity), grads);
+    return check_launch("voxel_slot_reduce");
+}
+
+template <typename S, bool kBeta, bool kVar>
+int launch_vrec_p(const VoxelRecordGeom& g, const Rec3D<S>* rec, const S* means_v, const int32_t* radii,
+                  const int64_t* item_cum, bool chain_var, const S* v_vol, const S* v_vol_var, Rec3D<S>* partials,
+                  cudaStream_t stream) {
+    // Persistent over the items: at most four resident 8-warp blocks per SM's worth of blocks.
+    const uint64_t needed = (g.n_items + kVoxBwdWarps - 1) / kVoxBwdWarps;
+    const unsigned grid = unsigned(needed < uint64_t(148 * 8) ? (needed > 0 ? needed : 1) : uint64_t(148 * 8));
+    const size_t smem = size_t(kVoxBwdWarps) * 32u * kRecStride * sizeof(S) * (kVar ? 2u : 1u);
+    R2S_TRY(allow_dynamic_smem(voxel_record_bwd_kernel<S, kBeta, kVar>, smem));
+    voxel_record_bwd_kernel<S, kBeta, kVar><<<grid, kVoxBwdThreads, smem, stream>>>(
+        rec, means_v, radii, item_cum, chain_var, g, v_vol, v_vol_var, partials);
+    return check_launch("voxel_record_bwd");
+}
+
+template <typename S>
+int launch_vrec(const VoxelRecordGeom& g, const Rec3D<S>* rec, const S* means_v, const int32_t* radii,
+                const int64_t* item_cum, bool beta, bool chain_var, const S* v_vol, const S* v_vol_var,
+                Rec3D<S>* partials, Rec3D<S>* grads, cudaStream_t stream) {
+    if (g.N == 0) return R2S_OK;
+    if (g.n_items > 0) {
+        const bool var = v_vol_var != nullptr;
+        int status;
+        if (beta)
+            status = var ? launch_vrec_p<S, true, true>(g, rec, means_v, radii, item_cum, chain_var, v_vol,
+                                                        v_vol_var, partials, stream)
+                         : launch_vrec_p<S, true, false>(g, rec, means_v, radii, item_cum, chain_var, v_vol,
+                                                         v_vol_var, partials, stream);
+        else
+            status = var ? launch_vrec_p<S, false, true>(g, rec, means_v, radii, item_cum, chain_var, v_vol,
+                                                         v_vol_var, partials, stream)
+                         : launch_vrec_p<S, false, false>(g, rec, means_v, radii, item_cum, chain_var, v_vol,
+                                                          v_vol_var, partials, stream);
+        R2S_TRY(status);
+    }
+    voxel_record_reduce_kernel<S><<<blocks_for(g.N, 256), 256, 0, stream>>>(partials, item_cum, g.N,
+                                                                           int64_t(g.n_items), grads);
+    return check_launch("voxel_record_reduce");
+}
+
+__global__ void item_capacity_check_kernel(const int64_t* __restrict__ used, uint64_t capacity,
+                                           uint32_t* __restrict__ overflow) {
+    if (uint64_t(*used) > capacity) *overflow = 1u;
 }
 
 template <typename S>
@@ -815,6 +1327,72 @@ int r2s_voxel_render_bwd_capacity(int dtype, const void* records, int beta, int 
                                               detach_variance == 0, tile_offsets, flatten_ids,
                                               static_cast<const S*>(v_volume), static_cast<const S*>(v_volume_var),
                                               static_cast<Rec3D<S>*>(grads), as_stream(stream)));
+}
+
+int r2s_voxel_render_bwd_slots(int dtype, const void* records, int beta, int detach_variance,
+                               const int32_t* tile_offsets, const int32_t* flatten_ids, uint64_t n_isects,
+                               const int64_t* n_used, const void* means_v, const int32_t* radii,
+                               const int64_t* tile_cum, const void* v_volume, const void* v_volume_var, uint32_t N,
+                               uint32_t dim2, uint32_t dim1, uint32_t dim0, uint32_t tile_size, uint32_t tiles_x,
+                               uint32_t tiles_y, uint32_t tiles_z, void* slots, uint64_t slot_capacity, void* grads,
+                               void* stream) {
+    if (N == 0) return R2S_OK;
+    R2S_REQUIRE(records != nullptr && means_v != nullptr && radii != nullptr && tile_cum != nullptr &&
+                    slots != nullptr && grads != nullptr,
+                R2S_ERR_ARGUMENT, "records, means_v, radii, tile_cum, slots and grads must be non-null");
+    R2S_REQUIRE(n_used != nullptr || n_isects <= slot_capacity, R2S_ERR_ARGUMENT,
+                "slot_capacity must hold n_isects slots");
+    R2S_REQUIRE(n_isects < (uint64_t(1) << 31), R2S_ERR_UNSUPPORTED, "too many 3D intersections");
+    VoxelGeom g{N, uint32_t(n_used != nullptr ? 1u : n_isects), dim2, dim1, dim0, tile_size, tiles_x, tiles_y,
+                tiles_z};
+    g.n_dev = n_used;
+    R2S_DISPATCH(dtype, {
+        VoxelSlots<S> sl;
+        sl.means_v = static_cast<const S*>(means_v);
+        sl.radii = radii;
+        sl.cum = tile_cum;
+        sl.slots = static_cast<S*>(slots);
+        sl.capacity = slot_capacity;
+        return launch_vbwd_slots<S>(g, static_cast<const Rec3D<S>*>(records), beta != 0, detach_variance == 0,
+                                    tile_offsets, flatten_ids, static_cast<const S*>(v_volume),
+                                    static_cast<const S*>(v_volume_var), sl, static_cast<Rec3D<S>*>(grads),
+                                    as_stream(stream));
+    });
+}
+
+int r2s_voxel_layer_counts(int dtype, const void* means_v, const int32_t* radii, uint32_t N, uint32_t dim2,
+                           uint32_t dim1, uint32_t dim0, uint32_t tile_size, uint32_t tiles_x, uint32_t tiles_y,
+                           uint32_t tiles_z, int32_t* layers, void* stream) {
+    if (N == 0) return R2S_OK;
+    R2S_REQUIRE(means_v != nullptr && radii != nullptr && layers != nullptr, R2S_ERR_ARGUMENT,
+                "means_v, radii and layers must be non-null");
+    VoxelRecordGeom g{N, dim2, dim1, dim0, tile_size, tiles_x, tiles_y, tiles_z, 0u, nullptr};
+    R2S_DISPATCH(dtype, voxel_layer_count_kernel<S><<<blocks_for(N, 256), 256, 0, as_stream(stream)>>>(
+        static_cast<const S*>(means_v), radii, g, layers));
+    return check_launch("voxel_layer_counts");
+}
+
+int r2s_voxel_record_bwd(int dtype, const void* records, const void* means_v, const int32_t* radii,
+                         const int64_t* layer_cum, uint64_t n_items, const int64_t* n_items_dev, int beta,
+                         int detach_variance, const void* v_volume, const void* v_volume_var, uint32_t N,
+                         uint32_t dim2, uint32_t dim1, uint32_t dim0, uint32_t tile_size, uint32_t tiles_x,
+                         uint32_t tiles_y, uint32_t tiles_z, void* partials, void* grads, uint32_t* overflow,
+                         void* stream) {
+    if (N == 0) return R2S_OK;
+    R2S_REQUIRE(records != nullptr && means_v != nullptr && radii != nullptr && layer_cum != nullptr &&
+                    grads != nullptr && (partials != nullptr || n_items == 0),
+                R2S_ERR_ARGUMENT, "records, means_v, radii, layer_cum, partials and grads must be non-null");
+    R2S_REQUIRE(tile_size >= 1 && tile_size <= 10, R2S_ERR_UNSUPPORTED, "3D tile_size must be in [1, 10]");
+    VoxelRecordGeom g{N, dim2, dim1, dim0, tile_size, tiles_x, tiles_y, tiles_z, n_items, n_items_dev};
+    cudaStream_t st = as_stream(stream);
+    if (n_items_dev != nullptr && overflow != nullptr) {
+        item_capacity_check_kernel<<<1, 1, 0, st>>>(n_items_dev, n_items, overflow);
+        R2S_TRY(check_launch("voxel_record_capacity"));
+    }
+    R2S_DISPATCH(dtype, return launch_vrec<S>(g, static_cast<const Rec3D<S>*>(records), static_cast<const S*>(means_v),
+                                              radii, layer_cum, beta != 0, detach_variance == 0,
+                                              static_cast<const S*>(v_volume), static_cast<const S*>(v_volume_var),
+                                              static_cast<Rec3D<S>*>(partials), static_cast<Rec3D<S>*>(grads), st));
 }
 
 }  // extern "C"

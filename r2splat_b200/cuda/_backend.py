@@ -69,6 +69,7 @@ SIGNATURES: dict[str, tuple] = {
     "r2s_volume_loss_workspace": (SZ, [U64]),
     "r2s_volume_loss_fwd": (I32, [I32, P, U32, U32, U32, U32, F32, P, P, P, P, SZ, P]),
     "r2s_volume_loss_bwd": (I32, [I32, P, P, U32, U32, U32, U32, F32, P, P]),
+    "r2s_volume_loss_fwd_bwd": (I32, [I32, P, P, U32, U32, U32, U32, F32, P, P, P, P, P, SZ, P]),
     "r2s_image_loss_l1_fwd": (I32, [I32, P, P, U32, U32, U32, F32, P, P, P, P, SZ, P]),
     "r2s_image_loss_l1_bwd": (I32, [I32, P, P, P, U32, U32, U32, F32, P, P]),
     "r2s_raster_project": (I32, [I32, P, P, P, P, P, P, P, U32, U32, U32, U32, F32, F64, F32, U32, U32, U32,
@@ -93,6 +94,15 @@ SIGNATURES: dict[str, tuple] = {
     "r2s_voxel_render_capacity": (I32, [I32, P, I32, P, P, P, U32, U32, U32, U32, U32, U32, U32, U32, P, P, P]),
     "r2s_voxel_render_bwd_capacity": (I32, [I32, P, I32, I32, P, P, P, P, P, U32, U32, U32, U32, U32, U32, U32,
                                             U32, P, P]),
+    # dtype, records, beta, detach, offsets, ids, n_isects, n_used, means_v, radii, tile_cum, v_volume, v_volume_var,
+    # N, dim2, dim1, dim0, tile, tiles_x, tiles_y, tiles_z, slots, slot_capacity, grads, stream
+    "r2s_voxel_render_bwd_slots": (I32, [I32, P, I32, I32, P, P, U64, P, P, P, P, P, P, U32, U32, U32, U32, U32, U32,
+                                         U32, U32, P, U64, P, P]),
+    "r2s_voxel_layer_counts": (I32, [I32, P, P, U32, U32, U32, U32, U32, U32, U32, U32, P, P]),
+    # dtype, records, means_v, radii, layer_cum, n_items, n_items_dev, beta, detach, v_volume, v_volume_var, N,
+    # dim2, dim1, dim0, tile, tiles_x, tiles_y, tiles_z, partials, grads, overflow, stream
+    "r2s_voxel_record_bwd": (I32, [I32, P, P, P, P, U64, P, I32, I32, P, P, U32, U32, U32, U32, U32, U32, U32, U32,
+                                   P, P, P, P]),
     "r2s_raster_image_loss_workspace": (SZ, [U32, U32, U32]),
     # dtype, records, unc, beta, offsets, ids, n_isects, n_used, C, N, W, H, tile, tiles_x, tiles_y, stage_batch,
     # target, kind, lambda, render, render_var, v_render, loss, loss_value, workspace, bytes, stream

@@ -800,6 +800,35 @@ def volume_loss_bwd(volume: Tensor, grad_output: Tensor, lambda_tv: float):
     return grad
 
 
+def volume_loss_fwd_bwd(volume: Tensor, grad_output: Tensor, lambda_tv: float, with_map: bool = False):
+    """``volume_loss_fwd`` and ``volume_loss_bwd`` in one pass over the volume.
+
+    No reference counterpart as one call: for a caller that knows the upstream
+    gradient before the forward (a fit step, where the TV term enters the loss
+    with weight one). Returns ``(lambda * tv, tv, grad_volume)``, plus
+    ``tv_map`` when ``with_map``; the map and the gradient equal the two
+    separate calls' bit for bit.
+    """
+    _check("volume", volume)
+    _check("grad_output", grad_output)
+    _require(grad_output.device == volume.device, "grad_output must be on the same CUDA device as volume")
+    _dtype(volume)
+    _require(volume.dim() == 4, "volume must be 4D (B, D, H, W)")
+    _require(grad_output.dtype == volume.dtype and grad_output.numel() >= 1, "grad_output must match volume's dtype")
+    b, d, h, w = volume.shape
+    grad = torch.empty_like(volume)
+    tv_map = torch.empty_like(volume) if with_map else None
+    loss = volume.new_empty(())
+    tv = volume.new_empty(())
+    with _Guard(volume.device):
+        lib = _backend.library()
+        ws = _workspace(lib.r2s_volume_loss_workspace(volume.numel()), volume.device)
+        _backend.call("r2s_volume_loss_fwd_bwd", _dtype(volume), _ptr(volume), _ptr(grad_output), b, d, h, w,
+                      float(lambda_tv), _ptr(loss), _ptr(tv), _ptr(tv_map), _ptr(grad), _ptr(ws), ws.numel(),
+                      _stream(volume.device))
+    return (loss, tv, grad) + ((tv_map,) if with_map else ())
+
+
 def image_loss_l1_fwd(prediction: Tensor, target: Tensor, lambda_l1: float):
     """Mean L1 of [B,H,W] images -> (lambda * l1, l1, l1_map)."""
     _check("prediction", prediction)

@@ -1,17 +1,18 @@
-"""Explicit CUDA forward/VJP calls for physical primitive parameters.
+"""The drop-in explicit operators: forward passes that hand back a one-shot VJP context.
 
-Same public contract as the reference's ``r2splat/explicit.py``:
+Public surface and error contract of the reference's ``r2splat/explicit.py``:
 ``rasterize_fwd`` (:102-188), ``rasterize_bwd`` (:191-242), ``voxelize_fwd``
-(:245-311), ``voxelize_bwd`` (:314-351), the one-shot context with tensor
-version guards (:37-99) and ``ParameterGradients`` (:25-34). Forward returns
-``(output, context)`` without recording an autograd graph; backward consumes
-the context once and returns gradients without writing ``.grad``. Geometry is
-constant; activations and loss derivatives belong to the caller.
+(:245-311), ``voxelize_bwd`` (:314-351) and ``ParameterGradients`` (:25-34).
+No autograd graph is built. A forward returns its output detached plus a
+context; the matching backward accepts that context exactly once, refuses it
+if any tensor it captured was written in place since, and returns the
+gradients as a ``ParameterGradients`` without touching ``.grad``. Cameras,
+volume extent and centre are constants; activations and loss derivatives are
+the caller's.
 
-The device work runs through the fused sm_100a pipelines in ``_fused``.
-``backward_mode`` is accepted for compatibility: "pixel" and "primitive" give
-the same VJP here (one tile kernel serves both; they differ only in float
-summation order in the reference).
+Device work runs through the fused sm_100a pipelines of ``_fused``. Both
+``backward_mode`` values are accepted and run the same VJP (in the reference
+they select two kernels that differ only in float summation order).
 """
 
 from __future__ import annotations
@@ -29,11 +30,17 @@ from ._validation import (FOCAL, HOMOGENEOUS_ROW, PINHOLE, POSITIVE, _constant, 
 Tensor = torch.Tensor
 Output = Union[Tensor, tuple[Tensor, Tensor]]
 _PRIMITIVE_NAMES = ("means", "quats", "scales", "densities", "beta", "uncertainty")
+# Launch geometry bounds of the reference's kernels, kept as input limits of the contract.
+_GRID_LIMIT = 65535
+_INDEX_LIMIT = 2**31 - 1
 
 
 @dataclass
 class ParameterGradients:
-    """VJP tensors matching the physical inputs; absent optional inputs give None."""
+    """Gradients with respect to the physical inputs of a forward call.
+
+    ``beta`` and ``uncertainty`` are None when the forward had no such input.
+    """
 
     means: Tensor
     quats: Tensor
@@ -43,17 +50,68 @@ class ParameterGradients:
     uncertainty: Optional[Tensor] = None
 
 
-@dataclass
 class _Context:
-    kind: str
-    shape: tuple
-    primitives: tuple
-    buffers: dict
-    versions: tuple
-    eps: float
-    backward_mode: str
-    detach_variance: bool
-    used: bool = False
+    """What one forward call leaves for its backward, usable once.
+
+    ``versions`` holds ``(name, tensor, version)`` for every distinct tensor
+    the forward read or produced for the backward; ``open`` compares them
+    again, so an in-place write in between is reported instead of silently
+    giving wrong gradients.
+    """
+
+    __slots__ = ("kind", "shape", "primitives", "buffers", "versions", "eps", "backward_mode",
+                 "detach_variance", "used")
+
+    def __init__(self, kind, shape, primitives, buffers, versions, eps, backward_mode, detach_variance):
+        self.kind, self.shape, self.eps = kind, shape, eps
+        self.primitives, self.buffers, self.versions = primitives, buffers, versions
+        self.backward_mode, self.detach_variance = backward_mode, detach_variance
+        self.used = False
+
+    @classmethod
+    def capture(cls, kind, shape, primitives, buffers, originals, eps, backward_mode, detach_variance):
+        """A context that watches the caller's originals, the validated primitives and the saved tensors."""
+        named = [*originals, *zip(_PRIMITIVE_NAMES, primitives), *buffers.items()]
+        versions, ids = [], set()
+        for name, value in named:
+            if not isinstance(value, Tensor) or id(value) in ids:
+                continue
+            ids.add(id(value))
+            try:
+                versions.append((name, value, value._version))
+            except RuntimeError as error:  # inference tensors carry no version counter
+                raise ValueError("explicit contexts require tensors with version counters") from error
+        return cls(kind, shape, primitives, buffers, tuple(versions), eps, backward_mode, detach_variance)
+
+    def open(self, kind):
+        """Checks that this is an unused, unmodified context of a ``kind`` forward."""
+        if self.kind != kind:
+            raise TypeError(f"expected a context returned by {kind}_fwd")
+        if self.used:
+            raise RuntimeError("this context has already been consumed by backward")
+        stale = next((name for name, value, version in self.versions if value._version != version), None)
+        if stale is not None:
+            raise RuntimeError(f"saved input {stale} was modified in-place after forward")
+
+    def close(self, gradients):
+        """Marks the context used, drops every reference it holds and passes ``gradients`` through."""
+        self.used = True
+        self.primitives, self.versions = (), ()
+        self.buffers.clear()
+        return gradients
+
+    def adjoint(self, name, value):
+        """``value`` checked against the forward output's shape, device and dtype (None passes through)."""
+        return None if value is None else _tensor(name, value, self.shape, self.primitives[0])
+
+    def zero_gradients(self):
+        return ParameterGradients(*(None if p is None else torch.zeros_like(p) for p in self.primitives))
+
+
+def _open_context(context, kind):
+    if not isinstance(context, _Context):
+        raise TypeError(f"expected a context returned by {kind}_fwd")
+    context.open(kind)
 
 
 @contextlib.contextmanager
@@ -74,53 +132,36 @@ def _resolving(checks):
     checks.check()
 
 
-def _mode(value):
-    value = str(value).lower()
-    if value not in ("pixel", "primitive"):
-        raise ValueError("backward_mode must be 'pixel' or 'primitive'")
-    return value
+def _backward_mode(value):
+    mode = str(value).lower()
+    if mode in ("pixel", "primitive"):
+        return mode
+    raise ValueError("backward_mode must be 'pixel' or 'primitive'")
+
+
+def release_intersection_lists(context) -> None:
+    """Frees a forward context's intersection lists before its backward runs.
+
+    Not part of the reference's surface: a memory-bounded caller (the serving
+    loop's recompute-in-backward mode) calls it between ``rasterize_fwd`` /
+    ``voxelize_fwd`` and the matching backward. Neither VJP reads the lists:
+    the raster VJP walks each record's tile rectangle and the voxel VJP then
+    walks each primitive's tile box. The gradients are unchanged up to the
+    voxel VJP's summation order.
+    """
+    if not isinstance(context, _Context) or context.used:
+        raise RuntimeError("expected an unconsumed explicit context")
+    state = context.buffers.get("state")
+    if state is None:
+        return
+    dropped = {id(t) for t in _fused.release_lists(state)}
+    for key in ("offsets", "isect_ids", "flatten_ids"):
+        context.buffers.pop(key, None)
+    context.versions = tuple(entry for entry in context.versions if id(entry[1]) not in dropped)
 
 
 def _context(kind, shape, primitives, buffers, originals, eps, mode, detach_variance):
-    """Snapshots the version counter of every input and saved tensor."""
-    watched, seen = [], set()
-    entries = list(originals) + list(zip(_PRIMITIVE_NAMES, primitives)) + [
-        (name, value) for name, value in buffers.items() if isinstance(value, Tensor)]
-    for name, value in entries:
-        if isinstance(value, Tensor) and id(value) not in seen:
-            try:
-                version = value._version
-            except RuntimeError as error:
-                raise ValueError("explicit contexts require tensors with version counters") from error
-            watched.append((name, value, version))
-            seen.add(id(value))
-    return _Context(kind, shape, primitives, buffers, tuple(watched), eps, mode, detach_variance)
-
-
-def _check_context(context, kind):
-    if not isinstance(context, _Context) or context.kind != kind:
-        raise TypeError(f"expected a context returned by {kind}_fwd")
-    if context.used:
-        raise RuntimeError("this context has already been consumed by backward")
-    for name, value, version in context.versions:
-        if value._version != version:
-            raise RuntimeError(f"saved input {name} was modified in-place after forward")
-
-
-def _adjoint(name, value, context):
-    return None if value is None else _tensor(name, value, context.shape, context.primitives[0])
-
-
-def _zero_gradients(context):
-    return ParameterGradients(*(None if value is None else torch.zeros_like(value) for value in context.primitives))
-
-
-def _consume(context, gradients):
-    context.used = True
-    context.primitives = ()
-    context.buffers.clear()
-    context.versions = ()
-    return gradients
+    return _Context.capture(kind, shape, primitives, buffers, originals, eps, mode, detach_variance)
 
 
 @torch.no_grad()
@@ -140,11 +181,12 @@ def rasterize_fwd(
     detach_variance: bool = False,
     backward_mode: str = "primitive",
 ) -> tuple[Output, _Context]:
-    """Project physical primitives, returning a detached image and VJP context.
+    """Line-integral images of the primitives for every camera, plus the context for ``rasterize_bwd``.
 
-    World-to-camera ``viewmats [C,4,4]`` and pinhole ``Ks [C,3,3]`` are
-    constant. Output is ``[C,height,width]`` or ``(image, variance)`` with
-    uncertainty. No input needs requires_grad.
+    ``viewmats [C,4,4]`` (world to camera) and the pinhole intrinsics ``Ks
+    [C,3,3]`` are constants. The output is ``[C,height,width]``, or the pair
+    ``(image, variance)`` when ``uncertainty`` is given; it never carries an
+    autograd graph, and the inputs need not require grad.
     """
     return _rasterize_fwd(means, quats, scales, densities, viewmats, Ks, image_size, beta, uncertainty, eps,
                           radius_clip, detach_variance, backward_mode, None)
@@ -208,8 +250,9 @@ def _rasterize_fwd(means, quats, scales, densities, viewmats, Ks, image_size, be
         primitives = _primitives(means, quats, scales, densities, beta, uncertainty)
         means, quats, scales, densities, beta, uncertainty = primitives
         eps, radius_clip = _options(beta, eps, radius_clip, detach_variance)
-        mode = _mode(backward_mode)
-        # Check the originals: a contiguous copy under no_grad drops requires_grad.
+        mode = _backward_mode(backward_mode)
+        # requires_grad must be judged on the caller's tensors: _tensor may hand back a
+        # contiguous copy, and under no_grad that copy no longer requires grad.
         for name, value in (("viewmats", viewmats), ("Ks", Ks)):
             if isinstance(value, Tensor):
                 _constant(name, value)
@@ -217,9 +260,10 @@ def _rasterize_fwd(means, quats, scales, densities, viewmats, Ks, image_size, be
         cameras = viewmats.shape[0]
         if cameras == 0:
             raise ValueError("viewmats must contain at least one camera")
-        if cameras * max(height * width, means.shape[0]) > 2**31 - 1 or cameras > 65535:
+        largest_index = cameras * max(height * width, means.shape[0])
+        if largest_index > _INDEX_LIMIT or cameras > _GRID_LIMIT:
             raise ValueError("camera batch exceeds CUDA indexing or grid limits")
-        if max(height, width) > 16 * 65535:
+        if max(height, width) > _fused.RASTER_TILE * _GRID_LIMIT:
             raise ValueError("image_size exceeds CUDA grid limits")
         Ks = _constant("Ks", _tensor("Ks", Ks, (cameras, 3, 3), means))
         _value_check(Ks, FOCAL, ValueError, "Ks must have positive fx and fy")
@@ -264,21 +308,23 @@ def _rasterize_fwd(means, quats, scales, densities, viewmats, Ks, image_size, be
 @torch.no_grad()
 def rasterize_bwd(context: _Context, v_image: Optional[Tensor], v_variance: Optional[Tensor] = None
                   ) -> ParameterGradients:
-    """Consume a projection context and return physical-parameter gradients.
+    """Gradients of ``<output, adjoint>`` with respect to the primitives, from a ``rasterize_fwd`` context.
 
-    Adjoint tensors match the output's shape, device, and dtype. None denotes
-    a zero adjoint, including variance-only losses. Inputs must remain unchanged.
+    Each adjoint has the shape, device and dtype of the output it belongs to;
+    None stands for a zero adjoint (so a loss on the variance alone passes
+    ``v_image=None``). The context is used up, and the forward's inputs must
+    not have been modified in place since the forward.
     """
-    _check_context(context, "rasterize")
+    _open_context(context, "rasterize")
     means, quats, scales, densities, beta, uncertainty = context.primitives
     if v_variance is not None and uncertainty is None:
         raise ValueError("v_variance requires uncertainty in the forward call")
     with deferred_value_checks(pending=True) as checks:
-        v_image = _adjoint("v_image", v_image, context)
-        v_variance = _adjoint("v_variance", v_variance, context)
+        v_image = context.adjoint("v_image", v_image)
+        v_variance = context.adjoint("v_variance", v_variance)
     if means.shape[0] == 0 or (v_image is None and v_variance is None):
         checks.check()
-        return _consume(context, _zero_gradients(context))
+        return context.close(context.zero_gradients())
     b = context.buffers
     # The VJP is enqueued before the adjoint checks resolve; on a failure its
     # result is dropped and the context stays unconsumed.
@@ -286,7 +332,7 @@ def rasterize_bwd(context: _Context, v_image: Optional[Tensor], v_variance: Opti
         grads = _fused.raster_backward(b["state"], means, quats, scales, densities, beta, uncertainty,
                                        b["viewmats"], b["Ks"], context.eps, v_image, v_variance,
                                        context.detach_variance)
-    return _consume(context, ParameterGradients(*grads))
+    return context.close(ParameterGradients(*grads))
 
 
 @torch.no_grad()
@@ -306,10 +352,11 @@ def voxelize_fwd(
     detach_variance: bool = False,
     backward_mode: str = "primitive",
 ) -> tuple[Output, _Context]:
-    """Sample physical primitives, returning a detached volume and VJP context.
+    """Densities of the primitives sampled at voxel centres, plus the context for ``voxelize_bwd``.
 
-    ``volume_shape`` and output use ``[depth,height,width]``; physical extent
-    and center use xyz order. With uncertainty, output is ``(volume, variance)``.
+    ``volume_shape`` and the output are ``[depth,height,width]``; the
+    physical ``volume_extent`` and ``volume_center`` are given in x, y, z
+    order. With ``uncertainty`` the output is ``(volume, variance)``.
     """
     originals = list(zip(
         ("means", "quats", "scales", "densities", "volume_extent", "volume_center", "beta", "uncertainty"),
@@ -317,12 +364,12 @@ def voxelize_fwd(
     ))
     with deferred_value_checks(pending=True) as checks:
         depth, height, width = _shape("volume_shape", volume_shape, 3)
-        if max(height, width) > 8 * 65535:
+        if max(height, width) > _fused.VOXEL_TILE * _GRID_LIMIT:
             raise ValueError("volume_shape exceeds CUDA grid limits")
         primitives = _primitives(means, quats, scales, densities, beta, uncertainty)
         means, quats, scales, densities, beta, uncertainty = primitives
         eps, radius_clip = _options(beta, eps, radius_clip, detach_variance)
-        mode = _mode(backward_mode)
+        mode = _backward_mode(backward_mode)
         for name, value in (("volume_extent", volume_extent), ("volume_center", volume_center)):
             if isinstance(value, Tensor):
                 _constant(name, value)
@@ -348,22 +395,25 @@ def voxelize_fwd(
 @torch.no_grad()
 def voxelize_bwd(context: _Context, v_volume: Optional[Tensor], v_variance: Optional[Tensor] = None
                  ) -> ParameterGradients:
-    """Consume a volume context and return gradients without updating inputs."""
-    _check_context(context, "voxelize")
+    """Gradients of ``<volume, adjoint>`` with respect to the primitives, from a ``voxelize_fwd`` context.
+
+    Adjoint rules as for ``rasterize_bwd``; no input's ``.grad`` is written.
+    """
+    _open_context(context, "voxelize")
     means, quats, scales, densities, beta, uncertainty = context.primitives
     if v_variance is not None and uncertainty is None:
         raise ValueError("v_variance requires uncertainty in the forward call")
     with deferred_value_checks(pending=True) as checks:
-        v_volume = _adjoint("v_volume", v_volume, context)
-        v_variance = _adjoint("v_variance", v_variance, context)
+        v_volume = context.adjoint("v_volume", v_volume)
+        v_variance = context.adjoint("v_variance", v_variance)
     if means.shape[0] == 0 or (v_volume is None and v_variance is None):
         checks.check()
-        return _consume(context, _zero_gradients(context))
+        return context.close(context.zero_gradients())
     b = context.buffers
     with _resolving(checks), torch.cuda.device(means.device):
         grads = _fused.voxel_backward(b["state"], means, quats, scales, beta, uncertainty, b["extent"],
                                       b["center"], context.eps, v_volume, v_variance, context.detach_variance)
-    return _consume(context, ParameterGradients(*grads))
+    return context.close(ParameterGradients(*grads))
 
 
 # rasterize_fwd_with_loss is an extension outside the reference's surface: it is

@@ -4,10 +4,14 @@ Requests name a reconstruction and ask for one fit step of it. The server
 keeps every admitted reconstruction's parameters and Adam moments resident on
 the device, and runs requests as follows:
 
-* Admission is by an HBM budget. A reconstruction whose full fit-step
-  footprint (all buffers of a ``FitScene`` plus its captured graph) fits the
-  remaining budget is kept *graphed*: one CUDA-graph replay per step. One that
-  does not fit is kept *lean*: parameters, Adam moments, cameras and target
+* Admission is by an HBM budget. Lean steps run one at a time, and the
+  largest transient peak of a lean step (measured by its first step at
+  admission) is held back from the budget. A reconstruction whose full
+  fit-step footprint (all buffers of a ``FitScene`` plus its captured graph)
+  fits the rest is kept *graphed*: one CUDA-graph replay per step. The
+  graph's private memory is only known after capture; if it tips the total
+  over the budget, the graph is dropped and the reconstruction kept lean. One
+  that does not fit is kept *lean*: parameters, Adam moments, cameras and target
   resident, every other buffer allocated for the step and released after it.
   A lean step runs the explicit API (which rebuilds the intersection lists each
   step) plus the same fused activation + Adam update. A reconstruction that
@@ -17,6 +21,18 @@ the device, and runs requests as follows:
   of ``slots`` CUDA streams is free, so requests that arrive while others run
   are started immediately and their kernels overlap on the device. Completion
   is detected with CUDA events; latency is arrival to completion.
+* A graphed step whose intersection lists outgrow their capacity skips its
+  update and raises the scene's overflow flag; each replay copies that flag
+  to pinned host memory ahead of its completion event. On completion the
+  server grows the capacity, redoes the step eagerly and captures the graph
+  again, so every completed request is one applied update.
+* Requests for a reconstruction that is still waiting for memory are dropped
+  and counted (``ServeStats.rejected``); a key that was never offered raises
+  ``KeyError`` before anything runs.
+
+``snapshot(key)`` / ``restore(key, snapshot)`` copy a reconstruction's
+parameters, activations, Adam moments and step counter to host memory and
+back; a restored reconstruction continues bit for bit as the original would.
 
 ``serve()`` replays a list of (arrival time, reconstruction) requests against
 the wall clock and reports fit-steps/s with p50/p99 latency. ``serve_serially``
@@ -51,6 +67,7 @@ class Reconstruction:
     busy: bool = False
     steps: int = 0
     footprint: int = 0
+    overflow_host: Optional[Tensor] = None  # pinned copy of the scene's overflow flag after each replay
 
 
 @dataclass
@@ -61,6 +78,8 @@ class ServeStats:
     lean: int = 0
     graphed: int = 0
     waited_for_memory: int = 0
+    rejected: int = 0
+    regrown: int = 0
 
     @property
     def steps_per_s(self) -> float:
@@ -76,23 +95,31 @@ class ServeStats:
     def summary(self) -> dict:
         return {"completed": self.completed, "wall_s": self.wall_s, "fit_steps_per_s": self.steps_per_s,
                 "p50_ms": self.percentile(50), "p99_ms": self.percentile(99), "graphed": self.graphed,
-                "lean": self.lean, "waited_for_memory": self.waited_for_memory}
+                "lean": self.lean, "waited_for_memory": self.waited_for_memory, "rejected": self.rejected,
+                "regrown": self.regrown}
 
 
-def lean_step(scene: batched.FitScene):
-    """One fit step through the explicit API with transient buffers, then the fused update."""
+def lean_step(scene: batched.FitScene, recompute: bool = False):
+    """One fit step through the explicit API with transient buffers, then the fused update.
+
+    ``recompute``: free each forward's intersection lists before its backward (the raster VJP never reads
+    them; the voxel VJP then walks the primitives' tile boxes), so the lists of the two passes are never
+    resident at the same time as the backward's buffers.
+    """
     cfg = scene.cfg
     _, ctx, v_image, image_loss, _ = explicit.rasterize_fwd_with_loss(
         scene.means, scene.quats, scene.scales, scene.densities, scene.viewmats, scene.Ks, cfg.image_size,
         scene.target, loss="mse", beta=scene.beta, eps=cfg.eps, radius_clip=cfg.radius_clip)
+    if recompute:
+        explicit.release_intersection_lists(ctx)
     g = explicit.rasterize_bwd(ctx, v_image)
     volume, vctx = explicit.voxelize_fwd(scene.means, scene.quats, scene.scales, scene.densities, cfg.volume_shape,
                                          volume_extent=cfg.volume_extent, volume_center=cfg.volume_center,
                                          beta=scene.beta, eps=cfg.eps, radius_clip=cfg.radius_clip)
-    vol4 = volume.unsqueeze(0)
-    tv, _, _ = low.volume_loss_fwd(vol4, cfg.lambda_tv)
-    g_vol = low.volume_loss_bwd(vol4, scene.ones, cfg.lambda_tv)[0]
-    gv = explicit.voxelize_bwd(vctx, g_vol)
+    if recompute:
+        explicit.release_intersection_lists(vctx)
+    tv, _, g_vol = low.volume_loss_fwd_bwd(volume.unsqueeze(0), scene.ones, cfg.lambda_tv)
+    gv = explicit.voxelize_bwd(vctx, g_vol[0])
     torch.add(image_loss.reshape(1), tv.reshape(1), out=scene.loss)
     ga = (ctypes.c_void_p * 5)(*[None if t is None else t.data_ptr() for t in (g.means, g.quats, g.scales,
                                                                                g.densities, g.beta)])
@@ -112,10 +139,16 @@ def lean_step(scene: batched.FitScene):
 class FitServer:
     """Admits reconstructions against an HBM budget and serves fit-step requests continuously."""
 
-    def __init__(self, budget_bytes: int, slots: int = 8, device="cuda"):
+    def __init__(self, budget_bytes: int, slots: int = 8, device="cuda", lean_recompute: bool = False):
+        """``lean_recompute``: lean reconstructions free each forward's intersection lists before the
+        backward (``lean_step(recompute=True)``), for budgets that large reconstructions press against."""
         self.device = torch.device(device)
+        self.lean_recompute = bool(lean_recompute)
         self.budget = int(budget_bytes)
         self.used = 0
+        # Peak transient memory of one lean step (the largest measured at admission). Lean steps run one at
+        # a time, so this much of the budget is held back from resident reconstructions.
+        self.lean_reserve = 0
         self.streams = [torch.cuda.Stream(device=self.device) for _ in range(slots)]
         self.recons: dict = {}
         self.waiting: deque = deque()  # (key, factory) not yet admitted
@@ -128,19 +161,41 @@ class FitServer:
         scene = factory()
         torch.cuda.synchronize(self.device)
         full = torch.cuda.memory_allocated(self.device) - before
-        if self.used + full <= self.budget:
+        recon, warm_steps = None, 0
+        if not scene.is_lean and self.used + full + self.lean_reserve <= self.budget:
             recon = Reconstruction(key, scene, graphed=True, footprint=full)
             self._capture(recon)
-        else:
+            if self.used + recon.footprint + self.lean_reserve > self.budget:
+                # The graph's private pool tipped it over: keep it lean instead (its warm-up step stays applied).
+                warm_steps, recon.graph, recon = recon.steps, None, None
+                torch.cuda.synchronize(self.device)
+        if recon is None:
             # Lean: release every fit-step buffer; keep parameters, moments, cameras, target.
             self._make_lean(scene)
             torch.cuda.synchronize(self.device)
             lean = torch.cuda.memory_allocated(self.device) - before
-            if self.used + lean > self.budget:
+            transient = 0
+            fits = self.used + lean + self.lean_reserve <= self.budget
+            if fits and warm_steps == 0:
+                # One real step measures the lean step's transient peak (and warms the scene up, as a
+                # graphed admission's first step does).
+                torch.cuda.reset_peak_memory_stats(self.device)
+                base = torch.cuda.memory_allocated(self.device)
+                try:
+                    lean_step(scene, recompute=self.lean_recompute)
+                    torch.cuda.synchronize(self.device)
+                    transient = torch.cuda.max_memory_allocated(self.device) - base
+                    warm_steps = 1
+                except torch.cuda.OutOfMemoryError:
+                    fits = False
+            fits = fits and self.used + lean + max(self.lean_reserve, transient) <= self.budget
+            if not fits:
                 del scene
+                torch.cuda.empty_cache()
                 self.waiting.append((key, factory))
                 return False
-            recon = Reconstruction(key, scene, graphed=False, footprint=lean)
+            self.lean_reserve = max(self.lean_reserve, transient)
+            recon = Reconstruction(key, scene, graphed=False, footprint=lean, steps=warm_steps)
         self.used += recon.footprint
         self.recons[key] = recon
         return True
@@ -153,11 +208,16 @@ class FitServer:
         for name in list(vars(scene)):
             if name not in keep and isinstance(getattr(scene, name), (torch.Tensor, list)):
                 setattr(scene, name, None)
+        scene.is_lean = True
 
-    def _capture(self, recon: Reconstruction):
+    def _capture(self, recon: Reconstruction, warm: bool = True):
+        """Captures the reconstruction's fit step; ``warm`` first runs one real eager step outside capture."""
         scene = recon.scene
-        scene.step()  # warm-up outside capture (a real step)
-        recon.steps += 1
+        if warm:
+            scene.step()
+            recon.steps += 1
+        if recon.overflow_host is None:
+            recon.overflow_host = torch.zeros(1, dtype=torch.int32, pin_memory=True)
         torch.cuda.synchronize(self.device)
         before = torch.cuda.memory_allocated(self.device)
         graph = torch.cuda.CUDAGraph()
@@ -166,6 +226,24 @@ class FitServer:
         torch.cuda.synchronize(self.device)
         recon.footprint += torch.cuda.memory_allocated(self.device) - before
         recon.graph = graph
+
+    # ----------------------------------------------------------- snapshot / restore
+    def snapshot(self, key) -> dict:
+        """Host copy of a resident reconstruction's parameters, activations, Adam moments and step counter.
+
+        Waits for the reconstruction's work in flight on the device; call it between ``serve()`` runs.
+        """
+        recon = self.recons[key]
+        torch.cuda.synchronize(self.device)
+        return {"steps": recon.steps, "state": recon.scene.state_dict()}
+
+    def restore(self, key, snapshot: dict):
+        """Puts a snapshot back into an admitted reconstruction of the same shape; its captured graph
+        (if any) stays valid, since the state is copied into the same device buffers."""
+        recon = self.recons[key]
+        torch.cuda.synchronize(self.device)
+        recon.scene.load_state_dict(snapshot["state"])
+        recon.steps = snapshot["steps"]
 
     def evict(self, key):
         recon = self.recons.pop(key)
@@ -185,16 +263,44 @@ class FitServer:
         with torch.cuda.stream(stream):
             if recon.graphed:
                 recon.graph.replay()
+                recon.overflow_host.copy_(recon.scene.overflow, non_blocking=True)
             else:
-                lean_step(recon.scene)
+                lean_step(recon.scene, recompute=self.lean_recompute)
             done = torch.cuda.Event()
             done.record(stream)
         return done
 
+    def _finish(self, recon: Reconstruction, stats: ServeStats):
+        """Completion of a step: a graphed step that overflowed is redone with room, then re-captured."""
+        if not recon.graphed or int(recon.overflow_host[0]) == 0:
+            return
+        scene = recon.scene
+        torch.cuda.synchronize(self.device)
+        before = torch.cuda.memory_allocated(self.device)
+        recon.graph = None
+        scene.set_capacity(*scene.needs_capacity())
+        scene.step()  # the skipped update, now with room (it grows again if it must)
+        self._capture(recon, warm=False)
+        torch.cuda.synchronize(self.device)
+        grown = torch.cuda.memory_allocated(self.device) - before
+        recon.footprint += grown
+        self.used += grown
+        stats.regrown += 1
+
     def serve(self, requests: list, poll_s: float = 2e-5) -> ServeStats:
-        """requests: [(arrival_s, key)] sorted by arrival, relative to the call. Runs them all."""
+        """requests: [(arrival_s, key)] relative to the call. Runs every request of an admitted reconstruction.
+
+        Requests for reconstructions still waiting for memory are dropped and
+        counted in ``rejected``; a key the server has never been offered raises
+        KeyError before anything runs.
+        """
+        waiting = {key for key, _ in self.waiting}
+        unknown = sorted({repr(key) for _, key in requests if key not in self.recons and key not in waiting})
+        if unknown:
+            raise KeyError(f"requests name reconstructions that were never admitted: {', '.join(unknown)}")
         pending: dict = {key: deque() for key in self.recons}
-        arrivals = deque(sorted(requests, key=lambda r: r[0]))
+        rejected = sum(1 for _, key in requests if key not in self.recons)
+        arrivals = deque(sorted((r for r in requests if r[1] in self.recons), key=lambda r: r[0]))
         free = list(range(len(self.streams)))
         in_flight: list = []  # (event, slot, key, arrival)
         ready: list = []  # heap of (arrival, seq, key)
@@ -202,7 +308,9 @@ class FitServer:
         stats.graphed = sum(r.graphed for r in self.recons.values())
         stats.lean = len(self.recons) - stats.graphed
         stats.waited_for_memory = len(self.waiting)
+        stats.rejected = rejected
         seq = 0
+        lean_in_flight = 0
         start = time.perf_counter()
         while arrivals or in_flight or ready or any(pending.values()):
             now = time.perf_counter() - start
@@ -216,9 +324,11 @@ class FitServer:
             still = []
             for event, slot, key, t in in_flight:
                 if event.query():
+                    recon = self.recons[key]
+                    lean_in_flight -= int(not recon.graphed)
+                    self._finish(recon, stats)
                     stats.completed += 1
                     stats.latencies_ms.append((time.perf_counter() - start - t) * 1e3)
-                    recon = self.recons[key]
                     recon.busy = False
                     recon.steps += 1
                     free.append(slot)
@@ -229,14 +339,22 @@ class FitServer:
                 else:
                     still.append((event, slot, key, t))
             in_flight = still
+            deferred = []
             while free and ready:
-                t, _, key = heapq.heappop(ready)
+                item = heapq.heappop(ready)
+                t, _, key = item
                 recon = self.recons[key]
+                if not recon.graphed and lean_in_flight:
+                    deferred.append(item)  # lean steps run one at a time (their transient is reserved once)
+                    continue
                 pending[key].popleft()
                 recon.busy = True
+                lean_in_flight += int(not recon.graphed)
                 slot = free.pop()
                 in_flight.append((self._launch(recon, self.streams[slot]), slot, key, t))
                 progressed = True
+            for item in deferred:
+                heapq.heappush(ready, item)
             if not progressed:
                 time.sleep(poll_s)
         stats.wall_s = time.perf_counter() - start

@@ -1,7 +1,8 @@
 """Generates the golden fixtures in tests/golden/ from the reference checkout.
 
-Run in a container that has the reference at /root/reference (read-only):
-    python tests/golden/make_golden.py [--reference /root/reference]
+Run where the reference checkout is readable, naming it by argument or by the
+R2SPLAT_REFERENCE environment variable:
+    python tests/golden/make_golden.py --reference <checkout>
 
 Outputs (small, committed):
 * dense_oracle.pt -- the reference's own float64 test oracle
@@ -22,6 +23,7 @@ import argparse
 import ast
 import importlib.util
 import json
+import os
 import sys
 from pathlib import Path
 
@@ -126,8 +128,11 @@ def tv_case():
 
 def main(argv=None) -> int:
     parser = argparse.ArgumentParser()
-    parser.add_argument("--reference", default="/root/reference")
+    parser.add_argument("--reference", default=os.environ.get("R2SPLAT_REFERENCE"),
+                        help="reference checkout (default: $R2SPLAT_REFERENCE)")
     args = parser.parse_args(argv)
+    if not args.reference:
+        parser.error("give --reference or set R2SPLAT_REFERENCE")
     reference = Path(args.reference)
     oracle = load_reference_oracle(reference)
     torch.save(dense_cases(oracle), HERE / "dense_oracle.pt")

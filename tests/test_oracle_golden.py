@@ -133,3 +133,45 @@ def test_l1_oracle_forward_and_backward():
     assert l1 == pytest.approx(0.625) and loss == pytest.approx(1.25)
     g = losses.l1_backward(p, t, [1.0], 2.0)
     assert g.tolist() == [[[0.5, 0.0], [-0.5, -0.5]]]
+
+
+@pytest.mark.parametrize("beta", [None, 2.6])
+def test_absgrad_oracle_is_the_sum_of_per_pixel_gradient_magnitudes(beta):
+    """absgrad_dense against autograd: the per-pixel terms v_p alpha_p(mean) differentiated one by one.
+
+    The statistic the reference's VJPs return with absgrad (RasterizeToPixelsBwd.cu:216-221,
+    :459-462) is sum_p |d(v_p alpha_p) / d mean| per component, over the samples the forward
+    counts; this derives it independently of the closed form the oracle writes out.
+    """
+    gen = torch.Generator().manual_seed(17)
+    h, w = 7, 9
+    means2d = torch.tensor([[[3.1, 2.7], [5.6, 4.2]]], dtype=torch.float64)
+    conics = torch.tensor([[[0.30, 0.05, 0.45], [0.12, -0.03, 0.10]]], dtype=torch.float64)
+    opac = torch.tensor([[1.3, 0.7]], dtype=torch.float64)
+    mus = torch.tensor([[0.9, 1.4]], dtype=torch.float64)
+    v = torch.randn((1, h, w), generator=gen, dtype=torch.float64)
+    betas = None if beta is None else torch.tensor([[beta, beta + 0.8]], dtype=torch.float64)
+    got = dense.absgrad_dense(means2d, conics, opac, mus, v, betas=betas)
+    yy, xx = torch.meshgrid(torch.arange(h, dtype=torch.float64) + 0.5, torch.arange(w, dtype=torch.float64) + 0.5,
+                            indexing="ij")
+    want = torch.zeros(1, 2, 2, dtype=torch.float64)
+    for n in range(2):
+        a, b, c = conics[0, n]
+
+        def terms(mean):
+            dx, dy = xx - mean[0], yy - mean[1]
+            if betas is None:
+                sigma = 0.5 * (a * dx * dx + c * dy * dy) + b * dx * dy
+                alpha = opac[0, n] * mus[0, n] * torch.exp(-sigma)
+                valid = (sigma >= 0) & (alpha.abs() >= 1e-5)
+            else:
+                d2 = a * dx * dx + 2 * b * dx * dy + c * dy * dy
+                hh = (1 - d2).clamp_min(1e-300)
+                alpha = opac[0, n] * mus[0, n] * hh.pow(betas[0, n])
+                valid = (d2 >= 0) & (d2 < 1) & (alpha.abs() >= 1e-5)
+            return torch.where(valid.detach(), v[0] * alpha, torch.zeros_like(alpha)).reshape(-1)
+
+        jac = torch.autograd.functional.jacobian(terms, means2d[0, n].clone())  # [H*W, 2]
+        want[0, n] = jac.abs().sum(0)
+    assert float(want.abs().max()) > 0
+    torch.testing.assert_close(got, want, rtol=1e-12, atol=1e-14)
