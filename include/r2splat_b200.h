@@ -367,12 +367,19 @@ int r2s_raster_render_bwd(int dtype, const void* records, const void* uncertaint
  * tile rectangle rects [C,N,4] (uint16 x0, y0, x1, y1 in tiles, upper bounds
  * exclusive, as r2s_raster_project writes them) and written to grads [C,N,8]
  * without atomics (every record written; the buffer needs no clearing).
- * v_means2d_abs [C,N,2] optional (written); v_uncertainties [N] accumulated
- * (clear it first). Same adjoints as r2s_raster_render_bwd. */
+ * v_means2d_abs [C,N,2] optional (written); v_uncertainties [C,N] with the
+ * variance branch: each record's uncertainty adjoint (written), to be summed
+ * over cameras by r2s_sum_over_cameras, so the result does not depend on the
+ * order the records finish in. Same adjoints as r2s_raster_render_bwd. */
 int r2s_raster_record_bwd(int dtype, const void* records, const uint16_t* rects, const void* uncertainties,
                           int beta, int detach_variance, const void* v_render, const void* v_render_var,
                           uint32_t C, uint32_t N, uint32_t width, uint32_t height, uint32_t tile_size,
                           void* grads, void* v_means2d_abs, void* v_uncertainties, void* stream);
+
+/* out [N] = sum over cameras c of per_record [C,N], in camera order (the
+ * record VJP's uncertainty adjoints; no reference counterpart as a call: the
+ * reference adds them with atomics inside K20/K22). */
+int r2s_sum_over_cameras(int dtype, const void* per_record, uint32_t C, uint32_t N, void* out, void* stream);
 
 /* Chain rule from packed adjoints to physical parameters (explicit.py:225-241):
  * conic/mu VJP, projection VJP summed over cameras, Beta path factor and the

@@ -280,12 +280,16 @@ def raster_backward(state: RasterState, means, quats, scales, densities, beta, u
     tile = state.tile_size
     stream = _stream(device)
     grads = means.new_empty((c, n, 8))  # every record is written by the record-parallel VJP
-    v_unc = means.new_zeros((n,)) if v_variance is not None else None
+    # With the variance branch: one uncertainty adjoint per record, summed over cameras in order.
+    v_unc_cn = means.new_empty((c, n)) if v_variance is not None else None
+    v_unc = means.new_empty((n,)) if v_variance is not None else None
     with _stage("raster_render_bwd"):
         _backend.call("r2s_raster_record_bwd", _dtype(means), _ptr(state.records), _ptr(state.extra["rects"]),
                       _ptr(uncertainty), int(beta is not None), int(bool(detach_variance)), _ptr(v_image),
-                      _ptr(v_variance), c, n, state.width, state.height, tile, _ptr(grads), None, _ptr(v_unc),
+                      _ptr(v_variance), c, n, state.width, state.height, tile, _ptr(grads), None, _ptr(v_unc_cn),
                       stream)
+    if v_unc is not None:
+        _backend.call("r2s_sum_over_cameras", _dtype(means), _ptr(v_unc_cn), c, n, _ptr(v_unc), stream)
     log_grad = _beta.beta_path_log_grad(beta) if beta is not None else None
     v_means = means.new_empty((n, 3))
     v_quats = means.new_empty((n, 4))

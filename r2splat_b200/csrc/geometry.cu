@@ -248,16 +248,40 @@ __global__ void raster_project_kernel(const S* __restrict__ means, const S* __re
 // every fourth camera, partial sums combined by shuffles (no atomics). grads
 // [C,N,8] holds the adjoints of the packed record slots.
 constexpr uint32_t kChainGroup = 4;  // lanes per primitive in the chain-rule pass
+constexpr uint32_t kChainThreads = 128;
+// Up to this many cameras the block first writes the camera table (extrinsics,
+// intrinsics and clamp limits) to shared memory; beyond it each pair loads its
+// camera and derives the limits itself.
+constexpr uint32_t kChainTableCameras = 256;
 
 template <typename S>
-__global__ void raster_chain_bwd_kernel(const S* __restrict__ means, const S* __restrict__ quats,
-                                        const S* __restrict__ scales, const S* __restrict__ covars,
-                                        const S* __restrict__ ratio, const S* __restrict__ log_grad,
-                                        const S* __restrict__ viewmats, const S* __restrict__ Ks, uint32_t C,
-                                        uint32_t N, uint32_t width, uint32_t height, S eps_blur, S eps,
-                                        const Rec2D<S>* __restrict__ grads, S* __restrict__ v_means,
-                                        S* __restrict__ v_quats, S* __restrict__ v_scales,
-                                        S* __restrict__ v_densities, S* __restrict__ v_betas) {
+struct CameraEntry {
+    Camera<S> cam;
+    CameraLimits<S> lim;
+};
+
+// Per (camera, primitive) pair: the projection's frame once, the projected
+// covariance from it, the conic/mu VJP, then the projection VJP from the same
+// frame (the forward projection and its VJP share the camera-space centre,
+// Jacobian and camera-space covariance).
+template <typename S, bool kTable>
+__global__ void __launch_bounds__(kChainThreads) raster_chain_bwd_kernel(
+    const S* __restrict__ means, const S* __restrict__ quats, const S* __restrict__ scales,
+    const S* __restrict__ covars, const S* __restrict__ ratio, const S* __restrict__ log_grad,
+    const S* __restrict__ viewmats, const S* __restrict__ Ks, uint32_t C, uint32_t N, uint32_t width,
+    uint32_t height, S eps, const Rec2D<S>* __restrict__ grads, S* __restrict__ v_means, S* __restrict__ v_quats,
+    S* __restrict__ v_scales, S* __restrict__ v_densities, S* __restrict__ v_betas) {
+    extern __shared__ __align__(16) unsigned char chain_smem[];
+    CameraEntry<S>* s_cams = reinterpret_cast<CameraEntry<S>*>(chain_smem);
+    if (kTable) {
+        for (uint32_t c = threadIdx.x; c < C; c += blockDim.x) {
+            CameraEntry<S> e;
+            e.cam = load_camera(viewmats, Ks, c);
+            e.lim = camera_limits(e.cam, width, height);
+            s_cams[c] = e;
+        }
+        __syncthreads();
+    }
     // kChainGroup consecutive lanes share a primitive, each taking every
     // kChainGroup-th camera; their partial sums are combined by shuffles in a
     // fixed order (deterministic).
@@ -282,10 +306,24 @@ __global__ void raster_chain_bwd_kernel(const S* __restrict__ means, const S* __
         acc_o += g.o;
         if (g.x == S(0) && g.y == S(0) && g.a == S(0) && g.b == S(0) && g.c == S(0) && g.mu == S(0) &&
             g.beta == S(0)) continue;
-        const Camera<S> cam = load_camera(viewmats, Ks, c);
-        Projected<S> p;
-        project(cam, px, py, pz, sig, width, height, eps_blur, S(1), p);
-        const S cov[6] = {p.c00, p.c01, p.c02, p.c11, p.c12, p.c22};
+        Camera<S> cam;
+        CameraLimits<S> lim;
+        if (kTable) {
+            cam = s_cams[c].cam;
+            lim = s_cams[c].lim;
+        } else {
+            cam = load_camera(viewmats, Ks, c);
+            lim = camera_limits(cam, width, height);
+        }
+        ProjectionFrame<S> f;
+        if (!projection_frame(cam, lim, px, py, pz, sig, f)) {
+            // Behind the camera: no covariance, mu = 0; only the Beta slot's
+            // own adjoint passes through.
+            if (is_beta) acc_beta += g.beta;
+            continue;
+        }
+        S cov[6];
+        projection_cov(f, cov);
         S u11, u12, u22, base_mu;
         conic_and_mu(cov, eps, u11, u12, u22, base_mu);
         S v_mu = g.mu;
@@ -297,7 +335,7 @@ __global__ void raster_chain_bwd_kernel(const S* __restrict__ means, const S* __
         }
         S vcov[6], vp[3], vs[6];
         conic_and_mu_vjp(cov, u11, u12, u22, base_mu, g.a, g.b, g.c, v_mu, vcov);
-        if (!project_vjp(cam, px, py, pz, sig, width, height, g.x, g.y, vcov, vp, vs)) continue;
+        projection_vjp(cam, f, g.x, g.y, vcov, vp, vs);
 #pragma unroll
         for (int k = 0; k < 3; ++k) acc_p[k] += vp[k];
 #pragma unroll
@@ -529,14 +567,32 @@ int r2s_raster_chain_bwd(int dtype, const void* means, const void* quats, const 
     const bool beta = betas != nullptr;
     R2S_REQUIRE(!beta || (ratio != nullptr && log_grad != nullptr && v_betas != nullptr), R2S_ERR_ARGUMENT,
                 "Beta chain rule needs ratio, log_grad and v_betas");
-    R2S_DISPATCH(dtype, raster_chain_bwd_kernel<S><<<blocks_for(uint64_t(N) * kChainGroup, 128), 128, 0,
-                                                    as_stream(stream)>>>(
-        static_cast<const S*>(means), static_cast<const S*>(quats), static_cast<const S*>(scales),
-        static_cast<const S*>(covars), beta ? static_cast<const S*>(ratio) : nullptr,
-        beta ? static_cast<const S*>(log_grad) : nullptr, static_cast<const S*>(viewmats),
-        static_cast<const S*>(Ks), C, N, width, height, static_cast<S>(eps_blur), static_cast<S>(eps),
-        static_cast<const Rec2D<S>*>(grads), static_cast<S*>(v_means), static_cast<S*>(v_quats),
-        static_cast<S*>(v_scales), static_cast<S*>(v_densities), static_cast<S*>(v_betas)));
+    (void)eps_blur;  // only the pixel radii depend on it, and the chain rule does not use them
+    R2S_DISPATCH(dtype, {
+        const unsigned blocks = blocks_for(uint64_t(N) * kChainGroup, kChainThreads);
+        const auto* mp = static_cast<const S*>(means);
+        const auto* qp = static_cast<const S*>(quats);
+        const auto* sp = static_cast<const S*>(scales);
+        const auto* cp = static_cast<const S*>(covars);
+        const auto* rp = beta ? static_cast<const S*>(ratio) : nullptr;
+        const auto* lp = beta ? static_cast<const S*>(log_grad) : nullptr;
+        const auto* vm = static_cast<const S*>(viewmats);
+        const auto* kp = static_cast<const S*>(Ks);
+        const auto* gp = static_cast<const Rec2D<S>*>(grads);
+        if (C <= kChainTableCameras) {
+            const size_t smem = size_t(C) * sizeof(CameraEntry<S>);
+            R2S_TRY(allow_dynamic_smem(raster_chain_bwd_kernel<S, true>, smem));
+            raster_chain_bwd_kernel<S, true><<<blocks, kChainThreads, smem, as_stream(stream)>>>(
+                mp, qp, sp, cp, rp, lp, vm, kp, C, N, width, height, static_cast<S>(eps), gp, static_cast<S*>(v_means),
+                static_cast<S*>(v_quats), static_cast<S*>(v_scales), static_cast<S*>(v_densities),
+                static_cast<S*>(v_betas));
+        } else {
+            raster_chain_bwd_kernel<S, false><<<blocks, kChainThreads, 0, as_stream(stream)>>>(
+                mp, qp, sp, cp, rp, lp, vm, kp, C, N, width, height, static_cast<S>(eps), gp, static_cast<S*>(v_means),
+                static_cast<S*>(v_quats), static_cast<S*>(v_scales), static_cast<S*>(v_densities),
+                static_cast<S*>(v_betas));
+        }
+    });
     return check_launch("raster_chain_bwd");
 }
 

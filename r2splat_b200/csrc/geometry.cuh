@@ -333,53 +333,70 @@ __device__ __forceinline__ void conic_and_mu_vjp(
     v_cov[3] = grad_d; v_cov[4] = grad_e; v_cov[5] = grad_f;
 }
 
-// VJP of project() for one (camera, primitive) pair with respect to the
-// world mean and packed world covariance (WorldToImageProjectionBwd.cu:97-545).
-// Returns false when the pair is behind the camera (no contribution).
+// Clamp limits of the normalised image coordinates x/z, y/z used for the
+// Jacobian (the same expressions as in project()): they depend only on the
+// intrinsics and the image size, so per-camera tables can hold them.
 template <typename S>
-__device__ __forceinline__ bool project_vjp(
-    const Camera<S>& cam, S px, S py, S pz, const S* sig, uint32_t width, uint32_t height,
-    S vm2_x, S vm2_y, const S* vcov, S* v_p, S* v_s
-) {
+struct CameraLimits {
+    S x_pos, x_neg, y_pos, y_neg;
+};
+
+template <typename S>
+__device__ __forceinline__ CameraLimits<S> camera_limits(const Camera<S>& cam, uint32_t width, uint32_t height) {
+    const S Wd = static_cast<S>(width);
+    const S Hd = static_cast<S>(height);
+    const S tan_fovx = static_cast<S>(0.5) * Wd / cam.fx;
+    const S tan_fovy = static_cast<S>(0.5) * Hd / cam.fy;
+    CameraLimits<S> lim;
+    lim.x_pos = (Wd - cam.cx) / cam.fx + static_cast<S>(0.3) * tan_fovx;
+    lim.x_neg = cam.cx / cam.fx + static_cast<S>(0.3) * tan_fovx;
+    lim.y_pos = (Hd - cam.cy) / cam.fy + static_cast<S>(0.3) * tan_fovy;
+    lim.y_neg = cam.cy / cam.fy + static_cast<S>(0.3) * tan_fovy;
+    return lim;
+}
+
+// The intermediates of the projection of one (camera, primitive) pair that
+// both its covariance and its VJP use: camera-space centre, clamped centre,
+// Jacobian and camera-space covariance.
+template <typename S>
+struct ProjectionFrame {
+    S x, y, z, rz, rz2, tx, ty, rl;
+    S J00, J02, J11, J12, J20, J21, J22;
+    S Sc00, Sc01, Sc02, Sc11, Sc12, Sc22;
+    bool x_clipped, y_clipped;
+};
+
+// Fills f; false when the pair is behind the camera (z <= 0.01).
+template <typename S>
+__device__ __forceinline__ bool projection_frame(const Camera<S>& cam, const CameraLimits<S>& lim, S px, S py, S pz,
+                                                 const S* sig, ProjectionFrame<S>& f) {
     const S R00 = cam.R00, R01 = cam.R01, R02 = cam.R02;
     const S R10 = cam.R10, R11 = cam.R11, R12 = cam.R12;
     const S R20 = cam.R20, R21 = cam.R21, R22 = cam.R22;
-    const S fx = cam.fx, fy = cam.fy, cx = cam.cx, cy = cam.cy;
     const S s00 = sig[0], s01 = sig[1], s02 = sig[2], s11 = sig[3], s12 = sig[4], s22 = sig[5];
 
     const S x = R00 * px + R01 * py + R02 * pz + cam.t0;
     const S y = R10 * px + R11 * py + R12 * pz + cam.t1;
     const S z = R20 * px + R21 * py + R22 * pz + cam.t2;
     if (z <= static_cast<S>(0.01)) return false;
-
     const S rz = static_cast<S>(1) / z;
     const S rz2 = rz * rz;
-    const S rz3 = rz2 * rz;
-    const S Wd = static_cast<S>(width);
-    const S Hd = static_cast<S>(height);
-    const S tan_fovx = static_cast<S>(0.5) * Wd / fx;
-    const S tan_fovy = static_cast<S>(0.5) * Hd / fy;
-    const S lim_x_pos = (Wd - cx) / fx + static_cast<S>(0.3) * tan_fovx;
-    const S lim_x_neg = cx / fx + static_cast<S>(0.3) * tan_fovx;
-    const S lim_y_pos = (Hd - cy) / fy + static_cast<S>(0.3) * tan_fovy;
-    const S lim_y_neg = cy / fy + static_cast<S>(0.3) * tan_fovy;
     const S xrz = x * rz;
     const S yrz = y * rz;
-    const S tx = z * min(lim_x_pos, max(-lim_x_neg, xrz));
-    const S ty = z * min(lim_y_pos, max(-lim_y_neg, yrz));
-    const bool x_clipped = (xrz > lim_x_pos) || (xrz < -lim_x_neg);
-    const bool y_clipped = (yrz > lim_y_pos) || (yrz < -lim_y_neg);
-
+    const S tx = z * min(lim.x_pos, max(-lim.x_neg, xrz));
+    const S ty = z * min(lim.y_pos, max(-lim.y_neg, yrz));
+    f.x_clipped = (xrz > lim.x_pos) || (xrz < -lim.x_neg);
+    f.y_clipped = (yrz > lim.y_pos) || (yrz < -lim.y_neg);
     const S l = sqrt(tx * tx + ty * ty + z * z);
     const S rl = static_cast<S>(1) / l;
-    const S rl2 = rl * rl;
-    const S J00 = fx * rz;
-    const S J02 = -fx * tx * rz2;
-    const S J11 = fy * rz;
-    const S J12 = -fy * ty * rz2;
-    const S J20 = tx * rl;
-    const S J21 = ty * rl;
-    const S J22 = z * rl;
+    f.x = x; f.y = y; f.z = z; f.rz = rz; f.rz2 = rz2; f.tx = tx; f.ty = ty; f.rl = rl;
+    f.J00 = cam.fx * rz;
+    f.J02 = -cam.fx * tx * rz2;
+    f.J11 = cam.fy * rz;
+    f.J12 = -cam.fy * ty * rz2;
+    f.J20 = tx * rl;
+    f.J21 = ty * rl;
+    f.J22 = z * rl;
 
     const S M00 = s00*R00 + s01*R01 + s02*R02;
     const S M01 = s00*R10 + s01*R11 + s02*R12;
@@ -390,12 +407,51 @@ __device__ __forceinline__ bool project_vjp(
     const S M20 = s02*R00 + s12*R01 + s22*R02;
     const S M21 = s02*R10 + s12*R11 + s22*R12;
     const S M22 = s02*R20 + s12*R21 + s22*R22;
-    const S Sc00 = R00*M00 + R01*M10 + R02*M20;
-    const S Sc01 = R00*M01 + R01*M11 + R02*M21;
-    const S Sc02 = R00*M02 + R01*M12 + R02*M22;
-    const S Sc11 = R10*M01 + R11*M11 + R12*M21;
-    const S Sc12 = R10*M02 + R11*M12 + R12*M22;
-    const S Sc22 = R20*M02 + R21*M12 + R22*M22;
+    f.Sc00 = R00*M00 + R01*M10 + R02*M20;
+    f.Sc01 = R00*M01 + R01*M11 + R02*M21;
+    f.Sc02 = R00*M02 + R01*M12 + R02*M22;
+    f.Sc11 = R10*M01 + R11*M11 + R12*M21;
+    f.Sc12 = R10*M02 + R11*M12 + R12*M22;
+    f.Sc22 = R20*M02 + R21*M12 + R22*M22;
+    return true;
+}
+
+// Projected covariance J Sigma_c J^T of a frame (project()'s c00..c22).
+template <typename S>
+__device__ __forceinline__ void projection_cov(const ProjectionFrame<S>& f, S* cov) {
+    const S N00 = f.Sc00*f.J00 +                f.Sc02*f.J02;
+    const S N01 = f.Sc01*f.J11 + f.Sc02*f.J12;
+    const S N02 = f.Sc00*f.J20 + f.Sc01*f.J21 + f.Sc02*f.J22;
+    const S N11 = f.Sc11*f.J11 + f.Sc12*f.J12;
+    const S N12 = f.Sc01*f.J20 + f.Sc11*f.J21 + f.Sc12*f.J22;
+    const S N20 = f.Sc02*f.J00 +                f.Sc22*f.J02;
+    const S N21 = f.Sc12*f.J11 + f.Sc22*f.J12;
+    const S N22 = f.Sc02*f.J20 + f.Sc12*f.J21 + f.Sc22*f.J22;
+    cov[0] = f.J00*N00 + f.J02*N20;
+    cov[1] = f.J00*N01 + f.J02*N21;
+    cov[2] = f.J00*N02 + f.J02*N22;
+    cov[3] = f.J11*N11 + f.J12*N21;
+    cov[4] = f.J11*N12 + f.J12*N22;
+    cov[5] = f.J20*N02 + f.J21*N12 + f.J22*N22;
+}
+
+// VJP of the projection of one pair from its frame, with respect to the world
+// mean and the packed world covariance (WorldToImageProjectionBwd.cu:97-545):
+// vm2 is the adjoint of the projected centre, vcov that of the packed
+// projected covariance.
+template <typename S>
+__device__ __forceinline__ void projection_vjp(const Camera<S>& cam, const ProjectionFrame<S>& f, S vm2_x, S vm2_y,
+                                               const S* vcov, S* v_p, S* v_s) {
+    const S R00 = cam.R00, R01 = cam.R01, R02 = cam.R02;
+    const S R10 = cam.R10, R11 = cam.R11, R12 = cam.R12;
+    const S R20 = cam.R20, R21 = cam.R21, R22 = cam.R22;
+    const S fx = cam.fx, fy = cam.fy;
+    const S x = f.x, y = f.y, z = f.z, rz = f.rz, rz2 = f.rz2, tx = f.tx, ty = f.ty, rl = f.rl;
+    const S rz3 = rz2 * rz;
+    const S rl2 = rl * rl;
+    const S J00 = f.J00, J02 = f.J02, J11 = f.J11, J12 = f.J12, J20 = f.J20, J21 = f.J21, J22 = f.J22;
+    const S Sc00 = f.Sc00, Sc01 = f.Sc01, Sc02 = f.Sc02, Sc11 = f.Sc11, Sc12 = f.Sc12, Sc22 = f.Sc22;
+    const bool x_clipped = f.x_clipped, y_clipped = f.y_clipped;
 
     const S va = vcov[0], vb = vcov[1], vc_ = vcov[2], vd = vcov[3], ve = vcov[4], vf = vcov[5];
 
@@ -403,7 +459,6 @@ __device__ __forceinline__ bool project_vjp(
     S v_pc_x = fx * rz * vm2_x;
     S v_pc_y = fy * rz * vm2_y;
     S v_pc_z = -(fx * x * rz2 * vm2_x + fy * y * rz2 * vm2_y);
-
     // Covariance: v_Sigma_c = J^T G_upper J with the packed (upper-triangular)
     // adjoint, then v_Sigma = R^T v_Sigma_c R; off-diagonal packed entries
     // collect both symmetric positions.
@@ -498,6 +553,19 @@ __device__ __forceinline__ bool project_vjp(
     v_p[0] = R00 * v_pc_x + R10 * v_pc_y + R20 * v_pc_z;
     v_p[1] = R01 * v_pc_x + R11 * v_pc_y + R21 * v_pc_z;
     v_p[2] = R02 * v_pc_x + R12 * v_pc_y + R22 * v_pc_z;
+}
+
+// VJP of project() for one (camera, primitive) pair with respect to the
+// world mean and packed world covariance (WorldToImageProjectionBwd.cu:97-545).
+// Returns false when the pair is behind the camera (no contribution).
+template <typename S>
+__device__ __forceinline__ bool project_vjp(
+    const Camera<S>& cam, S px, S py, S pz, const S* sig, uint32_t width, uint32_t height,
+    S vm2_x, S vm2_y, const S* vcov, S* v_p, S* v_s
+) {
+    ProjectionFrame<S> f;
+    if (!projection_frame(cam, camera_limits(cam, width, height), px, py, pz, sig, f)) return false;
+    projection_vjp(cam, f, vm2_x, vm2_y, vcov, v_p, v_s);
     return true;
 }
 

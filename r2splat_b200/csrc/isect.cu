@@ -105,6 +105,62 @@ __global__ void emit_rects_kernel(const ushort4* __restrict__ rects, uint32_t to
         }
 }
 
+// The same output as emit_rects_kernel, written cooperatively: a warp takes 32
+// consecutive elements, whose runs form one contiguous range of the output, and
+// its lanes stride over that range, so consecutive lanes write consecutive keys
+// and values (one-thread-per-element writes are scattered over 32 runs). Each
+// lane finds the element owning its position by a 5-step binary search over the
+// warp's 32 run starts, exchanged by shuffles.
+__global__ void __launch_bounds__(256) emit_rects_warp_kernel(const ushort4* __restrict__ rects, uint32_t total,
+                                                               uint32_t N, uint32_t tiles_x, uint32_t tiles_y,
+                                                               const int64_t* __restrict__ cum, int64_t capacity,
+                                                               uint32_t* __restrict__ keys,
+                                                               uint32_t* __restrict__ vals) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t i0 = warp * 32u;
+    if (i0 >= total) return;  // warp-uniform
+    const uint32_t i = uint32_t(i0) + lane;
+    const bool have = i < total;
+    ushort4 r = make_ushort4(0, 0, 0, 0);
+    int64_t start = 0, end = 0;
+    if (have) {
+        r = rects[i];
+        start = i == 0 ? 0 : cum[i - 1];
+        end = cum[i];
+    } else {
+        start = end = cum[total - 1];
+    }
+    const bool nonempty = have && r.z > r.x && r.w > r.y;
+    const uint32_t width = nonempty ? uint32_t(r.z - r.x) : 1u;
+    const int64_t range_start = __shfl_sync(0xffffffffu, start, 0);
+    const int64_t range_end = __shfl_sync(0xffffffffu, end, 31);
+    const uint32_t n_tiles = tiles_x * tiles_y;
+    // A warp-uniform trip count: every lane takes part in every shuffle.
+    const int64_t steps = (range_end - range_start + 31) / 32;
+    for (int64_t k = 0; k < steps; ++k) {
+        const int64_t p = range_start + k * 32 + lane;
+        // Owner: the last lane whose run starts at or before p (empty runs start where the next one does,
+        // so the search lands on the non-empty run that holds p).
+        uint32_t lo = 0u;
+#pragma unroll
+        for (uint32_t step = 16u; step > 0u; step >>= 1) {
+            const int64_t s_mid = __shfl_sync(0xffffffffu, start, int(lo + step));
+            if (s_mid <= p) lo += step;
+        }
+        const int64_t s_owner = __shfl_sync(0xffffffffu, start, int(lo));
+        const uint32_t w_owner = __shfl_sync(0xffffffffu, width, int(lo));
+        const uint32_t x0 = __shfl_sync(0xffffffffu, uint32_t(r.x), int(lo));
+        const uint32_t y0 = __shfl_sync(0xffffffffu, uint32_t(r.y), int(lo));
+        if (p >= range_end || p >= capacity) continue;
+        const uint32_t local = uint32_t(p - s_owner);
+        const uint32_t row = local / w_owner, col = local - row * w_owner;
+        const uint32_t elem = uint32_t(i0) + lo;
+        keys[p] = (elem / N) * n_tiles + (y0 + row) * tiles_x + (x0 + col);
+        vals[p] = elem;
+    }
+}
+
 template <typename S>
 __global__ void emit_3d_kernel(const S* __restrict__ means3d, const int32_t* __restrict__ radii, uint32_t N,
                                uint32_t tile_size, uint32_t tx, uint32_t ty, uint32_t tz,
@@ -124,7 +180,60 @@ __global__ void emit_3d_kernel(const S* __restrict__ means3d, const int32_t* __r
             }
 }
 
-// --------------------------------------------------------------- radix sort
+// 3D counterpart of emit_rects_warp_kernel (the output of emit_3d_kernel, written cooperatively).
+template <typename S>
+__global__ void __launch_bounds__(256) emit_3d_warp_kernel(const S* __restrict__ means3d,
+                                                            const int32_t* __restrict__ radii, uint32_t N,
+                                                            uint32_t tile_size, uint32_t tx, uint32_t ty, uint32_t tz,
+                                                            const int64_t* __restrict__ cum, int64_t capacity,
+                                                            uint32_t* __restrict__ keys,
+                                                            uint32_t* __restrict__ vals) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t i0 = ((uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5) * 32u;
+    if (i0 >= N) return;  // warp-uniform
+    const uint32_t i = uint32_t(i0) + lane;
+    uint32_t lo[3] = {0u, 0u, 0u}, hi[3] = {1u, 1u, 1u};
+    int64_t start, end;
+    if (i < N) {
+        if (!rect_3d(means3d, radii, i, tile_size, tx, ty, tz, lo, hi)) {
+            lo[0] = lo[1] = lo[2] = 0u;
+            hi[0] = hi[1] = hi[2] = 1u;
+        }
+        start = i == 0 ? 0 : cum[i - 1];
+        end = cum[i];
+    } else {
+        start = end = cum[N - 1];
+    }
+    const uint32_t nx = hi[0] - lo[0], ny = hi[1] - lo[1];
+    const int64_t range_start = __shfl_sync(0xffffffffu, start, 0);
+    const int64_t range_end = __shfl_sync(0xffffffffu, end, 31);
+    const int64_t steps = (range_end - range_start + 31) / 32;
+    for (int64_t k = 0; k < steps; ++k) {
+        const int64_t p = range_start + k * 32 + lane;
+        uint32_t owner = 0u;
+#pragma unroll
+        for (uint32_t step = 16u; step > 0u; step >>= 1) {
+            const int64_t s_mid = __shfl_sync(0xffffffffu, start, int(owner + step));
+            if (s_mid <= p) owner += step;
+        }
+        const int64_t s_owner = __shfl_sync(0xffffffffu, start, int(owner));
+        const uint32_t onx = __shfl_sync(0xffffffffu, nx, int(owner));
+        const uint32_t ony = __shfl_sync(0xffffffffu, ny, int(owner));
+        const uint32_t ox = __shfl_sync(0xffffffffu, lo[0], int(owner));
+        const uint32_t oy = __shfl_sync(0xffffffffu, lo[1], int(owner));
+        const uint32_t oz = __shfl_sync(0xffffffffu, lo[2], int(owner));
+        if (p >= range_end || p >= capacity) continue;
+        const uint32_t local = uint32_t(p - s_owner);
+        const uint32_t plane = onx * ony;
+        const uint32_t dz = local / plane;
+        const uint32_t rem = local - dz * plane;
+        const uint32_t dy = rem / onx, dx = rem - dy * onx;
+        keys[p] = ((oz + dz) * ty + (oy + dy)) * tx + (ox + dx);
+        vals[p] = uint32_t(i0) + owner;
+    }
+}
+
+// --------------------------------------------------------------- radix sort// --------------------------------------------------------------- radix sort
 
 constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / 32;
@@ -678,7 +787,7 @@ int r2s_raster_emit(const uint16_t* rects, uint32_t C, uint32_t N, uint32_t tile
         uint32_t* keys = arena.take<uint32_t>(size_t(n_isects));
         uint32_t* vals = arena.take<uint32_t>(size_t(n_isects));
         R2S_REQUIRE(keys && vals, R2S_ERR_WORKSPACE, "intersection workspace too small");
-        emit_rects_kernel<<<blocks_for(total, kIsectThreads), kIsectThreads, 0, as_stream(stream)>>>(
+        emit_rects_warp_kernel<<<blocks_for(total, 256), 256, 0, as_stream(stream)>>>(
             reinterpret_cast<const ushort4*>(rects), uint32_t(total), N, tiles_x, tiles_y, cum_tiles, INT64_MAX, keys,
             vals);
         R2S_TRY(check_launch("raster_emit"));
@@ -723,7 +832,7 @@ int r2s_isect_tiles_3d_emit(int dtype, const void* means3d, const int32_t* radii
         uint32_t* keys = arena.take<uint32_t>(size_t(n_isects));
         uint32_t* vals = arena.take<uint32_t>(size_t(n_isects));
         R2S_REQUIRE(keys && vals, R2S_ERR_WORKSPACE, "intersection workspace too small");
-        R2S_DISPATCH(dtype, emit_3d_kernel<S><<<blocks_for(N, kIsectThreads), kIsectThreads, 0, as_stream(stream)>>>(
+        R2S_DISPATCH(dtype, emit_3d_warp_kernel<S><<<blocks_for(N, 256), 256, 0, as_stream(stream)>>>(
             static_cast<const S*>(means3d), radii, N, tile_size, tiles_x, tiles_y, tiles_z, cum_tiles, INT64_MAX, keys,
             vals));
         R2S_TRY(check_launch("isect_emit_3d"));
@@ -760,7 +869,7 @@ int r2s_raster_emit_capacity(const uint16_t* rects, uint32_t C, uint32_t N, uint
     uint32_t* vals = arena.take<uint32_t>(size_t(capacity));
     R2S_REQUIRE(keys && vals, R2S_ERR_WORKSPACE, "intersection workspace too small");
     if (total > 0) {
-        emit_rects_kernel<<<blocks_for(total, kIsectThreads), kIsectThreads, 0, st>>>(
+        emit_rects_warp_kernel<<<blocks_for(total, 256), 256, 0, st>>>(
             reinterpret_cast<const ushort4*>(rects), uint32_t(total), N, tiles_x, tiles_y, cum_tiles, capacity, keys,
             vals);
         R2S_TRY(check_launch("raster_emit"));
@@ -788,7 +897,7 @@ int r2s_voxel_emit_capacity(int dtype, const void* means3d, const int32_t* radii
     uint32_t* vals = arena.take<uint32_t>(size_t(capacity));
     R2S_REQUIRE(keys && vals, R2S_ERR_WORKSPACE, "intersection workspace too small");
     if (N > 0) {
-        R2S_DISPATCH(dtype, emit_3d_kernel<S><<<blocks_for(N, kIsectThreads), kIsectThreads, 0, st>>>(
+        R2S_DISPATCH(dtype, emit_3d_warp_kernel<S><<<blocks_for(N, 256), 256, 0, st>>>(
             static_cast<const S*>(means3d), radii, N, tile_size, tiles_x, tiles_y, tiles_z, cum_tiles, capacity, keys,
             vals));
         R2S_TRY(check_launch("isect_emit_3d"));

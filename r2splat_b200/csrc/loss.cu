@@ -156,6 +156,100 @@ __global__ void __launch_bounds__(kLossThreads) tv_fused_kernel(
     if (threadIdx.x == 0) partials[blockIdx.x] = total_sum;
 }
 
+// The fused pass on fp32 volumes whose rows are whole float4s (W % 4 == 0, 16-byte aligned): each
+// lane owns four consecutive voxels of a row (one 16-byte load per slice), a warp 128 voxels of
+// one row, the block 8 rows; the slice two ahead is loaded while the current one is computed.
+// Per voxel the operations and their order are tv_fused_kernel's.
+constexpr uint32_t kTv4TileX = 128;
+
+__device__ __forceinline__ float tv_at(float cur, float next, float yp, float xp, bool dz, bool dy, bool dx) {
+    float tv = 0.f;
+    if (dz) tv += abs_diff(next - cur);
+    if (dy) tv += abs_diff(yp - cur);
+    if (dx) tv += abs_diff(xp - cur);
+    return tv;
+}
+
+__device__ __forceinline__ float tv_grad_at(float cur, float prev, float next, float yp, float ym, float xp,
+                                            float xm, bool zn, bool zp, bool yn, bool yq, bool xn, bool xq) {
+    float g = 0.f;
+    if (zn) g -= sign_of(next - cur);
+    if (zp) g += sign_of(cur - prev);
+    if (yn) g -= sign_of(yp - cur);
+    if (yq) g += sign_of(cur - ym);
+    if (xn) g -= sign_of(xp - cur);
+    if (xq) g += sign_of(cur - xm);
+    return g;
+}
+
+template <bool kMap>
+__global__ void __launch_bounds__(kLossThreads) tv_fused4_kernel(
+    const float* __restrict__ vol, uint32_t D, uint32_t H, uint32_t W, uint32_t tiles_x, uint32_t tiles_y,
+    uint32_t chunks, uint64_t n_tiles, const float* __restrict__ grad_output, int64_t edges, float lambda,
+    float* __restrict__ tv_map, float* __restrict__ grad, double* __restrict__ partials) {
+    const float grad_out = grad_output[0] / static_cast<float>(edges);
+    const float lam = lambda;
+    const uint64_t HW = uint64_t(H) * W;
+    const uint32_t lane = threadIdx.x & 31u, ly = threadIdx.x >> 5;
+    double sum = 0;
+    for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+        uint64_t t = tile;
+        const uint32_t tx = uint32_t(t % tiles_x);
+        t /= tiles_x;
+        const uint32_t ty = uint32_t(t % tiles_y);
+        t /= tiles_y;
+        const uint32_t chunk = uint32_t(t % chunks);
+        const uint64_t b = t / chunks;
+        const uint32_t x = tx * kTv4TileX + 4u * lane, y = ty * kTvTileY + ly;
+        const uint32_t d0 = chunk * kTvChunk, d1 = min(D, d0 + kTvChunk);
+        const bool active = x < W && y < H;  // W % 4 == 0: a lane's four voxels are all in or all out
+        const uint64_t column = b * D * HW + uint64_t(y) * W + x;
+        const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        auto load4 = [&](uint32_t d) {
+            return (active && d < D) ? __ldg(reinterpret_cast<const float4*>(vol + column + uint64_t(d) * HW))
+                                     : zero4;
+        };
+        float4 prev = (active && d0 > 0) ? load4(d0 - 1) : zero4;
+        float4 cur = load4(d0);
+        float4 next = load4(d0 + 1);
+        for (uint32_t d = d0; d < d1; ++d) {
+            const float4 ahead = load4(d + 2);  // in flight while this slice is computed
+            const uint64_t idx = column + uint64_t(d) * HW;
+            // x neighbours: the adjacent lanes' edge voxels; the warp's first and last lanes load them.
+            float xp = __shfl_down_sync(0xffffffffu, cur.x, 1);
+            float xm = __shfl_up_sync(0xffffffffu, cur.w, 1);
+            if (active) {
+                if (lane == 31u && x + 4 < W) xp = vol[idx + 4];
+                if (lane == 0u && x > 0) xm = vol[idx - 1];
+                const float4 yp = y + 1 < H ? __ldg(reinterpret_cast<const float4*>(vol + idx + W)) : zero4;
+                const float4 ym = y > 0 ? __ldg(reinterpret_cast<const float4*>(vol + idx - W)) : zero4;
+                const bool zn = d + 1 < D, zp = d > 0, yn = y + 1 < H, yq = y > 0;
+                const bool xn3 = x + 4 < W, xq0 = x > 0;
+                float4 m, g;
+                m.x = tv_at(cur.x, next.x, yp.x, cur.y, zn, yn, true);
+                m.y = tv_at(cur.y, next.y, yp.y, cur.z, zn, yn, true);
+                m.z = tv_at(cur.z, next.z, yp.z, cur.w, zn, yn, true);
+                m.w = tv_at(cur.w, next.w, yp.w, xp, zn, yn, xn3);
+                g.x = tv_grad_at(cur.x, prev.x, next.x, yp.x, ym.x, cur.y, xm, zn, zp, yn, yq, true, xq0);
+                g.y = tv_grad_at(cur.y, prev.y, next.y, yp.y, ym.y, cur.z, cur.x, zn, zp, yn, yq, true, true);
+                g.z = tv_grad_at(cur.z, prev.z, next.z, yp.z, ym.z, cur.w, cur.y, zn, zp, yn, yq, true, true);
+                g.w = tv_grad_at(cur.w, prev.w, next.w, yp.w, ym.w, xp, cur.z, zn, zp, yn, yq, xn3, true);
+                if (kMap) *reinterpret_cast<float4*>(tv_map + idx) = m;
+                *reinterpret_cast<float4*>(grad + idx) =
+                    make_float4((g.x * grad_out) * lam, (g.y * grad_out) * lam, (g.z * grad_out) * lam,
+                                (g.w * grad_out) * lam);
+                sum += static_cast<double>(m.x) + static_cast<double>(m.y) + static_cast<double>(m.z) +
+                       static_cast<double>(m.w);
+            }
+            prev = cur;
+            cur = next;
+            next = ahead;
+        }
+    }
+    const double total_sum = block_sum(sum);
+    if (threadIdx.x == 0) partials[blockIdx.x] = total_sum;
+}
+
 template <typename S>
 __global__ void __launch_bounds__(kLossThreads) l1_fwd_kernel(const S* __restrict__ pred, const S* __restrict__ tgt,
                                                               int64_t total, S* __restrict__ l1_map,
@@ -314,6 +408,30 @@ int r2s_volume_loss_fwd_bwd(int dtype, const void* volume, const void* grad_outp
     double* partials = arena.take<double>(blocks);
     R2S_REQUIRE(partials, R2S_ERR_WORKSPACE, "loss workspace too small");
     cudaStream_t st = as_stream(stream);
+    const bool vec4 = dtype == R2S_F32 && W % 4 == 0 && reinterpret_cast<uintptr_t>(volume) % 16 == 0 &&
+                      reinterpret_cast<uintptr_t>(grad_volume) % 16 == 0 &&
+                      (tv_map == nullptr || reinterpret_cast<uintptr_t>(tv_map) % 16 == 0);
+    if (vec4 && total > 0) {
+        const uint32_t tiles4_x = (W + kTv4TileX - 1) / kTv4TileX;
+        const uint64_t n4 = uint64_t(B) * chunks * tiles_y * tiles4_x;
+        const unsigned blocks4 = unsigned(n4 < uint64_t(kLossMaxBlocks) ? n4 : uint64_t(kLossMaxBlocks));
+        double* partials4 = partials;  // blocks4 <= blocks: the 128-voxel rows make no more tiles than 32
+        if (tv_map != nullptr) {
+            tv_fused4_kernel<true><<<blocks4, kLossThreads, 0, st>>>(
+                static_cast<const float*>(volume), D, H, W, tiles4_x, tiles_y, chunks, n4,
+                static_cast<const float*>(grad_output), edges, lambda_tv, static_cast<float*>(tv_map),
+                static_cast<float*>(grad_volume), partials4);
+        } else {
+            tv_fused4_kernel<false><<<blocks4, kLossThreads, 0, st>>>(
+                static_cast<const float*>(volume), D, H, W, tiles4_x, tiles_y, chunks, n4,
+                static_cast<const float*>(grad_output), edges, lambda_tv, nullptr, static_cast<float*>(grad_volume),
+                partials4);
+        }
+        R2S_TRY(check_launch("volume_loss_fwd_bwd"));
+        finish_mean_kernel<float><<<1, kLossThreads, 0, st>>>(partials4, int(blocks4), edges, lambda_tv,
+                                                              static_cast<float*>(loss), static_cast<float*>(tv));
+        return check_launch("volume_loss_finish");
+    }
     R2S_DISPATCH(dtype, {
         if (total > 0) {
             if (tv_map != nullptr) {

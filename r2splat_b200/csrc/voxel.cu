@@ -2,11 +2,13 @@
 // densities at voxel centres, and its VJP, on packed per-primitive records.
 //
 // Same schedule as the rasterizer: one CTA per 3D tile, the tile's
-// intersection list gathered into shared memory with cp.async in
-// double-buffered batches (records are [N] x 64 B and stay in L2), forward
-// threads own up to 4 voxels, backward warps own one record at a time over a
-// 256-voxel sub-tile (8 voxels per lane), warp-reduce, then issue three
-// vector atomics per record.
+// intersection list gathered into shared memory with cp.async in buffered
+// batches (records are [N] x 64 B and stay in L2). Forward threads own a row
+// of 8 voxels (Gaussian fp32 at T = 8), 4 voxels of a row, or single voxels;
+// backward warps own one record at a time over the record's box in the tile,
+// warp-reduce, and either write the record's partial adjoints to its own slot
+// (reduced per primitive in a fixed order afterwards) or add them with vector
+// atomics.
 //
 // Per-sample arithmetic keeps the reference's expression forms
 // (VoxelizeToVoxelsFwd.cu:180-215, :555-580; VoxelizeToVoxelsBwd.cu:397-433,
@@ -63,36 +65,44 @@ __global__ void __launch_bounds__(256) voxel_fwd_kernel(const Rec3D<S>* __restri
     const uint32_t rem = key - tz * g.tiles_x * g.tiles_y;
     const uint32_t ty = rem / g.tiles_x, tx = rem - ty * g.tiles_x;
     const uint32_t t = threadIdx.x;
-    constexpr bool kRowShared = PPT == 4 && !kBeta && std::is_same<S, float>::value;
+    // PPT = 4 or 8: a thread owns PPT consecutive voxels of one row (same y,
+    // z), so the Gaussian terms in d2 and d3 alone are computed once per
+    // record and the record's shared-memory reads are spread over PPT samples.
+    // PPT = 1: voxels placed by tile_voxel.
+    constexpr bool kRows = PPT >= 4;
+    constexpr bool kRowShared = kRows && !kBeta && std::is_same<S, float>::value;
 
     S px[PPT], py[PPT], pz[PPT], acc[PPT], accv[PPT];
-    size_t vid[PPT];
     bool inside[PPT];
-    // PPT = 4: a thread owns 4 consecutive voxels of one row (same y, z), so
-    // the Gaussian terms in d2 and d3 alone are computed once per record.
-    const uint32_t segs = (T + 3u) / 4u;
-    const uint32_t row = PPT == 4 ? t / segs : 0u;
-    const uint32_t seg = PPT == 4 ? t - row * segs : 0u;
-#pragma unroll
-    for (int k = 0; k < PPT; ++k) {
+    const uint32_t segs = (T + uint32_t(PPT) - 1u) / uint32_t(PPT);
+    const uint32_t row = kRows ? t / segs : 0u;
+    const uint32_t seg = kRows ? t - row * segs : 0u;
+    // Global voxel coordinates (i = z, j = y, kk = x) of the thread's k-th voxel.
+    auto voxel_of = [&](int k, uint32_t& i, uint32_t& j, uint32_t& kk) {
         uint32_t lz, ly, lx;
         bool in_tile;
-        if (PPT == 4) {
+        if (kRows) {
             lz = row / T;
             ly = row - lz * T;
-            lx = 4u * seg + uint32_t(k);
+            lx = uint32_t(PPT) * seg + uint32_t(k);
             in_tile = row < T * T && lx < T;
         } else {
             const uint32_t p = t + uint32_t(k) * nthreads;
             tile_voxel(p, T, lz, ly, lx);
             in_tile = p < T * T * T;
         }
-        const uint32_t i = tz * T + lz, j = ty * T + ly, kk = tx * T + lx;
-        inside[k] = in_tile && i < g.dim0 && j < g.dim1 && kk < g.dim2;
+        i = tz * T + lz;
+        j = ty * T + ly;
+        kk = tx * T + lx;
+        return in_tile && i < g.dim0 && j < g.dim1 && kk < g.dim2;
+    };
+#pragma unroll
+    for (int k = 0; k < PPT; ++k) {
+        uint32_t i, j, kk;
+        inside[k] = voxel_of(k, i, j, kk);
         px[k] = static_cast<S>(kk) + static_cast<S>(0.5);
         py[k] = static_cast<S>(j) + static_cast<S>(0.5);
         pz[k] = static_cast<S>(i) + static_cast<S>(0.5);
-        vid[k] = (size_t(i) * g.dim1 + j) * g.dim2 + kk;
         acc[k] = S(0);
         accv[k] = S(0);
     }
@@ -149,37 +159,37 @@ __global__ void __launch_bounds__(256) voxel_fwd_kernel(const Rec3D<S>* __restri
                         if (kVar) accv[k + 1] = fmaf(__fmul_rn(r.q, alpha1), alpha1, accv[k + 1]);
                     }
                 }
-                continue;
-            }
+            } else {
 #pragma unroll
-            for (int k = 0; k < PPT; ++k) {
-                if (!kBeta) {
-                    // Same contraction as above (VoxelizeToVoxelsFwd.cu:200-205, :390-396).
-                    const S d1 = px[k] - r.x, d2 = py[k] - r.y, d3 = pz[k] - r.z;
-                    const S s3 = fma(mul_rn(r.c22, d3), d3, fma(mul_rn(r.c00, d1), d1, mul_rn(mul_rn(r.c11, d2), d2)));
-                    const S sigma = fma(mul_rn(r.c12, d2), d3,
-                                        fma(mul_rn(r.c02, d1), d3,
-                                            fma(mul_rn(r.c01, d1), d2, mul_rn(static_cast<S>(0.5), s3))));
-                    const S alpha = r.o * exp(-sigma);
-                    if (!(sigma < static_cast<S>(0) || fabs(alpha) < static_cast<S>(1e-6))) {
-                        acc[k] += alpha;
-                        if (kVar) accv[k] = fma(mul_rn(r.q, alpha), alpha, accv[k]);
-                    }
-                } else {
-                    // The reference's d^T Q d (VoxelizeToVoxelsFwd.cu:563-567) with its contraction
-                    // explicit: s = fma(c d3, d3, fma(a d1, d1, (bb d2) d2)), then
-                    // q = fma((2 r) d2, d3, fma((2 q) d1, d3, fma((2 p) d1, d2, s))).
-                    const S d1 = r.x - px[k], d2 = r.y - py[k], d3 = r.z - pz[k];
-                    const S two = static_cast<S>(2);
-                    const S sq = fma(mul_rn(r.c22, d3), d3, fma(mul_rn(r.c00, d1), d1, mul_rn(mul_rn(r.c11, d2), d2)));
-                    const S qf = fma(mul_rn(mul_rn(two, r.c12), d2), d3,
-                                     fma(mul_rn(mul_rn(two, r.c02), d1), d3, fma(mul_rn(mul_rn(two, r.c01), d1), d2, sq)));
-                    if (!(qf < static_cast<S>(0) || qf >= static_cast<S>(1))) {
-                        const S h = static_cast<S>(1) - qf;
-                        const S alpha = r.o * pow(h, r.beta);
-                        if (!(fabs(alpha) < static_cast<S>(1e-5))) {
+                for (int k = 0; k < PPT; ++k) {
+                    if (!kBeta) {
+                        // Same contraction as above (VoxelizeToVoxelsFwd.cu:200-205, :390-396).
+                        const S d1 = px[k] - r.x, d2 = py[k] - r.y, d3 = pz[k] - r.z;
+                        const S s3 = fma(mul_rn(r.c22, d3), d3, fma(mul_rn(r.c00, d1), d1, mul_rn(mul_rn(r.c11, d2), d2)));
+                        const S sigma = fma(mul_rn(r.c12, d2), d3,
+                                            fma(mul_rn(r.c02, d1), d3,
+                                                fma(mul_rn(r.c01, d1), d2, mul_rn(static_cast<S>(0.5), s3))));
+                        const S alpha = r.o * exp(-sigma);
+                        if (!(sigma < static_cast<S>(0) || fabs(alpha) < static_cast<S>(1e-6))) {
                             acc[k] += alpha;
                             if (kVar) accv[k] = fma(mul_rn(r.q, alpha), alpha, accv[k]);
+                        }
+                    } else {
+                        // The reference's d^T Q d (VoxelizeToVoxelsFwd.cu:563-567) with its contraction
+                        // explicit: s = fma(c d3, d3, fma(a d1, d1, (bb d2) d2)), then
+                        // q = fma((2 r) d2, d3, fma((2 q) d1, d3, fma((2 p) d1, d2, s))).
+                        const S d1 = r.x - px[k], d2 = r.y - py[k], d3 = r.z - pz[k];
+                        const S two = static_cast<S>(2);
+                        const S sq = fma(mul_rn(r.c22, d3), d3, fma(mul_rn(r.c00, d1), d1, mul_rn(mul_rn(r.c11, d2), d2)));
+                        const S qf = fma(mul_rn(mul_rn(two, r.c12), d2), d3,
+                                         fma(mul_rn(mul_rn(two, r.c02), d1), d3, fma(mul_rn(mul_rn(two, r.c01), d1), d2, sq)));
+                        if (!(qf < static_cast<S>(0) || qf >= static_cast<S>(1))) {
+                            const S h = static_cast<S>(1) - qf;
+                            const S alpha = r.o * pow(h, r.beta);
+                            if (!(fabs(alpha) < static_cast<S>(1e-5))) {
+                                acc[k] += alpha;
+                                if (kVar) accv[k] = fma(mul_rn(r.q, alpha), alpha, accv[k]);
+                            }
                         }
                     }
                 }
@@ -191,8 +201,11 @@ __global__ void __launch_bounds__(256) voxel_fwd_kernel(const Rec3D<S>* __restri
 #pragma unroll
     for (int k = 0; k < PPT; ++k) {
         if (inside[k]) {
-            volume[vid[k]] = acc[k];
-            if (kVar) volume_var[vid[k]] = accv[k];
+            uint32_t i, j, kk;
+            voxel_of(k, i, j, kk);
+            const size_t vid = (size_t(i) * g.dim1 + j) * g.dim2 + kk;
+            volume[vid] = acc[k];
+            if (kVar) volume_var[vid] = accv[k];
         }
     }
 }
@@ -280,15 +293,44 @@ __device__ __forceinline__ VoxelBox voxel_box(const Rec3D<S>& r, uint32_t ox, ui
 // span of IsectTiles3DKernel.cu:38-112 on the voxel-space mean and radii):
 // [lo, hi) per axis; false when it has no tiles.
 template <typename S>
+__device__ __forceinline__ bool tile_box_3d(const S* mean_v, const int32_t* radius, uint32_t T, uint32_t tiles_x,
+                                            uint32_t tiles_y, uint32_t tiles_z, uint32_t* lo, uint32_t* hi) {
+    const int32_t rx = radius[0], ry = radius[1], rz = radius[2];
+    if (rx <= 0 || ry <= 0 || rz <= 0) return false;
+    tile_span(mean_v[0], static_cast<S>(rx), T, tiles_x, lo[0], hi[0]);
+    tile_span(mean_v[1], static_cast<S>(ry), T, tiles_y, lo[1], hi[1]);
+    tile_span(mean_v[2], static_cast<S>(rz), T, tiles_z, lo[2], hi[2]);
+    return hi[0] > lo[0] && hi[1] > lo[1] && hi[2] > lo[2];
+}
+
+template <typename S>
 __device__ __forceinline__ bool tile_box_3d(const S* means_v, const int32_t* radii, uint32_t n, uint32_t T,
                                             uint32_t tiles_x, uint32_t tiles_y, uint32_t tiles_z, uint32_t* lo,
                                             uint32_t* hi) {
-    const int32_t rx = radii[3 * size_t(n)], ry = radii[3 * size_t(n) + 1], rz = radii[3 * size_t(n) + 2];
-    if (rx <= 0 || ry <= 0 || rz <= 0) return false;
-    tile_span(means_v[3 * size_t(n)], static_cast<S>(rx), T, tiles_x, lo[0], hi[0]);
-    tile_span(means_v[3 * size_t(n) + 1], static_cast<S>(ry), T, tiles_y, lo[1], hi[1]);
-    tile_span(means_v[3 * size_t(n) + 2], static_cast<S>(rz), T, tiles_z, lo[2], hi[2]);
-    return hi[0] > lo[0] && hi[1] > lo[1] && hi[2] > lo[2];
+    return tile_box_3d(means_v + 3 * size_t(n), radii + 3 * size_t(n), T, tiles_x, tiles_y, tiles_z, lo, hi);
+}
+
+// What the tile VJP needs to find a record's slot, staged into the record's
+// padding in shared memory by cp.async alongside the record (so the slot
+// costs no dependent global round trip): the primitive's voxel radii (its
+// tile box, with the record's voxel-space centre x, y, z) and its first slot
+// cum[n - 1]. fp32 records have 16 bytes of padding, which hold the radii and
+// the low 32 bits of cum[n - 1] (slots fit 31 bits, and a step whose count
+// outgrew that is discarded); fp64 records have 32, and hold all 64 bits.
+struct SlotPad {
+    int32_t radius[3];
+    uint32_t first32;  // fp32 records
+    uint64_t first64;  // fp64 records
+};
+static_assert(sizeof(Rec3D<float>) - 12 * sizeof(float) >= offsetof(SlotPad, first64), "fp32 record padding");
+static_assert(sizeof(Rec3D<double>) - 12 * sizeof(double) >= sizeof(SlotPad), "fp64 record padding");
+template <typename S>
+__device__ __forceinline__ SlotPad* slot_pad(Rec3D<S>* rec) {
+    return reinterpret_cast<SlotPad*>(&rec->pad0);
+}
+template <typename S>
+__device__ __forceinline__ const SlotPad* slot_pad(const Rec3D<S>* rec) {
+    return reinterpret_cast<const SlotPad*>(&rec->pad0);
 }
 
 // Deterministic output of the tile VJP: instead of adding a (tile, primitive)
@@ -334,8 +376,15 @@ struct VoxelSlots {
 // -(log2 e): exp(-s) = 2^(-s log2 e).
 constexpr float kVoxNegLog2e = -1.4426950408889634f;
 
+// Resident blocks the VJP is compiled for: the plain Gaussian walk is left to
+// ptxas (60 registers, so four blocks of 46 KB shared memory fit an SM; a cap
+// of 64 registers made it spill), the Beta and variance forms are held to
+// three blocks, for which ptxas would otherwise use 80-120 registers and two.
+template <bool kBeta, bool kVar>
+constexpr int kVoxBwdMinBlocks = (kBeta || kVar) ? 3 : 0;
+
 template <typename S, bool kBeta, bool kVar>
-__global__ void __launch_bounds__(kVoxBwdThreads) voxel_bwd_kernel(
+__global__ void __launch_bounds__(kVoxBwdThreads, kVoxBwdMinBlocks<kBeta, kVar>) voxel_bwd_kernel(
     const Rec3D<S>* __restrict__ records, bool chain_var, const int32_t* __restrict__ offsets,
     const int32_t* __restrict__ flatten_ids, VoxelGeom g, const S* __restrict__ v_volume,
     const S* __restrict__ v_volume_var, Rec3D<S>* __restrict__ grads, VoxelSlots<S> sl) {
@@ -390,20 +439,27 @@ __global__ void __launch_bounds__(kVoxBwdThreads) voxel_bwd_kernel(
         const int32_t idx = start + b * kVoxBwdThreads + int32_t(t);
         if (idx < end) {
             const int32_t gid = flatten_ids[idx];
-            gather_record3(s_rec + stage * kVoxBwdThreads + t, records + gid);
-            s_id[stage * kVoxBwdThreads + t] = gid;
-            if (sl.slots != nullptr) {
-                // The pair's slot, found while the previous batch is walked (slots fit 31 bits).
-                uint32_t slot = 0xffffffffu;
-                uint32_t blo[3], bhi[3];
-                if (tile_box_3d(sl.means_v, sl.radii, uint32_t(gid), T, g.tiles_x, g.tiles_y, g.tiles_z, blo, bhi)) {
-                    const uint64_t local = (uint64_t(tz - blo[2]) * (bhi[1] - blo[1]) + (ty - blo[1])) *
-                                               (bhi[0] - blo[0]) + (tx - blo[0]);
-                    const uint64_t j = (gid > 0 ? uint64_t(sl.cum[gid - 1]) : 0u) + local;
-                    if (j < sl.capacity) slot = uint32_t(j);
+            Rec3D<S>* dst = s_rec + stage * kVoxBwdThreads + t;
+            if (sl.slots == nullptr) {
+                gather_record3(dst, records + gid);
+            } else {
+                // The record's 12 values, then the slot inputs into its padding.
+                const char* src = reinterpret_cast<const char*>(records + gid);
+#pragma unroll
+                for (int k = 0; k < int(12 * sizeof(S) / 16); ++k)
+                    cp_async16(reinterpret_cast<char*>(dst) + 16 * k, src + 16 * k);
+                SlotPad* pad = slot_pad(dst);
+#pragma unroll
+                for (int k = 0; k < 3; ++k) cp_async4(pad->radius + k, sl.radii + 3 * size_t(gid) + k);
+                if constexpr (sizeof(S) == 4) {
+                    if (gid > 0) cp_async4(&pad->first32, sl.cum + (gid - 1));  // the low word
+                    else pad->first32 = 0u;
+                } else {
+                    if (gid > 0) cp_async8(&pad->first64, sl.cum + (gid - 1));
+                    else pad->first64 = 0u;
                 }
-                s_slot[stage * kVoxBwdThreads + t] = slot;
             }
+            s_id[stage * kVoxBwdThreads + t] = gid;
         }
         cp_async_commit();
     };
@@ -418,7 +474,27 @@ __global__ void __launch_bounds__(kVoxBwdThreads) voxel_bwd_kernel(
         __syncthreads();
         const uint32_t stage = uint32_t(b) & 1u;
         const int32_t batch = min(int32_t(kVoxBwdThreads), count - b * kVoxBwdThreads);
-        if (int32_t(t) < batch) s_box[t] = voxel_box<S, kBeta>(s_rec[stage * kVoxBwdThreads + t], ox, oy, oz, vx, vy, vz);
+        if (int32_t(t) < batch) {
+            s_box[t] = voxel_box<S, kBeta>(s_rec[stage * kVoxBwdThreads + t], ox, oy, oz, vx, vy, vz);
+            if (sl.slots != nullptr) {
+                // The pair's slot: the primitive's first slot plus this tile's index in its tile box
+                // (slots fit 31 bits).
+                const Rec3D<S>& rec = s_rec[stage * kVoxBwdThreads + t];
+                const SlotPad* pad = slot_pad(&rec);
+                uint64_t first;
+                if constexpr (sizeof(S) == 4) first = pad->first32;
+                else first = pad->first64;
+                uint32_t slot = 0xffffffffu;
+                uint32_t blo[3], bhi[3];
+                if (tile_box_3d(&rec.x, pad->radius, T, g.tiles_x, g.tiles_y, g.tiles_z, blo, bhi)) {
+                    const uint64_t local = (uint64_t(tz - blo[2]) * (bhi[1] - blo[1]) + (ty - blo[1])) *
+                                               (bhi[0] - blo[0]) + (tx - blo[0]);
+                    const uint64_t j = first + local;
+                    if (j < sl.capacity) slot = uint32_t(j);
+                }
+                s_slot[stage * kVoxBwdThreads + t] = slot;
+            }
+        }
         __syncthreads();
         for (int32_t s = int32_t(warp); s < batch; s += kVoxBwdWarps) {
             const VoxelBox box = s_box[s];
@@ -1074,6 +1150,11 @@ int launch_vfwd_p(const VoxelGeom& g, const Rec3D<S>* rec, const int32_t* offset
         const unsigned nt = (voxels + 31) / 32 * 32;
         return launch_vfwd_t<S, kBeta, kVar, 1>(g, rec, offsets, ids, vol, vol_var, nt, stream);
     }
+    if (!kBeta && std::is_same<S, float>::value && g.T % 8 == 0) {
+        // Whole rows of eight voxels per thread: T^2 rows of T / 8 segments.
+        const unsigned nt = (g.T * g.T * (g.T / 8) + 31) / 32 * 32;
+        return launch_vfwd_t<S, kBeta, kVar, 8>(g, rec, offsets, ids, vol, vol_var, nt, stream);
+    }
     // Four consecutive voxels of a row per thread: T^2 rows of ceil(T / 4) segments.
     const unsigned nt = (g.T * g.T * ((g.T + 3) / 4) + 31) / 32 * 32;
     return launch_vfwd_t<S, kBeta, kVar, 4>(g, rec, offsets, ids, vol, vol_var, nt, stream);
@@ -1343,6 +1424,7 @@ int r2s_voxel_render_bwd_slots(int dtype, const void* records, int beta, int det
     R2S_REQUIRE(n_used != nullptr || n_isects <= slot_capacity, R2S_ERR_ARGUMENT,
                 "slot_capacity must hold n_isects slots");
     R2S_REQUIRE(n_isects < (uint64_t(1) << 31), R2S_ERR_UNSUPPORTED, "too many 3D intersections");
+    R2S_REQUIRE(slot_capacity < (uint64_t(1) << 31), R2S_ERR_UNSUPPORTED, "slot_capacity must be below 2^31");
     VoxelGeom g{N, uint32_t(n_used != nullptr ? 1u : n_isects), dim2, dim1, dim0, tile_size, tiles_x, tiles_y,
                 tiles_z};
     g.n_dev = n_used;

@@ -79,6 +79,7 @@ SIGNATURES: dict[str, tuple] = {
     "r2s_raster_render_bwd": (I32, [I32, P, P, I32, I32, P, P, P, P, U32, U32, U32, U32, U32, U32, U32, U32,
                                     P, P, P, P]),
     "r2s_raster_record_bwd": (I32, [I32, P, P, P, I32, I32, P, P, U32, U32, U32, U32, U32, P, P, P, P]),
+    "r2s_sum_over_cameras": (I32, [I32, P, U32, U32, P, P]),
     "r2s_raster_chain_bwd": (I32, [I32, P, P, P, P, P, P, P, P, P, U32, U32, U32, U32, F32, F64, P, P, P, P,
                                    P, P, P]),
     "r2s_voxel_project": (I32, [I32, P, P, P, P, P, P, P, U32, U32, U32, U32, F64, F64, U32, U32, U32, U32,

@@ -19,8 +19,12 @@ the device, and runs requests as follows:
 * Scheduling is continuous. A scheduler thread of control launches each
   arrived request as soon as its reconstruction has no step in flight and one
   of ``slots`` CUDA streams is free, so requests that arrive while others run
-  are started immediately and their kernels overlap on the device. Completion
-  is detected with CUDA events; latency is arrival to completion.
+  are started immediately and their kernels overlap on the device. A graphed
+  step is one replay. A lean step reads intersection counts back to the host
+  while it runs, so it runs on a worker thread of its own: the scheduler keeps
+  launching graphed steps on the other streams meanwhile, and a large lean
+  reconstruction does not hold up the small ones. Completion is detected with
+  CUDA events; latency is arrival to completion.
 * A graphed step whose intersection lists outgrow their capacity skips its
   update and raises the scene's overflow flag; each replay copies that flag
   to pinned host memory ahead of its completion event. On completion the
@@ -46,6 +50,7 @@ import ctypes
 import heapq
 import time
 from collections import deque
+from concurrent.futures import Future, ThreadPoolExecutor
 from dataclasses import dataclass, field
 from typing import Callable, Optional
 
@@ -80,23 +85,33 @@ class ServeStats:
     waited_for_memory: int = 0
     rejected: int = 0
     regrown: int = 0
+    lean_latencies_ms: list = field(default_factory=list)
 
     @property
     def steps_per_s(self) -> float:
         return self.completed / self.wall_s if self.wall_s > 0 else 0.0
 
-    def percentile(self, q: float) -> float:
-        if not self.latencies_ms:
+    def percentile(self, q: float, values: Optional[list] = None) -> float:
+        values = sorted(self.latencies_ms if values is None else values)
+        if not values:
             return float("nan")
-        values = sorted(self.latencies_ms)
         index = min(len(values) - 1, max(0, int(round(q / 100.0 * (len(values) - 1)))))
         return values[index]
 
     def summary(self) -> dict:
-        return {"completed": self.completed, "wall_s": self.wall_s, "fit_steps_per_s": self.steps_per_s,
-                "p50_ms": self.percentile(50), "p99_ms": self.percentile(99), "graphed": self.graphed,
-                "lean": self.lean, "waited_for_memory": self.waited_for_memory, "rejected": self.rejected,
-                "regrown": self.regrown}
+        out = {"completed": self.completed, "wall_s": self.wall_s, "fit_steps_per_s": self.steps_per_s,
+               "p50_ms": self.percentile(50), "p99_ms": self.percentile(99), "graphed": self.graphed,
+               "lean": self.lean, "waited_for_memory": self.waited_for_memory, "rejected": self.rejected,
+               "regrown": self.regrown}
+        if self.lean_latencies_ms:
+            lean = self.lean_latencies_ms
+            other = sorted(self.latencies_ms)
+            for x in lean:
+                other.remove(x)
+            out.update(lean_requests=len(lean), lean_p50_ms=self.percentile(50, lean),
+                       lean_p99_ms=self.percentile(99, lean), graphed_p50_ms=self.percentile(50, other),
+                       graphed_p99_ms=self.percentile(99, other))
+        return out
 
 
 def lean_step(scene: batched.FitScene, recompute: bool = False):
@@ -139,19 +154,25 @@ def lean_step(scene: batched.FitScene, recompute: bool = False):
 class FitServer:
     """Admits reconstructions against an HBM budget and serves fit-step requests continuously."""
 
-    def __init__(self, budget_bytes: int, slots: int = 8, device="cuda", lean_recompute: bool = False):
+    def __init__(self, budget_bytes: int, slots: int = 8, device="cuda", lean_recompute: bool = False,
+                 lean_reserve_bytes: int = 0):
         """``lean_recompute``: lean reconstructions free each forward's intersection lists before the
-        backward (``lean_step(recompute=True)``), for budgets that large reconstructions press against."""
+        backward (``lean_step(recompute=True)``), for budgets that large reconstructions press against.
+        ``lean_reserve_bytes``: memory held back for lean steps from the start (it grows to the largest
+        transient peak measured at a lean admission)."""
         self.device = torch.device(device)
         self.lean_recompute = bool(lean_recompute)
         self.budget = int(budget_bytes)
         self.used = 0
         # Peak transient memory of one lean step (the largest measured at admission). Lean steps run one at
         # a time, so this much of the budget is held back from resident reconstructions.
-        self.lean_reserve = 0
+        self.lean_reserve = int(lean_reserve_bytes)
         self.streams = [torch.cuda.Stream(device=self.device) for _ in range(slots)]
         self.recons: dict = {}
         self.waiting: deque = deque()  # (key, factory) not yet admitted
+        # Lean steps run here, one at a time, so their host reads do not stall the scheduler.
+        self._lean_worker = ThreadPoolExecutor(max_workers=1, thread_name_prefix="r2s-lean-step")
+        self._lean_future: Optional[Future] = None
 
     # ----------------------------------------------------------- admission
     def admit(self, key, factory: Callable[[], batched.FitScene]) -> bool:
@@ -259,22 +280,39 @@ class FitServer:
             self.waiting.popleft()
 
     # ----------------------------------------------------------- serving
-    def _launch(self, recon: Reconstruction, stream: torch.cuda.Stream) -> torch.cuda.Event:
-        with torch.cuda.stream(stream):
-            if recon.graphed:
+    def _launch(self, recon: Reconstruction, stream: torch.cuda.Stream):
+        """Starts one step on ``stream``; returns an object whose ``query()`` is True once it is done."""
+        if recon.graphed:
+            with torch.cuda.stream(stream):
                 recon.graph.replay()
                 recon.overflow_host.copy_(recon.scene.overflow, non_blocking=True)
-            else:
-                lean_step(recon.scene, recompute=self.lean_recompute)
-            done = torch.cuda.Event()
-            done.record(stream)
-        return done
+                done = torch.cuda.Event()
+                done.record(stream)
+            return done
+        recompute = self.lean_recompute
+
+        def run():
+            with torch.cuda.device(self.device), torch.cuda.stream(stream):
+                lean_step(recon.scene, recompute=recompute)
+                done = torch.cuda.Event()
+                done.record(stream)
+            return done
+
+        self._lean_future = self._lean_worker.submit(run)
+        return _LeanStep(self._lean_future)
+
+    def _wait_lean(self):
+        """Waits for the lean step on the worker thread, if any (re-raising its error)."""
+        if self._lean_future is not None:
+            self._lean_future.result().synchronize()
 
     def _finish(self, recon: Reconstruction, stats: ServeStats):
         """Completion of a step: a graphed step that overflowed is redone with room, then re-captured."""
         if not recon.graphed or int(recon.overflow_host[0]) == 0:
             return
         scene = recon.scene
+        # Capturing while the worker thread launches a lean step would put its work into the graph.
+        self._wait_lean()
         torch.cuda.synchronize(self.device)
         before = torch.cuda.memory_allocated(self.device)
         recon.graph = None
@@ -328,7 +366,10 @@ class FitServer:
                     lean_in_flight -= int(not recon.graphed)
                     self._finish(recon, stats)
                     stats.completed += 1
-                    stats.latencies_ms.append((time.perf_counter() - start - t) * 1e3)
+                    latency = (time.perf_counter() - start - t) * 1e3
+                    stats.latencies_ms.append(latency)
+                    if not recon.graphed:
+                        stats.lean_latencies_ms.append(latency)
                     recon.busy = False
                     recon.steps += 1
                     free.append(slot)
@@ -358,7 +399,20 @@ class FitServer:
             if not progressed:
                 time.sleep(poll_s)
         stats.wall_s = time.perf_counter() - start
+        self._wait_lean()
         return stats
+
+
+class _LeanStep:
+    """A lean step running on the worker thread: done once the thread has launched it and its event fired."""
+
+    def __init__(self, future: Future):
+        self.future = future
+
+    def query(self) -> bool:
+        if not self.future.done():
+            return False
+        return self.future.result().query()  # re-raises an error of the step
 
 
 def serve_serially(recons: dict, requests: list) -> ServeStats:

@@ -9,9 +9,10 @@ back to the float64 VJP of the same fp32 forward, computed with the
 reference's own kernels in float64 ("truth"): this build must be no farther
 from it than the reference build is. "No farther" allows 25 % on three
 statistics of the normalised error |x - truth| / (1e-6 + 1e-5 |truth|): the
-norm-wise error, the count of elements above 1, and (for tensors of at least
-100,000 elements, where it is not just one of the few largest errors) the
-99.9th percentile. On
+norm-wise error (or, whichever is larger, the contract's relative 1e-5 applied
+to the whole tensor), the count of elements above 1, and (for tensors of at
+least 100,000 elements, where it is not just one of the few largest errors)
+the 99.9th percentile. On
 the 500k-primitive Beta scene with the variance branch (128 views at 768^2,
 volume 384^3) these statistics of this build were 0.26 to 1.08 times the
 reference build's.
@@ -51,7 +52,9 @@ def assert_gradient_parity(name, ours, ref, truth=None, report=None):
     mine, theirs = truth_errors(ours, truth), truth_errors(ref, truth)
     stats.update(ours_vs_truth=mine, ref_vs_truth=theirs)
     norm_t = float(truth.norm())
-    assert mine["norm"] <= 1.25 * theirs["norm"] + 1e-7 * norm_t, (name, stats)
+    # Norm-wise: within 25 % of the reference's distance, or within the contract's relative 1e-5 of the
+    # truth as a whole.
+    assert mine["norm"] <= max(1.25 * theirs["norm"], 1e-5 * norm_t), (name, stats)
     assert mine["count"] <= 1.25 * theirs["count"] + 16, (name, stats)
     if ours.numel() >= 100_000:
         assert mine["p999"] <= 1.25 * theirs["p999"] + 0.05, (name, stats)

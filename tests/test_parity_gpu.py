@@ -641,3 +641,21 @@ def test_released_lists_give_the_same_gradients(device, beta):
         a, b = getattr(v0, name), getattr(v1, name)
         if a is not None:
             torch.testing.assert_close(b, a, rtol=1e-4, atol=1e-5 * float(a.abs().max()), msg=name)
+
+
+@pytest.mark.parametrize("shape", [(2, 33, 40, 48), (1, 20, 21, 22), (1, 64, 64, 256)])
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+def test_tv_forward_backward_in_one_pass_equals_the_two_calls(device, shape, dtype):
+    """r2s_volume_loss_fwd_bwd: map and gradient bit for bit those of volume_loss_fwd + volume_loss_bwd
+    (the vectorised form for fp32 rows of whole float4s, the scalar form otherwise)."""
+    vol = torch.randn(shape, generator=torch.Generator().manual_seed(12), dtype=dtype).to(device)
+    g = torch.full((1,), 0.7, dtype=dtype, device=device)
+    loss, tv, tv_map = low.volume_loss_fwd(vol, 0.05)
+    grad = low.volume_loss_bwd(vol, g, 0.05)
+    loss2, tv2, grad2, map2 = low.volume_loss_fwd_bwd(vol, g, 0.05, with_map=True)
+    assert torch.equal(map2, tv_map)
+    assert torch.equal(grad2, grad)
+    torch.testing.assert_close(tv2, tv, rtol=1e-6, atol=0)
+    torch.testing.assert_close(loss2, loss, rtol=1e-6, atol=0)
+    loss3, _, grad3 = low.volume_loss_fwd_bwd(vol, g, 0.05)
+    assert torch.equal(grad3, grad) and torch.equal(loss3, loss2)

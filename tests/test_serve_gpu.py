@@ -65,9 +65,11 @@ def test_admission_by_budget(device):
     lean_probe.admit("q", lambda: batched.make_synthetic_scene(1500, 3, 48, 24, seed=31, device=device, lean=True))
     lean_fp, reserve = lean_probe.recons["q"].footprint, lean_probe.lean_reserve
     assert not lean_probe.recons["q"].graphed and reserve > 0
-    budget = full + lean_fp + reserve + (1 << 20)
-    assert budget < 2 * full  # room for one full footprint and one lean reconstruction, not two full ones
-    server = serve.FitServer(budget_bytes=budget, slots=2, device=device)
+    # Room for one full footprint plus one lean reconstruction and its reserved transient, but (the reserve
+    # being held back from the start) not for a second full footprint.
+    budget = full + lean_fp + reserve + (64 << 10)
+    assert full > lean_fp + (64 << 10)
+    server = serve.FitServer(budget_bytes=budget, slots=2, device=device, lean_reserve_bytes=reserve)
     assert server.admit("g", _factory(device, 32))
     assert server.recons["g"].graphed
     assert server.admit("l", _factory(device, 33))  # no room for a second full footprint: lean
