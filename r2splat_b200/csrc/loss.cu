@@ -158,9 +158,12 @@ __global__ void __launch_bounds__(kLossThreads) tv_fused_kernel(
 
 // The fused pass on fp32 volumes whose rows are whole float4s (W % 4 == 0, 16-byte aligned): each
 // lane owns four consecutive voxels of a row (one 16-byte load per slice), a warp 128 voxels of
-// one row, the block 8 rows; the slice two ahead is loaded while the current one is computed.
+// one row, the block 8 rows, over kTv4Chunk slices; the centre row two slices ahead and the two
+// neighbouring rows one slice ahead are loaded while the current slice is computed. Short chunks
+// keep enough warps in flight to cover the loads (a 256^3 volume makes 2048 block tiles).
 // Per voxel the operations and their order are tv_fused_kernel's.
 constexpr uint32_t kTv4TileX = 128;
+constexpr uint32_t kTv4Chunk = 8;
 
 __device__ __forceinline__ float tv_at(float cur, float next, float yp, float xp, bool dz, bool dy, bool dx) {
     float tv = 0.f;
@@ -201,19 +204,27 @@ __global__ void __launch_bounds__(kLossThreads) tv_fused4_kernel(
         const uint32_t chunk = uint32_t(t % chunks);
         const uint64_t b = t / chunks;
         const uint32_t x = tx * kTv4TileX + 4u * lane, y = ty * kTvTileY + ly;
-        const uint32_t d0 = chunk * kTvChunk, d1 = min(D, d0 + kTvChunk);
+        const uint32_t d0 = chunk * kTv4Chunk, d1 = min(D, d0 + kTv4Chunk);
         const bool active = x < W && y < H;  // W % 4 == 0: a lane's four voxels are all in or all out
         const uint64_t column = b * D * HW + uint64_t(y) * W + x;
         const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
-        auto load4 = [&](uint32_t d) {
-            return (active && d < D) ? __ldg(reinterpret_cast<const float4*>(vol + column + uint64_t(d) * HW))
-                                     : zero4;
+        const bool has_yp = active && y + 1 < H, has_ym = active && y > 0;
+        auto load4 = [&](bool ok, uint32_t d, int64_t dy) {
+            return (ok && d < D)
+                       ? __ldg(reinterpret_cast<const float4*>(vol + column + uint64_t(d) * HW + dy * int64_t(W)))
+                       : zero4;
         };
-        float4 prev = (active && d0 > 0) ? load4(d0 - 1) : zero4;
-        float4 cur = load4(d0);
-        float4 next = load4(d0 + 1);
+        float4 prev = d0 > 0 ? load4(active, d0 - 1, 0) : zero4;
+        float4 cur = load4(active, d0, 0);
+        float4 next = load4(active, d0 + 1, 0);
+        float4 yp_next = load4(has_yp, d0, 1), ym_next = load4(has_ym, d0, -1);
         for (uint32_t d = d0; d < d1; ++d) {
-            const float4 ahead = load4(d + 2);  // in flight while this slice is computed
+            // In flight while this slice is computed: the centre row two slices ahead, the
+            // neighbouring rows one ahead.
+            const float4 ahead = load4(active, d + 2, 0);
+            const float4 yp = yp_next, ym = ym_next;
+            yp_next = load4(has_yp, d + 1, 1);
+            ym_next = load4(has_ym, d + 1, -1);
             const uint64_t idx = column + uint64_t(d) * HW;
             // x neighbours: the adjacent lanes' edge voxels; the warp's first and last lanes load them.
             float xp = __shfl_down_sync(0xffffffffu, cur.x, 1);
@@ -221,8 +232,6 @@ __global__ void __launch_bounds__(kLossThreads) tv_fused4_kernel(
             if (active) {
                 if (lane == 31u && x + 4 < W) xp = vol[idx + 4];
                 if (lane == 0u && x > 0) xm = vol[idx - 1];
-                const float4 yp = y + 1 < H ? __ldg(reinterpret_cast<const float4*>(vol + idx + W)) : zero4;
-                const float4 ym = y > 0 ? __ldg(reinterpret_cast<const float4*>(vol + idx - W)) : zero4;
                 const bool zn = d + 1 < D, zp = d > 0, yn = y + 1 < H, yq = y > 0;
                 const bool xn3 = x + 4 < W, xq0 = x > 0;
                 float4 m, g;
@@ -413,17 +422,21 @@ int r2s_volume_loss_fwd_bwd(int dtype, const void* volume, const void* grad_outp
                       (tv_map == nullptr || reinterpret_cast<uintptr_t>(tv_map) % 16 == 0);
     if (vec4 && total > 0) {
         const uint32_t tiles4_x = (W + kTv4TileX - 1) / kTv4TileX;
-        const uint64_t n4 = uint64_t(B) * chunks * tiles_y * tiles4_x;
+        const uint32_t chunks4 = (D + kTv4Chunk - 1) / kTv4Chunk;
+        const uint64_t n4 = uint64_t(B) * chunks4 * tiles_y * tiles4_x;
         const unsigned blocks4 = unsigned(n4 < uint64_t(kLossMaxBlocks) ? n4 : uint64_t(kLossMaxBlocks));
-        double* partials4 = partials;  // blocks4 <= blocks: the 128-voxel rows make no more tiles than 32
+        // blocks4 <= kLossMaxBlocks, the partials the workspace was sized for.
+        Arena arena4(workspace, workspace_bytes);
+        double* partials4 = arena4.take<double>(blocks4);
+        R2S_REQUIRE(partials4, R2S_ERR_WORKSPACE, "loss workspace too small");
         if (tv_map != nullptr) {
             tv_fused4_kernel<true><<<blocks4, kLossThreads, 0, st>>>(
-                static_cast<const float*>(volume), D, H, W, tiles4_x, tiles_y, chunks, n4,
+                static_cast<const float*>(volume), D, H, W, tiles4_x, tiles_y, chunks4, n4,
                 static_cast<const float*>(grad_output), edges, lambda_tv, static_cast<float*>(tv_map),
                 static_cast<float*>(grad_volume), partials4);
         } else {
             tv_fused4_kernel<false><<<blocks4, kLossThreads, 0, st>>>(
-                static_cast<const float*>(volume), D, H, W, tiles4_x, tiles_y, chunks, n4,
+                static_cast<const float*>(volume), D, H, W, tiles4_x, tiles_y, chunks4, n4,
                 static_cast<const float*>(grad_output), edges, lambda_tv, nullptr, static_cast<float*>(grad_volume),
                 partials4);
         }

@@ -406,6 +406,9 @@ __global__ void __launch_bounds__(kMaxThreads) raster_fwd_pair_kernel(
                 if (hit) my_hits[__popc(hits & ((1u << lane) - 1u))] = uint16_t(base + int32_t(lane));
                 __syncwarp();
                 const int32_t n_hits = __popc(hits);
+                // Four records per loop trip: their sample math overlaps, while each pixel
+                // still adds them in list order (4.80 -> 4.33 ms at the CT workload).
+#pragma unroll 4
                 for (int32_t e = 0; e < n_hits; ++e) {
                     const int32_t s = my_hits[e];
                     const Rec2D<float>& r = buf[s];
