@@ -9,6 +9,9 @@ trajectory of radius 3, 512x512 detector (f=600, c=(256,256)). One fit step:
   from means perturbed by N(0, 0.005), seed 2) -> rasterize_bwd;
   voxelize_fwd on 256^3 of extent 1 -> TV loss fwd/bwd (lambda 0.05) ->
   voxelize_bwd with the TV gradient as the upstream adjoint.
+This package's arm takes the image-loss gradient from the forward's epilogue
+(``explicit.rasterize_fwd_with_loss``) and the TV loss and gradient from one
+pass; the reference's arm runs its own separate passes.
 A "Gaussian-sample evaluation" is one (primitive, pixel) or (primitive, voxel)
 pair inside an intersected tile: per pass, the sum over intersections of the
 in-bounds pixels (voxels) of the intersection's tile. value counts the raster
@@ -76,7 +79,7 @@ CONTRACTED_OPS = {"raster_render": 11, "raster_render_bwd": 30, "voxel_render": 
 ACCUMULATE_KERNELS = {
     "raster_render": "raster_fwd_pair_kernel (tile forward, two pixels per lane)",
     "raster_render_bwd": "raster_record_bwd_kernel (record-parallel raster VJP)",
-    "voxel_render": "voxel_fwd_kernel (tile forward, four voxels per thread)",
+    "voxel_render": "voxel_fwd_kernel (tile forward, a row of eight voxels per thread)",
     "voxel_render_bwd": "voxel_bwd_kernel (row-wise voxel VJP)",
 }
 # FP32 operations per sample of the Beta raster VJP with the variance branch in the reference's form
@@ -322,10 +325,11 @@ class OursStep:
     def __call__(self, means, quats, scales, densities):
         sc, st = self.scene, self.stages
         with st("rasterize_fwd"):
-            image, ctx = self.r2s.rasterize_fwd(means, quats, scales, densities, sc.viewmats, sc.Ks, sc.image_size)
+            # The MSE image loss and its gradient (image - target) * 2 / numel come from the
+            # forward's epilogue (the reference's step computes the gradient in a separate pass).
+            image, ctx, v_image, _, _ = self.r2s.explicit.rasterize_fwd_with_loss(
+                means, quats, scales, densities, sc.viewmats, sc.Ks, sc.image_size, self.target)
         self.last["raster_state"] = ctx.buffers["state"]
-        with st("image_loss_grad"):
-            v_image = 2 * (image - self.target) / image.numel()
         with st("rasterize_bwd"):
             g = self.r2s.rasterize_bwd(ctx, v_image)
         with st("voxelize_fwd"):
