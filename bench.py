@@ -11,7 +11,9 @@ trajectory of radius 3, 512x512 detector (f=600, c=(256,256)). One fit step:
   voxelize_bwd with the TV gradient as the upstream adjoint.
 This package's arm takes the image-loss gradient from the forward's epilogue
 (``explicit.rasterize_fwd_with_loss``) and the TV loss and gradient from one
-pass; the reference's arm runs its own separate passes.
+pass, and issues the raster and voxel halves of the step, which share nothing
+until the gradient sum, on two streams (``HalfStreams``); the reference's arm
+runs its own separate passes, one after the other, as its package does.
 A "Gaussian-sample evaluation" is one (primitive, pixel) or (primitive, voxel)
 pair inside an intersected tile: per pass, the sum over intersections of the
 in-bounds pixels (voxels) of the intersection's tile. value counts the raster
@@ -309,6 +311,51 @@ def count_evals_3d(offsets: torch.Tensor, n_isects: int, shape: tuple, tile: int
 
 # --------------------------------------------------------------------------- the fit step
 
+class HalfStreams:
+    """Streams for the two independent halves of a fit step.
+
+    The raster half (rasterize_fwd, its loss gradient, rasterize_bwd) and the voxel half
+    (voxelize_fwd, TV, voxelize_bwd) share nothing until the gradient sum. With ``concurrent``
+    the voxel half is issued first on a low-priority stream and the raster half on a
+    high-priority one: each half's host read of its intersection count waits only for its own
+    projection, and the voxel kernels fill the SMs around the raster kernels. Without it both
+    halves run on the current stream in the reference's order (raster, then voxel), which is
+    how the per-kernel stage timers and rooflines are taken.
+    """
+
+    def __init__(self):
+        least, greatest = torch.cuda.Stream.priority_range()
+        self.raster = torch.cuda.Stream(priority=greatest)
+        self.voxel = torch.cuda.Stream(priority=least)
+        self.concurrent = True
+
+    def run(self, raster_fwd, raster_bwd, voxel_fwd, voxel_bwd, outputs):
+        """Calls the four parts (each returning tensors the gradient sum reads) and joins them
+        onto the current stream."""
+        cur = torch.cuda.current_stream()
+        if not self.concurrent:
+            raster_fwd()
+            raster_bwd()
+            voxel_fwd()
+            voxel_bwd()
+            return
+        self.raster.wait_stream(cur)
+        self.voxel.wait_stream(cur)
+        with torch.cuda.stream(self.voxel):
+            voxel_fwd()
+        with torch.cuda.stream(self.raster):
+            raster_fwd()
+        with torch.cuda.stream(self.voxel):
+            voxel_bwd()
+        with torch.cuda.stream(self.raster):
+            raster_bwd()
+        cur.wait_stream(self.raster)
+        cur.wait_stream(self.voxel)
+        for t in outputs():
+            if t is not None:
+                t.record_stream(cur)
+
+
 class OursStep:
     """One fit step through this package's public explicit operators."""
 
@@ -321,29 +368,46 @@ class OursStep:
         self.ones = torch.ones(1, device=scene.means.device)
         self.last = {}
         self.stages = ApiStages()
+        self.streams = HalfStreams()
 
     def __call__(self, means, quats, scales, densities):
         sc, st = self.scene, self.stages
-        with st("rasterize_fwd"):
-            # The MSE image loss and its gradient (image - target) * 2 / numel come from the
-            # forward's epilogue (the reference's step computes the gradient in a separate pass).
-            image, ctx, v_image, _, _ = self.r2s.explicit.rasterize_fwd_with_loss(
-                means, quats, scales, densities, sc.viewmats, sc.Ks, sc.image_size, self.target)
-        self.last["raster_state"] = ctx.buffers["state"]
-        with st("rasterize_bwd"):
-            g = self.r2s.rasterize_bwd(ctx, v_image)
-        with st("voxelize_fwd"):
-            volume, vctx = self.r2s.voxelize_fwd(means, quats, scales, densities, sc.volume_shape,
-                                                 volume_extent=sc.volume_extent)
-        self.last["voxel_state"] = vctx.buffers["state"]
-        with st("volume_loss_fwd_bwd"):
-            # One pass: the TV term's upstream gradient (one) is known before its forward.
-            loss, _, g_vol = self.low.volume_loss_fwd_bwd(volume.unsqueeze(0), self.ones, self.lam)
-        with st("voxelize_bwd"):
-            gv = self.r2s.voxelize_bwd(vctx, g_vol[0])
+        out = {}
+
+        def raster_fwd():
+            with st("rasterize_fwd"):
+                # The MSE image loss and its gradient (image - target) * 2 / numel come from the
+                # forward's epilogue (the reference's step computes the gradient in a separate pass).
+                _, ctx, v_image, _, _ = self.r2s.explicit.rasterize_fwd_with_loss(
+                    means, quats, scales, densities, sc.viewmats, sc.Ks, sc.image_size, self.target)
+            self.last["raster_state"] = ctx.buffers["state"]
+            out["raster"] = (ctx, v_image)
+
+        def raster_bwd():
+            with st("rasterize_bwd"):
+                out["g"] = self.r2s.rasterize_bwd(*out.pop("raster"))
+
+        def voxel_fwd():
+            with st("voxelize_fwd"):
+                volume, vctx = self.r2s.voxelize_fwd(means, quats, scales, densities, sc.volume_shape,
+                                                     volume_extent=sc.volume_extent)
+            self.last["voxel_state"] = vctx.buffers["state"]
+            with st("volume_loss_fwd_bwd"):
+                # One pass: the TV term's upstream gradient (one) is known before its forward.
+                loss, _, g_vol = self.low.volume_loss_fwd_bwd(volume.unsqueeze(0), self.ones, self.lam)
+            out["voxel"] = (vctx, g_vol[0])
+            out["loss"] = loss
+
+        def voxel_bwd():
+            with st("voxelize_bwd"):
+                out["gv"] = self.r2s.voxelize_bwd(*out.pop("voxel"))
+
+        self.streams.run(raster_fwd, raster_bwd, voxel_fwd, voxel_bwd,
+                         lambda: (*_grad_fields(out["g"], 4), *_grad_fields(out["gv"], 4), out["loss"]))
+        g, gv = out["g"], out["gv"]
         with st("gradient_sum"):
             grads = (g.means + gv.means, g.quats + gv.quats, g.scales + gv.scales, g.densities + gv.densities)
-        return loss, grads
+        return out["loss"], grads
 
     def eval_counts(self):
         rs, vs = self.last["raster_state"], self.last["voxel_state"]
@@ -351,6 +415,12 @@ class OursStep:
         raster = count_evals_2d(rs.offsets, rs.n_isects, h, w, rs.tile_size)
         voxel = count_evals_3d(vs.offsets, vs.n_isects, vs.shape, vs.tile_size)
         return raster, voxel, rs.n_isects, vs.n_isects
+
+
+def _grad_fields(g, k: int) -> tuple:
+    """The first k gradient tensors of a ParameterGradients (means, quats, scales, densities, beta,
+    uncertainty)."""
+    return (g.means, g.quats, g.scales, g.densities, g.beta, g.uncertainty)[:k]
 
 
 class ReferenceStep:
@@ -425,25 +495,39 @@ class OursBetaStep(_BetaAdjoints):
         super().__init__(scene)
         self.r2s, self.scene, self.last = r2s, scene, {}
         self.stages = ApiStages()
+        self.streams = HalfStreams()
 
     def __call__(self, means, quats, scales, densities, beta, uncertainty):
         sc, st = self.scene, self.stages
-        with st("rasterize_fwd"):
-            _, ctx = self.r2s.rasterize_fwd(means, quats, scales, densities, sc.viewmats, sc.Ks, sc.image_size,
-                                            beta=beta, uncertainty=uncertainty)
-        self.last["raster_state"] = ctx.buffers["state"]
-        with st("rasterize_bwd"):
-            g = self.r2s.rasterize_bwd(ctx, self.v_image, self.v_image_var)
-        with st("voxelize_fwd"):
-            _, vctx = self.r2s.voxelize_fwd(means, quats, scales, densities, sc.volume_shape,
-                                            volume_extent=sc.volume_extent, beta=beta, uncertainty=uncertainty)
-        self.last["voxel_state"] = vctx.buffers["state"]
-        with st("voxelize_bwd"):
-            gv = self.r2s.voxelize_bwd(vctx, self.v_volume, self.v_volume_var)
+        out = {}
+
+        def raster_fwd():
+            with st("rasterize_fwd"):
+                _, ctx = self.r2s.rasterize_fwd(means, quats, scales, densities, sc.viewmats, sc.Ks, sc.image_size,
+                                                beta=beta, uncertainty=uncertainty)
+            self.last["raster_state"] = ctx.buffers["state"]
+            out["ctx"] = ctx
+
+        def raster_bwd():
+            with st("rasterize_bwd"):
+                out["g"] = self.r2s.rasterize_bwd(out.pop("ctx"), self.v_image, self.v_image_var)
+
+        def voxel_fwd():
+            with st("voxelize_fwd"):
+                _, vctx = self.r2s.voxelize_fwd(means, quats, scales, densities, sc.volume_shape,
+                                                volume_extent=sc.volume_extent, beta=beta, uncertainty=uncertainty)
+            self.last["voxel_state"] = vctx.buffers["state"]
+            out["vctx"] = vctx
+
+        def voxel_bwd():
+            with st("voxelize_bwd"):
+                out["gv"] = self.r2s.voxelize_bwd(out.pop("vctx"), self.v_volume, self.v_volume_var)
+
+        self.streams.run(raster_fwd, raster_bwd, voxel_fwd, voxel_bwd,
+                         lambda: (*_grad_fields(out["g"], 6), *_grad_fields(out["gv"], 6)))
+        g, gv = out["g"], out["gv"]
         with st("gradient_sum"):
-            grads = tuple(a + b for a, b in zip(
-                (g.means, g.quats, g.scales, g.densities, g.beta, g.uncertainty),
-                (gv.means, gv.quats, gv.scales, gv.densities, gv.beta, gv.uncertainty)))
+            grads = tuple(a + b for a, b in zip(_grad_fields(g, 6), _grad_fields(gv, 6)))
         return grads[3].sum(), grads
 
     eval_counts = OursStep.eval_counts
@@ -686,25 +770,57 @@ def library_launches() -> int:
 
 
 def e2e_run(step, scene, steps, warmup, device):
-    """Public API with pinned host inputs copied in and gradients copied out each step."""
+    """Public API with pinned host inputs copied in and gradients copied out each step.
+
+    The copies run on a stream of their own, double-buffered: step i+1's inputs are copied in
+    while step i computes (once step i-1, the last reader of that buffer, is done), and step
+    i's gradients are copied out as soon as it ends. Every step's copies are inside the timed
+    region; the clock stops when the last gradients have reached the host.
+    """
     host = [t.detach().cpu().pin_memory() for t in step_inputs(scene)]
-    outs = None
     h2d = sum(t.numel() * t.element_size() for t in host)
+    cur = torch.cuda.current_stream()
+    copy = torch.cuda.Stream()
+    dev = [[torch.empty_like(t, device=device) for t in host] for _ in range(2)]
+    loaded = [torch.cuda.Event(), torch.cuda.Event()]
+    outs = None
     d2h = 0
-    for i in range(warmup + steps):
+    last_step = None
+    total = warmup + steps
+
+    def load(i):
+        with torch.cuda.stream(copy):
+            for d, h in zip(dev[i % 2], host):
+                d.copy_(h, non_blocking=True)
+            loaded[i % 2].record(copy)
+
+    load(0)
+    for i in range(total):
         if i == warmup:
             torch.cuda.synchronize()
             start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            start.record()
-        dev = [t.to(device, non_blocking=True) for t in host]
-        loss, grads = step(*dev)
+            start.record(cur)
+            copy.wait_stream(cur)
+            load(i)  # this step's inputs inside the timed region
+        cur.wait_event(loaded[i % 2])
+        loss, grads = step(*dev[i % 2])
+        done = torch.cuda.Event()
+        done.record(cur)
+        if i + 1 < total and i + 1 != warmup:
+            if last_step is not None:
+                copy.wait_event(last_step)  # the previous step read the buffer about to be overwritten
+            load(i + 1)
+        last_step = done
+        results = list(grads) + [loss]
         if outs is None:
-            outs = [torch.empty(g.shape, dtype=g.dtype, pin_memory=True) for g in grads] + [
-                torch.empty((), dtype=loss.dtype, pin_memory=True)]
-            d2h = sum(o.numel() * o.element_size() for o in outs)
-        for o, g in zip(outs, list(grads) + [loss]):
-            o.copy_(g, non_blocking=True)
-    end.record()
+            outs = [[torch.empty(g.shape, dtype=g.dtype, pin_memory=True) for g in results] for _ in range(2)]
+            d2h = sum(o.numel() * o.element_size() for o in outs[0])
+        copy.wait_event(done)
+        with torch.cuda.stream(copy):
+            for o, g in zip(outs[i % 2], results):
+                g.record_stream(copy)
+                o.copy_(g, non_blocking=True)
+    end.record(copy)
     end.synchronize()
     return start.elapsed_time(end), h2d, d2h
 
@@ -1034,6 +1150,9 @@ def main(argv=None) -> int:
         step = OursBetaStep(scene) if ours else ReferenceBetaStep(scene)
     else:
         step = OursStep(scene, target) if ours else ReferenceStep(scene, target)
+    if ours and args.workload == "small":
+        # The small step is host-bound (about a millisecond): a second stream only adds host work.
+        step.streams.concurrent = False
     if args.profile_only:
         for _ in range(args.warmup):
             step(*step_inputs(scene))
@@ -1047,6 +1166,7 @@ def main(argv=None) -> int:
     with ClockSampler(local) as clocks:
         total_ms, stages, api_stages, own_launches = timed_run(step, scene, args.steps, args.warmup, device,
                                                                flush_buf, clocks, ours=ours)
+    per_step = sorted(getattr(timed_run, "per_step_ms", []))
     ranks = world if ours else 1
     total_ms = max_over_ranks(total_ms, ranks, device)
     ms_per_step = total_ms / args.steps
@@ -1057,10 +1177,23 @@ def main(argv=None) -> int:
     e2e_ms, h2d, d2h = e2e_run(step, scene, args.steps, args.warmup, device)
     e2e_ms = max_over_ranks(e2e_ms, ranks, device)
     e2e_value = job_rate(evals_per_step, ranks, e2e_ms / args.steps)
-    per_step = sorted(getattr(timed_run, "per_step_ms", []))
-    api_ms = {k: v / args.steps for k, v in api_stages.items()}
+
+    concurrent = None
+    stage_steps, stage_ms = args.steps, ms_per_step
+    if ours and step.streams.concurrent:
+        # In the timed steps the two halves overlap, so a kernel's CUDA-event time includes the
+        # other half's blocks sharing the SMs. The stage tables and rooflines are taken from a
+        # second pass of the same step with both halves on one stream (the reference's order).
+        concurrent = {"stages_ms_per_step": {k: v / args.steps for k, v in stages.items()},
+                      "api_stages_ms_per_step": {k: v / args.steps for k, v in api_stages.items()}}
+        step.streams.concurrent = False
+        stage_steps = min(args.steps, 10)
+        seq_ms, stages, api_stages, _ = timed_run(step, scene, stage_steps, 1, device, flush_buf, None, ours=True)
+        step.streams.concurrent = True
+        stage_ms = seq_ms / stage_steps
+    api_ms = {k: v / stage_steps for k, v in api_stages.items()}
     api_ms["sum_of_stages"] = sum(api_ms.values())
-    api_ms["outside_stages"] = ms_per_step - api_ms["sum_of_stages"]
+    api_ms["outside_stages"] = stage_ms - api_ms["sum_of_stages"]
 
     peaks = measured_peaks()
     result = {
@@ -1106,10 +1239,17 @@ def main(argv=None) -> int:
         })
     else:
         result["gpu_launches"] = own_launches
-        result["stages_ms_per_step"] = {k: v / args.steps for k, v in stages.items()}
+        result["stages_ms_per_step"] = {k: v / stage_steps for k, v in stages.items()}
+        if concurrent is not None:
+            result["step_schedule"] = (
+                "timed steps: the voxel half (voxelize_fwd, TV, voxelize_bwd) on a low-priority stream, issued "
+                "first, and the raster half (rasterize_fwd with the loss epilogue, rasterize_bwd) on a "
+                "high-priority stream; api_stages_ms_per_step, stages_ms_per_step and the rooflines come from "
+                f"{stage_steps} further steps with both halves on one stream ({stage_ms:.3f} ms per step)")
+            result["concurrent_stages"] = concurrent
         fp32_peak = fp32_peak_tflops(device)
         sfu_peak = sfu_peak_gops(device)
-        result["rooflines"] = accumulate_rooflines(args.workload, stages, args.steps, raster_evals, voxel_evals,
+        result["rooflines"] = accumulate_rooflines(args.workload, stages, stage_steps, raster_evals, voxel_evals,
                                                    fp32_peak)
         result["roofline"] = dominant_roofline(args.workload, result["rooflines"], fp32_peak, sfu_peak,
                                                peaks.get("hbm_gbs"))

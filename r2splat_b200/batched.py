@@ -116,6 +116,7 @@ class FitScene:
         self.overflow = torch.zeros(1, dtype=torch.int32, device=dev)
         self.loss = torch.zeros(1, dtype=dt, device=dev)
         self.ones = torch.ones(1, dtype=dt, device=dev)
+        self._voxel_stream: Optional[torch.cuda.Stream] = None
         self.capacity_2d = 0
         self.capacity_3d = 0
         if self.is_lean:
@@ -191,6 +192,7 @@ class FitScene:
     def measure_counts(self) -> tuple[int, int]:
         """2D and 3D intersection counts of the current parameters (host read; used outside capture)."""
         stream = torch.cuda.current_stream(self.device).cuda_stream
+        self._transform(stream)
         self._project(stream)
         self._project3(stream)
         torch.cuda.current_stream(self.device).synchronize()
@@ -204,10 +206,14 @@ class FitScene:
         return self.measure_counts()
 
     # ------------------------------------------------------------------ kernels
-    def _project(self, stream):
+    def _transform(self, stream):
+        """Covariances from the activated quaternions and scales (read by both halves of the step)."""
         d = _dt(self.means)
         _backend.call("r2s_parameter_transform_fwd", d, _p(self.quats), _p(self.scales), _p(self.covars),
                       _p(self.max_scales), self.n, stream)
+
+    def _project(self, stream):
+        d = _dt(self.means)
         self.ratio = _beta.beta_path_ratio(self.beta) if self.beta is not None else None
         _backend.call("r2s_raster_project", d, _p(self.means), _p(self.covars), _p(self.densities), _p(self.beta),
                       _p(self.ratio), _p(self.viewmats), _p(self.Ks), self.c, self.n, self.width, self.height,
@@ -226,12 +232,26 @@ class FitScene:
                       self.scan3_ws.numel(), stream)
 
     def enqueue(self, stream: torch.cuda.Stream):
-        """Issues one complete fit step on `stream` (capturable: no host synchronisation)."""
+        """Issues one complete fit step on `stream` (capturable: no host synchronisation).
+
+        The raster half runs on `stream`; the voxel half (projection, lists, forward, TV, VJP,
+        chain rule) forks onto a stream of the scene's own and joins back before the update, so
+        the two halves' kernels overlap on the device (and in a captured graph they are two
+        branches). Both read the covariances computed before the fork; neither reads what the other
+        writes, and both only raise the shared overflow flag.
+        """
         s = stream.cuda_stream
         d = _dt(self.means)
         beta_flag = int(self.beta is not None)
+        if self._voxel_stream is None:
+            self._voxel_stream = torch.cuda.Stream(device=self.device)
+        vstream = self._voxel_stream
         with torch.cuda.stream(stream):
             self.overflow.zero_()
+            self._transform(s)
+        vstream.wait_stream(stream)
+        self._enqueue_voxel_half(vstream, d, beta_flag)
+        with torch.cuda.stream(stream):
             # Raster forward, loss gradient, VJP.
             self._project(s)
             _backend.call("r2s_raster_emit_capacity", _p(self.rects), self.c, self.n, self.tx, self.ty, _p(self.cum),
@@ -252,7 +272,21 @@ class FitScene:
                           _p(self.covars), _p(self.beta), _p(self.ratio), _p(log_grad), _p(self.viewmats),
                           _p(self.Ks), self.c, self.n, self.width, self.height, float(self.cfg.eps),
                           float(self.cfg.eps), _p(self.grads2d), _p(g[0]), _p(g[1]), _p(g[2]), _p(g[3]), _p(g[4]), s)
-            # Voxel forward, TV, VJP.
+            stream.wait_stream(vstream)
+            # Loss (image MSE + lambda TV), then the update unless this step overflowed.
+            torch.add(self.image_loss, self.tv_loss, out=self.loss)
+            grads_a = (ctypes.c_void_p * 5)(*[None if t is None else t.data_ptr() for t in self.g_raster])
+            grads_b = (ctypes.c_void_p * 5)(*[None if t is None else t.data_ptr() for t in self.g_voxel])
+            self._grad_tables = (grads_a, grads_b)  # kept alive for the captured call's duration
+            _backend.call("r2s_adam_activation_step", d, self.n, _p(self.means), _p(self.quats),
+                          _p(self.raw_scales), _p(self.raw_densities), _p(self.raw_beta), _p(self.scales),
+                          _p(self.densities), _p(self.beta), _p(self.adam_m), _p(self.adam_v), grads_a, grads_b,
+                          float(self.cfg.lr), 0.9, 0.999, 1e-8, _p(self.step_count), _p(self.overflow), s)
+
+    def _enqueue_voxel_half(self, stream: torch.cuda.Stream, d: int, beta_flag: int):
+        """Voxel forward, TV, VJP and chain rule of one fit step on `stream`."""
+        s = stream.cuda_stream
+        with torch.cuda.stream(stream):
             self._project3(s)
             _backend.call("r2s_voxel_emit_capacity", d, _p(self.means_v), _p(self.radii3), self.n,
                           self.cfg.voxel_tile, self.vtx, self.vty, self.vtz, _p(self.cum3), self.capacity_3d,
@@ -276,15 +310,6 @@ class FitScene:
                           _p(self.extent), _p(self.center), self.n, self.vwidth, self.vheight, self.depth,
                           float(self.cfg.eps), _p(self.grads3d), _p(v[0]), _p(v[1]), _p(v[2]), _p(v[3]), _p(v[4]),
                           None, s)
-            # Loss (image MSE + lambda TV), then the update unless this step overflowed.
-            torch.add(self.image_loss, self.tv_loss, out=self.loss)
-            grads_a = (ctypes.c_void_p * 5)(*[None if t is None else t.data_ptr() for t in self.g_raster])
-            grads_b = (ctypes.c_void_p * 5)(*[None if t is None else t.data_ptr() for t in self.g_voxel])
-            self._grad_tables = (grads_a, grads_b)  # kept alive for the captured call's duration
-            _backend.call("r2s_adam_activation_step", d, self.n, _p(self.means), _p(self.quats),
-                          _p(self.raw_scales), _p(self.raw_densities), _p(self.raw_beta), _p(self.scales),
-                          _p(self.densities), _p(self.beta), _p(self.adam_m), _p(self.adam_v), grads_a, grads_b,
-                          float(self.cfg.lr), 0.9, 0.999, 1e-8, _p(self.step_count), _p(self.overflow), s)
 
     def step(self):
         """One eager fit step on the current stream (grows the capacity and repeats on overflow)."""

@@ -306,6 +306,13 @@ class FitServer:
         if self._lean_future is not None:
             self._lean_future.result().synchronize()
 
+    def close(self):
+        """Waits for a lean step in flight and stops the worker thread."""
+        try:
+            self._wait_lean()
+        finally:
+            self._lean_worker.shutdown(wait=True)
+
     def _finish(self, recon: Reconstruction, stats: ServeStats):
         """Completion of a step: a graphed step that overflowed is redone with room, then re-captured."""
         if not recon.graphed or int(recon.overflow_host[0]) == 0:

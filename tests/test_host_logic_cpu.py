@@ -27,6 +27,41 @@ def test_serve_stats_percentiles_and_summary():
     assert summary["p50_ms"] == 3.0 and summary["fit_steps_per_s"] == 2.5
     assert serve.ServeStats(0, 0.0).steps_per_s == 0.0
     assert serve.ServeStats(0, 1.0).percentile(50) != serve.ServeStats(0, 1.0).percentile(50)  # nan
+    assert "lean_p50_ms" not in summary
+
+
+def test_serve_stats_split_lean_and_graphed_latencies():
+    stats = serve.ServeStats(completed=6, wall_s=1.0, latencies_ms=[1.0, 2.0, 900.0, 3.0, 1000.0, 4.0],
+                             lean_latencies_ms=[900.0, 1000.0])
+    summary = stats.summary()
+    assert summary["lean_requests"] == 2
+    assert summary["lean_p50_ms"] in (900.0, 1000.0) and summary["lean_p99_ms"] == 1000.0
+    assert summary["graphed_p99_ms"] == 4.0 and summary["graphed_p50_ms"] in (2.0, 3.0)
+    assert summary["p99_ms"] == 1000.0
+
+
+def test_lean_step_handle_is_done_only_when_launched_and_finished():
+    from concurrent.futures import Future
+
+    class Event:
+        def __init__(self, done):
+            self.done = done
+
+        def query(self):
+            return self.done
+
+    pending = Future()
+    step = serve._LeanStep(pending)
+    assert not step.query()  # the worker thread has not launched it yet
+    pending.set_result(Event(False))
+    assert not step.query()  # launched, still running on the device
+    finished = Future()
+    finished.set_result(Event(True))
+    assert serve._LeanStep(finished).query()
+    failed = Future()
+    failed.set_exception(RuntimeError("lean step failed"))
+    with pytest.raises(RuntimeError, match="lean step failed"):
+        serve._LeanStep(failed).query()
 
 
 def test_scene_config_defaults_and_autotuner_keys():
