@@ -1163,10 +1163,28 @@ def main(argv=None) -> int:
     if world > 1 and ours:
         dist.barrier()
     torch.cuda.synchronize()
+    concurrent = None
+    stage_steps = args.steps
+    if ours and step.streams.concurrent:
+        # In the timed steps the two halves overlap, so a kernel's CUDA-event time includes the
+        # other half's blocks sharing the SMs. The stage tables and rooflines are taken first, from
+        # steps of the same fit step with both halves on one stream (the reference's order).
+        step.streams.concurrent = False
+        stage_steps = min(args.steps, 10)
+        seq_ms, seq_stages, seq_api, _ = timed_run(step, scene, stage_steps, args.warmup, device, flush_buf, None,
+                                                   ours=True)
+        step.streams.concurrent = True
+        step.stages = ApiStages()
+        concurrent = {"sequential_ms_per_step": seq_ms / stage_steps}
     with ClockSampler(local) as clocks:
         total_ms, stages, api_stages, own_launches = timed_run(step, scene, args.steps, args.warmup, device,
                                                                flush_buf, clocks, ours=ours)
     per_step = sorted(getattr(timed_run, "per_step_ms", []))
+    if concurrent is not None:
+        concurrent.update(stages_ms_per_step={k: v / args.steps for k, v in stages.items()},
+                          api_stages_ms_per_step={k: v / args.steps for k, v in api_stages.items()})
+        stages, api_stages = seq_stages, seq_api
+    stage_ms = concurrent["sequential_ms_per_step"] if concurrent is not None else None
     ranks = world if ours else 1
     total_ms = max_over_ranks(total_ms, ranks, device)
     ms_per_step = total_ms / args.steps
@@ -1178,19 +1196,8 @@ def main(argv=None) -> int:
     e2e_ms = max_over_ranks(e2e_ms, ranks, device)
     e2e_value = job_rate(evals_per_step, ranks, e2e_ms / args.steps)
 
-    concurrent = None
-    stage_steps, stage_ms = args.steps, ms_per_step
-    if ours and step.streams.concurrent:
-        # In the timed steps the two halves overlap, so a kernel's CUDA-event time includes the
-        # other half's blocks sharing the SMs. The stage tables and rooflines are taken from a
-        # second pass of the same step with both halves on one stream (the reference's order).
-        concurrent = {"stages_ms_per_step": {k: v / args.steps for k, v in stages.items()},
-                      "api_stages_ms_per_step": {k: v / args.steps for k, v in api_stages.items()}}
-        step.streams.concurrent = False
-        stage_steps = min(args.steps, 10)
-        seq_ms, stages, api_stages, _ = timed_run(step, scene, stage_steps, 1, device, flush_buf, None, ours=True)
-        step.streams.concurrent = True
-        stage_ms = seq_ms / stage_steps
+    if stage_ms is None:
+        stage_ms = ms_per_step
     api_ms = {k: v / stage_steps for k, v in api_stages.items()}
     api_ms["sum_of_stages"] = sum(api_ms.values())
     api_ms["outside_stages"] = stage_ms - api_ms["sum_of_stages"]
@@ -1245,7 +1252,7 @@ def main(argv=None) -> int:
                 "timed steps: the voxel half (voxelize_fwd, TV, voxelize_bwd) on a low-priority stream, issued "
                 "first, and the raster half (rasterize_fwd with the loss epilogue, rasterize_bwd) on a "
                 "high-priority stream; api_stages_ms_per_step, stages_ms_per_step and the rooflines come from "
-                f"{stage_steps} further steps with both halves on one stream ({stage_ms:.3f} ms per step)")
+                f"{stage_steps} steps run before them with both halves on one stream ({stage_ms:.3f} ms per step)")
             result["concurrent_stages"] = concurrent
         fp32_peak = fp32_peak_tflops(device)
         sfu_peak = sfu_peak_gops(device)
