@@ -466,10 +466,12 @@ int r2s_voxel_render_bwd_capacity(int dtype, const void* records, int beta, int 
  * sums to slot tile_cum[n - 1] + (the tile's index in primitive n's 3D tile box,
  * z then y then x), and a second pass adds each primitive's slots in order into
  * grads [N] (written, not accumulated): the same result on every run. means_v [N,3]
- * and radii [N,3] are r2s_voxel_project's, tile_cum [N] int64 the inclusive scan of
- * its tile counts; slots [slot_capacity, 12] is caller scratch. Capacity-bounded
- * form: n_used (device count) instead of n_isects; slots past slot_capacity are
- * neither written nor read (such a step overflowed and is discarded). */
+ * and radii [N,3] are r2s_voxel_project's (the tile box is taken from the records'
+ * voxel-space centre, which r2s_voxel_project writes equal to means_v), tile_cum [N]
+ * int64 the inclusive scan of its tile counts; slots [slot_capacity, 12] is caller
+ * scratch, slot_capacity below 2^31. Capacity-bounded form: n_used (device count)
+ * instead of n_isects; slots past slot_capacity are neither written nor read (such a
+ * step overflowed and is discarded). */
 int r2s_voxel_render_bwd_slots(int dtype, const void* records, int beta, int detach_variance,
                                const int32_t* tile_offsets, const int32_t* flatten_ids, uint64_t n_isects,
                                const int64_t* n_used, const void* means_v, const int32_t* radii,
