@@ -480,6 +480,43 @@ int r2s_voxel_render_bwd_slots(int dtype, const void* records, int beta, int det
                                uint32_t tiles_y, uint32_t tiles_z, void* slots, uint64_t slot_capacity, void* grads,
                                void* stream);
 
+/* Per-tile packed record layout of the 3D tile pipeline (replaces the reference's
+ * per-intersection gathers through flatten_ids in K29-K32, VoxelizeToVoxelsFwd.cu:73-139
+ * and VoxelizeToVoxelsBwd.cu:322-380, which read means3d/conics/opacities at
+ * g = flatten_ids[i] for every list entry). packed [n_isects] Rec3D (64 B fp32,
+ * 128 B fp64, caller-allocated) receives records[flatten_ids[i]] for each sorted
+ * intersection i, so a tile's list is one contiguous range that the tile kernels stage
+ * with one bulk copy per batch. The padding carries the pair's VJP slot, as in
+ * r2s_voxel_render_bwd_slots (0xffffffff past slot_capacity). tile_offsets and
+ * flatten_ids are the sorted 3D lists, radii [N,3] and tile_cum [N] r2s_voxel_project's
+ * and its tile-count scan; workspace holds r2s_voxel_pack_workspace(N) bytes.
+ * Capacity-bounded form: n_isects is the capacity and n_used the device count. */
+size_t r2s_voxel_pack_workspace(uint32_t N);
+int r2s_voxel_pack_tile_records(int dtype, const void* records, const int32_t* tile_offsets,
+                                const int32_t* flatten_ids, const int32_t* radii, const int64_t* tile_cum, uint32_t N,
+                                uint64_t n_isects, const int64_t* n_used, uint32_t tile_size, uint32_t tiles_x,
+                                uint32_t tiles_y, uint32_t tiles_z, uint64_t slot_capacity, void* packed,
+                                void* workspace, size_t workspace_bytes, void* stream);
+/* r2s_voxel_render (K29/K31) on the packed layout: the same volume and variance bit for
+ * bit. n_used null: n_isects is the count; else the device count (n_isects unused). */
+int r2s_voxel_render_packed(int dtype, const void* packed, int beta, const int32_t* tile_offsets,
+                            uint64_t n_isects, const int64_t* n_used, uint32_t dim2, uint32_t dim1, uint32_t dim0,
+                            uint32_t tile_size, uint32_t tiles_x, uint32_t tiles_y, uint32_t tiles_z, void* volume,
+                            void* volume_var, void* stream);
+/* r2s_voxel_render_bwd_slots (K30/K32, deterministic slots) on the packed layout, with
+ * the slots taken from the records' padding: the same grads bit for bit. */
+int r2s_voxel_render_bwd_packed(int dtype, const void* packed, int beta, int detach_variance,
+                                const int32_t* tile_offsets, uint64_t n_isects, const int64_t* n_used,
+                                const int64_t* tile_cum, const void* v_volume, const void* v_volume_var, uint32_t N,
+                                uint32_t dim2, uint32_t dim1, uint32_t dim0, uint32_t tile_size, uint32_t tiles_x,
+                                uint32_t tiles_y, uint32_t tiles_z, void* slots, uint64_t slot_capacity, void* grads,
+                                void* stream);
+/* Number of bulk-staging waits on `device` that ran out (a batch copy that did not
+ * complete within 0.2 s; the kernel then left the rest of that tile unwritten) since
+ * the last clear; clear != 0 resets it. Synchronous: reads a device word. No
+ * counterpart in the reference (its tile kernels stage with plain loads). */
+int r2s_bulk_wait_faults(int device, int clear, uint32_t* count);
+
 /* Record-parallel voxel VJP, for a backward that keeps no intersection lists
  * (recompute-in-backward under a memory budget), replacing the tile-parallel
  * per-primitive VJP with atomics (VoxelizeToVoxelsBwd.cu:322-514, K30/K32, for

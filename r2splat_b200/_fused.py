@@ -138,6 +138,7 @@ class VoxelState:
     tile_cum: Optional[Tensor] = None
     layer_cum: Optional[Tensor] = None
     n_items: int = 0
+    packed: Optional[Tensor] = None  # per-tile packed records [M,16], the VJP slot in each padding
 
 
 def raster_intersections(means, covars, densities, beta, ratio, viewmats, Ks, width, height, eps, radius_clip,
@@ -380,9 +381,25 @@ def release_lists(state):
     """Drops a forward state's intersection lists (raster or voxel): neither VJP needs them (the raster VJP
     walks tile rectangles; the voxel VJP then takes its list-free form), so a caller short of memory can
     free them between forward and backward. Returns the tensors dropped."""
-    dropped = [t for t in (state.isect_ids, state.flatten_ids, state.offsets) if t is not None]
+    dropped = [t for t in (state.isect_ids, state.flatten_ids, state.offsets, getattr(state, "packed", None))
+               if t is not None]
     state.isect_ids = state.flatten_ids = state.offsets = None
+    if hasattr(state, "packed"):
+        state.packed = None
     return dropped
+
+
+def pack_tile_records(records, offsets, flatten_ids, radii, tile_cum, m, shape, tile_size):
+    """Per-tile packed copy of the 3D records ([M,16], the sorted intersections' records in list order, each
+    pair's VJP slot in the padding): each tile's batch is then one contiguous range, staged by one bulk copy."""
+    tx, ty, tz = _voxel_tiles(shape, tile_size)
+    n = records.shape[0]
+    packed = records.new_empty((max(m, 1), records.shape[1]))
+    ws = _ws(_backend.library().r2s_voxel_pack_workspace(n), records.device)
+    _backend.call("r2s_voxel_pack_tile_records", _dtype(records), _ptr(records), _ptr(offsets), _ptr(flatten_ids),
+                  _ptr(radii), _ptr(tile_cum), n, m, None, tile_size, tx, ty, tz, m, _ptr(packed), _ptr(ws),
+                  ws.numel(), _stream(records.device))
+    return packed
 
 
 def voxel_forward(means, quats, scales, densities, shape, extent, center, beta, uncertainty, eps, radius_clip,
@@ -398,12 +415,14 @@ def voxel_forward(means, quats, scales, densities, shape, extent, center, beta, 
     tx = (width + tile_size - 1) // tile_size
     ty = (height + tile_size - 1) // tile_size
     tz = (depth + tile_size - 1) // tile_size
+    with _stage("voxel_pack"):
+        packed = pack_tile_records(records, offsets, flatten_ids, radii, tile_cum, m, shape, tile_size)
     with _stage("voxel_render"):
-        _backend.call("r2s_voxel_render", _dtype(means), _ptr(records), int(beta is not None), _ptr(offsets),
-                      _ptr(flatten_ids), means.shape[0], m, width, height, depth, tile_size, tx, ty, tz,
-                      _ptr(volume), _ptr(variance), _stream(device))
+        _backend.call("r2s_voxel_render_packed", _dtype(means), _ptr(packed), int(beta is not None), _ptr(offsets),
+                      m, None, width, height, depth, tile_size, tx, ty, tz, _ptr(volume), _ptr(variance),
+                      _stream(device))
     state = VoxelState(covars, records, offsets, isect_ids, flatten_ids, m, tuple(shape), tile_size, means_v, radii,
-                       tile_cum)
+                       tile_cum, packed=packed)
     return (volume if uncertainty is None else (volume, variance)), state
 
 
@@ -420,7 +439,7 @@ def voxel_backward(state: VoxelState, means, quats, scales, beta, uncertainty, e
     # The list-free form when no lists were kept, or when per-intersection slots would take more memory
     # than the budget (it needs one slot per primitive and tile-box z-layer instead).
     slot_bytes = state.n_isects * 12 * means.element_size()
-    list_free = state.offsets is None or slot_bytes > VOXEL_SLOT_BUDGET_BYTES
+    list_free = state.offsets is None or state.packed is None or slot_bytes > VOXEL_SLOT_BUDGET_BYTES
     if list_free and state.layer_cum is None:
         state.layer_cum = _layer_scan(state.means_v, state.radii, state.shape, state.tile_size)
         state.n_items = int(state.layer_cum[-1].item()) if n else 0
@@ -428,11 +447,10 @@ def voxel_backward(state: VoxelState, means, quats, scales, beta, uncertainty, e
         if not list_free:
             # Tile-parallel over the forward's sorted lists, one slot per (tile, primitive) pair.
             slots = means.new_empty((max(state.n_isects, 1), 12))
-            _backend.call("r2s_voxel_render_bwd_slots", _dtype(means), _ptr(state.records), int(beta is not None),
-                          int(bool(detach_variance)), _ptr(state.offsets), _ptr(state.flatten_ids), state.n_isects,
-                          None, _ptr(state.means_v), _ptr(state.radii), _ptr(state.tile_cum), _ptr(v_volume),
-                          _ptr(v_variance), n, width, height, depth, tile, tx, ty, tz, _ptr(slots), slots.shape[0],
-                          _ptr(grads), stream)
+            _backend.call("r2s_voxel_render_bwd_packed", _dtype(means), _ptr(state.packed), int(beta is not None),
+                          int(bool(detach_variance)), _ptr(state.offsets), state.n_isects, None,
+                          _ptr(state.tile_cum), _ptr(v_volume), _ptr(v_variance), n, width, height, depth, tile, tx,
+                          ty, tz, _ptr(slots), slots.shape[0], _ptr(grads), stream)
         else:
             # No lists kept: record-parallel over the primitives' tile-box layers.
             partials = means.new_empty((max(state.n_items, 1), 16))

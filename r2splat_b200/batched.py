@@ -187,6 +187,9 @@ class FitScene:
         self.emit_ws = _ws(lib.r2s_isect_emit_workspace(self.capacity_2d, self.c * self.tx * self.ty), dev)
         self.isect3_ids = torch.empty((self.capacity_3d,), dtype=torch.int64, device=dev)
         self.flatten3_ids = torch.empty((self.capacity_3d,), dtype=torch.int32, device=dev)
+        # Per-tile packed 3D records (list order, VJP slot in the padding) for the bulk-staged tile kernels.
+        self.packed3 = torch.empty((self.capacity_3d, 16), dtype=self.means.dtype, device=dev)
+        self.pack3_ws = _ws(lib.r2s_voxel_pack_workspace(self.n), dev)
         self.emit3_ws = _ws(lib.r2s_isect_emit_workspace(self.capacity_3d, self.vtx * self.vty * self.vtz), dev)
 
     def measure_counts(self) -> tuple[int, int]:
@@ -292,19 +295,22 @@ class FitScene:
                           self.cfg.voxel_tile, self.vtx, self.vty, self.vtz, _p(self.cum3), self.capacity_3d,
                           _p(self.n_used3), _p(self.overflow), _p(self.isect3_ids), _p(self.flatten3_ids),
                           _p(self.offsets3), _p(self.emit3_ws), self.emit3_ws.numel(), s)
-            _backend.call("r2s_voxel_render_capacity", d, _p(self.records3), beta_flag, _p(self.offsets3),
-                          _p(self.flatten3_ids), _p(self.n_used3), self.n, self.vwidth, self.vheight, self.depth,
-                          self.cfg.voxel_tile, self.vtx, self.vty, self.vtz, _p(self.volume), None, s)
+            _backend.call("r2s_voxel_pack_tile_records", d, _p(self.records3), _p(self.offsets3),
+                          _p(self.flatten3_ids), _p(self.radii3), _p(self.cum3), self.n, self.capacity_3d,
+                          _p(self.n_used3), self.cfg.voxel_tile, self.vtx, self.vty, self.vtz, self.capacity_3d,
+                          _p(self.packed3), _p(self.pack3_ws), self.pack3_ws.numel(), s)
+            _backend.call("r2s_voxel_render_packed", d, _p(self.packed3), beta_flag, _p(self.offsets3), 0,
+                          _p(self.n_used3), self.vwidth, self.vheight, self.depth, self.cfg.voxel_tile, self.vtx,
+                          self.vty, self.vtz, _p(self.volume), None, s)
             # TV forward and backward in one pass (the TV term enters the loss with weight one).
             _backend.call("r2s_volume_loss_fwd_bwd", d, _p(self.volume), _p(self.ones), 1, self.depth, self.vheight,
                           self.vwidth, float(self.cfg.lambda_tv), _p(self.tv_loss), _p(self.tv_value), None,
                           _p(self.g_volume), _p(self.tv_ws), self.tv_ws.numel(), s)
             # Deterministic tile VJP: one slot per 3D intersection, summed per primitive in a fixed order.
-            _backend.call("r2s_voxel_render_bwd_slots", d, _p(self.records3), beta_flag, 1, _p(self.offsets3),
-                          _p(self.flatten3_ids), 0, _p(self.n_used3), _p(self.means_v), _p(self.radii3),
-                          _p(self.cum3), _p(self.g_volume), None, self.n, self.vwidth, self.vheight, self.depth,
-                          self.cfg.voxel_tile, self.vtx, self.vty, self.vtz, _p(self.slots3), self.capacity_3d,
-                          _p(self.grads3d), s)
+            _backend.call("r2s_voxel_render_bwd_packed", d, _p(self.packed3), beta_flag, 1, _p(self.offsets3), 0,
+                          _p(self.n_used3), _p(self.cum3), _p(self.g_volume), None, self.n, self.vwidth,
+                          self.vheight, self.depth, self.cfg.voxel_tile, self.vtx, self.vty, self.vtz,
+                          _p(self.slots3), self.capacity_3d, _p(self.grads3d), s)
             v = self.g_voxel
             _backend.call("r2s_voxel_chain_bwd", d, _p(self.means), _p(self.quats), _p(self.scales), _p(self.covars),
                           _p(self.extent), _p(self.center), self.n, self.vwidth, self.vheight, self.depth,

@@ -60,14 +60,31 @@ def _fingerprint() -> str:
     return digest.hexdigest()
 
 
+def _object_fingerprint(source: Path, extra: list[str]) -> str:
+    """Flags, the translation unit and every header it may include (all of csrc/*.cuh and include/*.h)."""
+    digest = hashlib.sha256()
+    digest.update(" ".join(NVCC_FLAGS + extra).encode())
+    digest.update(source.read_bytes())
+    for path in sorted(list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h"))):
+        digest.update(path.name.encode())
+        digest.update(path.read_bytes())
+    return digest.hexdigest()
+
+
 def _compile(source: Path, extra: list[str]) -> Path:
+    """Compiles one translation unit unless its object is up to date with its fingerprint."""
     obj = OBJ_DIR / (source.stem + ".o")
+    stamp = OBJ_DIR / (source.stem + ".o.stamp")
+    fingerprint = _object_fingerprint(source, extra)
+    if obj.exists() and stamp.exists() and stamp.read_text() == fingerprint:
+        return obj
     cmd = [nvcc(), *NVCC_FLAGS, *extra, f"-I{INCLUDE}", "-c", str(source), "-o", str(obj)]
     proc = subprocess.run(cmd, capture_output=True, text=True)
     if proc.returncode != 0:
         raise RuntimeError(f"nvcc failed for {source.name}:\n{proc.stdout}\n{proc.stderr}")
     if proc.stderr.strip():
         sys.stderr.write(proc.stderr)
+    stamp.write_text(fingerprint)
     return obj
 
 
@@ -83,6 +100,9 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False, e
         return lib
     sources = _sources()
     workers = jobs or min(len(sources), os.cpu_count() or 4)
+    if force:
+        for source in sources:
+            (OBJ_DIR / (source.stem + ".o.stamp")).unlink(missing_ok=True)
     with concurrent.futures.ThreadPoolExecutor(max_workers=workers) as pool:
         objects = list(pool.map(lambda s: _compile(s, extra), sources))
     tmp = lib.with_suffix(".so.tmp")

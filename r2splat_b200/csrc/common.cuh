@@ -121,6 +121,53 @@ __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;\n" :: "n"(N) : "memory");
 }
 
+// Bulk global->shared copies completed on a shared-memory mbarrier (the
+// non-tensor form of TMA, sm_90+): one thread arms the barrier with the byte
+// count and issues one copy of a contiguous range; every thread then waits on
+// the barrier's phase. Source and destination must be 16-byte aligned and the
+// size a multiple of 16. Only this GPU's own memory is read, never with
+// cluster multicast.
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" :: "r"(smem_u32(bar)), "r"(count) : "memory");
+}
+// Makes the initialised barriers visible to the bulk-copy unit.
+__device__ __forceinline__ void mbar_init_fence() {
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n"
+                 :: "r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// Orders this thread's earlier shared-memory accesses (and, after a block
+// barrier, the block's) before later bulk copies into shared memory.
+__device__ __forceinline__ void fence_proxy_async_shared() {
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+__device__ __forceinline__ void bulk_load_g2s(void* smem_dst, const void* gmem_src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
+                 :: "r"(smem_u32(smem_dst)), "l"(gmem_src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                 " selp.u32 %0, 1, 0, p;\n}\n"
+                 : "=r"(done) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+    return done != 0u;
+}
+// A staging copy of a few KB completes in microseconds; a wait that has not
+// seen its phase complete after this long gives up.
+constexpr uint64_t kBulkWaitLimitNs = 200ull * 1000ull * 1000ull;
+// Waits for the barrier's phase with the given parity; false when it did not
+// complete within kBulkWaitLimitNs.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_timer_ns();
+    while (!mbar_try_wait(bar, parity)) {
+        if (global_timer_ns() - t0 > kBulkWaitLimitNs) return false;
+    }
+    return true;
+}
+
 // Vector reductions into global memory (sm_90+ red.global.add.v4.f32).
 __device__ __forceinline__ void red_add_v4(float* addr, float a, float b, float c, float d) {
     asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};\n"
@@ -211,10 +258,11 @@ __device__ __forceinline__ float gt_mask(float a, float b) {
 }
 
 // Raises a kernel's dynamic shared-memory limit when a launch needs more than
-// the default 48 KB.
+// the default 48 KB in all (its dynamic bytes plus `static_bytes` of static
+// shared memory).
 template <typename Kernel>
-inline int allow_dynamic_smem(Kernel kernel, size_t bytes) {
-    if (bytes <= 48 * 1024) return R2S_OK;
+inline int allow_dynamic_smem(Kernel kernel, size_t bytes, size_t static_bytes = 0) {
+    if (bytes + static_bytes <= 48 * 1024) return R2S_OK;
     const cudaError_t err =
         cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
     if (err != cudaSuccess)

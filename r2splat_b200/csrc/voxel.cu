@@ -47,12 +47,22 @@ struct VoxelGeom {
     const int64_t* n_dev = nullptr;  // device-side intersection count, overrides n_isects
 };
 
-template <typename S, bool kBeta, bool kVar, int PPT>
+// Bulk-staging waits that ran out (a tile batch's copy did not complete
+// within kBulkWaitLimitNs): counted per device, read and cleared by
+// r2s_bulk_wait_faults(). A kernel that gives up on a wait waits (bounded)
+// for its copies in flight and leaves the rest of its tile unwritten.
+static __device__ unsigned int g_bulk_wait_faults;
+
+// kBulk: `records` is the per-tile packed copy (packed[i] is the record of
+// sorted intersection i, flatten_ids unused), and each batch is staged by one
+// bulk copy; otherwise records are gathered through flatten_ids by cp.async.
+template <typename S, bool kBeta, bool kVar, int PPT, bool kBulk>
 __global__ void __launch_bounds__(256) voxel_fwd_kernel(const Rec3D<S>* __restrict__ records,
                                                         const int32_t* __restrict__ offsets,
                                                         const int32_t* __restrict__ flatten_ids, VoxelGeom g,
                                                         S* __restrict__ volume, S* __restrict__ volume_var) {
     extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ uint64_t s_bar[3];
     const uint32_t nthreads = blockDim.x;
     Rec3D<S>* s_rec = reinterpret_cast<Rec3D<S>*>(smem);  // [3][nthreads]
     const uint32_t T = g.T;
@@ -109,20 +119,52 @@ __global__ void __launch_bounds__(256) voxel_fwd_kernel(const Rec3D<S>* __restri
 
     const int32_t count = end - start;
     const int32_t n_batches = count > 0 ? (count + int32_t(nthreads) - 1) / int32_t(nthreads) : 0;
+    if (kBulk && n_batches > 0) {
+        if (t == 0) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) mbar_init(&s_bar[k], 1u);
+            mbar_init_fence();
+        }
+        __syncthreads();
+    }
     auto load = [&](int32_t b, int stage) {
-        const int32_t idx = start + b * int32_t(nthreads) + int32_t(t);
-        if (idx < end) gather_record3(s_rec + stage * nthreads + t, records + flatten_ids[idx]);
-        cp_async_commit();
+        if (kBulk) {
+            if (t == 0) {
+                const int32_t first = start + b * int32_t(nthreads);
+                const uint32_t bytes = uint32_t(min(int32_t(nthreads), end - first)) * uint32_t(sizeof(Rec3D<S>));
+                fence_proxy_async_shared();
+                mbar_arrive_expect_tx(&s_bar[stage], bytes);
+                bulk_load_g2s(s_rec + stage * nthreads, records + first, bytes, &s_bar[stage]);
+            }
+        } else {
+            const int32_t idx = start + b * int32_t(nthreads) + int32_t(t);
+            if (idx < end) gather_record3(s_rec + stage * nthreads + t, records + flatten_ids[idx]);
+            cp_async_commit();
+        }
     };
     if (n_batches > 0) load(0, 0);
     for (int32_t b = 0; b < n_batches; ++b) {
         if (b + 1 < n_batches) {
             load(b + 1, (b + 1) % 3);
-            cp_async_wait<1>();
-        } else {
+            if (!kBulk) cp_async_wait<1>();
+        } else if (!kBulk) {
             cp_async_wait<0>();
         }
-        __syncthreads();
+        if (kBulk) {
+            // Batch b is the (b / 3)-th use of its stage's barrier.
+            const bool ok = mbar_wait_bounded(&s_bar[b % 3], uint32_t(b / 3) & 1u);
+            if (__syncthreads_or(!ok)) {
+                if (t == 0) {
+                    atomicAdd(&g_bulk_wait_faults, 1u);
+                    mbar_wait_bounded(&s_bar[b % 3], uint32_t(b / 3) & 1u);
+                    if (b + 1 < n_batches) mbar_wait_bounded(&s_bar[(b + 1) % 3], uint32_t((b + 1) / 3) & 1u);
+                }
+                __syncthreads();
+                return;
+            }
+        } else {
+            __syncthreads();
+        }
         const Rec3D<S>* buf = s_rec + (b % 3) * nthreads;
         const int32_t batch = min(int32_t(nthreads), count - b * int32_t(nthreads));
         for (int32_t s = 0; s < batch; ++s) {
@@ -383,12 +425,16 @@ constexpr float kVoxNegLog2e = -1.4426950408889634f;
 template <bool kBeta, bool kVar>
 constexpr int kVoxBwdMinBlocks = (kBeta || kVar) ? 3 : 0;
 
-template <typename S, bool kBeta, bool kVar>
+// kBulk: `records` is the per-tile packed copy whose padding holds each
+// pair's slot (slot output only; flatten_ids unused), staged one bulk copy
+// per batch.
+template <typename S, bool kBeta, bool kVar, bool kBulk>
 __global__ void __launch_bounds__(kVoxBwdThreads, kVoxBwdMinBlocks<kBeta, kVar>) voxel_bwd_kernel(
     const Rec3D<S>* __restrict__ records, bool chain_var, const int32_t* __restrict__ offsets,
     const int32_t* __restrict__ flatten_ids, VoxelGeom g, const S* __restrict__ v_volume,
     const S* __restrict__ v_volume_var, Rec3D<S>* __restrict__ grads, VoxelSlots<S> sl) {
     extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ uint64_t s_bar[2];
     const uint32_t T = g.T;
     const uint32_t tile_voxels = T * T * T;
     // The tile's adjoints are stored by rows of T voxels at a stride of T + 1,
@@ -435,7 +481,25 @@ __global__ void __launch_bounds__(kVoxBwdThreads, kVoxBwdMinBlocks<kBeta, kVar>)
         s_v[p < T * T ? p * RS + T : T * T * RS + (p - T * T)] = S(0);
 
     const int32_t n_batches = (count + kVoxBwdThreads - 1) / kVoxBwdThreads;
+    if (kBulk) {
+        if (t == 0) {
+            mbar_init(&s_bar[0], 1u);
+            mbar_init(&s_bar[1], 1u);
+            mbar_init_fence();
+        }
+        __syncthreads();
+    }
     auto load = [&](int32_t b, uint32_t stage) {
+        if constexpr (kBulk) {
+            if (t == 0) {
+                const int32_t first = start + b * kVoxBwdThreads;
+                const uint32_t bytes = uint32_t(min(kVoxBwdThreads, end - first)) * uint32_t(sizeof(Rec3D<S>));
+                fence_proxy_async_shared();
+                mbar_arrive_expect_tx(&s_bar[stage], bytes);
+                bulk_load_g2s(s_rec + stage * kVoxBwdThreads, records + first, bytes, &s_bar[stage]);
+            }
+            return;
+        }
         const int32_t idx = start + b * kVoxBwdThreads + int32_t(t);
         if (idx < end) {
             const int32_t gid = flatten_ids[idx];
@@ -467,16 +531,34 @@ __global__ void __launch_bounds__(kVoxBwdThreads, kVoxBwdMinBlocks<kBeta, kVar>)
     for (int32_t b = 0; b < n_batches; ++b) {
         if (b + 1 < n_batches) {
             load(b + 1, uint32_t(b + 1) & 1u);
-            cp_async_wait<1>();
-        } else {
+            if (!kBulk) cp_async_wait<1>();
+        } else if (!kBulk) {
             cp_async_wait<0>();
         }
-        __syncthreads();
+        if (kBulk) {
+            // Batch b is the (b / 2)-th use of its stage's barrier.
+            const bool ok = mbar_wait_bounded(&s_bar[b & 1], uint32_t(b >> 1) & 1u);
+            if (__syncthreads_or(!ok)) {
+                if (t == 0) {
+                    atomicAdd(&g_bulk_wait_faults, 1u);
+                    mbar_wait_bounded(&s_bar[b & 1], uint32_t(b >> 1) & 1u);
+                    if (b + 1 < n_batches) mbar_wait_bounded(&s_bar[(b + 1) & 1], uint32_t((b + 1) >> 1) & 1u);
+                }
+                __syncthreads();
+                return;
+            }
+        } else {
+            __syncthreads();
+        }
         const uint32_t stage = uint32_t(b) & 1u;
         const int32_t batch = min(int32_t(kVoxBwdThreads), count - b * kVoxBwdThreads);
         if (int32_t(t) < batch) {
             s_box[t] = voxel_box<S, kBeta>(s_rec[stage * kVoxBwdThreads + t], ox, oy, oz, vx, vy, vz);
-            if (sl.slots != nullptr) {
+            if (kBulk) {
+                // The pack kernel put the pair's slot (or 0xffffffff) in the padding.
+                s_slot[stage * kVoxBwdThreads + t] =
+                    *reinterpret_cast<const uint32_t*>(&s_rec[stage * kVoxBwdThreads + t].pad0);
+            } else if (sl.slots != nullptr) {
                 // The pair's slot: the primitive's first slot plus this tile's index in its tile box
                 // (slots fit 31 bits).
                 const Rec3D<S>& rec = s_rec[stage * kVoxBwdThreads + t];
@@ -500,7 +582,7 @@ __global__ void __launch_bounds__(kVoxBwdThreads, kVoxBwdMinBlocks<kBeta, kVar>)
             const VoxelBox box = s_box[s];
             const uint32_t w = box.extent & 0xffu, h = (box.extent >> 8) & 0xffu, d = (box.extent >> 16) & 0xffu;
             const uint32_t rows = h * d;
-            const int32_t gid = s_id[stage * kVoxBwdThreads + s];
+            const int32_t gid = kBulk ? 0 : s_id[stage * kVoxBwdThreads + s];
             // This pair's slot (deterministic output), written by the leaders of lane groups 0..2.
             const uint32_t slot = sl.slots != nullptr ? s_slot[stage * kVoxBwdThreads + s] : 0xffffffffu;
             if (rows * w == 0u) {
@@ -691,7 +773,7 @@ __global__ void __launch_bounds__(kVoxBwdThreads, kVoxBwdMinBlocks<kBeta, kVar>)
                     e2 = w4[2];
                     e3 = w4[3];
                 }
-                if (sl.slots == nullptr) {
+                if (!kBulk && sl.slots == nullptr) {
                     red_add_v4(reinterpret_cast<S*>(grads + gid) + 4 * grp, e0, e1, e2, e3);
                 } else if (slot != 0xffffffffu && grp < 3u) {
                     S* out = sl.slots + size_t(slot) * 12u + 4u * grp;
@@ -1079,6 +1161,82 @@ __global__ void voxel_record_reduce_kernel(const Rec3D<S>* __restrict__ partials
     for (int i = 12; i < 16; ++i) out[i] = S(0);
 }
 
+// Per-tile packed copy of the 3D records for the explicit and batched
+// pipelines: packed[i] = records[flatten_ids[i]] for each sorted intersection
+// i, so the records of a tile's list are one contiguous range, staged by one
+// bulk copy per batch in the tile forward and VJP. The padding carries the
+// pair's VJP slot (the primitive's first slot cum[n - 1] plus the tile's index
+// in the primitive's tile box, z then y then x), or 0xffffffff past
+// slot_capacity.
+//
+// The slot is an affine function of the tile coordinates per primitive:
+// slot = base + tz * nxny + ty * nx + tx with base = cum[n - 1] - (lo_z * nxny +
+// lo_y * nx + lo_x) for the box [lo, hi), nx and ny its extents. A first pass
+// tabulates (base, nx, nxny) per primitive into caller workspace.
+struct alignas(16) SlotAffine {
+    int64_t base;
+    uint32_t nx, nxny;
+};
+
+template <typename S>
+__global__ void voxel_slot_affine_kernel(const Rec3D<S>* __restrict__ records, const int32_t* __restrict__ radii,
+                                         const int64_t* __restrict__ cum, uint32_t N, uint32_t T, uint32_t tiles_x,
+                                         uint32_t tiles_y, uint32_t tiles_z, SlotAffine* __restrict__ table) {
+    const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    const S centre[3] = {records[n].x, records[n].y, records[n].z};
+    SlotAffine e{0, 0u, 0u};
+    uint32_t lo[3], hi[3];
+    if (tile_box_3d(centre, radii + 3 * size_t(n), T, tiles_x, tiles_y, tiles_z, lo, hi)) {
+        e.nx = hi[0] - lo[0];
+        e.nxny = e.nx * (hi[1] - lo[1]);
+        e.base = (n > 0u ? cum[n - 1] : int64_t(0)) -
+                 (int64_t(lo[2]) * e.nxny + int64_t(lo[1]) * e.nx + int64_t(lo[0]));
+    }
+    table[n] = e;
+}
+
+// One warp per tile; four lanes move one record, each a quarter of it (16 B
+// fp32, 32 B fp64), so a warp reads and writes eight whole records per
+// instruction. With n_used set (capacity-bounded steps) the lists hold
+// min(*n_used, n_isects) entries.
+template <typename S>
+__global__ void __launch_bounds__(256) pack_tile_records3_kernel(
+    const Rec3D<S>* __restrict__ records, const int32_t* __restrict__ offsets,
+    const int32_t* __restrict__ flatten_ids, const SlotAffine* __restrict__ table, uint32_t tiles_x,
+    uint32_t tiles_y, uint32_t tiles_z, uint64_t n_isects, const int64_t* __restrict__ n_used,
+    uint64_t slot_capacity, Rec3D<S>* __restrict__ packed) {
+    using Quarter = typename std::conditional<sizeof(S) == 4, float4, double4>::type;
+    static_assert(sizeof(Rec3D<S>) == 4 * sizeof(Quarter), "a record is four quarters");
+    const uint64_t n_tiles = uint64_t(tiles_x) * tiles_y * tiles_z;
+    const uint64_t key = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    if (key >= n_tiles) return;  // warp-uniform
+    const int64_t n = n_used != nullptr ? min(max(*n_used, int64_t(0)), int64_t(n_isects)) : int64_t(n_isects);
+    const int64_t start = offsets[key];
+    const int64_t end = key + 1 == n_tiles ? n : int64_t(offsets[key + 1]);
+    const uint32_t plane = tiles_x * tiles_y;
+    const uint32_t tz = uint32_t(key) / plane;
+    const uint32_t rem = uint32_t(key) - tz * plane;
+    const uint32_t ty = rem / tiles_x, tx = rem - ty * tiles_x;
+    const uint32_t lane = threadIdx.x & 31u, part = lane & 3u;
+    for (int64_t i = start + (lane >> 2); i < end; i += 8) {
+        const int32_t gid = flatten_ids[i];
+        Quarter v = reinterpret_cast<const Quarter*>(records + gid)[part];
+        if (part == 3u) {
+            const SlotAffine e = table[gid];
+            const int64_t j = e.base + int64_t(tz) * e.nxny + int64_t(ty) * e.nx + int64_t(tx);
+            const uint32_t slot = (j >= 0 && uint64_t(j) < slot_capacity) ? uint32_t(j) : 0xffffffffu;
+            // pad0 is the first value of the last quarter.
+            if constexpr (sizeof(S) == 4) {
+                v.x = __uint_as_float(slot);
+            } else {
+                v.x = __longlong_as_double(static_cast<long long>(slot));
+            }
+        }
+        reinterpret_cast<Quarter*>(packed + i)[part] = v;
+    }
+}
+
 template <typename S>
 __global__ void pack_records3_kernel(const S* __restrict__ means3d, const S* __restrict__ conics,
                                      const S* __restrict__ opacities, const S* __restrict__ betas,
@@ -1130,84 +1288,102 @@ inline int check_vgeom(const VoxelGeom& g) {
     return R2S_OK;
 }
 
-template <typename S, bool kBeta, bool kVar, int PPT>
+template <typename S, bool kBeta, bool kVar, int PPT, bool kBulk>
 int launch_vfwd_t(const VoxelGeom& g, const Rec3D<S>* rec, const int32_t* offsets, const int32_t* ids, S* vol,
                   S* vol_var, unsigned nthreads, cudaStream_t stream) {
     const size_t smem = 3 * nthreads * sizeof(Rec3D<S>);
-    if (smem > 48 * 1024)
-        cudaFuncSetAttribute(voxel_fwd_kernel<S, kBeta, kVar, PPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(smem));
+    R2S_TRY(allow_dynamic_smem(voxel_fwd_kernel<S, kBeta, kVar, PPT, kBulk>, smem, 3 * sizeof(uint64_t)));
     const unsigned grid = g.tiles_x * g.tiles_y * g.tiles_z;
-    voxel_fwd_kernel<S, kBeta, kVar, PPT><<<grid, nthreads, smem, stream>>>(rec, offsets, ids, g, vol, vol_var);
+    voxel_fwd_kernel<S, kBeta, kVar, PPT, kBulk><<<grid, nthreads, smem, stream>>>(rec, offsets, ids, g, vol,
+                                                                                    vol_var);
     return check_launch("voxelize_to_voxels_fwd");
 }
 
-template <typename S, bool kBeta, bool kVar>
+template <typename S, bool kBeta, bool kVar, bool kBulk>
 int launch_vfwd_p(const VoxelGeom& g, const Rec3D<S>* rec, const int32_t* offsets, const int32_t* ids, S* vol,
                   S* vol_var, cudaStream_t stream) {
     const uint32_t voxels = g.T * g.T * g.T;
     if (voxels <= 128) {
         const unsigned nt = (voxels + 31) / 32 * 32;
-        return launch_vfwd_t<S, kBeta, kVar, 1>(g, rec, offsets, ids, vol, vol_var, nt, stream);
+        return launch_vfwd_t<S, kBeta, kVar, 1, kBulk>(g, rec, offsets, ids, vol, vol_var, nt, stream);
     }
     if (!kBeta && std::is_same<S, float>::value && g.T % 8 == 0) {
         // Whole rows of eight voxels per thread: T^2 rows of T / 8 segments.
         const unsigned nt = (g.T * g.T * (g.T / 8) + 31) / 32 * 32;
-        return launch_vfwd_t<S, kBeta, kVar, 8>(g, rec, offsets, ids, vol, vol_var, nt, stream);
+        return launch_vfwd_t<S, kBeta, kVar, 8, kBulk>(g, rec, offsets, ids, vol, vol_var, nt, stream);
     }
     // Four consecutive voxels of a row per thread: T^2 rows of ceil(T / 4) segments.
     const unsigned nt = (g.T * g.T * ((g.T + 3) / 4) + 31) / 32 * 32;
-    return launch_vfwd_t<S, kBeta, kVar, 4>(g, rec, offsets, ids, vol, vol_var, nt, stream);
+    return launch_vfwd_t<S, kBeta, kVar, 4, kBulk>(g, rec, offsets, ids, vol, vol_var, nt, stream);
 }
 
+// bulk: `rec` is the per-tile packed copy and `ids` is unused.
 template <typename S>
 int launch_vfwd(const VoxelGeom& g, const Rec3D<S>* rec, bool beta, const int32_t* offsets, const int32_t* ids,
-                S* vol, S* vol_var, cudaStream_t stream) {
+                S* vol, S* vol_var, cudaStream_t stream, bool bulk = false) {
     R2S_TRY(check_vgeom(g));
     if (uint64_t(g.tiles_x) * g.tiles_y * g.tiles_z == 0) return R2S_OK;
     const bool var = vol_var != nullptr;
-    if (beta) return var ? launch_vfwd_p<S, true, true>(g, rec, offsets, ids, vol, vol_var, stream)
-                         : launch_vfwd_p<S, true, false>(g, rec, offsets, ids, vol, vol_var, stream);
-    return var ? launch_vfwd_p<S, false, true>(g, rec, offsets, ids, vol, vol_var, stream)
-               : launch_vfwd_p<S, false, false>(g, rec, offsets, ids, vol, vol_var, stream);
+    if (bulk) {
+        if (beta) return var ? launch_vfwd_p<S, true, true, true>(g, rec, offsets, ids, vol, vol_var, stream)
+                             : launch_vfwd_p<S, true, false, true>(g, rec, offsets, ids, vol, vol_var, stream);
+        return var ? launch_vfwd_p<S, false, true, true>(g, rec, offsets, ids, vol, vol_var, stream)
+                   : launch_vfwd_p<S, false, false, true>(g, rec, offsets, ids, vol, vol_var, stream);
+    }
+    if (beta) return var ? launch_vfwd_p<S, true, true, false>(g, rec, offsets, ids, vol, vol_var, stream)
+                         : launch_vfwd_p<S, true, false, false>(g, rec, offsets, ids, vol, vol_var, stream);
+    return var ? launch_vfwd_p<S, false, true, false>(g, rec, offsets, ids, vol, vol_var, stream)
+               : launch_vfwd_p<S, false, false, false>(g, rec, offsets, ids, vol, vol_var, stream);
 }
 
-template <typename S, bool kBeta, bool kVar>
+template <typename S, bool kBeta, bool kVar, bool kBulk>
 int launch_vbwd_p(const VoxelGeom& g, const Rec3D<S>* rec, bool chain_var, const int32_t* offsets,
                   const int32_t* ids, const S* v_vol, const S* v_vol_var, Rec3D<S>* grads, cudaStream_t stream,
                   const VoxelSlots<S>& sl) {
     const size_t tile_slots = size_t(g.T) * g.T * (g.T + 1) + (g.T + 1);
     const size_t smem = 2 * size_t(kVoxBwdThreads) * (sizeof(Rec3D<S>) + 2 * sizeof(int32_t)) +
                         size_t(kVoxBwdThreads) * sizeof(VoxelBox) + 2 * tile_slots * sizeof(S);
-    R2S_TRY(allow_dynamic_smem(voxel_bwd_kernel<S, kBeta, kVar>, smem));
+    R2S_TRY(allow_dynamic_smem(voxel_bwd_kernel<S, kBeta, kVar, kBulk>, smem, 2 * sizeof(uint64_t)));
     const unsigned grid = g.tiles_x * g.tiles_y * g.tiles_z;
-    voxel_bwd_kernel<S, kBeta, kVar><<<grid, kVoxBwdThreads, smem, stream>>>(rec, chain_var, offsets, ids, g, v_vol,
-                                                                           v_vol_var, grads, sl);
+    voxel_bwd_kernel<S, kBeta, kVar, kBulk><<<grid, kVoxBwdThreads, smem, stream>>>(
+        rec, chain_var, offsets, ids, g, v_vol, v_vol_var, grads, sl);
     return check_launch("voxelize_to_voxels_bwd");
 }
 
+template <typename S, bool kBulk>
+int launch_vbwd_b(const VoxelGeom& g, const Rec3D<S>* rec, bool beta, bool chain_var, const int32_t* offsets,
+                  const int32_t* ids, const S* v_vol, const S* v_vol_var, Rec3D<S>* grads, cudaStream_t stream,
+                  const VoxelSlots<S>& sl) {
+    const bool var = v_vol_var != nullptr;
+    if (beta)
+        return var ? launch_vbwd_p<S, true, true, kBulk>(g, rec, chain_var, offsets, ids, v_vol, v_vol_var, grads,
+                                                         stream, sl)
+                   : launch_vbwd_p<S, true, false, kBulk>(g, rec, chain_var, offsets, ids, v_vol, v_vol_var, grads,
+                                                          stream, sl);
+    return var ? launch_vbwd_p<S, false, true, kBulk>(g, rec, chain_var, offsets, ids, v_vol, v_vol_var, grads,
+                                                      stream, sl)
+               : launch_vbwd_p<S, false, false, kBulk>(g, rec, chain_var, offsets, ids, v_vol, v_vol_var, grads,
+                                                       stream, sl);
+}
+
+// bulk: `rec` is the per-tile packed copy with the slots in its padding (slot output only).
 template <typename S>
 int launch_vbwd(const VoxelGeom& g, const Rec3D<S>* rec, bool beta, bool chain_var, const int32_t* offsets,
                 const int32_t* ids, const S* v_vol, const S* v_vol_var, Rec3D<S>* grads, cudaStream_t stream,
-                const VoxelSlots<S>& sl = VoxelSlots<S>{}) {
+                const VoxelSlots<S>& sl = VoxelSlots<S>{}, bool bulk = false) {
     R2S_TRY(check_vgeom(g));
     if (g.n_isects == 0 || uint64_t(g.tiles_x) * g.tiles_y * g.tiles_z == 0) return R2S_OK;
-    const bool var = v_vol_var != nullptr;
-    if (beta)
-        return var ? launch_vbwd_p<S, true, true>(g, rec, chain_var, offsets, ids, v_vol, v_vol_var, grads, stream, sl)
-                   : launch_vbwd_p<S, true, false>(g, rec, chain_var, offsets, ids, v_vol, v_vol_var, grads, stream,
-                                                   sl);
-    return var ? launch_vbwd_p<S, false, true>(g, rec, chain_var, offsets, ids, v_vol, v_vol_var, grads, stream, sl)
-               : launch_vbwd_p<S, false, false>(g, rec, chain_var, offsets, ids, v_vol, v_vol_var, grads, stream, sl);
+    if (bulk) return launch_vbwd_b<S, true>(g, rec, beta, chain_var, offsets, ids, v_vol, v_vol_var, grads, stream, sl);
+    return launch_vbwd_b<S, false>(g, rec, beta, chain_var, offsets, ids, v_vol, v_vol_var, grads, stream, sl);
 }
 
 // Tile VJP into slots, then the in-order per-primitive sum into grads (written, not accumulated).
 template <typename S>
 int launch_vbwd_slots(const VoxelGeom& g, const Rec3D<S>* rec, bool beta, bool chain_var, const int32_t* offsets,
                       const int32_t* ids, const S* v_vol, const S* v_vol_var, const VoxelSlots<S>& sl,
-                      Rec3D<S>* grads, cudaStream_t stream) {
+                      Rec3D<S>* grads, cudaStream_t stream, bool bulk = false) {
     if (g.N == 0) return R2S_OK;
-    R2S_TRY(launch_vbwd<S>(g, rec, beta, chain_var, offsets, ids, v_vol, v_vol_var, grads, stream, sl));
+    R2S_TRY(launch_vbwd<S>(g, rec, beta, chain_var, offsets, ids, v_vol, v_vol_var, grads, stream, sl, bulk));
     voxel_slot_reduce_kernel<S><<<blocks_for(g.N, 256), 256, 0, stream>>>(sl.slots, sl.cum, g.N,
                                                                          int64_t(sl.capacity), grads);
     return check_launch("voxel_slot_reduce");
@@ -1440,6 +1616,96 @@ int r2s_voxel_render_bwd_slots(int dtype, const void* records, int beta, int det
                                     static_cast<const S*>(v_volume_var), sl, static_cast<Rec3D<S>*>(grads),
                                     as_stream(stream));
     });
+}
+
+size_t r2s_voxel_pack_workspace(uint32_t N) { return size_t(N) * sizeof(SlotAffine) + 256; }
+
+int r2s_voxel_pack_tile_records(int dtype, const void* records, const int32_t* tile_offsets,
+                                const int32_t* flatten_ids, const int32_t* radii, const int64_t* tile_cum, uint32_t N,
+                                uint64_t n_isects, const int64_t* n_used, uint32_t tile_size, uint32_t tiles_x,
+                                uint32_t tiles_y, uint32_t tiles_z, uint64_t slot_capacity, void* packed,
+                                void* workspace, size_t workspace_bytes, void* stream) {
+    if (n_isects == 0 || N == 0) return R2S_OK;
+    R2S_REQUIRE(records != nullptr && tile_offsets != nullptr && flatten_ids != nullptr && radii != nullptr &&
+                    tile_cum != nullptr && packed != nullptr,
+                R2S_ERR_ARGUMENT, "records, tile_offsets, flatten_ids, radii, tile_cum and packed must be non-null");
+    R2S_REQUIRE(n_isects < (uint64_t(1) << 31), R2S_ERR_UNSUPPORTED, "too many 3D intersections");
+    R2S_REQUIRE(slot_capacity < (uint64_t(1) << 31), R2S_ERR_UNSUPPORTED, "slot_capacity must be below 2^31");
+    R2S_REQUIRE(tile_size >= 1 && uint64_t(tiles_x) * tiles_y * tiles_z < (uint64_t(1) << 31), R2S_ERR_UNSUPPORTED,
+                "3D tile grid out of range");
+    Arena arena(workspace, workspace_bytes);
+    SlotAffine* table = arena.take<SlotAffine>(N);
+    R2S_REQUIRE(table != nullptr, R2S_ERR_WORKSPACE, "pack workspace too small (r2s_voxel_pack_workspace)");
+    const uint64_t n_tiles = uint64_t(tiles_x) * tiles_y * tiles_z;
+    R2S_DISPATCH(dtype, {
+        voxel_slot_affine_kernel<S><<<blocks_for(N, 256), 256, 0, as_stream(stream)>>>(
+            static_cast<const Rec3D<S>*>(records), radii, tile_cum, N, tile_size, tiles_x, tiles_y, tiles_z, table);
+        R2S_TRY(check_launch("voxel_slot_affine"));
+        pack_tile_records3_kernel<S><<<blocks_for(int64_t(n_tiles) * 32, 256), 256, 0, as_stream(stream)>>>(
+            static_cast<const Rec3D<S>*>(records), tile_offsets, flatten_ids, table, tiles_x, tiles_y, tiles_z,
+            n_isects, n_used, slot_capacity, static_cast<Rec3D<S>*>(packed));
+    });
+    return check_launch("voxel_pack_tile_records");
+}
+
+int r2s_voxel_render_packed(int dtype, const void* packed, int beta, const int32_t* tile_offsets,
+                            uint64_t n_isects, const int64_t* n_used, uint32_t dim2, uint32_t dim1, uint32_t dim0,
+                            uint32_t tile_size, uint32_t tiles_x, uint32_t tiles_y, uint32_t tiles_z, void* volume,
+                            void* volume_var, void* stream) {
+    R2S_REQUIRE(n_isects < (uint64_t(1) << 31), R2S_ERR_UNSUPPORTED, "too many 3D intersections");
+    R2S_REQUIRE(tile_offsets != nullptr && volume != nullptr && (packed != nullptr || n_isects == 0),
+                R2S_ERR_ARGUMENT, "packed, tile_offsets and volume must be non-null");
+    VoxelGeom g{0u, uint32_t(n_isects), dim2, dim1, dim0, tile_size, tiles_x, tiles_y, tiles_z};
+    g.n_dev = n_used;
+    R2S_DISPATCH(dtype, return launch_vfwd<S>(g, static_cast<const Rec3D<S>*>(packed), beta != 0, tile_offsets,
+                                              nullptr, static_cast<S*>(volume), static_cast<S*>(volume_var),
+                                              as_stream(stream), true));
+}
+
+int r2s_voxel_render_bwd_packed(int dtype, const void* packed, int beta, int detach_variance,
+                                const int32_t* tile_offsets, uint64_t n_isects, const int64_t* n_used,
+                                const int64_t* tile_cum, const void* v_volume, const void* v_volume_var, uint32_t N,
+                                uint32_t dim2, uint32_t dim1, uint32_t dim0, uint32_t tile_size, uint32_t tiles_x,
+                                uint32_t tiles_y, uint32_t tiles_z, void* slots, uint64_t slot_capacity, void* grads,
+                                void* stream) {
+    if (N == 0) return R2S_OK;
+    R2S_REQUIRE(tile_offsets != nullptr && tile_cum != nullptr && slots != nullptr && grads != nullptr &&
+                    (packed != nullptr || n_isects == 0),
+                R2S_ERR_ARGUMENT, "packed, tile_offsets, tile_cum, slots and grads must be non-null");
+    R2S_REQUIRE(n_used != nullptr || n_isects <= slot_capacity, R2S_ERR_ARGUMENT,
+                "slot_capacity must hold n_isects slots");
+    R2S_REQUIRE(n_isects < (uint64_t(1) << 31), R2S_ERR_UNSUPPORTED, "too many 3D intersections");
+    R2S_REQUIRE(slot_capacity < (uint64_t(1) << 31), R2S_ERR_UNSUPPORTED, "slot_capacity must be below 2^31");
+    VoxelGeom g{N, uint32_t(n_used != nullptr ? 1u : n_isects), dim2, dim1, dim0, tile_size, tiles_x, tiles_y,
+                tiles_z};
+    g.n_dev = n_used;
+    R2S_DISPATCH(dtype, {
+        VoxelSlots<S> sl;
+        sl.cum = tile_cum;
+        sl.slots = static_cast<S*>(slots);
+        sl.capacity = slot_capacity;
+        return launch_vbwd_slots<S>(g, static_cast<const Rec3D<S>*>(packed), beta != 0, detach_variance == 0,
+                                    tile_offsets, nullptr, static_cast<const S*>(v_volume),
+                                    static_cast<const S*>(v_volume_var), sl, static_cast<Rec3D<S>*>(grads),
+                                    as_stream(stream), true);
+    });
+}
+
+int r2s_bulk_wait_faults(int device, int clear, uint32_t* count) {
+    R2S_REQUIRE(count != nullptr, R2S_ERR_ARGUMENT, "count must be non-null");
+    int previous = 0;
+    cudaError_t err = cudaGetDevice(&previous);
+    if (err == cudaSuccess && previous != device) err = cudaSetDevice(device);
+    unsigned int value = 0u;
+    if (err == cudaSuccess) err = cudaMemcpyFromSymbol(&value, g_bulk_wait_faults, sizeof(value));
+    if (err == cudaSuccess && clear != 0) {
+        const unsigned int zero = 0u;
+        err = cudaMemcpyToSymbol(g_bulk_wait_faults, &zero, sizeof(zero));
+    }
+    if (previous != device) cudaSetDevice(previous);
+    if (err != cudaSuccess) return fail(R2S_ERR_CUDA, std::string("bulk wait fault counter: ") + cudaGetErrorString(err));
+    *count = value;
+    return R2S_OK;
 }
 
 int r2s_voxel_layer_counts(int dtype, const void* means_v, const int32_t* radii, uint32_t N, uint32_t dim2,

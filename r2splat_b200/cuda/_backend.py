@@ -99,6 +99,18 @@ SIGNATURES: dict[str, tuple] = {
     # N, dim2, dim1, dim0, tile, tiles_x, tiles_y, tiles_z, slots, slot_capacity, grads, stream
     "r2s_voxel_render_bwd_slots": (I32, [I32, P, I32, I32, P, P, U64, P, P, P, P, P, P, U32, U32, U32, U32, U32, U32,
                                          U32, U32, P, U64, P, P]),
+    "r2s_voxel_pack_workspace": (SZ, [U32]),
+    # dtype, records, offsets, flatten_ids, radii, tile_cum, N, n_isects, n_used, tile, tiles_x, tiles_y, tiles_z,
+    # slot_capacity, packed, workspace, bytes, stream
+    "r2s_voxel_pack_tile_records": (I32, [I32, P, P, P, P, P, U32, U64, P, U32, U32, U32, U32, U64, P, P, SZ, P]),
+    # dtype, packed, beta, offsets, n_isects, n_used, dim2, dim1, dim0, tile, tiles_x, tiles_y, tiles_z, volume,
+    # volume_var, stream
+    "r2s_voxel_render_packed": (I32, [I32, P, I32, P, U64, P, U32, U32, U32, U32, U32, U32, U32, P, P, P]),
+    # dtype, packed, beta, detach, offsets, n_isects, n_used, tile_cum, v_volume, v_volume_var, N, dim2, dim1, dim0,
+    # tile, tiles_x, tiles_y, tiles_z, slots, slot_capacity, grads, stream
+    "r2s_voxel_render_bwd_packed": (I32, [I32, P, I32, I32, P, U64, P, P, P, P, U32, U32, U32, U32, U32, U32, U32,
+                                          U32, P, U64, P, P]),
+    "r2s_bulk_wait_faults": (I32, [I32, I32, P]),
     "r2s_voxel_layer_counts": (I32, [I32, P, P, U32, U32, U32, U32, U32, U32, U32, U32, P, P]),
     # dtype, records, means_v, radii, layer_cum, n_items, n_items_dev, beta, detach, v_volume, v_volume_var, N,
     # dim2, dim1, dim0, tile, tiles_x, tiles_y, tiles_z, partials, grads, overflow, stream
