@@ -56,8 +56,11 @@ static __device__ unsigned int g_bulk_wait_faults;
 // kBulk: `records` is the per-tile packed copy (packed[i] is the record of
 // sorted intersection i, flatten_ids unused), and each batch is staged by one
 // bulk copy; otherwise records are gathered through flatten_ids by cp.async.
+// The two-row form (PPT = 16) runs only at T = 8 (3D tiles are at most 10
+// wide), one warp per tile; bounding it to 80 registers keeps its accumulators
+// out of local memory.
 template <typename S, bool kBeta, bool kVar, int PPT, bool kBulk>
-__global__ void __launch_bounds__(256) voxel_fwd_kernel(const Rec3D<S>* __restrict__ records,
+__global__ void __launch_bounds__(PPT == 16 ? 32 : 256, PPT == 16 ? 24 : 1) voxel_fwd_kernel(const Rec3D<S>* __restrict__ records,
                                                         const int32_t* __restrict__ offsets,
                                                         const int32_t* __restrict__ flatten_ids, VoxelGeom g,
                                                         S* __restrict__ volume, S* __restrict__ volume_var) {
@@ -78,24 +81,29 @@ __global__ void __launch_bounds__(256) voxel_fwd_kernel(const Rec3D<S>* __restri
     // PPT = 4 or 8: a thread owns PPT consecutive voxels of one row (same y,
     // z), so the Gaussian terms in d2 and d3 alone are computed once per
     // record and the record's shared-memory reads are spread over PPT samples.
+    // PPT = 16: eight consecutive voxels of each of two adjacent rows (y and
+    // y + 1 of one z-plane; T even), which also share the terms in d1 alone.
     // PPT = 1: voxels placed by tile_voxel.
     constexpr bool kRows = PPT >= 4;
     constexpr bool kRowShared = kRows && !kBeta && std::is_same<S, float>::value;
+    constexpr int kRowsPer = PPT == 16 ? 2 : 1;   // rows per thread
+    constexpr int kRowLen = PPT / kRowsPer;      // voxels per row segment
 
     S px[PPT], py[PPT], pz[PPT], acc[PPT], accv[PPT];
     bool inside[PPT];
-    const uint32_t segs = (T + uint32_t(PPT) - 1u) / uint32_t(PPT);
-    const uint32_t row = kRows ? t / segs : 0u;
-    const uint32_t seg = kRows ? t - row * segs : 0u;
+    const uint32_t segs = (T + uint32_t(kRowLen) - 1u) / uint32_t(kRowLen);
+    const uint32_t row = kRows ? (t / segs) * uint32_t(kRowsPer) : 0u;  // the thread's first row
+    const uint32_t seg = kRows ? t - (t / segs) * segs : 0u;
     // Global voxel coordinates (i = z, j = y, kk = x) of the thread's k-th voxel.
     auto voxel_of = [&](int k, uint32_t& i, uint32_t& j, uint32_t& kk) {
         uint32_t lz, ly, lx;
         bool in_tile;
         if (kRows) {
-            lz = row / T;
-            ly = row - lz * T;
-            lx = uint32_t(PPT) * seg + uint32_t(k);
-            in_tile = row < T * T && lx < T;
+            const uint32_t r = row + uint32_t(k / kRowLen);
+            lz = r / T;
+            ly = r - lz * T;
+            lx = uint32_t(kRowLen) * seg + uint32_t(k % kRowLen);
+            in_tile = r < T * T && lx < T;
         } else {
             const uint32_t p = t + uint32_t(k) * nthreads;
             tile_voxel(p, T, lz, ly, lx);
@@ -169,7 +177,43 @@ __global__ void __launch_bounds__(256) voxel_fwd_kernel(const Rec3D<S>* __restri
         const int32_t batch = min(int32_t(nthreads), count - b * int32_t(nthreads));
         for (int32_t s = 0; s < batch; ++s) {
             const Rec3D<S> r = buf[s];
-            if constexpr (kRowShared) {
+            if constexpr (kRowShared && PPT == 16) {
+                // As below, for two rows (d2 = da, db) of one z-plane: the
+                // factors in d1 alone (d1, c00 d1, c01 d1, c02 d1) are shared
+                // by the rows; each sample's expression and rounding are the
+                // single-row form's.
+                const float da = py[0] - r.y, db = py[kRowLen] - r.y, d3 = pz[0] - r.z;
+                const float b2a = __fmul_rn(__fmul_rn(r.c11, da), da);
+                const float b2b = __fmul_rn(__fmul_rn(r.c11, db), db);
+                const float c22d3 = __fmul_rn(r.c22, d3);
+                const float c12da = __fmul_rn(r.c12, da), c12db = __fmul_rn(r.c12, db);
+                const float2 nx = splat2(-r.x), c00 = splat2(r.c00), c01 = splat2(r.c01), c02 = splat2(r.c02);
+                const float2 b22a = splat2(b2a), b22b = splat2(b2b), c22d32 = splat2(c22d3);
+                const float2 c12a2 = splat2(c12da), c12b2 = splat2(c12db);
+                const float2 da2 = splat2(da), db2 = splat2(db), d32 = splat2(d3), half = splat2(0.5f);
+                auto add_sample = [&](int k, float sigma) {
+                    const float alpha = r.o * exp(-sigma);
+                    if (!(sigma < 0.f || fabs(alpha) < 1e-6f)) {
+                        acc[k] += alpha;
+                        if (kVar) accv[k] = fmaf(__fmul_rn(r.q, alpha), alpha, accv[k]);
+                    }
+                };
+#pragma unroll
+                for (int k = 0; k < kRowLen; k += 2) {
+                    const float2 d1 = add2(make_float2(px[k], px[k + 1]), nx);
+                    const float2 c00d1 = mul2(c00, d1), c01d1 = mul2(c01, d1), c02d1 = mul2(c02, d1);
+                    const float2 s3a = fma2(c22d32, d32, fma2(c00d1, d1, b22a));
+                    const float2 s3b = fma2(c22d32, d32, fma2(c00d1, d1, b22b));
+                    const float2 laa = fma2(c01d1, da2, mul2(half, s3a));
+                    const float2 lab = fma2(c01d1, db2, mul2(half, s3b));
+                    const float2 sa = fma2(c12a2, d32, fma2(c02d1, d32, laa));
+                    const float2 sb = fma2(c12b2, d32, fma2(c02d1, d32, lab));
+                    add_sample(k, sa.x);
+                    add_sample(k + 1, sa.y);
+                    add_sample(kRowLen + k, sb.x);
+                    add_sample(kRowLen + k + 1, sb.y);
+                }
+            } else if constexpr (kRowShared) {
                 // The reference's sigma with its contraction made explicit, as
                 // nvcc -O3 --use_fast_math compiles the reference's kernel
                 // (VoxelizeToVoxelsFwd.cu:200-205): S3 = fma(c22 d3, d3,
@@ -1307,10 +1351,10 @@ int launch_vfwd_p(const VoxelGeom& g, const Rec3D<S>* rec, const int32_t* offset
         const unsigned nt = (voxels + 31) / 32 * 32;
         return launch_vfwd_t<S, kBeta, kVar, 1, kBulk>(g, rec, offsets, ids, vol, vol_var, nt, stream);
     }
-    if (!kBeta && std::is_same<S, float>::value && g.T % 8 == 0) {
-        // Whole rows of eight voxels per thread: T^2 rows of T / 8 segments.
-        const unsigned nt = (g.T * g.T * (g.T / 8) + 31) / 32 * 32;
-        return launch_vfwd_t<S, kBeta, kVar, 8, kBulk>(g, rec, offsets, ids, vol, vol_var, nt, stream);
+    if (!kBeta && std::is_same<S, float>::value && g.T == 8) {
+        // Eight voxels of each of two adjacent rows per thread: 32 row pairs, one warp.
+        const unsigned nt = 32;
+        return launch_vfwd_t<S, kBeta, kVar, 16, kBulk>(g, rec, offsets, ids, vol, vol_var, nt, stream);
     }
     // Four consecutive voxels of a row per thread: T^2 rows of ceil(T / 4) segments.
     const unsigned nt = (g.T * g.T * ((g.T + 3) / 4) + 31) / 32 * 32;
