@@ -301,8 +301,13 @@ __global__ void __launch_bounds__(kChainThreads) raster_chain_bwd_kernel(
     S& acc_o = acc[9];
     S& acc_beta = acc[10];
     S& acc_mu_mu = acc[11];
-    for (uint32_t c = active ? part : C; c < C; c += kChainGroup) {
-        const Rec2D<S> g = grads[size_t(c) * N + n];
+    // The next camera's adjoint record is loaded before this one's arithmetic.
+    uint32_t c = active ? part : C;
+    Rec2D<S> g_next{};
+    if (c < C) g_next = grads[size_t(c) * N + n];
+    for (; c < C; c += kChainGroup) {
+        const Rec2D<S> g = g_next;
+        if (c + kChainGroup < C) g_next = grads[size_t(c + kChainGroup) * N + n];
         acc_o += g.o;
         if (g.x == S(0) && g.y == S(0) && g.a == S(0) && g.b == S(0) && g.c == S(0) && g.mu == S(0) &&
             g.beta == S(0)) continue;
