@@ -81,8 +81,8 @@ CONTRACTED_OPS = {"raster_render": 11, "raster_render_bwd": 30, "voxel_render": 
 ACCUMULATE_KERNELS = {
     "raster_render": "raster_fwd_pair_kernel (tile forward, two pixels per lane)",
     "raster_render_bwd": "raster_record_bwd_kernel (record-parallel raster VJP)",
-    "voxel_render": "voxel_fwd_kernel (tile forward, a row of eight voxels per thread)",
-    "voxel_render_bwd": "voxel_bwd_kernel (row-wise voxel VJP)",
+    "voxel_render": "voxel_fwd_kernel (tile forward, two rows of eight voxels per thread, bulk-staged packed records)",
+    "voxel_render_bwd": "voxel_bwd_kernel (row-wise voxel VJP, bulk-staged packed records)",
 }
 # FP32 operations per sample of the Beta raster VJP with the variance branch in the reference's form
 # (RasterizeToPixelsBwd.cu:817-1046), counted by the same rule: offsets 2, d^2 9, h 1, pow argument 1,
@@ -105,8 +105,9 @@ WORKLOAD_TEXT = {
 }
 # DRAM bytes (read + write) of one record-parallel raster VJP launch, from ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum, one pass, one full-size launch of the
-# shipped kernel): 536.03 MB read, 369.60 MB written at the CT workload.
-RASTER_VJP_TRAFFIC_BYTES = {"ct": 536.03e6 + 369.60e6}
+# shipped kernel, profiles/ct_fit_step_launch_list.md): 552.60 MB read, 372.58 MB written
+# at the CT workload.
+RASTER_VJP_TRAFFIC_BYTES = {"ct": 552.60e6 + 372.58e6}
 
 
 # --------------------------------------------------------------------------- utilities
@@ -1055,6 +1056,20 @@ def accumulate_rooflines(workload, stages, steps, raster_evals, voxel_evals, fp3
     return out
 
 
+def pack_roofline(stages, steps, n_prims, voxel_isects, hbm_peak) -> dict:
+    """HBM roofline of the 3D pack pass (voxel_slot_affine + pack_tile_records3 kernels): its algorithmic bytes
+    read each input once (records N x 64 B, radii N x 12 B, tile-count scan N x 8 B, the slot table N x 16 B
+    written and read, flatten_ids M x 4 B, offsets) and write the packed records (M x 64 B)."""
+    if not stages.get("voxel_pack"):
+        return {}
+    ms = stages["voxel_pack"] / steps
+    nbytes = n_prims * (64 + 12 + 8 + 2 * 16) + voxel_isects * (4 + 64)
+    achieved = nbytes / (ms * 1e-3) / 1e9
+    return {"kernel": "voxel_slot_affine_kernel + pack_tile_records3_kernel (per-tile packed 3D records)",
+            "bound": "hbm", "ms": ms, "algorithmic_bytes": nbytes, "achieved": achieved, "peak": hbm_peak,
+            "unit": "GB/s", "frac": achieved / hbm_peak, "peak_source": "MEASURED_PEAKS.json hbm_gbs"}
+
+
 def dominant_roofline(workload, rooflines, fp32_peak, sfu_peak, hbm_peak) -> dict:
     """The roofline object of the step's dominant kernel, the record-parallel raster VJP."""
     entry = rooflines.get("raster_render_bwd", {})
@@ -1260,6 +1275,9 @@ def main(argv=None) -> int:
                                                    fp32_peak)
         result["roofline"] = dominant_roofline(args.workload, result["rooflines"], fp32_peak, sfu_peak,
                                                peaks.get("hbm_gbs"))
+        pack = pack_roofline(stages, stage_steps, int(scene.means.shape[0]), m3, peaks.get("hbm_gbs"))
+        if pack:
+            result["rooflines"]["voxel_pack"] = pack
         if rank == 0 and not args.no_cpu_baseline and args.workload in ("ct", "small"):
             result["cpu_baseline"] = cpu_baseline(device, args.cpu_budget)
         if args.workload == "ct" and not args.no_mix and rank == 0:
