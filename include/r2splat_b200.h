@@ -464,7 +464,7 @@ int r2s_voxel_render_bwd_capacity(int dtype, const void* records, int beta, int 
  * reference's K30/K32, VoxelizeToVoxelsBwd.cu:322-514, add every (tile, primitive)
  * pair's sums into the primitive's adjoints with atomics). Each pair writes its 12
  * sums to slot tile_cum[n - 1] + (the tile's index in primitive n's 3D tile box,
- * z then y then x), and a second pass adds each primitive's slots in order into
+ * z then y then x), and a second pass adds each primitive's slots in a fixed order into
  * grads [N] (written, not accumulated): the same result on every run. means_v [N,3]
  * and radii [N,3] are r2s_voxel_project's (the tile box is taken from the records'
  * voxel-space centre, which r2s_voxel_project writes equal to means_v), tile_cum [N]

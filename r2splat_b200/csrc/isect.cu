@@ -136,6 +136,8 @@ __global__ void __launch_bounds__(256) emit_rects_warp_kernel(const ushort4* __r
     const int64_t range_start = __shfl_sync(0xffffffffu, start, 0);
     const int64_t range_end = __shfl_sync(0xffffffffu, end, 31);
     const uint32_t n_tiles = tiles_x * tiles_y;
+    // The key of the record's first tile, cam * n_tiles + y0 * tiles_x + x0, once per record.
+    const uint32_t key0 = (i / N) * n_tiles + uint32_t(r.y) * tiles_x + uint32_t(r.x);
     // A warp-uniform trip count: every lane takes part in every shuffle.
     const int64_t steps = (range_end - range_start + 31) / 32;
     for (int64_t k = 0; k < steps; ++k) {
@@ -150,14 +152,12 @@ __global__ void __launch_bounds__(256) emit_rects_warp_kernel(const ushort4* __r
         }
         const int64_t s_owner = __shfl_sync(0xffffffffu, start, int(lo));
         const uint32_t w_owner = __shfl_sync(0xffffffffu, width, int(lo));
-        const uint32_t x0 = __shfl_sync(0xffffffffu, uint32_t(r.x), int(lo));
-        const uint32_t y0 = __shfl_sync(0xffffffffu, uint32_t(r.y), int(lo));
+        const uint32_t k_owner = __shfl_sync(0xffffffffu, key0, int(lo));
         if (p >= range_end || p >= capacity) continue;
         const uint32_t local = uint32_t(p - s_owner);
         const uint32_t row = local / w_owner, col = local - row * w_owner;
-        const uint32_t elem = uint32_t(i0) + lo;
-        keys[p] = (elem / N) * n_tiles + (y0 + row) * tiles_x + (x0 + col);
-        vals[p] = elem;
+        keys[p] = k_owner + row * tiles_x + col;
+        vals[p] = uint32_t(i0) + lo;
     }
 }
 

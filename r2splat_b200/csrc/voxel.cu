@@ -423,7 +423,7 @@ __device__ __forceinline__ const SlotPad* slot_pad(const Rec3D<S>* rec) {
 // pair's 12 sums into the primitive's adjoints with atomics, the pair writes
 // them to a slot of its own, slot = cum[n - 1] + the tile's index in the
 // primitive's tile box (z, then y, then x), and voxel_slot_reduce_kernel adds
-// each primitive's slots in that order. cum is the inclusive scan of the
+// each primitive's slots in a fixed order. cum is the inclusive scan of the
 // per-primitive tile counts, so the slots of the primitives are consecutive;
 // slots past `capacity` (an overflowing capacity-bounded step, which is
 // discarded) are not written.
@@ -832,17 +832,29 @@ __global__ void __launch_bounds__(kVoxBwdThreads, kVoxBwdMinBlocks<kBeta, kVar>)
     }
 }
 
-// grads[n] = the sum of primitive n's slots in order (12 sums), zero pads.
+// grads[n] = the sum of primitive n's slots (12 sums), zero pads. Four lanes
+// share a primitive: lane q sums slots q, q + 4, ... in order, and the four
+// partial sums are combined by a fixed butterfly ((s0 + s1) + (s2 + s3)), so
+// the result does not depend on scheduling. Lane q then writes quarter q of
+// the primitive's 16-value entry.
+constexpr uint32_t kSlotLanes = 4u;
 template <typename S>
 __global__ void voxel_slot_reduce_kernel(const S* __restrict__ slots, const int64_t* __restrict__ cum, uint32_t N,
                                          int64_t capacity, Rec3D<S>* __restrict__ grads) {
-    const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= N) return;
-    const int64_t first = n == 0u ? 0 : min(cum[n - 1], capacity), last = min(cum[n], capacity);
+    const uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const uint32_t q = uint32_t(t) & (kSlotLanes - 1u);
+    const uint64_t n = t / kSlotLanes;
+    if ((t & ~uint64_t(31)) / kSlotLanes >= N) return;  // warp-uniform: the warp holds no primitive
+    const bool active = n < N;
+    int64_t first = 0, last = 0;
+    if (active) {
+        first = n == 0u ? 0 : min(cum[n - 1], capacity);
+        last = min(cum[n], capacity);
+    }
     S acc[12];
 #pragma unroll
     for (int i = 0; i < 12; ++i) acc[i] = S(0);
-    for (int64_t j = first; j < last; ++j) {
+    for (int64_t j = first + q; j < last; j += kSlotLanes) {
         if constexpr (sizeof(S) == 4) {
             // A slot is 48 bytes, 16-byte aligned: three vector loads.
             const float4* p = reinterpret_cast<const float4*>(slots + size_t(j) * 12u);
@@ -860,11 +872,15 @@ __global__ void voxel_slot_reduce_kernel(const S* __restrict__ slots, const int6
             for (int i = 0; i < 12; ++i) acc[i] += p[i];
         }
     }
-    S* out = reinterpret_cast<S*>(grads + n);
 #pragma unroll
-    for (int i = 0; i < 12; ++i) out[i] = acc[i];
+    for (uint32_t offset = 1u; offset < kSlotLanes; offset <<= 1) {
 #pragma unroll
-    for (int i = 12; i < 16; ++i) out[i] = S(0);
+        for (int i = 0; i < 12; ++i) acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], offset);
+    }
+    if (!active) return;
+    S* out = reinterpret_cast<S*>(grads + n) + 4u * q;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) out[i] = q == 0u ? acc[i] : q == 1u ? acc[4 + i] : q == 2u ? acc[8 + i] : S(0);
 }
 
 // ---------------------------------------------------------------------------
@@ -1428,8 +1444,8 @@ int launch_vbwd_slots(const VoxelGeom& g, const Rec3D<S>* rec, bool beta, bool c
                       Rec3D<S>* grads, cudaStream_t stream, bool bulk = false) {
     if (g.N == 0) return R2S_OK;
     R2S_TRY(launch_vbwd<S>(g, rec, beta, chain_var, offsets, ids, v_vol, v_vol_var, grads, stream, sl, bulk));
-    voxel_slot_reduce_kernel<S><<<blocks_for(g.N, 256), 256, 0, stream>>>(sl.slots, sl.cum, g.N,
-                                                                         int64_t(sl.capacity), grads);
+    voxel_slot_reduce_kernel<S><<<blocks_for(int64_t(g.N) * kSlotLanes, 256), 256, 0, stream>>>(
+        sl.slots, sl.cum, g.N, int64_t(sl.capacity), grads);
     return check_launch("voxel_slot_reduce");
 }
 
