@@ -709,13 +709,20 @@ def cpu_baseline(device, budget_s: float = 15.0) -> dict:
         if time.perf_counter() - t0 > budget_s:
             break
     elapsed = time.perf_counter() - t0
+    dense_rate = dense_per_step * steps / elapsed
+    # The CT step (N=200k, 64 views at 512^2, volume 256^3) through the same dense oracle: not run, its
+    # dense evaluation count divided by the rate measured here.
+    ct_dense = 2 * 200_000 * (64 * 512 * 512 + 256 ** 3)
     return {"value": algorithmic * steps / elapsed, "unit": "evals/s", "cores": threads, "kind": "port",
             "cpu_model": cpu_model(), "torch_threads": torch.get_num_threads(),
             "sample": f"small configuration in full (N=2000, 4 views at 64x64, volume 32^3, TV): {steps} float64 "
                       f"fit steps of the dense oracle (oracle/dense.py, autograd VJPs) in {elapsed:.1f} s",
             "seconds_per_fit_step": elapsed / steps,
             "algorithmic_evals_per_step": algorithmic,
-            "dense_evals_per_s": dense_per_step * steps / elapsed}
+            "dense_evals_per_s": dense_rate,
+            "ct_step_seconds_extrapolated": ct_dense / dense_rate,
+            "ct_step_extrapolation": "not measured: the CT step's 2 N (C H W + D H W) dense evaluations divided by "
+                                     "dense_evals_per_s"}
 
 
 def timed_run(step, scene, steps, warmup, device, flush_buf, clocks=None, ours=True):
