@@ -78,6 +78,7 @@ def test_workspace_queries_run_without_a_gpu():
     assert lib.r2s_isect_emit_workspace(40_000_000, 65536) >= 40_000_000 * 16
     assert lib.r2s_raster_workspace(0, 64, 200_000, 1) >= 2 * 64 * 200_000 * 32
     assert lib.r2s_voxel_workspace(1, 1000, 1) >= 2 * 1000 * 128
+    assert lib.r2s_voxel_pack_workspace(200_000) >= 200_000 * 16  # one 16-byte slot-table entry per primitive
 
 
 @pytest.mark.parametrize("shape", [(0, 3), (True, 3), (2.5, 3), (3,), (2**30, 4)])

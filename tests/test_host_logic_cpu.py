@@ -86,3 +86,17 @@ def test_mixed_benchmark_scene_shapes_follow_the_stated_distribution():
     assert specs == bench._mixed_scene_specs(64, small=False)
     small = bench._mixed_scene_specs(16, small=True)
     assert all(s["n"] <= 100_000 and s["side"] <= 256 for s in small)
+
+
+def test_pack_roofline_counts_the_algorithmic_bytes():
+    """The 3D pack pass's HBM roofline: per primitive its record, radii, first slot and slot table (written and
+    read); per intersection a 4-byte id read and a 64-byte packed record written."""
+    import bench
+
+    stages = {"voxel_pack": 2.0}  # ms over two steps
+    out = bench.pack_roofline(stages, 2, 1000, 10_000, 5000.0)
+    nbytes = 1000 * (64 + 12 + 8 + 32) + 10_000 * 68
+    assert out["algorithmic_bytes"] == nbytes and out["bound"] == "hbm"
+    assert abs(out["achieved"] - nbytes / 1e-3 / 1e9) < 1e-9
+    assert abs(out["frac"] - out["achieved"] / 5000.0) < 1e-12
+    assert bench.pack_roofline({}, 2, 1000, 10_000, 5000.0) == {}
