@@ -961,12 +961,13 @@ def mixed_workload(args, device, autotune: bool = True) -> dict:
 
 
 def _estimated_full_bytes(spec: dict) -> float:
-    """Rough device footprint of a fully allocated FitScene (step buffers, lists with slack, slots)."""
+    """Rough device footprint of a fully allocated FitScene (step buffers, lists with slack, slots and the
+    per-tile packed 3D records)."""
     n, c, side, vol = spec["n"], spec["cameras"], spec["side"], spec["volume"]
     sigma_vox = 0.01 * vol
     m2 = 4.0 * c * n
     m3 = n * (6 * sigma_vox / 8 + 1) ** 3
-    return (c * n * 84 + 3 * 4 * c * side * side + n * 160 + 8 * vol ** 3 + 1.3 * (12 * m2 + 60 * m3))
+    return (c * n * 84 + 3 * 4 * c * side * side + n * 160 + 8 * vol ** 3 + 1.3 * (12 * m2 + 124 * m3))
 
 
 def serving_at_scale(args, device) -> dict:

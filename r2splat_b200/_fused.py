@@ -40,6 +40,10 @@ VOXEL_TILE = 8
 # Largest scratch the deterministic voxel VJP takes for its per-intersection slots (12 values each);
 # past it the VJP walks the primitives' tile boxes instead (one slot per primitive and z-layer).
 VOXEL_SLOT_BUDGET_BYTES = 8 << 30
+# The voxel forward copies the 3D records into per-tile packed order (16 values per intersection) when
+# that copy and the VJP's slots fit this budget together; otherwise the tile kernels gather the records
+# through the lists, as the reference's do.
+VOXEL_PACK_BUDGET_BYTES = VOXEL_SLOT_BUDGET_BYTES
 
 
 def _ptr(t: Optional[Tensor]):
@@ -415,12 +419,19 @@ def voxel_forward(means, quats, scales, densities, shape, extent, center, beta, 
     tx = (width + tile_size - 1) // tile_size
     ty = (height + tile_size - 1) // tile_size
     tz = (depth + tile_size - 1) // tile_size
-    with _stage("voxel_pack"):
-        packed = pack_tile_records(records, offsets, flatten_ids, radii, tile_cum, m, shape, tile_size)
+    packed = None
+    if m * (16 + 12) * means.element_size() <= VOXEL_PACK_BUDGET_BYTES:
+        with _stage("voxel_pack"):
+            packed = pack_tile_records(records, offsets, flatten_ids, radii, tile_cum, m, shape, tile_size)
     with _stage("voxel_render"):
-        _backend.call("r2s_voxel_render_packed", _dtype(means), _ptr(packed), int(beta is not None), _ptr(offsets),
-                      m, None, width, height, depth, tile_size, tx, ty, tz, _ptr(volume), _ptr(variance),
-                      _stream(device))
+        if packed is not None:
+            _backend.call("r2s_voxel_render_packed", _dtype(means), _ptr(packed), int(beta is not None),
+                          _ptr(offsets), m, None, width, height, depth, tile_size, tx, ty, tz, _ptr(volume),
+                          _ptr(variance), _stream(device))
+        else:
+            _backend.call("r2s_voxel_render", _dtype(means), _ptr(records), int(beta is not None), _ptr(offsets),
+                          _ptr(flatten_ids), means.shape[0], m, width, height, depth, tile_size, tx, ty, tz,
+                          _ptr(volume), _ptr(variance), _stream(device))
     state = VoxelState(covars, records, offsets, isect_ids, flatten_ids, m, tuple(shape), tile_size, means_v, radii,
                        tile_cum, packed=packed)
     return (volume if uncertainty is None else (volume, variance)), state
@@ -439,7 +450,7 @@ def voxel_backward(state: VoxelState, means, quats, scales, beta, uncertainty, e
     # The list-free form when no lists were kept, or when per-intersection slots would take more memory
     # than the budget (it needs one slot per primitive and tile-box z-layer instead).
     slot_bytes = state.n_isects * 12 * means.element_size()
-    list_free = state.offsets is None or state.packed is None or slot_bytes > VOXEL_SLOT_BUDGET_BYTES
+    list_free = state.offsets is None or slot_bytes > VOXEL_SLOT_BUDGET_BYTES
     if list_free and state.layer_cum is None:
         state.layer_cum = _layer_scan(state.means_v, state.radii, state.shape, state.tile_size)
         state.n_items = int(state.layer_cum[-1].item()) if n else 0
@@ -447,10 +458,18 @@ def voxel_backward(state: VoxelState, means, quats, scales, beta, uncertainty, e
         if not list_free:
             # Tile-parallel over the forward's sorted lists, one slot per (tile, primitive) pair.
             slots = means.new_empty((max(state.n_isects, 1), 12))
-            _backend.call("r2s_voxel_render_bwd_packed", _dtype(means), _ptr(state.packed), int(beta is not None),
-                          int(bool(detach_variance)), _ptr(state.offsets), state.n_isects, None,
-                          _ptr(state.tile_cum), _ptr(v_volume), _ptr(v_variance), n, width, height, depth, tile, tx,
-                          ty, tz, _ptr(slots), slots.shape[0], _ptr(grads), stream)
+            if state.packed is not None:
+                _backend.call("r2s_voxel_render_bwd_packed", _dtype(means), _ptr(state.packed),
+                              int(beta is not None), int(bool(detach_variance)), _ptr(state.offsets),
+                              state.n_isects, None, _ptr(state.tile_cum), _ptr(v_volume), _ptr(v_variance), n,
+                              width, height, depth, tile, tx, ty, tz, _ptr(slots), slots.shape[0], _ptr(grads),
+                              stream)
+            else:
+                _backend.call("r2s_voxel_render_bwd_slots", _dtype(means), _ptr(state.records),
+                              int(beta is not None), int(bool(detach_variance)), _ptr(state.offsets),
+                              _ptr(state.flatten_ids), state.n_isects, None, _ptr(state.means_v), _ptr(state.radii),
+                              _ptr(state.tile_cum), _ptr(v_volume), _ptr(v_variance), n, width, height, depth,
+                              tile, tx, ty, tz, _ptr(slots), slots.shape[0], _ptr(grads), stream)
         else:
             # No lists kept: record-parallel over the primitives' tile-box layers.
             partials = means.new_empty((max(state.n_items, 1), 16))

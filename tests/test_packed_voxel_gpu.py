@@ -137,3 +137,39 @@ def test_packed_capacity_form_writes_only_the_used_entries(device):
     assert int((slot == 0xFFFFFFFF).sum()) == m - small
     torch.cuda.synchronize(device)
     assert _faults(device) == 0
+
+
+@pytest.mark.parametrize("beta", [False, True])
+def test_explicit_path_gathers_past_the_pack_budget_with_the_same_results(device, monkeypatch, beta):
+    """A voxelize forward whose packed copy and VJP slots would exceed the pack budget keeps the gather
+    form (tile kernels reading records through flatten_ids); volume, variance and gradients are the same
+    bits as the packed form's."""
+    import r2splat_b200 as r2s
+
+    if beta:
+        sc = scenes.beta_scene(n=4096, cameras=8, side=64, focal=100.0, volume=32).to(device)
+    else:
+        sc = scenes.small_scene().to(device)
+    gen = torch.Generator().manual_seed(12)
+    adjoints = None
+    results = []
+    for budget in (None, 0):
+        if budget is not None:
+            monkeypatch.setattr(_fused, "VOXEL_PACK_BUDGET_BYTES", budget)
+        out, ctx = r2s.voxelize_fwd(*sc.primitives, sc.volume_shape, volume_extent=(1, 1, 1), beta=sc.beta,
+                                    uncertainty=sc.uncertainty)
+        state = ctx.buffers["state"]
+        assert (state.packed is None) == (budget == 0)
+        outs = out if isinstance(out, tuple) else (out,)
+        if adjoints is None:
+            adjoints = [torch.randn(o.shape, generator=gen).to(device) for o in outs]
+        grads = r2s.voxelize_bwd(ctx, *adjoints)
+        results.append((outs, grads))
+    (o0, g0), (o1, g1) = results
+    for a, b in zip(o0, o1):
+        assert torch.equal(a, b)
+    for name in ("means", "quats", "scales", "densities", "beta", "uncertainty"):
+        a, b = getattr(g0, name), getattr(g1, name)
+        assert (a is None and b is None) or torch.equal(a, b), name
+    torch.cuda.synchronize(device)
+    assert _faults(device) == 0
