@@ -175,3 +175,61 @@ def test_absgrad_oracle_is_the_sum_of_per_pixel_gradient_magnitudes(beta):
         want[0, n] = jac.abs().sum(0)
     assert float(want.abs().max()) > 0
     torch.testing.assert_close(got, want, rtol=1e-12, atol=1e-14)
+
+
+@pytest.mark.parametrize("use_beta", [False, True])
+def test_dense_oracle_on_axis_projection_matches_its_closed_form(use_beta):
+    """An axis-aligned primitive on the optical axis at depth 2, seen with fx = 12, fy = 10: an
+    axis-aligned profile of standard deviations (6 s_x, 5 s_y) around the principal point, scaled by
+    the path factor sqrt(2 pi) s_z (Gaussian) or s_z Gamma(1/2) Gamma(b + 1) / Gamma(b + 3/2) with the
+    profile (1 - d^2)^(b + 1/2) (Beta); the same case as the GPU test of the explicit operators."""
+    dtype = torch.float64
+    means = torch.tensor([[0.0, 0.0, 2.0]], dtype=dtype)
+    quats = torch.tensor([[1.0, 0.0, 0.0, 0.0]], dtype=dtype)
+    scales = torch.tensor([[0.4, 0.3, 0.25]], dtype=dtype)
+    density = torch.tensor([0.8], dtype=dtype)
+    beta = torch.tensor([3.5], dtype=dtype) if use_beta else None
+    viewmats = torch.eye(4, dtype=dtype)[None]
+    Ks = torch.tensor([[[12.0, 0.0, 4.5], [0.0, 10.0, 3.5], [0.0, 0.0, 1.0]]], dtype=dtype)
+    image = dense.rasterize_dense(means, quats, scales, density, viewmats, Ks, (7, 9), beta=beta, eps=0.0)
+    yy, xx = torch.meshgrid(torch.arange(7, dtype=dtype) + 0.5, torch.arange(9, dtype=dtype) + 0.5, indexing="ij")
+    d2 = ((xx - 4.5) / (6 * 0.4)) ** 2 + ((yy - 3.5) / (5 * 0.3)) ** 2
+    if use_beta:
+        log_path = math.lgamma(0.5) + math.lgamma(4.5) - math.lgamma(5.0)
+        expected = 0.8 * 0.25 * math.exp(log_path) * (1 - d2).clamp_min(0) ** 4.0
+    else:
+        expected = 0.8 * math.sqrt(2 * math.pi) * 0.25 * torch.exp(-d2 / 2)
+    expected = torch.where(expected.abs() >= 1e-5, expected, torch.zeros_like(expected))[None]
+    torch.testing.assert_close(image, expected, atol=1e-13, rtol=1e-12)
+
+
+@pytest.mark.parametrize("eps", [0.0, 1e-4])
+def test_dense_oracle_path_factor_at_the_principal_point(eps):
+    """An isotropic Gaussian of scale s on the axis, a one-pixel image at the principal point: the
+    image is the path factor sqrt(2 pi (s^2 + eps)), and its s_z derivative sqrt(2 pi) s / sqrt(s^2 + eps)."""
+    scale = 0.01
+    means = torch.tensor([[0.0, 0.0, 2.0]], dtype=torch.float64)
+    quats = torch.tensor([[1.0, 0.0, 0.0, 0.0]], dtype=torch.float64)
+    scales = torch.full((1, 3), scale, dtype=torch.float64, requires_grad=True)
+    Ks = torch.tensor([[[2.0, 0.0, 0.5], [0.0, 2.0, 0.5], [0.0, 0.0, 1.0]]], dtype=torch.float64)
+    image = dense.rasterize_dense(means, quats, scales, torch.ones(1, dtype=torch.float64),
+                                  torch.eye(4, dtype=torch.float64)[None], Ks, (1, 1), eps=eps)
+    (grad,) = torch.autograd.grad(image.sum(), scales)
+    assert math.isclose(float(image), math.sqrt(2 * math.pi * (scale ** 2 + eps)), rel_tol=1e-12)
+    assert math.isclose(float(grad[0, 2]), math.sqrt(2 * math.pi) * scale / math.sqrt(scale ** 2 + eps),
+                        rel_tol=1e-10)
+
+
+def test_dense_oracle_voxel_centre_holds_the_densities():
+    """Primitives centred on the single voxel of a 1^3 volume contribute their densities (Gaussian: e^0;
+    Beta: (1 - 0)^b), and the variance is the q-weighted sum of their squares."""
+    means = torch.tensor([[0.0, 0.0, 2.0], [0.0, 0.0, 2.0]], dtype=torch.float64)
+    quats = torch.tensor([[2.0, 0.0, 0.0, 0.0], [3.0, 0.0, 0.0, 0.0]], dtype=torch.float64)
+    scales = torch.tensor([[0.2, 0.3, 0.4], [0.3, 0.4, 0.5]], dtype=torch.float64)
+    densities = torch.tensor([1.2, 0.8], dtype=torch.float64)
+    q = torch.tensor([0.2, 0.3], dtype=torch.float64)
+    for beta in (None, torch.tensor([3.5, 1.25], dtype=torch.float64)):
+        volume, variance = dense.voxelize_dense(means, quats, scales, densities, (1, 1, 1), volume_extent=(1, 1, 1),
+                                                volume_center=(0, 0, 2), beta=beta, uncertainty=q, eps=0.0)
+        torch.testing.assert_close(volume, torch.full((1, 1, 1), 2.0, dtype=torch.float64))
+        torch.testing.assert_close(variance, torch.full((1, 1, 1), 0.2 * 1.44 + 0.3 * 0.64, dtype=torch.float64))
