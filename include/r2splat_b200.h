@@ -469,7 +469,7 @@ int r2s_voxel_render_bwd_capacity(int dtype, const void* records, int beta, int 
  * and radii [N,3] are r2s_voxel_project's (the tile box is taken from the records'
  * voxel-space centre, which r2s_voxel_project writes equal to means_v), tile_cum [N]
  * int64 the inclusive scan of its tile counts; slots [slot_capacity, 12] is caller
- * scratch, slot_capacity below 2^31. Capacity-bounded form: n_used (device count)
+ * scratch, 16-byte aligned, slot_capacity below 2^31. Capacity-bounded form: n_used (device count)
  * instead of n_isects; slots past slot_capacity are neither written nor read (such a
  * step overflowed and is discarded). */
 int r2s_voxel_render_bwd_slots(int dtype, const void* records, int beta, int detach_variance,

@@ -883,6 +883,179 @@ __global__ void voxel_slot_reduce_kernel(const S* __restrict__ slots, const int6
     for (int i = 0; i < 4; ++i) out[i] = q == 0u ? acc[i] : q == 1u ? acc[4 + i] : q == 2u ? acc[8 + i] : S(0);
 }
 
+// Tile VJP of fp32 Gaussian records on 8^3 tiles without the variance branch
+// (the CT fit step's form), one lane per (tile, primitive) pair. The warp
+// walks the tile's 512 voxels in lockstep, z, then pairs of rows, then x; the
+// voxel is the same for every lane, so its adjoint is one broadcast shared-
+// memory read for 32 records, and each lane sums its own record's moments
+// serially: no per-pair reduction across lanes, no box set-up. The whole tile
+// is walked: a voxel outside the record's conservative box fails the
+// contribution test (zero adjoint outside the volume), as every sample the
+// reference skips does. The two samples of a packed step are two adjacent rows
+// at the same x, so d1 and the record's x terms are shared and the row terms
+// come as pairs. With the exponent e = -sigma log2(e) = qa d1^2 + ql d1 + qk
+// (conic prescaled by -log2(e); ql and qk per row from d2 and d3), a sample
+// counts when e <= 0 and e >= log2(1e-6 / |o|), as in voxel_bwd_kernel, and
+// adds g vis, g vis d1 and g vis d1^2 to the row sums. A pair of rows folds
+// them with its d2 values, a z slab with its d3; the record's sums are then
+// the ones voxel_bwd_kernel forms (w = -o g vis), and the 12 values written
+// per pair are the same quantities in the same layout.
+constexpr int kVoxLaneWarps = 4;
+constexpr int kVoxLaneThreads = kVoxLaneWarps * 32;
+
+template <bool kBulk>
+__global__ void __launch_bounds__(kVoxLaneThreads, 6) voxel_bwd_lanes_kernel(
+    const Rec3D<float>* __restrict__ records, const int32_t* __restrict__ offsets,
+    const int32_t* __restrict__ flatten_ids, VoxelGeom g, const float* __restrict__ v_volume,
+    Rec3D<float>* __restrict__ grads, VoxelSlots<float> sl) {
+    constexpr uint32_t T = 8u;
+    // The tile's adjoint as row pairs: s_g[(z * 4 + yp) * 8 + x] = (g(z, 2 yp, x), g(z, 2 yp + 1, x)).
+    __shared__ float2 s_g[T * T * T / 2];
+    const uint32_t n_tiles = g.tiles_x * g.tiles_y * g.tiles_z;
+    const uint32_t key = blockIdx.x;
+    const uint32_t tz = key / (g.tiles_x * g.tiles_y);
+    const uint32_t rem = key - tz * g.tiles_x * g.tiles_y;
+    const uint32_t ty = rem / g.tiles_x, tx = rem - ty * g.tiles_x;
+    const uint32_t ox = tx * T, oy = ty * T, oz = tz * T;
+    if (ox >= g.dim2 || oy >= g.dim1 || oz >= g.dim0) return;
+    const uint32_t vx = min(T, g.dim2 - ox), vy = min(T, g.dim1 - oy), vz = min(T, g.dim0 - oz);
+    const int32_t start = offsets[key];
+    const int32_t n_total = g.n_dev != nullptr ? int32_t(*g.n_dev) : int32_t(g.n_isects);
+    const int32_t end = (key + 1 == n_tiles) ? n_total : offsets[key + 1];
+    const int32_t count = end - start;
+    if (count <= 0) return;
+    const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+    for (uint32_t p = t; p < T * T * T / 2; p += kVoxLaneThreads) {
+        const uint32_t x = p & 7u, yp = (p >> 3) & 3u, z = p >> 5;
+        float ga = 0.f, gb = 0.f;
+        if (v_volume != nullptr && x < vx && z < vz) {
+            const size_t vid = (size_t(oz + z) * g.dim1 + (oy + 2u * yp)) * g.dim2 + (ox + x);
+            if (2u * yp < vy) ga = v_volume[vid];
+            if (2u * yp + 1u < vy) gb = v_volume[vid + g.dim2];
+        }
+        s_g[p] = make_float2(ga, gb);
+    }
+    __syncthreads();
+
+    const float fx = static_cast<float>(ox) + 0.5f, fy = static_cast<float>(oy) + 0.5f;
+    const float fz = static_cast<float>(oz) + 0.5f;
+    const int32_t n_chunks = (count + 31) / 32;
+    for (int32_t chunk = int32_t(warp); chunk < n_chunks; chunk += kVoxLaneWarps) {
+        const int32_t idx = start + chunk * 32 + int32_t(lane);
+        const bool active = idx < end;
+        // Idle lanes walk a record with o = 0, whose threshold rejects every sample.
+        const Rec3D<float>* rp = nullptr;
+        int32_t gid = 0;
+        uint32_t slot = 0xffffffffu;
+        if (active) {
+            if constexpr (kBulk) {
+                rp = records + idx;
+                slot = __float_as_uint(__ldg(&rp->pad0));  // the pack kernel's slot (or 0xffffffff)
+            } else {
+                gid = flatten_ids[idx];
+                rp = records + gid;
+                if (sl.slots != nullptr) {
+                    const uint64_t first = gid > 0 ? uint64_t(sl.cum[gid - 1]) : 0u;
+                    const float mv[3] = {__ldg(&rp->x), __ldg(&rp->y), __ldg(&rp->z)};
+                    uint32_t blo[3], bhi[3];
+                    if (tile_box_3d(mv, sl.radii + 3 * size_t(gid), T, g.tiles_x, g.tiles_y, g.tiles_z, blo, bhi)) {
+                        const uint64_t local = (uint64_t(tz - blo[2]) * (bhi[1] - blo[1]) + (ty - blo[1])) *
+                                                   (bhi[0] - blo[0]) + (tx - blo[0]);
+                        if (first + local < sl.capacity) slot = uint32_t(first + local);
+                    }
+                }
+            }
+        }
+        float4 q0 = make_float4(0.f, 0.f, 0.f, 0.f), q1 = q0, q2 = q0;  // (x, y, z, o), (c00, c01, c02, c11), (c12, c22, ..)
+        if (active) {
+            const float4* r4 = reinterpret_cast<const float4*>(rp);
+            q0 = __ldg(r4);
+            q1 = __ldg(r4 + 1);
+            q2 = __ldg(r4 + 2);
+        }
+        const float ry = q0.y, rz = q0.z, opac = q0.w;
+        const float e_min = log2f(1e-6f / fabsf(opac));
+        const float2 qa = splat2(0.5f * q1.x * kVoxNegLog2e);
+        const float pl = q1.y * kVoxNegLog2e, ql3 = q1.z * kVoxNegLog2e;
+        const float hb = 0.5f * q1.w * kVoxNegLog2e, rl = q2.x * kVoxNegLog2e, hc = 0.5f * q2.y * kVoxNegLog2e;
+        const float2 d1_0 = splat2(fx - q0.x), one = splat2(1.f);
+        // Record sums: g vis d1^2, g vis d2^2, g vis d1 d2 (packed over the row pair),
+        // then g vis, g vis d1, g vis d2 and the d3 moments.
+        float2 r11 = splat2(0.f), r22 = r11, r12 = r11;
+        float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f, s13 = 0.f, s23 = 0.f, s33 = 0.f;
+        for (uint32_t z = 0; z < T; ++z) {
+            const float d3 = (fz + static_cast<float>(z)) - rz;
+            const float qd3 = ql3 * d3, rd3 = rl * d3, cd3 = hc * d3 * d3;
+            float2 z0 = splat2(0.f), z1 = z0, z2 = z0;
+            const float2* gz = s_g + z * (T * T / 2);
+#pragma unroll 1
+            for (uint32_t yp = 0; yp < T / 2; ++yp) {
+                const float fyp = fy + static_cast<float>(2u * yp);
+                const float2 d2 = make_float2(fyp - ry, (fyp + 1.f) - ry);
+                const float2 ql = make_float2(fmaf(pl, d2.x, qd3), fmaf(pl, d2.y, qd3));
+                const float2 qk = make_float2(fmaf(hb * d2.x, d2.x, fmaf(rd3, d2.x, cd3)),
+                                              fmaf(hb * d2.y, d2.y, fmaf(rd3, d2.y, cd3)));
+                float2 a1 = splat2(0.f), a2 = a1, a3 = a1;
+                float2 d1 = d1_0;
+#pragma unroll
+                for (uint32_t x = 0; x < T; ++x) {
+                    const float2 gg = gz[yp * T + x];
+                    const float2 e = fma2(fma2(qa, d1, ql), d1, qk);
+                    const float2 vis = make_float2(exp2f(e.x), exp2f(e.y));
+                    const bool ka = !(e.x > 0.f || e.x < e_min);
+                    const bool kb = !(e.y > 0.f || e.y < e_min);
+                    // Select after the product: a skipped sample may have vis = inf (e > 0).
+                    const float2 gvr = mul2(gg, vis);
+                    const float2 gv = make_float2(ka ? gvr.x : 0.f, kb ? gvr.y : 0.f);
+                    a3 = add2(a3, gv);
+                    const float2 gvd = mul2(gv, d1);
+                    a1 = add2(a1, gvd);
+                    a2 = fma2(gvd, d1, a2);
+                    d1 = add2(d1, one);
+                }
+                z0 = add2(z0, a3);
+                z1 = add2(z1, a1);
+                r11 = add2(r11, a2);
+                const float2 gd2 = mul2(d2, a3);
+                z2 = add2(z2, gd2);
+                r22 = fma2(d2, gd2, r22);
+                r12 = fma2(d2, a1, r12);
+            }
+            const float g0 = z0.x + z0.y, g1 = z1.x + z1.y, g2 = z2.x + z2.y;
+            s0 += g0;
+            s1 += g1;
+            s2 += g2;
+            s3 = fmaf(d3, g0, s3);
+            s13 = fmaf(d3, g1, s13);
+            s23 = fmaf(d3, g2, s23);
+            s33 = fmaf(d3 * d3, g0, s33);
+        }
+        if (!active) continue;
+        const float nom = -opac;
+        const float S1 = nom * s1, S2 = nom * s2, S3 = nom * s3;
+        const float S11 = nom * (r11.x + r11.y), S12 = nom * (r12.x + r12.y), S13 = nom * s13;
+        const float S22 = nom * (r22.x + r22.y), S23 = nom * s23, S33 = nom * s33;
+        // The conic again (read once more rather than held through the walk).
+        const float4 c4 = __ldg(reinterpret_cast<const float4*>(rp) + 1);
+        const float a = c4.x, p = c4.y, q = c4.z, bb = c4.w, rr = __ldg(&rp->c12), c = __ldg(&rp->c22);
+        const float4 o0 = make_float4(-(a * S1 + p * S2 + q * S3), -(bb * S2 + p * S1 + rr * S3),
+                                      -(c * S3 + q * S1 + rr * S2), s0);
+        const float4 o1 = make_float4(0.5f * S11, S12, S13, 0.5f * S22);
+        const float4 o2 = make_float4(S23, 0.5f * S33, 0.f, 0.f);
+        if (!kBulk && sl.slots == nullptr) {
+            float* out = reinterpret_cast<float*>(grads + gid);
+            red_add_v4(out, o0.x, o0.y, o0.z, o0.w);
+            red_add_v4(out + 4, o1.x, o1.y, o1.z, o1.w);
+            red_add_v4(out + 8, o2.x, o2.y, o2.z, o2.w);
+        } else if (slot != 0xffffffffu) {
+            float4* out = reinterpret_cast<float4*>(sl.slots + size_t(slot) * 12u);
+            out[0] = o0;
+            out[1] = o1;
+            out[2] = o2;
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Record-parallel voxel VJP (the explicit path).
 //
@@ -1400,6 +1573,14 @@ template <typename S, bool kBeta, bool kVar, bool kBulk>
 int launch_vbwd_p(const VoxelGeom& g, const Rec3D<S>* rec, bool chain_var, const int32_t* offsets,
                   const int32_t* ids, const S* v_vol, const S* v_vol_var, Rec3D<S>* grads, cudaStream_t stream,
                   const VoxelSlots<S>& sl) {
+    if constexpr (std::is_same<S, float>::value && !kBeta && !kVar) {
+        if (g.T == 8) {
+            const unsigned grid = g.tiles_x * g.tiles_y * g.tiles_z;
+            voxel_bwd_lanes_kernel<kBulk><<<grid, kVoxLaneThreads, 0, stream>>>(rec, offsets, ids, g, v_vol, grads,
+                                                                                  sl);
+            return check_launch("voxelize_to_voxels_bwd");
+        }
+    }
     const size_t tile_slots = size_t(g.T) * g.T * (g.T + 1) + (g.T + 1);
     const size_t smem = 2 * size_t(kVoxBwdThreads) * (sizeof(Rec3D<S>) + 2 * sizeof(int32_t)) +
                         size_t(kVoxBwdThreads) * sizeof(VoxelBox) + 2 * tile_slots * sizeof(S);
@@ -1657,6 +1838,7 @@ int r2s_voxel_render_bwd_slots(int dtype, const void* records, int beta, int det
     R2S_REQUIRE(records != nullptr && means_v != nullptr && radii != nullptr && tile_cum != nullptr &&
                     slots != nullptr && grads != nullptr,
                 R2S_ERR_ARGUMENT, "records, means_v, radii, tile_cum, slots and grads must be non-null");
+    R2S_REQUIRE(reinterpret_cast<uintptr_t>(slots) % 16 == 0, R2S_ERR_ARGUMENT, "slots must be 16-byte aligned");
     R2S_REQUIRE(n_used != nullptr || n_isects <= slot_capacity, R2S_ERR_ARGUMENT,
                 "slot_capacity must hold n_isects slots");
     R2S_REQUIRE(n_isects < (uint64_t(1) << 31), R2S_ERR_UNSUPPORTED, "too many 3D intersections");
@@ -1732,6 +1914,7 @@ int r2s_voxel_render_bwd_packed(int dtype, const void* packed, int beta, int det
     R2S_REQUIRE(tile_offsets != nullptr && tile_cum != nullptr && slots != nullptr && grads != nullptr &&
                     (packed != nullptr || n_isects == 0),
                 R2S_ERR_ARGUMENT, "packed, tile_offsets, tile_cum, slots and grads must be non-null");
+    R2S_REQUIRE(reinterpret_cast<uintptr_t>(slots) % 16 == 0, R2S_ERR_ARGUMENT, "slots must be 16-byte aligned");
     R2S_REQUIRE(n_used != nullptr || n_isects <= slot_capacity, R2S_ERR_ARGUMENT,
                 "slot_capacity must hold n_isects slots");
     R2S_REQUIRE(n_isects < (uint64_t(1) << 31), R2S_ERR_UNSUPPORTED, "too many 3D intersections");

@@ -215,7 +215,7 @@ def test_dense_oracle_path_factor_at_the_principal_point(eps):
     image = dense.rasterize_dense(means, quats, scales, torch.ones(1, dtype=torch.float64),
                                   torch.eye(4, dtype=torch.float64)[None], Ks, (1, 1), eps=eps)
     (grad,) = torch.autograd.grad(image.sum(), scales)
-    assert math.isclose(float(image), math.sqrt(2 * math.pi * (scale ** 2 + eps)), rel_tol=1e-12)
+    assert math.isclose(float(image.detach()), math.sqrt(2 * math.pi * (scale ** 2 + eps)), rel_tol=1e-12)
     assert math.isclose(float(grad[0, 2]), math.sqrt(2 * math.pi) * scale / math.sqrt(scale ** 2 + eps),
                         rel_tol=1e-10)
 
