@@ -82,7 +82,8 @@ ACCUMULATE_KERNELS = {
     "raster_render": "raster_fwd_pair_kernel (tile forward, two pixels per lane)",
     "raster_render_bwd": "raster_record_bwd_kernel (record-parallel raster VJP)",
     "voxel_render": "voxel_fwd_kernel (tile forward, two rows of eight voxels per thread, bulk-staged packed records)",
-    "voxel_render_bwd": "voxel_bwd_kernel (row-wise voxel VJP, bulk-staged packed records)",
+    "voxel_render_bwd": ("voxel_bwd_lanes_kernel (one lane per (tile, primitive) pair walking the 8^3 tile in "
+                         "lockstep, packed records)"),
 }
 # FP32 operations per sample of the Beta raster VJP with the variance branch in the reference's form
 # (RasterizeToPixelsBwd.cu:817-1046), counted by the same rule: offsets 2, d^2 9, h 1, pow argument 1,
