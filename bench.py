@@ -218,12 +218,24 @@ class ClockSampler:
                 "samples": len(clocks)}
 
 
+# HBM copy bandwidth of an earlier STREAM-style measurement on B200, used only when
+# MEASURED_PEAKS.json is absent.
+FALLBACK_HBM_GBS = 6650.0
+
+
 def measured_peaks() -> dict:
     path = ROOT / "MEASURED_PEAKS.json"
     try:
         return json.loads(path.read_text())
     except (OSError, ValueError):
         return {}
+
+
+def hbm_peak_gbs(peaks: dict) -> tuple:
+    """(HBM peak in GB/s, where it comes from): MEASURED_PEAKS.json's hbm_gbs, else the fallback."""
+    if peaks.get("hbm_gbs"):
+        return float(peaks["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs"
+    return FALLBACK_HBM_GBS, "fallback: an earlier STREAM-style copy on B200 (MEASURED_PEAKS.json absent)"
 
 
 def flush_l2(buf: torch.Tensor):
@@ -1065,7 +1077,7 @@ def accumulate_rooflines(workload, stages, steps, raster_evals, voxel_evals, fp3
     return out
 
 
-def pack_roofline(stages, steps, n_prims, voxel_isects, hbm_peak) -> dict:
+def pack_roofline(stages, steps, n_prims, voxel_isects, hbm_peak, peak_source="MEASURED_PEAKS.json hbm_gbs") -> dict:
     """HBM roofline of the 3D pack pass (voxel_slot_affine + pack_tile_records3 kernels): its algorithmic bytes
     read each input once (records N x 64 B, radii N x 12 B, tile-count scan N x 8 B, the slot table N x 16 B
     written and read, flatten_ids M x 4 B, offsets) and write the packed records (M x 64 B)."""
@@ -1076,7 +1088,7 @@ def pack_roofline(stages, steps, n_prims, voxel_isects, hbm_peak) -> dict:
     achieved = nbytes / (ms * 1e-3) / 1e9
     return {"kernel": "voxel_slot_affine_kernel + pack_tile_records3_kernel (per-tile packed 3D records)",
             "bound": "hbm", "ms": ms, "algorithmic_bytes": nbytes, "achieved": achieved, "peak": hbm_peak,
-            "unit": "GB/s", "frac": achieved / hbm_peak, "peak_source": "MEASURED_PEAKS.json hbm_gbs"}
+            "unit": "GB/s", "frac": achieved / hbm_peak, "peak_source": peak_source}
 
 
 def dominant_roofline(workload, rooflines, fp32_peak, sfu_peak, hbm_peak) -> dict:
@@ -1283,8 +1295,8 @@ def main(argv=None) -> int:
         result["rooflines"] = accumulate_rooflines(args.workload, stages, stage_steps, raster_evals, voxel_evals,
                                                    fp32_peak)
         result["roofline"] = dominant_roofline(args.workload, result["rooflines"], fp32_peak, sfu_peak,
-                                               peaks.get("hbm_gbs"))
-        pack = pack_roofline(stages, stage_steps, int(scene.means.shape[0]), m3, peaks.get("hbm_gbs"))
+                                               hbm_peak_gbs(peaks)[0])
+        pack = pack_roofline(stages, stage_steps, int(scene.means.shape[0]), m3, *hbm_peak_gbs(peaks))
         if pack:
             result["rooflines"]["voxel_pack"] = pack
         if rank == 0 and not args.no_cpu_baseline and args.workload in ("ct", "small"):

@@ -100,3 +100,15 @@ def test_pack_roofline_counts_the_algorithmic_bytes():
     assert abs(out["achieved"] - nbytes / 1e-3 / 1e9) < 1e-9
     assert abs(out["frac"] - out["achieved"] / 5000.0) < 1e-12
     assert bench.pack_roofline({}, 2, 1000, 10_000, 5000.0) == {}
+
+
+def test_hbm_peak_falls_back_when_the_measured_file_has_no_figure():
+    """The HBM denominator is MEASURED_PEAKS.json's hbm_gbs when present; without it the bench uses the fallback
+    figure and says so, instead of failing on a missing peak."""
+    import bench
+
+    assert bench.hbm_peak_gbs({"hbm_gbs": 6455.0}) == (6455.0, "MEASURED_PEAKS.json hbm_gbs")
+    peak, source = bench.hbm_peak_gbs({})
+    assert peak == bench.FALLBACK_HBM_GBS and source.startswith("fallback")
+    out = bench.pack_roofline({"voxel_pack": 2.0}, 2, 1000, 10_000, *bench.hbm_peak_gbs({}))
+    assert out["peak"] == bench.FALLBACK_HBM_GBS and out["peak_source"].startswith("fallback")
