@@ -173,3 +173,27 @@ def test_explicit_path_gathers_past_the_pack_budget_with_the_same_results(device
         assert (a is None and b is None) or torch.equal(a, b), name
     torch.cuda.synchronize(device)
     assert _faults(device) == 0
+
+
+def test_slot_buffers_must_be_16_byte_aligned(device):
+    """The slot writes and the per-primitive reduction use 16-byte vectors, so both slot entry points refuse a
+    slot buffer that is not 16-byte aligned, before any launch."""
+    dtype, shape, tile = torch.float32, (16, 16, 16), 8
+    n, (records, offsets, isect_ids, flatten_ids, m, means_v, radii, cum) = _lists(device, dtype, False, False,
+                                                                                   shape, tile)
+    depth, height, width = shape
+    tx, ty, tz = _fused._voxel_tiles(shape, tile)
+    stream = torch.cuda.current_stream(device).cuda_stream
+    v_vol = torch.ones(shape, dtype=dtype, device=device)
+    grads = torch.empty((n, 16), dtype=dtype, device=device)
+    backing = torch.empty(m * 12 + 4, dtype=dtype, device=device)
+    misaligned = backing[1:].view(-1)  # 4 bytes past a 16-byte boundary
+    assert misaligned.data_ptr() % 16 == 4
+    with pytest.raises(RuntimeError, match="16-byte aligned"):
+        _backend.call("r2s_voxel_render_bwd_slots", 0, _p(records), 0, 0, _p(offsets), _p(flatten_ids), m, None,
+                      _p(means_v), _p(radii), _p(cum), _p(v_vol), None, n, width, height, depth, tile, tx, ty, tz,
+                      _p(misaligned), m, _p(grads), stream)
+    packed = _fused.pack_tile_records(records, offsets, flatten_ids, radii, cum, m, shape, tile)
+    with pytest.raises(RuntimeError, match="16-byte aligned"):
+        _backend.call("r2s_voxel_render_bwd_packed", 0, _p(packed), 0, 0, _p(offsets), m, None, _p(cum), _p(v_vol),
+                      None, n, width, height, depth, tile, tx, ty, tz, _p(misaligned), m, _p(grads), stream)
